@@ -1,0 +1,21 @@
+"""B200-native (sm_100a) implementation of HeddleMD's per-timestep
+force-and-constraint path: packed neighbour list, LJ + erfc real-space pair
+kernel, SPME spread / FFT / convolution / gather, SETTLE / SHAKE, deterministic
+fixed-point and FP64 reductions, behind a C ABI (include/heddle_b200.h)."""
+
+from ._native import HeddleError, load  # noqa: F401
+from .api import (  # noqa: F401
+    Constraints,
+    Context,
+    ForceField,
+    Integrator,
+    LennardJonesParams,
+    PotentialRegistry,
+    SpmeParams,
+    System,
+)
+
+__all__ = [
+    "Context", "System", "ForceField", "Constraints", "Integrator",
+    "PotentialRegistry", "LennardJonesParams", "SpmeParams", "HeddleError", "load",
+]

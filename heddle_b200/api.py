@@ -1,0 +1,406 @@
+"""Host-side mirror of the reference's force / constraint / integrator plugin
+surface over the C ABI.
+
+  * PotentialRegistry -- builders keyed by label in the reference's canonical
+    order (LJ, SPME real, SPME reciprocal; src/forces/mod.rs:277-289), with
+    compositional activation driven by which sections a configuration holds
+    and the reference's validation errors (src/forces/mod.rs:394-447);
+  * ConstraintRegistry -- "settle" and "shake" groups
+    (src/integrator/constraint.rs:205-212, :227-300);
+  * IntegratorRegistry -- "velocity-verlet" (with a "lossless" flag) and
+    "langevin-baoab" (src/integrator/mod.rs:627-677).
+
+Objects wrap the opaque C handles and raise HeddleError with the library's
+status on failure.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+from .systems import SystemSpec
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint32))
+
+
+class Context:
+    """A device, its streams and loaded kernels (init_device,
+    src/gpu/device.rs:67-74)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = N.load()
+        h = C.c_void_p()
+        N.check(self.lib.hb_context_create(device, C.byref(h)))
+        self.h = h
+
+    def synchronize(self) -> None:
+        N.check(self.lib.hb_context_synchronize(self.h))
+
+    def timing(self, enable: bool) -> None:
+        N.check(self.lib.hb_timing_enable(self.h, 1 if enable else 0))
+
+    def timings(self) -> np.ndarray:
+        out = np.zeros(8)
+        N.check(self.lib.hb_timing_get(self.h, N.dptr(out)))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.hb_context_destroy(self.h)
+            self.h = None
+
+
+class System:
+    """Device-resident particle state (ParticleBuffers + SimulationBox)."""
+
+    def __init__(self, ctx: Context, positions, masses, charges, types, box,
+                 velocities=None, images=None):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self._pos = _f64(positions).reshape(-1)
+        self._vel = None if velocities is None else _f64(velocities).reshape(-1)
+        self._m = _f64(masses)
+        self._q = _f64(charges)
+        self._t = _u32(types)
+        self._img = None if images is None else np.ascontiguousarray(np.asarray(images, dtype=np.int32)).reshape(-1)
+        self.n = int(self._m.shape[0])
+        d = N.SystemDesc()
+        d.n_atoms = self.n
+        d.positions = N.dptr(self._pos)
+        d.velocities = N.dptr(self._vel)
+        d.masses = N.dptr(self._m)
+        d.charges = N.dptr(self._q)
+        d.types = N.u32ptr(self._t)
+        d.images = N.i32ptr(self._img)
+        for k in range(6):
+            d.box[k] = float(box[k])
+        h = C.c_void_p()
+        N.check(self.lib.hb_system_create(ctx.h, C.byref(d), C.byref(h)))
+        self.h = h
+
+    @classmethod
+    def from_spec(cls, ctx: Context, spec: SystemSpec) -> "System":
+        return cls(ctx, spec.positions, spec.masses, spec.charges, spec.types, spec.box,
+                   velocities=spec.velocities)
+
+    def state(self):
+        pos = np.zeros(3 * self.n)
+        vel = np.zeros(3 * self.n)
+        img = np.zeros(3 * self.n, dtype=np.int32)
+        frc = np.zeros(3 * self.n)
+        N.check(self.lib.hb_system_get_state(self.h, N.dptr(pos), N.dptr(vel), N.i32ptr(img), N.dptr(frc)))
+        return pos.reshape(-1, 3), vel.reshape(-1, 3), img.reshape(-1, 3), frc.reshape(-1, 3)
+
+    def positions(self) -> np.ndarray:
+        pos = np.zeros(3 * self.n)
+        N.check(self.lib.hb_system_get_state(self.h, N.dptr(pos), None, None, None))
+        return pos.reshape(-1, 3)
+
+    def forces(self) -> np.ndarray:
+        f = np.zeros(3 * self.n)
+        N.check(self.lib.hb_system_get_state(self.h, None, None, None, N.dptr(f)))
+        return f.reshape(-1, 3)
+
+    def set_state(self, positions=None, velocities=None) -> None:
+        p = None if positions is None else _f64(positions).reshape(-1)
+        v = None if velocities is None else _f64(velocities).reshape(-1)
+        N.check(self.lib.hb_system_set_state(self.h, N.dptr(p), N.dptr(v)))
+
+    def set_box(self, box) -> None:
+        b = _f64(box)
+        N.check(self.lib.hb_system_set_box(self.h, N.dptr(b)))
+
+    def kinetic(self) -> np.ndarray:
+        out = np.zeros(4)
+        N.check(self.lib.hb_reduce_kinetic(self.h, N.dptr(out)))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.hb_system_destroy(self.h)
+            self.h = None
+
+
+# ---------------------------------------------------------------------------
+# potentials and their registry
+# ---------------------------------------------------------------------------
+@dataclass
+class LennardJonesParams:
+    sigma: np.ndarray
+    epsilon: np.ndarray
+    cutoff: np.ndarray
+    switch: np.ndarray
+
+
+@dataclass
+class SpmeParams:
+    alpha: float
+    r_cut_real: float
+    grid: tuple
+    spline_order: int = 4
+    reciprocal: bool = True
+
+
+class PotentialBuilder:
+    label = ""
+
+    def build(self, config: dict, desc: N.ForceFieldDesc, keep: list) -> bool:
+        raise NotImplementedError
+
+
+class LennardJonesBuilder(PotentialBuilder):
+    label = "lennard_jones"
+
+    def build(self, config, desc, keep):
+        p = config.get(self.label)
+        if p is None:
+            return False
+        nt = int(np.asarray(p.sigma).shape[0])
+        arrs = [_f64(np.asarray(x).reshape(-1)) for x in (p.sigma, p.epsilon, p.cutoff, p.switch)]
+        keep.extend(arrs)
+        desc.lj_enabled = 1
+        desc.n_types = nt
+        desc.lj_sigma, desc.lj_epsilon, desc.lj_cutoff, desc.lj_switch = [N.dptr(a) for a in arrs]
+        return True
+
+
+class SpmeBuilder(PotentialBuilder):
+    """SPME real-space erfc slot plus, unless disabled, the reciprocal slot."""
+
+    label = "spme"
+
+    def build(self, config, desc, keep):
+        p = config.get(self.label)
+        if p is None:
+            return False
+        desc.coulomb_enabled = 1
+        desc.alpha = float(p.alpha)
+        desc.r_cut_coulomb = float(p.r_cut_real)
+        if p.reciprocal:
+            desc.recip_enabled = 1
+            for k in range(3):
+                desc.grid[k] = int(p.grid[k])
+            desc.spline_order = int(p.spline_order)
+        return True
+
+
+class PotentialRegistry:
+    """Builders in canonical order; a slot is active when its section is
+    present (compositional activation)."""
+
+    def __init__(self):
+        self.builders: list[PotentialBuilder] = [LennardJonesBuilder(), SpmeBuilder()]
+
+    def register(self, builder: PotentialBuilder) -> None:
+        if any(b.label == builder.label for b in self.builders):
+            raise ValueError(f"duplicate potential label {builder.label!r}")
+        self.builders.append(builder)
+
+    def labels(self) -> list[str]:
+        return [b.label for b in self.builders]
+
+
+DEFAULT_POTENTIALS = PotentialRegistry()
+
+
+class ForceField:
+    """ForceField::new / step over the C ABI."""
+
+    def __init__(self, system: System, config: dict, exclusions=None, r_skin: float = 0.0,
+                 registry: PotentialRegistry | None = None):
+        self.system = system
+        self.lib = system.lib
+        reg = registry or DEFAULT_POTENTIALS
+        unknown = set(config) - set(reg.labels())
+        if unknown:
+            raise ValueError(f"unknown potential sections: {sorted(unknown)}")
+        d = N.ForceFieldDesc()
+        self._keep: list = []
+        self.active = [b.label for b in reg.builders if b.build(config, d, self._keep)]
+        if exclusions is not None:
+            off, part, slj, sc = exclusions
+            arrs = [_u32(off), _u32(part), _f64(slj), _f64(sc)]
+            self._keep.extend(arrs)
+            d.excl_offsets, d.excl_partners = N.u32ptr(arrs[0]), N.u32ptr(arrs[1])
+            d.excl_lj_scale, d.excl_coulomb_scale = N.dptr(arrs[2]), N.dptr(arrs[3])
+        d.r_skin = float(r_skin)
+        h = C.c_void_p()
+        N.check(self.lib.hb_forcefield_create(system.h, C.byref(d), C.byref(h)))
+        self.h = h
+
+    @classmethod
+    def from_spec(cls, system: System, spec: SystemSpec, r_skin: float | None = None,
+                  reciprocal: bool = True) -> "ForceField":
+        cfg = {}
+        if spec.lj_sigma is not None:
+            cfg["lennard_jones"] = LennardJonesParams(spec.lj_sigma, spec.lj_epsilon,
+                                                      spec.lj_cutoff, spec.lj_switch)
+        if spec.alpha is not None:
+            cfg["spme"] = SpmeParams(spec.alpha, spec.r_cut_coul, spec.grid, spec.order,
+                                     reciprocal=reciprocal and spec.grid is not None)
+        excl = None
+        if spec.excl_offsets is not None:
+            excl = (spec.excl_offsets, spec.excl_partners, spec.excl_lj, spec.excl_coul)
+        return cls(system, cfg, excl, spec.r_skin if r_skin is None else r_skin)
+
+    def step(self, scalars: bool = False) -> None:
+        N.check(self.lib.hb_forcefield_step(
+            self.h, N.HB_FORCES_AND_SCALARS if scalars else N.HB_FORCES_ONLY))
+
+    def pre_step(self, force: bool = False) -> bool:
+        r = C.c_int(0)
+        N.check(self.lib.hb_forcefield_pre_step(self.h, 1 if force else 0, C.byref(r)))
+        return bool(r.value)
+
+    def scalars(self) -> dict:
+        out = np.zeros(8)
+        N.check(self.lib.hb_forcefield_scalars(self.h, N.dptr(out)))
+        keys = ["lj", "coulomb_real", "recip", "self", "potential", "virial_pair",
+                "virial_recip", "virial"]
+        return dict(zip(keys, out.tolist()))
+
+    def per_atom(self):
+        e = np.zeros(self.system.n)
+        w = np.zeros(self.system.n)
+        N.check(self.lib.hb_forcefield_get_per_atom(self.h, N.dptr(e), N.dptr(w)))
+        return e, w
+
+    def neighbor_pairs(self):
+        cnt = C.c_uint64(0)
+        dup = C.c_uint64(0)
+        N.check(self.lib.hb_neighbor_pairs(self.h, None, 0, C.byref(cnt), C.byref(dup)))
+        buf = np.zeros(2 * max(cnt.value, 1), dtype=np.uint32)
+        N.check(self.lib.hb_neighbor_pairs(self.h, N.u32ptr(buf), cnt.value, C.byref(cnt), C.byref(dup)))
+        return buf[: 2 * cnt.value].reshape(-1, 2), int(dup.value)
+
+    def stats(self) -> dict:
+        out = np.zeros(6, dtype=np.uint64)
+        N.check(self.lib.hb_neighbor_stats(self.h, out.ctypes.data_as(N.PU64)))
+        keys = ["tiles", "entries", "capacity", "rebuilds", "status", "pair_slots"]
+        return dict(zip(keys, [int(x) for x in out]))
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.hb_forcefield_destroy(self.h)
+            self.h = None
+
+
+# ---------------------------------------------------------------------------
+# constraints
+# ---------------------------------------------------------------------------
+CONSTRAINT_KINDS = {"settle": N.HB_CONSTRAINT_SETTLE, "shake": N.HB_CONSTRAINT_SHAKE}
+
+
+class Constraints:
+    """Constraint hooks of SETTLE / SHAKE groups (Constraint trait,
+    src/integrator/constraint.rs:43-122)."""
+
+    def __init__(self, system: System, group_offsets, group_atoms, group_kind,
+                 settle_geometry=None, shake=None, shake_tol: float = 3.57e-6,
+                 shake_max_iter: int = 32):
+        self.system = system
+        self.lib = system.lib
+        d = N.ConstraintsDesc()
+        go, ga, gk = _u32(group_offsets), _u32(group_atoms), _u32(group_kind)
+        self._keep = [go, ga, gk]
+        d.n_groups = int(gk.shape[0])
+        d.group_offsets, d.group_atoms, d.group_kind = N.u32ptr(go), N.u32ptr(ga), N.u32ptr(gk)
+        if settle_geometry is not None:
+            ra, rb, rc = [_f64(x) for x in settle_geometry]
+            self._keep += [ra, rb, rc]
+            d.settle_ra, d.settle_rb, d.settle_rc = N.dptr(ra), N.dptr(rb), N.dptr(rc)
+        if shake is not None:
+            co, ci, cj, cd = _u32(shake[0]), _u32(shake[1]), _u32(shake[2]), _f64(shake[3])
+            self._keep += [co, ci, cj, cd]
+            d.con_offsets, d.con_i, d.con_j, d.con_dist = N.u32ptr(co), N.u32ptr(ci), N.u32ptr(cj), N.dptr(cd)
+        d.shake_tol = float(shake_tol)
+        d.shake_max_iter = int(shake_max_iter)
+        h = C.c_void_p()
+        N.check(self.lib.hb_constraints_create(system.h, C.byref(d), C.byref(h)))
+        self.h = h
+
+    @classmethod
+    def from_spec(cls, system: System, spec: SystemSpec, **kw) -> "Constraints":
+        geo = None
+        if spec.settle_ra is not None:
+            geo = (spec.settle_ra, spec.settle_rb, spec.settle_rc)
+        shake = None
+        if spec.con_offsets is not None:
+            shake = (spec.con_offsets, spec.con_i, spec.con_j, spec.con_dist)
+        return cls(system, spec.group_offsets, spec.group_atoms, spec.group_kind, geo, shake, **kw)
+
+    def before_drift(self):
+        N.check(self.lib.hb_constraints_before_drift(self.h))
+
+    def after_drift(self, dt: float):
+        N.check(self.lib.hb_constraints_after_drift(self.h, float(dt)))
+
+    def after_kick(self, dt: float):
+        N.check(self.lib.hb_constraints_after_kick(self.h, float(dt)))
+
+    def virial(self) -> np.ndarray:
+        out = np.zeros(self.system.n)
+        N.check(self.lib.hb_constraints_get_virial(self.h, N.dptr(out)))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.hb_constraints_destroy(self.h)
+            self.h = None
+
+
+# ---------------------------------------------------------------------------
+# integrators
+# ---------------------------------------------------------------------------
+INTEGRATOR_KINDS = {
+    "velocity-verlet": N.HB_INTEGRATOR_VV,
+    "velocity-verlet-lossless": N.HB_INTEGRATOR_VV_LOSSLESS,
+    "langevin-baoab": N.HB_INTEGRATOR_LANGEVIN,
+}
+
+
+class Integrator:
+    def __init__(self, system: System, kind: str, dt: float, friction: float = 0.0,
+                 temperature: float = 0.0, seed: int = 0, step0: int = 0):
+        if kind not in INTEGRATOR_KINDS:
+            raise ValueError(f"unknown integrator {kind!r}; known: {sorted(INTEGRATOR_KINDS)}")
+        self.system = system
+        self.lib = system.lib
+        d = N.IntegratorDesc()
+        d.kind = INTEGRATOR_KINDS[kind]
+        d.dt = float(dt)
+        d.friction = float(friction)
+        d.temperature = float(temperature)
+        d.seed = int(seed)
+        d.step0 = int(step0)
+        h = C.c_void_p()
+        N.check(self.lib.hb_integrator_create(system.h, C.byref(d), C.byref(h)))
+        self.h = h
+
+    def step(self, ff: ForceField, cons: Constraints | None = None, n_steps: int = 1,
+             scalar_every: int = 0) -> None:
+        N.check(self.lib.hb_integrator_step(self.h, ff.h, cons.h if cons else None,
+                                            int(n_steps), int(scalar_every)))
+
+    def step_graph(self, ff: ForceField, cons: Constraints | None = None, n_steps: int = 1) -> None:
+        N.check(self.lib.hb_integrator_step_graph(self.h, ff.h, cons.h if cons else None, int(n_steps)))
+
+    def count_launches(self, ff: ForceField, cons: Constraints | None = None) -> int:
+        out = C.c_uint64(0)
+        N.check(self.lib.hb_integrator_count_launches(self.h, ff.h, cons.h if cons else None, C.byref(out)))
+        return int(out.value)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.hb_integrator_destroy(self.h)
+            self.h = None

@@ -1,0 +1,948 @@
+// hb_api.cu -- C ABI of the B200-native force-and-constraint path: object
+// lifetimes, validation with the reference's error semantics, and the
+// per-step orchestration (integrator sub-steps, constraint hooks, device-
+// gated neighbour rebuild, pair kernel overlapped with SPME on a second
+// stream, force combine).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "hb_internal.cuh"
+
+static thread_local std::string g_err;
+
+void hb_set_error(const std::string &msg) { g_err = msg; }
+int hb_fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+extern "C" const char *hb_last_error(void) { return g_err.c_str(); }
+extern "C" const char *hb_version(void) { return "heddle_b200 0.1 (sm_100a)"; }
+
+#define HB_REQUIRE(cond, code, msg) \
+  do {                              \
+    if (!(cond)) return hb_fail((code), (msg)); \
+  } while (0)
+
+// ---------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------
+extern "C" int hb_context_create(int device_ordinal, hb_context **out) {
+  HB_REQUIRE(out != nullptr, HB_ERR_INVALID_ARGUMENT, "out is null");
+  int count = 0;
+  HB_CUDA(cudaGetDeviceCount(&count));
+  HB_REQUIRE(device_ordinal >= 0 && device_ordinal < count, HB_ERR_INVALID_ARGUMENT,
+             "device ordinal out of range");
+  HB_CUDA(cudaSetDevice(device_ordinal));
+  hb_context *c = new hb_context();
+  c->device = device_ordinal;
+  cudaDeviceProp prop;
+  HB_CUDA(cudaGetDeviceProperties(&prop, device_ordinal));
+  if (prop.major < 10) {
+    delete c;
+    return hb_fail(HB_ERR_UNSUPPORTED, "heddle_b200 is built for sm_100a (B200)");
+  }
+  c->n_sm = prop.multiProcessorCount;
+  HB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  HB_CUDA(cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking));
+  HB_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+  HB_CUDA(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+  *out = c;
+  return HB_OK;
+}
+
+extern "C" int hb_context_destroy(hb_context *ctx) {
+  if (!ctx) return HB_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaStreamSynchronize(ctx->stream2);
+  for (auto e : ctx->tev) cudaEventDestroy(e);
+  cudaEventDestroy(ctx->ev_fork);
+  cudaEventDestroy(ctx->ev_join);
+  cudaStreamDestroy(ctx->stream);
+  cudaStreamDestroy(ctx->stream2);
+  delete ctx;
+  return HB_OK;
+}
+
+extern "C" int hb_context_synchronize(hb_context *ctx) {
+  HB_REQUIRE(ctx, HB_ERR_INVALID_ARGUMENT, "null context");
+  HB_CUDA(cudaStreamSynchronize(ctx->stream));
+  HB_CUDA(cudaStreamSynchronize(ctx->stream2));
+  return HB_OK;
+}
+
+// ---------------------------------------------------------------------
+// timing: event pairs per stage, summed at the end of a call
+// ---------------------------------------------------------------------
+struct StageTimer {
+  hb_context *ctx;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+  size_t used = 0;
+  cudaEvent_t get() {
+    if (used < ctx->tev.size()) return ctx->tev[used++];
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    ctx->tev.push_back(e);
+    used++;
+    return e;
+  }
+};
+static thread_local StageTimer *g_timer = nullptr;
+
+static cudaEvent_t stage_begin(cudaStream_t s) {
+  if (!g_timer) return nullptr;
+  cudaEvent_t e = g_timer->get();
+  cudaEventRecord(e, s);
+  return e;
+}
+static void stage_end(int stage, cudaEvent_t b, cudaStream_t s) {
+  if (!g_timer || !b) return;
+  cudaEvent_t e = g_timer->get();
+  cudaEventRecord(e, s);
+  g_timer->marks.push_back({stage, {b, e}});
+}
+
+// ---------------------------------------------------------------------
+// system
+// ---------------------------------------------------------------------
+static DBox make_dbox(const double b[6]) {
+  DBox d;
+  d.lx = (float)b[0];
+  d.ly = (float)b[1];
+  d.lz = (float)b[2];
+  d.xy = (float)b[3];
+  d.xz = (float)b[4];
+  d.yz = (float)b[5];
+  d.ilx = (float)(1.0 / b[0]);
+  d.ily = (float)(1.0 / b[1]);
+  d.ilz = (float)(1.0 / b[2]);
+  d.ortho = (b[3] == 0.0 && b[4] == 0.0 && b[5] == 0.0) ? 1 : 0;
+  return d;
+}
+
+static bool finite6(const double b[6]) {
+  for (int d = 0; d < 6; ++d)
+    if (!std::isfinite(b[d])) return false;
+  return b[0] > 0.0 && b[1] > 0.0 && b[2] > 0.0;
+}
+
+static void perp_widths(const double b[6], double w[3]) {
+  const double a[3] = {b[0], 0.0, 0.0}, bb[3] = {b[3], b[1], 0.0}, c[3] = {b[4], b[5], b[2]};
+  const double vol = b[0] * b[1] * b[2];
+  auto cr = [](const double *x, const double *y, double *o) {
+    o[0] = x[1] * y[2] - x[2] * y[1];
+    o[1] = x[2] * y[0] - x[0] * y[2];
+    o[2] = x[0] * y[1] - x[1] * y[0];
+  };
+  double t[3];
+  cr(bb, c, t);
+  w[0] = vol / std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+  cr(c, a, t);
+  w[1] = vol / std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+  cr(a, bb, t);
+  w[2] = vol / std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+}
+
+// wrap a position into the primary cell in FP64 (kernels/pbc.cuh:73-91)
+static void wrap_host(const double b[6], double &x, double &y, double &z, int &ka, int &kb,
+                      int &kc) {
+  double sc = z / b[2];
+  double sb = (y - sc * b[5]) / b[1];
+  double sa = (x - sb * b[3] - sc * b[4]) / b[0];
+  double fa = std::floor(sa + 0.5), fb = std::floor(sb + 0.5), fc = std::floor(sc + 0.5);
+  x -= fa * b[0] + fb * b[3] + fc * b[4];
+  y -= fb * b[1] + fc * b[5];
+  z -= fc * b[2];
+  ka = (int)fa;
+  kb = (int)fb;
+  kc = (int)fc;
+}
+
+static int upload_state(hb_system *sys, const double *pos, const double *vel,
+                        const int32_t *images_in, bool keep_images) {
+  const uint32_t n = sys->n;
+  std::vector<float4> posq(n), v(n);
+  std::vector<int4> img(n);
+  std::vector<int4> old_img;
+  if (keep_images && n) {
+    old_img.resize(n);
+    HB_CUDA(cudaMemcpy(old_img.data(), sys->d_image, sizeof(int4) * n, cudaMemcpyDeviceToHost));
+  }
+  for (uint32_t i = 0; i < n; ++i) {
+    double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+    if (!std::isfinite(x) || !std::isfinite(y) || !std::isfinite(z))
+      return hb_fail(HB_ERR_NOT_FINITE, "non-finite position for atom " + std::to_string(i));
+    int ka, kb, kc;
+    wrap_host(sys->box, x, y, z, ka, kb, kc);
+    posq[i] = make_float4((float)x, (float)y, (float)z, (float)sys->h_charge[i]);
+    int4 im;
+    if (keep_images) {
+      im = old_img[i];
+      im.x += ka;
+      im.y += kb;
+      im.z += kc;
+    } else {
+      im.x = ka + (images_in ? images_in[3 * i] : 0);
+      im.y = kb + (images_in ? images_in[3 * i + 1] : 0);
+      im.z = kc + (images_in ? images_in[3 * i + 2] : 0);
+    }
+    im.w = (int)sys->h_type[i];
+    img[i] = im;
+    const double m = sys->h_mass[i];
+    v[i] = make_float4(vel ? (float)vel[3 * i] : 0.f, vel ? (float)vel[3 * i + 1] : 0.f,
+                       vel ? (float)vel[3 * i + 2] : 0.f, (float)(1.0 / m));
+  }
+  if (n) {
+    HB_CUDA(cudaMemcpy(sys->d_posq, posq.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+    HB_CUDA(cudaMemcpy(sys->d_image, img.data(), sizeof(int4) * n, cudaMemcpyHostToDevice));
+    if (vel || !keep_images)
+      HB_CUDA(cudaMemcpy(sys->d_vel, v.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+    // the pre-drift snapshot is the constraints' reference frame: only a
+    // new system initialises it
+    if (!keep_images)
+      HB_CUDA(cudaMemcpy(sys->d_pos_prev, posq.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+  }
+  return HB_OK;
+}
+
+extern "C" int hb_system_create(hb_context *ctx, const hb_system_desc *d, hb_system **out) {
+  HB_REQUIRE(ctx && d && out, HB_ERR_INVALID_ARGUMENT, "null argument");
+  HB_REQUIRE(finite6(d->box), HB_ERR_NOT_FINITE, "box must be finite with positive diagonal");
+  const uint32_t n = d->n_atoms;
+  HB_REQUIRE(n == 0 || (d->positions && d->masses && d->charges && d->types),
+             HB_ERR_INVALID_ARGUMENT, "positions, masses, charges and types are required");
+  for (uint32_t i = 0; i < n; ++i) {
+    HB_REQUIRE(std::isfinite(d->masses[i]) && d->masses[i] > 0.0, HB_ERR_INVALID_ARGUMENT,
+               "masses must be finite and positive");
+    HB_REQUIRE(std::isfinite(d->charges[i]), HB_ERR_NOT_FINITE, "charges must be finite");
+  }
+  HB_CUDA(cudaSetDevice(ctx->device));
+  hb_system *s = new hb_system();
+  s->ctx = ctx;
+  s->n = n;
+  std::memcpy(s->box, d->box, sizeof(double) * 6);
+  s->h_mass.assign(d->masses, d->masses + n);
+  s->h_charge.assign(d->charges, d->charges + n);
+  s->h_type.assign(d->types, d->types + n);
+  const size_t nn = std::max<size_t>(n, 1);
+  HB_CUDA(cudaMalloc(&s->d_box, sizeof(DBox)));
+  DBox db = make_dbox(d->box);
+  HB_CUDA(cudaMemcpy(s->d_box, &db, sizeof(DBox), cudaMemcpyHostToDevice));
+  HB_CUDA(cudaMalloc(&s->d_posq, sizeof(float4) * nn));
+  HB_CUDA(cudaMalloc(&s->d_vel, sizeof(float4) * nn));
+  HB_CUDA(cudaMalloc(&s->d_image, sizeof(int4) * nn));
+  HB_CUDA(cudaMalloc(&s->d_force, sizeof(float4) * nn));
+  HB_CUDA(cudaMemset(s->d_force, 0, sizeof(float4) * nn));
+  HB_CUDA(cudaMalloc(&s->d_pos_prev, sizeof(float4) * nn));
+  HB_CUDA(cudaMalloc(&s->d_vlo, sizeof(double) * 3 * nn));
+  HB_CUDA(cudaMemset(s->d_vlo, 0, sizeof(double) * 3 * nn));
+  HB_CUDA(cudaMalloc(&s->d_xlo, sizeof(double) * 3 * nn));
+  HB_CUDA(cudaMemset(s->d_xlo, 0, sizeof(double) * 3 * nn));
+  HB_CUDA(cudaMalloc(&s->d_red, sizeof(double) * (4 * 296 + 8)));
+  HB_CUDA(cudaMallocHost(&s->h_red, sizeof(double) * 8));
+  int rc = upload_state(s, d->positions, d->velocities, d->images, false);
+  if (rc != HB_OK) {
+    hb_system_destroy(s);
+    return rc;
+  }
+  *out = s;
+  return HB_OK;
+}
+
+extern "C" int hb_system_destroy(hb_system *s) {
+  if (!s) return HB_OK;
+  cudaSetDevice(s->ctx->device);
+  cudaStreamSynchronize(s->ctx->stream);
+  cudaFree(s->d_box);
+  cudaFree(s->d_posq);
+  cudaFree(s->d_vel);
+  cudaFree(s->d_image);
+  cudaFree(s->d_force);
+  cudaFree(s->d_pos_prev);
+  cudaFree(s->d_vlo);
+  cudaFree(s->d_xlo);
+  cudaFree(s->d_red);
+  cudaFreeHost(s->h_red);
+  delete s;
+  return HB_OK;
+}
+
+extern "C" int hb_system_set_state(hb_system *sys, const double *positions,
+                                   const double *velocities) {
+  HB_REQUIRE(sys, HB_ERR_INVALID_ARGUMENT, "null system");
+  HB_CUDA(cudaStreamSynchronize(sys->ctx->stream));
+  const uint32_t n = sys->n;
+  if (positions) {
+    HB_TRY(upload_state(sys, positions, velocities, nullptr, true));
+  } else if (velocities && n) {
+    std::vector<float4> v(n);
+    for (uint32_t i = 0; i < n; ++i)
+      v[i] = make_float4((float)velocities[3 * i], (float)velocities[3 * i + 1],
+                         (float)velocities[3 * i + 2], (float)(1.0 / sys->h_mass[i]));
+    HB_CUDA(cudaMemcpy(sys->d_vel, v.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+  }
+  return HB_OK;
+}
+
+extern "C" int hb_system_get_state(hb_system *sys, double *positions, double *velocities,
+                                   int32_t *images, double *forces) {
+  HB_REQUIRE(sys, HB_ERR_INVALID_ARGUMENT, "null system");
+  HB_CUDA(cudaStreamSynchronize(sys->ctx->stream));
+  HB_CUDA(cudaStreamSynchronize(sys->ctx->stream2));
+  const uint32_t n = sys->n;
+  if (!n) return HB_OK;
+  std::vector<float4> buf(n);
+  if (positions) {
+    HB_CUDA(cudaMemcpy(buf.data(), sys->d_posq, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < n; ++i) {
+      positions[3 * i] = buf[i].x;
+      positions[3 * i + 1] = buf[i].y;
+      positions[3 * i + 2] = buf[i].z;
+    }
+  }
+  if (velocities) {
+    HB_CUDA(cudaMemcpy(buf.data(), sys->d_vel, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < n; ++i) {
+      velocities[3 * i] = buf[i].x;
+      velocities[3 * i + 1] = buf[i].y;
+      velocities[3 * i + 2] = buf[i].z;
+    }
+  }
+  if (forces) {
+    HB_CUDA(cudaMemcpy(buf.data(), sys->d_force, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < n; ++i) {
+      forces[3 * i] = buf[i].x;
+      forces[3 * i + 1] = buf[i].y;
+      forces[3 * i + 2] = buf[i].z;
+    }
+  }
+  if (images) {
+    std::vector<int4> im(n);
+    HB_CUDA(cudaMemcpy(im.data(), sys->d_image, sizeof(int4) * n, cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < n; ++i) {
+      images[3 * i] = im[i].x;
+      images[3 * i + 1] = im[i].y;
+      images[3 * i + 2] = im[i].z;
+    }
+  }
+  return HB_OK;
+}
+
+extern "C" int hb_system_set_box(hb_system *sys, const double box[6]) {
+  HB_REQUIRE(sys && box, HB_ERR_INVALID_ARGUMENT, "null argument");
+  HB_REQUIRE(finite6(box), HB_ERR_NOT_FINITE, "box must be finite with positive diagonal");
+  std::memcpy(sys->box, box, sizeof(double) * 6);
+  DBox db = make_dbox(box);
+  HB_CUDA(cudaMemcpyAsync(sys->d_box, &db, sizeof(DBox), cudaMemcpyHostToDevice, sys->ctx->stream));
+  HB_CUDA(cudaStreamSynchronize(sys->ctx->stream));
+  return HB_OK;
+}
+
+extern "C" int hb_system_get_box(hb_system *sys, double box[6]) {
+  HB_REQUIRE(sys && box, HB_ERR_INVALID_ARGUMENT, "null argument");
+  std::memcpy(box, sys->box, sizeof(double) * 6);
+  return HB_OK;
+}
+
+// ---------------------------------------------------------------------
+// force field
+// ---------------------------------------------------------------------
+extern "C" int hb_forcefield_destroy(hb_forcefield *ff) {
+  if (!ff) return HB_OK;
+  cudaSetDevice(ff->sys->ctx->device);
+  hb_context_synchronize(ff->sys->ctx);
+  nl_free(ff);
+  if (ff->spme.on) spme_free(ff);
+  cudaFree(ff->d_lj);
+  cudaFree(ff->d_excl_off);
+  cudaFree(ff->d_excl_partner);
+  cudaFree(ff->d_excl_scale);
+  cudaFree(ff->d_scalars);
+  cudaFree(ff->d_acc);
+  cudaFree(ff->d_energy);
+  cudaFree(ff->d_virial);
+  delete ff;
+  return HB_OK;
+}
+
+extern "C" int hb_forcefield_create(hb_system *sys, const hb_forcefield_desc *d,
+                                    hb_forcefield **out) {
+  HB_REQUIRE(sys && d && out, HB_ERR_INVALID_ARGUMENT, "null argument");
+  const uint32_t n = sys->n;
+  hb_forcefield tmp;
+  double rc_max = 0.0;
+  if (d->lj_enabled) {
+    HB_REQUIRE(d->n_types >= 1 && d->n_types <= 64, HB_ERR_INVALID_ARGUMENT,
+               "LJ needs 1..64 particle types");
+    HB_REQUIRE(d->lj_sigma && d->lj_epsilon && d->lj_cutoff && d->lj_switch,
+               HB_ERR_INVALID_ARGUMENT, "LJ tables are required");
+    for (uint32_t i = 0; i < n; ++i)
+      HB_REQUIRE(sys->h_type[i] < d->n_types, HB_ERR_INVALID_ARGUMENT,
+                 "particle type index out of range");
+    const uint32_t nt2 = d->n_types * d->n_types;
+    for (uint32_t k = 0; k < nt2; ++k) {
+      const double sg = d->lj_sigma[k], ep = d->lj_epsilon[k], c = d->lj_cutoff[k],
+                   sw = d->lj_switch[k];
+      HB_REQUIRE(std::isfinite(sg) && std::isfinite(ep) && std::isfinite(c) && std::isfinite(sw),
+                 HB_ERR_NOT_FINITE, "LJ parameters must be finite");
+      HB_REQUIRE(c > 0.0 && sw > 0.0 && sw <= c, HB_ERR_INVALID_ARGUMENT,
+                 "LJ needs 0 < r_switch <= cutoff");
+      if (ep != 0.0) rc_max = std::max(rc_max, c);
+      if (sw < c) tmp.any_switch = 1;
+      tmp.h_lj.push_back(make_float4((float)(sg * sg), (float)(24.0 * ep), (float)(c * c),
+                                     (float)(sw * sw)));
+    }
+    tmp.lj_on = 1;
+    tmp.n_types = d->n_types;
+  }
+  if (d->coulomb_enabled) {
+    HB_REQUIRE(std::isfinite(d->alpha) && d->alpha > 0.0 && std::isfinite(d->r_cut_coulomb) &&
+                   d->r_cut_coulomb > 0.0,
+               HB_ERR_INVALID_ARGUMENT, "Coulomb needs alpha > 0 and r_cut > 0");
+    tmp.coul_on = 1;
+    tmp.alpha = (float)d->alpha;
+    tmp.coul_rc2 = (float)(d->r_cut_coulomb * d->r_cut_coulomb);
+    rc_max = std::max(rc_max, d->r_cut_coulomb);
+  }
+  if (d->recip_enabled) {
+    HB_REQUIRE(d->coulomb_enabled, HB_ERR_UNSUPPORTED,
+               "SPME reciprocal needs the erfc real-space slot");
+    HB_REQUIRE(d->spline_order >= 4 && d->spline_order <= 8, HB_ERR_INVALID_ARGUMENT,
+               "spline order must be 4..8");
+  }
+  HB_REQUIRE(std::isfinite(d->r_skin) && d->r_skin >= 0.0, HB_ERR_INVALID_ARGUMENT,
+             "r_skin must be finite and >= 0");
+  if (!tmp.lj_on) tmp.n_types = 1;
+  if (tmp.h_lj.empty()) tmp.h_lj.push_back(make_float4(0.f, 0.f, 0.f, 0.f));
+  tmp.rc_max = (float)rc_max;
+  tmp.r_skin = (float)d->r_skin;
+  tmp.r_search = (float)(rc_max + d->r_skin);
+  // minimum image is well defined only for r_search <= half the smallest
+  // perpendicular width (src/integrator/mc_barostat.rs:290-297)
+  double w[3];
+  perp_widths(sys->box, w);
+  const double wmin = std::min(w[0], std::min(w[1], w[2]));
+  if ((tmp.lj_on || tmp.coul_on) && n > 1 && wmin < 2.0 * (rc_max + d->r_skin) * (1.0 + 1e-4))
+    return hb_fail(HB_ERR_BOX_TOO_SMALL,
+                   "box perpendicular width " + std::to_string(wmin) +
+                       " is below 2 * (r_cut + r_skin) = " +
+                       std::to_string(2.0 * (rc_max + d->r_skin)));
+  // exclusions: symmetric CSR with ids in range
+  std::vector<uint32_t> eoff, epart;
+  std::vector<float2> escale;
+  if (d->excl_offsets) {
+    HB_REQUIRE(d->excl_offsets[0] == 0, HB_ERR_INVALID_ARGUMENT, "exclusion offsets must start at 0");
+    eoff.assign(d->excl_offsets, d->excl_offsets + n + 1);
+    const uint32_t ne = eoff[n];
+    HB_REQUIRE(ne == 0 || (d->excl_partners && d->excl_lj_scale && d->excl_coulomb_scale),
+               HB_ERR_INVALID_ARGUMENT, "exclusion arrays are required");
+    std::set<std::pair<uint32_t, uint32_t>> keys;
+    for (uint32_t i = 0; i < n; ++i) {
+      HB_REQUIRE(eoff[i] <= eoff[i + 1], HB_ERR_INVALID_ARGUMENT, "exclusion offsets must be monotone");
+      for (uint32_t q = eoff[i]; q < eoff[i + 1]; ++q) {
+        uint32_t j = d->excl_partners[q];
+        HB_REQUIRE(j < n && j != i, HB_ERR_INVALID_ARGUMENT, "bad exclusion partner");
+        keys.insert({i, j});
+        double sl = d->excl_lj_scale[q], sc = d->excl_coulomb_scale[q];
+        HB_REQUIRE(std::isfinite(sl) && std::isfinite(sc), HB_ERR_NOT_FINITE, "exclusion scales must be finite");
+        if (sl != 0.0 || sc != 0.0) tmp.excl_scaled = 1;
+        escale.push_back(make_float2((float)sl, (float)sc));
+      }
+    }
+    for (auto &k : keys)
+      HB_REQUIRE(keys.count({k.second, k.first}), HB_ERR_INVALID_ARGUMENT,
+                 "exclusion lists must be symmetric");
+    epart.assign(d->excl_partners, d->excl_partners + ne);
+  }
+  hb_forcefield *ff = new hb_forcefield();
+  *ff = tmp;
+  ff->sys = sys;
+  HB_CUDA(cudaSetDevice(sys->ctx->device));
+  HB_CUDA(cudaMalloc(&ff->d_lj, sizeof(float4) * ff->h_lj.size()));
+  HB_CUDA(cudaMemcpy(ff->d_lj, ff->h_lj.data(), sizeof(float4) * ff->h_lj.size(),
+                     cudaMemcpyHostToDevice));
+  if (!eoff.empty()) {
+    HB_CUDA(cudaMalloc(&ff->d_excl_off, sizeof(uint32_t) * eoff.size()));
+    HB_CUDA(cudaMemcpy(ff->d_excl_off, eoff.data(), sizeof(uint32_t) * eoff.size(), cudaMemcpyHostToDevice));
+    const size_t ne = std::max<size_t>(epart.size(), 1);
+    HB_CUDA(cudaMalloc(&ff->d_excl_partner, sizeof(uint32_t) * ne));
+    HB_CUDA(cudaMalloc(&ff->d_excl_scale, sizeof(float2) * ne));
+    if (!epart.empty()) {
+      HB_CUDA(cudaMemcpy(ff->d_excl_partner, epart.data(), sizeof(uint32_t) * epart.size(), cudaMemcpyHostToDevice));
+      HB_CUDA(cudaMemcpy(ff->d_excl_scale, escale.data(), sizeof(float2) * escale.size(), cudaMemcpyHostToDevice));
+    }
+    ff->n_excl = (uint32_t)epart.size();
+  }
+  HB_CUDA(cudaMalloc(&ff->d_scalars, sizeof(double) * 8));
+  HB_CUDA(cudaMemset(ff->d_scalars, 0, sizeof(double) * 8));
+  HB_CUDA(cudaMalloc(&ff->d_acc, sizeof(unsigned long long) * 4));
+  HB_CUDA(cudaMemset(ff->d_acc, 0, sizeof(unsigned long long) * 4));
+  const size_t nn = std::max<size_t>(n, 1);
+  HB_CUDA(cudaMalloc(&ff->d_energy, sizeof(float) * nn));
+  HB_CUDA(cudaMalloc(&ff->d_virial, sizeof(float) * nn));
+  HB_CUDA(cudaMemset(ff->d_energy, 0, sizeof(float) * nn));
+  HB_CUDA(cudaMemset(ff->d_virial, 0, sizeof(float) * nn));
+  int rc = nl_setup(ff);
+  if (rc == HB_OK && d->recip_enabled) rc = spme_setup(ff, d);
+  if (rc == HB_OK) rc = nl_first_build(ff);
+  if (rc != HB_OK) {
+    std::string msg = g_err;
+    hb_forcefield_destroy(ff);
+    return hb_fail(rc, msg);
+  }
+  *out = ff;
+  return HB_OK;
+}
+
+// ForceField::step body: gated neighbour rebuild, pair kernel on the main
+// stream overlapped with the SPME chain on the second stream, combine.
+static int force_eval(hb_forcefield *ff, bool ev) {
+  hb_context *ctx = ff->sys->ctx;
+  cudaStream_t s = ctx->stream, s2 = ctx->stream2;
+  cudaEvent_t t0 = stage_begin(s);
+  HB_TRY(nl_displacement_check(ff, s));
+  HB_TRY(nl_rebuild(ff, true, s));
+  HB_TRY(nl_gather_positions(ff, s));
+  stage_end(3, t0, s);
+  if (ff->spme.on) {
+    HB_CUDA(cudaEventRecord(ctx->ev_fork, s));
+    HB_CUDA(cudaStreamWaitEvent(s2, ctx->ev_fork, 0));
+    cudaEvent_t t2 = stage_begin(s2);
+    HB_TRY(spme_launch(ff, ev, s2));
+    stage_end(2, t2, s2);
+    HB_CUDA(cudaEventRecord(ctx->ev_join, s2));
+  }
+  cudaEvent_t t1 = stage_begin(s);
+  HB_TRY(pair_launch(ff, ev, s));
+  stage_end(1, t1, s);
+  if (ff->spme.on) HB_CUDA(cudaStreamWaitEvent(s, ctx->ev_join, 0));
+  HB_TRY(forces_finalize(ff, ev, s));
+  return HB_OK;
+}
+
+// host check of the status word: overflow is an error (the reference's
+// PackedNeighborOverflow), high water grows the buffers
+static int check_status(hb_forcefield *ff) {
+  cudaStream_t s = ff->sys->ctx->stream;
+  HB_CUDA(cudaMemcpyAsync(ff->h_status, ff->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  HB_CUDA(cudaStreamSynchronize(s));
+  const uint32_t st = ff->h_status[0];
+  if (st & HB_ST_ENTRY_OVERFLOW)
+    return hb_fail(HB_ERR_NL_OVERFLOW, "packed neighbour entries overflowed their capacity");
+  if (st & HB_ST_ENTRY_HIGHWATER) HB_TRY(nl_first_build(ff));
+  return HB_OK;
+}
+
+extern "C" int hb_forcefield_step(hb_forcefield *ff, int level) {
+  HB_REQUIRE(ff, HB_ERR_INVALID_ARGUMENT, "null force field");
+  HB_REQUIRE(level == HB_FORCES_ONLY || level == HB_FORCES_AND_SCALARS, HB_ERR_INVALID_ARGUMENT,
+             "bad aggregate level");
+  HB_TRY(force_eval(ff, level == HB_FORCES_AND_SCALARS));
+  return check_status(ff);
+}
+
+extern "C" int hb_forcefield_pre_step(hb_forcefield *ff, int force, int *rebuilt) {
+  HB_REQUIRE(ff, HB_ERR_INVALID_ARGUMENT, "null force field");
+  cudaStream_t s = ff->sys->ctx->stream;
+  uint32_t before = 0, after = 0;
+  HB_CUDA(cudaMemcpyAsync(&before, ff->d_counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  if (force) {
+    HB_TRY(nl_rebuild(ff, false, s));
+  } else {
+    HB_TRY(nl_displacement_check(ff, s));
+    HB_TRY(nl_rebuild(ff, true, s));
+  }
+  HB_CUDA(cudaMemcpyAsync(&after, ff->d_counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  HB_CUDA(cudaStreamSynchronize(s));
+  if (rebuilt) *rebuilt = after != before ? 1 : 0;
+  return check_status(ff);
+}
+
+extern "C" int hb_forcefield_scalars(hb_forcefield *ff, double out[8]) {
+  HB_REQUIRE(ff && out, HB_ERR_INVALID_ARGUMENT, "null argument");
+  HB_CUDA(cudaStreamSynchronize(ff->sys->ctx->stream));
+  HB_CUDA(cudaMemcpy(out, ff->d_scalars, sizeof(double) * 8, cudaMemcpyDeviceToHost));
+  return HB_OK;
+}
+
+extern "C" int hb_forcefield_get_per_atom(hb_forcefield *ff, double *energy, double *virial) {
+  HB_REQUIRE(ff, HB_ERR_INVALID_ARGUMENT, "null force field");
+  HB_CUDA(cudaStreamSynchronize(ff->sys->ctx->stream));
+  const uint32_t n = ff->sys->n;
+  std::vector<float> b(std::max(n, 1u));
+  if (energy && n) {
+    HB_CUDA(cudaMemcpy(b.data(), ff->d_energy, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < n; ++i) energy[i] = b[i];
+  }
+  if (virial && n) {
+    HB_CUDA(cudaMemcpy(b.data(), ff->d_virial, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < n; ++i) virial[i] = b[i];
+  }
+  return HB_OK;
+}
+
+extern "C" int hb_neighbor_pairs(hb_forcefield *ff, uint32_t *pairs, uint64_t cap,
+                                 uint64_t *count, uint64_t *duplicates) {
+  HB_REQUIRE(ff && count, HB_ERR_INVALID_ARGUMENT, "null argument");
+  std::vector<uint32_t> p;
+  uint64_t dups = 0;
+  HB_TRY(nl_pairs(ff, p, dups));
+  const uint64_t cnt = p.size() / 2;
+  *count = cnt;
+  if (duplicates) *duplicates = dups;
+  if (pairs) std::memcpy(pairs, p.data(), sizeof(uint32_t) * 2 * std::min(cnt, cap));
+  return HB_OK;
+}
+
+extern "C" int hb_neighbor_stats(hb_forcefield *ff, uint64_t out[6]) {
+  HB_REQUIRE(ff && out, HB_ERR_INVALID_ARGUMENT, "null argument");
+  cudaStream_t s = ff->sys->ctx->stream;
+  uint32_t cnt[4] = {0, 0, 0, 0}, st = 0;
+  HB_CUDA(cudaMemcpyAsync(cnt, ff->d_counters, sizeof(uint32_t) * 4, cudaMemcpyDeviceToHost, s));
+  HB_CUDA(cudaMemcpyAsync(&st, ff->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  uint32_t total = 0;
+  if (ff->n_tiles)
+    HB_CUDA(cudaMemcpyAsync(&total, ff->d_entry_off + ff->n_tiles, sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, s));
+  HB_CUDA(cudaStreamSynchronize(s));
+  out[0] = ff->n_tiles;
+  out[1] = total;
+  out[2] = ff->entry_cap;
+  out[3] = cnt[0];
+  out[4] = st;
+  out[5] = (uint64_t)total * 32u * 32u;
+  return HB_OK;
+}
+
+// ---------------------------------------------------------------------
+// constraints
+// ---------------------------------------------------------------------
+extern "C" int hb_constraints_destroy(hb_constraints *c) {
+  if (!c) return HB_OK;
+  cudaSetDevice(c->sys->ctx->device);
+  cudaStreamSynchronize(c->sys->ctx->stream);
+  cudaFree(c->d_settle_atoms);
+  cudaFree(c->d_settle_geom);
+  cudaFree(c->d_settle_mass);
+  cudaFree(c->d_shake_aoff);
+  cudaFree(c->d_shake_atoms);
+  cudaFree(c->d_shake_coff);
+  cudaFree(c->d_shake_pairs);
+  cudaFree(c->d_shake_d2);
+  cudaFree(c->d_virial);
+  cudaFree(c->d_iters);
+  delete c;
+  return HB_OK;
+}
+
+extern "C" int hb_constraints_create(hb_system *sys, const hb_constraints_desc *d,
+                                     hb_constraints **out) {
+  HB_REQUIRE(sys && d && out, HB_ERR_INVALID_ARGUMENT, "null argument");
+  const uint32_t n = sys->n, ng = d->n_groups;
+  HB_REQUIRE(ng == 0 || (d->group_offsets && d->group_atoms && d->group_kind),
+             HB_ERR_INVALID_ARGUMENT, "group arrays are required");
+  std::vector<uint4> s_atoms;
+  std::vector<float4> s_geom;
+  std::vector<float2> s_mass;
+  std::vector<uint32_t> h_aoff{0}, h_atoms, h_coff{0};
+  std::vector<uint2> h_pairs;
+  std::vector<double> h_d2;
+  std::vector<char> seen(n, 0);
+  for (uint32_t g = 0; g < ng; ++g) {
+    const uint32_t a0 = d->group_offsets[g], a1 = d->group_offsets[g + 1];
+    HB_REQUIRE(a1 > a0, HB_ERR_CONSTRAINT_SHAPE, "empty constraint group");
+    for (uint32_t a = a0; a < a1; ++a) {
+      const uint32_t id = d->group_atoms[a];
+      HB_REQUIRE(id < n, HB_ERR_CONSTRAINT_SHAPE, "constraint atom out of range");
+      HB_REQUIRE(!seen[id], HB_ERR_CONSTRAINT_SHAPE, "an atom belongs to two constraint groups");
+      seen[id] = 1;
+    }
+    if (d->group_kind[g] == HB_CONSTRAINT_SETTLE) {
+      HB_REQUIRE(a1 - a0 == 3, HB_ERR_CONSTRAINT_SHAPE, "SETTLE groups hold exactly 3 atoms (O, H, H)");
+      HB_REQUIRE(d->settle_ra && d->settle_rb && d->settle_rc, HB_ERR_INVALID_ARGUMENT,
+                 "SETTLE geometry is required");
+      const uint32_t o = d->group_atoms[a0], h1 = d->group_atoms[a0 + 1], h2 = d->group_atoms[a0 + 2];
+      HB_REQUIRE(sys->h_mass[h1] == sys->h_mass[h2], HB_ERR_CONSTRAINT_SHAPE,
+                 "SETTLE needs equal hydrogen masses");
+      s_atoms.push_back(make_uint4(o, h1, h2, 0));
+      s_geom.push_back(make_float4((float)d->settle_ra[g], (float)d->settle_rb[g],
+                                   (float)d->settle_rc[g], 0.f));
+      s_mass.push_back(make_float2((float)sys->h_mass[o], (float)sys->h_mass[h1]));
+    } else if (d->group_kind[g] == HB_CONSTRAINT_SHAKE) {
+      HB_REQUIRE(a1 - a0 <= 8, HB_ERR_CONSTRAINT_SHAPE, "SHAKE groups hold at most 8 atoms");
+      HB_REQUIRE(d->con_offsets && d->con_i && d->con_j && d->con_dist, HB_ERR_INVALID_ARGUMENT,
+                 "SHAKE constraints are required");
+      const uint32_t c0 = d->con_offsets[g], c1 = d->con_offsets[g + 1];
+      HB_REQUIRE(c1 >= c0 && c1 - c0 <= 12, HB_ERR_CONSTRAINT_SHAPE,
+                 "SHAKE groups hold at most 12 constraints");
+      for (uint32_t a = a0; a < a1; ++a) h_atoms.push_back(d->group_atoms[a]);
+      h_aoff.push_back((uint32_t)h_atoms.size());
+      for (uint32_t k = c0; k < c1; ++k) {
+        HB_REQUIRE(d->con_i[k] < a1 - a0 && d->con_j[k] < a1 - a0 && d->con_i[k] != d->con_j[k],
+                   HB_ERR_CONSTRAINT_SHAPE, "bad SHAKE constraint pair");
+        HB_REQUIRE(std::isfinite(d->con_dist[k]) && d->con_dist[k] > 0.0, HB_ERR_CONSTRAINT_SHAPE,
+                   "SHAKE distances must be positive");
+        h_pairs.push_back(make_uint2(d->con_i[k], d->con_j[k]));
+        h_d2.push_back(d->con_dist[k] * d->con_dist[k]);
+      }
+      h_coff.push_back((uint32_t)h_pairs.size());
+    } else {
+      return hb_fail(HB_ERR_CONSTRAINT_SHAPE, "unknown constraint kind");
+    }
+  }
+  hb_constraints *c = new hb_constraints();
+  c->sys = sys;
+  c->n_settle = (uint32_t)s_atoms.size();
+  c->n_shake = (uint32_t)h_aoff.size() - 1;
+  if (d->shake_tol > 0.0) c->shake_tol = d->shake_tol;
+  if (d->shake_max_iter > 0) c->shake_max_iter = d->shake_max_iter;
+  auto up = [](void **dst, const void *src, size_t bytes) -> int {
+    HB_CUDA(cudaMalloc(dst, std::max<size_t>(bytes, 16)));
+    if (bytes) HB_CUDA(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+    return HB_OK;
+  };
+  int rc = HB_OK;
+  if (rc == HB_OK) rc = up((void **)&c->d_settle_atoms, s_atoms.data(), sizeof(uint4) * s_atoms.size());
+  if (rc == HB_OK) rc = up((void **)&c->d_settle_geom, s_geom.data(), sizeof(float4) * s_geom.size());
+  if (rc == HB_OK) rc = up((void **)&c->d_settle_mass, s_mass.data(), sizeof(float2) * s_mass.size());
+  if (rc == HB_OK) rc = up((void **)&c->d_shake_aoff, h_aoff.data(), sizeof(uint32_t) * h_aoff.size());
+  if (rc == HB_OK) rc = up((void **)&c->d_shake_atoms, h_atoms.data(), sizeof(uint32_t) * h_atoms.size());
+  if (rc == HB_OK) rc = up((void **)&c->d_shake_coff, h_coff.data(), sizeof(uint32_t) * h_coff.size());
+  if (rc == HB_OK) rc = up((void **)&c->d_shake_pairs, h_pairs.data(), sizeof(uint2) * h_pairs.size());
+  if (rc == HB_OK) rc = up((void **)&c->d_shake_d2, h_d2.data(), sizeof(double) * h_d2.size());
+  if (rc == HB_OK) {
+    const size_t nn = std::max<size_t>(n, 1);
+    if (cudaMalloc(&c->d_virial, sizeof(float) * nn) != cudaSuccess ||
+        cudaMemset(c->d_virial, 0, sizeof(float) * nn) != cudaSuccess ||
+        cudaMalloc(&c->d_iters, sizeof(uint32_t)) != cudaSuccess ||
+        cudaMemset(c->d_iters, 0, sizeof(uint32_t)) != cudaSuccess)
+      rc = hb_fail(HB_ERR_CUDA, "constraint buffer allocation failed");
+  }
+  if (rc != HB_OK) {
+    hb_constraints_destroy(c);
+    return rc;
+  }
+  *out = c;
+  return HB_OK;
+}
+
+extern "C" int hb_constraints_before_drift(hb_constraints *c) {
+  HB_REQUIRE(c, HB_ERR_INVALID_ARGUMENT, "null constraints");
+  hb_system *sys = c->sys;
+  if (sys->n)
+    HB_CUDA(cudaMemcpyAsync(sys->d_pos_prev, sys->d_posq, sizeof(float4) * sys->n,
+                            cudaMemcpyDeviceToDevice, sys->ctx->stream));
+  return HB_OK;
+}
+
+extern "C" int hb_constraints_after_drift(hb_constraints *c, double dt) {
+  HB_REQUIRE(c, HB_ERR_INVALID_ARGUMENT, "null constraints");
+  return cons_positions(c, dt, c->sys->ctx->stream);
+}
+
+extern "C" int hb_constraints_after_kick(hb_constraints *c, double dt) {
+  HB_REQUIRE(c, HB_ERR_INVALID_ARGUMENT, "null constraints");
+  return cons_velocities(c, dt, dt > 0.0, c->sys->ctx->stream);
+}
+
+extern "C" int hb_constraints_get_virial(hb_constraints *c, double *virial) {
+  HB_REQUIRE(c && virial, HB_ERR_INVALID_ARGUMENT, "null argument");
+  const uint32_t n = c->sys->n;
+  HB_CUDA(cudaStreamSynchronize(c->sys->ctx->stream));
+  std::vector<float> b(std::max(n, 1u));
+  if (n) HB_CUDA(cudaMemcpy(b.data(), c->d_virial, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  for (uint32_t i = 0; i < n; ++i) virial[i] = b[i];
+  return HB_OK;
+}
+
+// ---------------------------------------------------------------------
+// integrator
+// ---------------------------------------------------------------------
+extern "C" int hb_integrator_create(hb_system *sys, const hb_integrator_desc *d,
+                                    hb_integrator **out) {
+  HB_REQUIRE(sys && d && out, HB_ERR_INVALID_ARGUMENT, "null argument");
+  HB_REQUIRE(d->kind == HB_INTEGRATOR_VV || d->kind == HB_INTEGRATOR_VV_LOSSLESS ||
+                 d->kind == HB_INTEGRATOR_LANGEVIN,
+             HB_ERR_INVALID_ARGUMENT, "unknown integrator kind");
+  HB_REQUIRE(std::isfinite(d->dt) && d->dt > 0.0, HB_ERR_INVALID_ARGUMENT, "dt must be > 0");
+  if (d->kind == HB_INTEGRATOR_LANGEVIN)
+    HB_REQUIRE(std::isfinite(d->friction) && d->friction > 0.0 && std::isfinite(d->temperature) &&
+                   d->temperature > 0.0,
+               HB_ERR_INVALID_ARGUMENT, "Langevin needs friction > 0 and temperature > 0");
+  hb_integrator *it = new hb_integrator();
+  it->sys = sys;
+  it->kind = d->kind;
+  it->dt = d->dt;
+  it->friction = d->friction;
+  it->temperature = d->temperature;
+  it->seed = d->seed;
+  it->step = d->step0;
+  *out = it;
+  return HB_OK;
+}
+
+extern "C" int hb_integrator_destroy(hb_integrator *it) {
+  if (!it) return HB_OK;
+  if (it->graph_exec) cudaGraphExecDestroy(it->graph_exec);
+  delete it;
+  return HB_OK;
+}
+
+// One step.  Velocity Verlet keeps the reference's hook order
+// (src/integrator/mod.rs:344-429 with the post-force kick of
+// src/runner.rs:2673-2686): snapshot, kick-drift, position constraint,
+// forces, velocity projection, final half kick.  Langevin (middle scheme):
+// full kick, velocity projection, half drift, O, half drift, position
+// constraint, forces.
+static int one_step(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons, bool ev) {
+  cudaStream_t s = it->sys->ctx->stream;
+  cudaEvent_t t4 = stage_begin(s);
+  if (it->kind == HB_INTEGRATOR_LANGEVIN) {
+    HB_TRY(integ_lang_kick(it, s));
+    if (cons) HB_TRY(cons_velocities(cons, 0.0, false, s));
+    HB_TRY(integ_lang_drift_ou(it, s));
+    if (cons) HB_TRY(cons_positions(cons, it->dt, s));
+    stage_end(4, t4, s);
+    HB_TRY(force_eval(ff, ev));
+  } else {
+    HB_TRY(integ_vv_kick_drift(it, s));
+    if (cons) HB_TRY(cons_positions(cons, it->dt, s));
+    stage_end(4, t4, s);
+    HB_TRY(force_eval(ff, ev));
+    cudaEvent_t t5 = stage_begin(s);
+    if (cons) HB_TRY(cons_velocities(cons, it->dt, true, s));
+    HB_TRY(integ_vv_kick(it, s));
+    stage_end(4, t5, s);
+  }
+  it->step++;
+  return HB_OK;
+}
+
+extern "C" int hb_integrator_step(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons,
+                                  uint32_t n_steps, uint32_t scalar_every) {
+  HB_REQUIRE(it && ff, HB_ERR_INVALID_ARGUMENT, "null argument");
+  HB_REQUIRE(ff->sys == it->sys && (!cons || cons->sys == it->sys), HB_ERR_INVALID_ARGUMENT,
+             "integrator, force field and constraints must share one system");
+  hb_context *ctx = it->sys->ctx;
+  StageTimer timer{ctx, {}, 0};
+  if (ctx->timing) g_timer = &timer;
+  cudaEvent_t t_all = stage_begin(ctx->stream);
+  int rc = HB_OK;
+  if (!it->forces_valid) {
+    rc = force_eval(ff, false);
+    it->forces_valid = rc == HB_OK;
+  }
+  for (uint32_t k = 0; k < n_steps && rc == HB_OK; ++k) {
+    const bool ev = scalar_every > 0 && ((k + 1) % scalar_every == 0);
+    rc = one_step(it, ff, cons, ev);
+  }
+  stage_end(0, t_all, ctx->stream);
+  g_timer = nullptr;
+  if (rc != HB_OK) return rc;
+  HB_TRY(check_status(ff));
+  if (ctx->timing) {
+    HB_CUDA(cudaStreamSynchronize(ctx->stream));
+    HB_CUDA(cudaStreamSynchronize(ctx->stream2));
+    for (int q = 0; q < 8; ++q) ctx->t_ms[q] = 0.0;
+    for (auto &m : timer.marks) {
+      float ms = 0.f;
+      HB_CUDA(cudaEventElapsedTime(&ms, m.second.first, m.second.second));
+      ctx->t_ms[m.first] += ms;
+    }
+  }
+  return HB_OK;
+}
+
+extern "C" int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
+                                        hb_constraints *cons, uint32_t n_steps) {
+  HB_REQUIRE(it && ff, HB_ERR_INVALID_ARGUMENT, "null argument");
+  hb_context *ctx = it->sys->ctx;
+  cudaStream_t s = ctx->stream;
+  if (!it->forces_valid) {
+    HB_TRY(force_eval(ff, false));
+    it->forces_valid = true;
+  }
+  if (it->kind == HB_INTEGRATOR_LANGEVIN) {
+    // the Philox step counter is a kernel argument; per-step graphs would
+    // freeze it, so the stochastic integrator runs eagerly
+    return hb_integrator_step(it, ff, cons, n_steps, 0);
+  }
+  if (!it->graph_exec || it->graph_ff != ff || it->graph_cons != cons) {
+    if (it->graph_exec) cudaGraphExecDestroy(it->graph_exec);
+    it->graph_exec = nullptr;
+    HB_CUDA(cudaStreamSynchronize(s));
+    cudaGraph_t g;
+    HB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int rc = one_step(it, ff, cons, false);
+    it->step--;
+    cudaError_t ce = cudaStreamEndCapture(s, &g);
+    if (rc != HB_OK) return rc;
+    if (ce != cudaSuccess) return hb_fail(HB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+    HB_CUDA(cudaGraphInstantiate(&it->graph_exec, g, 0));
+    cudaGraphDestroy(g);
+    it->graph_ff = ff;
+    it->graph_cons = cons;
+  }
+  for (uint32_t k = 0; k < n_steps; ++k) {
+    HB_CUDA(cudaGraphLaunch(it->graph_exec, s));
+    it->step++;
+  }
+  const uint64_t cap_before = ff->entry_cap;
+  HB_TRY(check_status(ff));
+  if (ff->entry_cap != cap_before) {
+    // buffers moved: the captured graph holds stale pointers
+    cudaGraphExecDestroy(it->graph_exec);
+    it->graph_exec = nullptr;
+  }
+  return HB_OK;
+}
+
+extern "C" int hb_integrator_count_launches(hb_integrator *it, hb_forcefield *ff,
+                                            hb_constraints *cons, uint64_t *kernels) {
+  HB_REQUIRE(it && ff && kernels, HB_ERR_INVALID_ARGUMENT, "null argument");
+  cudaStream_t s = it->sys->ctx->stream;
+  HB_CUDA(cudaStreamSynchronize(s));
+  cudaGraph_t g;
+  HB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  const uint64_t step = it->step;
+  int rc = one_step(it, ff, cons, false);
+  it->step = step;
+  cudaError_t ce = cudaStreamEndCapture(s, &g);
+  if (rc != HB_OK) return rc;
+  if (ce != cudaSuccess) return hb_fail(HB_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(ce));
+  size_t nn = 0;
+  HB_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  if (nn) HB_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+  uint64_t k = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    HB_CUDA(cudaGraphNodeGetType(nd, &t));
+    if (t == cudaGraphNodeTypeKernel) ++k;
+  }
+  cudaGraphDestroy(g);
+  *kernels = k;
+  return HB_OK;
+}
+
+extern "C" int hb_reduce_kinetic(hb_system *sys, double out[4]) {
+  HB_REQUIRE(sys && out, HB_ERR_INVALID_ARGUMENT, "null argument");
+  return reduce_kinetic(sys, out);
+}
+
+extern "C" int hb_timing_enable(hb_context *ctx, int enable) {
+  HB_REQUIRE(ctx, HB_ERR_INVALID_ARGUMENT, "null context");
+  ctx->timing = enable != 0;
+  return HB_OK;
+}
+
+extern "C" int hb_timing_get(hb_context *ctx, double out[8]) {
+  HB_REQUIRE(ctx && out, HB_ERR_INVALID_ARGUMENT, "null argument");
+  for (int q = 0; q < 8; ++q) out[q] = ctx->t_ms[q];
+  return HB_OK;
+}

@@ -1,0 +1,402 @@
+// hb_integ.cu -- force combine, FP64 scalar reductions and the integrator
+// kernels of the B200 force-and-constraint path.
+//
+//   * k_finalize: int64 fixed-point pair sums + SPME reciprocal terms ->
+//     f32 force per atom (atom order), clearing the accumulators for the
+//     next step (replaces finalize_packed_forces + combine_class_totals,
+//     kernels/neighbor.cu:728-760, kernels/forces.cu:13-41);
+//   * energy / virial totals are exact int64 sums of the fixed-point
+//     per-atom shares (order-independent), the reciprocal terms are FP64
+//     fixed-shape trees -> byte-identical scalars run to run
+//     (kernels/nose_hoover.cu:22-103, kernels/barostat.cu:11-78);
+//   * velocity Verlet kick-drift / kick (kernels/integrate.cu:24-265) with
+//     the lossless (f32 value + f64 low part) variant, and the Langevin
+//     middle scheme whose O step draws Philox-4x32-10 Gaussians keyed by
+//     (seed, step, atom, axis) (kernels/langevin.cu:13-80,
+//     kernels/philox.cuh).
+#include <cmath>
+
+#include "hb_internal.cuh"
+
+namespace {
+
+__device__ __forceinline__ float from_fixed(unsigned long long v) {
+  return (float)((double)(long long)v * HB_FP_INV_SCALE);
+}
+
+template <bool EV>
+__global__ void k_finalize(unsigned long long *__restrict__ fp, const float4 *__restrict__ recip,
+                           const uint32_t *__restrict__ sorted_ids, float4 *__restrict__ force,
+                           float *__restrict__ energy, float *__restrict__ virial,
+                           const double *__restrict__ spme_sums,
+                           unsigned long long *__restrict__ acc, uint32_t n, uint32_t np) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  long long e_fix = 0, w_fix = 0;
+  if (k < n) {
+    const uint32_t id = sorted_ids[k];
+    float fx = from_fixed(fp[k]);
+    float fy = from_fixed(fp[np + k]);
+    float fz = from_fixed(fp[2 * np + k]);
+    fp[k] = 0ull;
+    fp[np + k] = 0ull;
+    fp[2 * np + k] = 0ull;
+    float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (recip) r = recip[k];
+    force[id] = make_float4(fx + r.x, fy + r.y, fz + r.z, 0.0f);
+    if (EV) {
+      e_fix = (long long)fp[3 * np + k];
+      w_fix = (long long)fp[4 * np + k];
+      fp[3 * np + k] = 0ull;
+      fp[4 * np + k] = 0ull;
+      float wr = spme_sums ? (float)(spme_sums[1] / (double)n) : 0.0f;
+      energy[id] = (float)((double)e_fix * HB_FP_INV_SCALE) + r.w;
+      virial[id] = (float)((double)w_fix * HB_FP_INV_SCALE) + wr;
+    }
+  }
+  if (EV) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      e_fix += __shfl_xor_sync(0xFFFFFFFFu, e_fix, o);
+      w_fix += __shfl_xor_sync(0xFFFFFFFFu, w_fix, o);
+    }
+    if ((threadIdx.x & 31u) == 0u) {
+      if (e_fix) atomicAdd(&acc[1], (unsigned long long)e_fix);
+      if (w_fix) atomicAdd(&acc[2], (unsigned long long)w_fix);
+    }
+  }
+}
+
+__global__ void k_scalars(unsigned long long *__restrict__ acc,
+                          const double *__restrict__ spme_sums, double e_self,
+                          const float4 *__restrict__ recip_unused, double *__restrict__ out) {
+  const double lj = (double)(long long)acc[0] * HB_FP_INV_SCALE;
+  const double pair = (double)(long long)acc[1] * HB_FP_INV_SCALE;
+  const double wp = (double)(long long)acc[2] * HB_FP_INV_SCALE;
+  const double er = spme_sums ? spme_sums[0] : 0.0;
+  const double wr = spme_sums ? spme_sums[1] : 0.0;
+  out[0] = lj;
+  out[1] = pair - lj;
+  out[2] = er;
+  out[3] = spme_sums ? e_self : 0.0;
+  out[4] = pair + er - (spme_sums ? e_self : 0.0);
+  out[5] = wp;
+  out[6] = wr;
+  out[7] = wp + wr;
+  acc[0] = 0ull;
+  acc[1] = 0ull;
+  acc[2] = 0ull;
+}
+
+// ---- Philox-4x32-10 (Salmon et al. 2011), counter (step_lo, step_hi,
+// atom, axis), key = seed, as kernels/philox.cuh uses it
+__device__ __forceinline__ void philox(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1,
+                                       uint32_t c2, uint32_t c3, uint32_t &o0, uint32_t &o1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t hi0 = __umulhi(c0, 0xD2511F53u), lo0 = c0 * 0xD2511F53u;
+    const uint32_t hi2 = __umulhi(c2, 0xCD9E8D57u), lo2 = c2 * 0xCD9E8D57u;
+    const uint32_t n0 = hi2 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0;
+    c1 = lo2;
+    c2 = n2;
+    c3 = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  o0 = c0;
+  o1 = c1;
+}
+
+// Box-Muller cosine branch on the first two words, u = (x + 1/2) 2^-32
+// (kernels/philox.cuh:135-150), evaluated in single precision.
+__device__ __forceinline__ float gaussian(uint32_t s_lo, uint32_t s_hi, uint64_t step,
+                                          uint32_t atom, uint32_t axis) {
+  uint32_t o0, o1;
+  philox(s_lo, s_hi, (uint32_t)step, (uint32_t)(step >> 32), atom, axis, o0, o1);
+  const float u1 = ((float)(o0 >> 8) + 0.5f) * (1.0f / 16777216.0f);
+  const float u2 = ((float)(o1 >> 8) + 0.5f) * (1.0f / 16777216.0f);
+  return sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
+}
+
+__global__ void k_vv_kick_drift(float4 *__restrict__ posq, float4 *__restrict__ vel,
+                                int4 *__restrict__ image, const float4 *__restrict__ force,
+                                float4 *__restrict__ prev, const DBox *__restrict__ box, float dt,
+                                uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const DBox b = *box;
+  float4 p = posq[i];
+  float4 v = vel[i];
+  const float4 f = force[i];
+  prev[i] = p;
+  const float h = 0.5f * dt * v.w;
+  v.x += f.x * h;
+  v.y += f.y * h;
+  v.z += f.z * h;
+  p.x += v.x * dt;
+  p.y += v.y * dt;
+  p.z += v.z * dt;
+  int ka, kb, kc;
+  hb_wrap(p.x, p.y, p.z, ka, kb, kc, b);
+  int4 im = image[i];
+  im.x += ka;
+  im.y += kb;
+  im.z += kc;
+  image[i] = im;
+  posq[i] = p;
+  vel[i] = v;
+}
+
+__global__ void k_vv_kick(float4 *__restrict__ vel, const float4 *__restrict__ force, float dt,
+                          uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 v = vel[i];
+  const float4 f = force[i];
+  const float h = 0.5f * dt * v.w;
+  v.x += f.x * h;
+  v.y += f.y * h;
+  v.z += f.z * h;
+  vel[i] = v;
+}
+
+// lossless variant: (v_hi + v_lo) and (x_hi + x_lo) carried in f32 + f64
+// (kernels/integrate.cu:46-110)
+__global__ void k_vvl_kick_drift(float4 *__restrict__ posq, float4 *__restrict__ vel,
+                                 int4 *__restrict__ image, const float4 *__restrict__ force,
+                                 float4 *__restrict__ prev, double *__restrict__ xlo,
+                                 double *__restrict__ vlo, const DBox *__restrict__ box, float dt,
+                                 uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const DBox b = *box;
+  float4 p = posq[i];
+  float4 v = vel[i];
+  const float4 f = force[i];
+  prev[i] = p;
+  const float h = 0.5f * dt * v.w;
+  float a[3] = {f.x * h, f.y * h, f.z * h};
+  float *vv[3] = {&v.x, &v.y, &v.z};
+  float *pp[3] = {&p.x, &p.y, &p.z};
+  for (int d = 0; d < 3; ++d) {
+    double ext = (double)*vv[d] + vlo[3 * i + d] + (double)a[d];
+    float hi = (float)ext;
+    vlo[3 * i + d] = ext - (double)hi;
+    *vv[d] = hi;
+    double dx = ((double)hi + vlo[3 * i + d]) * (double)dt;
+    double xe = (double)*pp[d] + xlo[3 * i + d] + dx;
+    float xh = (float)xe;
+    xlo[3 * i + d] = xe - (double)xh;
+    *pp[d] = xh;
+  }
+  int ka, kb, kc;
+  hb_wrap(p.x, p.y, p.z, ka, kb, kc, b);
+  int4 im = image[i];
+  im.x += ka;
+  im.y += kb;
+  im.z += kc;
+  image[i] = im;
+  posq[i] = p;
+  vel[i] = v;
+}
+
+__global__ void k_vvl_kick(float4 *__restrict__ vel, const float4 *__restrict__ force,
+                           double *__restrict__ vlo, float dt, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 v = vel[i];
+  const float4 f = force[i];
+  const float h = 0.5f * dt * v.w;
+  float a[3] = {f.x * h, f.y * h, f.z * h};
+  float *vv[3] = {&v.x, &v.y, &v.z};
+  for (int d = 0; d < 3; ++d) {
+    double ext = (double)*vv[d] + vlo[3 * i + d] + (double)a[d];
+    float hi = (float)ext;
+    vlo[3 * i + d] = ext - (double)hi;
+    *vv[d] = hi;
+  }
+  vel[i] = v;
+}
+
+__global__ void k_lang_kick(float4 *__restrict__ vel, const float4 *__restrict__ force, float dt,
+                            uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 v = vel[i];
+  const float4 f = force[i];
+  const float h = dt * v.w;
+  v.x += f.x * h;
+  v.y += f.y * h;
+  v.z += f.z * h;
+  vel[i] = v;
+}
+
+__global__ void k_lang_drift_ou(float4 *__restrict__ posq, float4 *__restrict__ vel,
+                                int4 *__restrict__ image, float4 *__restrict__ prev,
+                                const DBox *__restrict__ box, float dt, float a, float kt,
+                                uint32_t s_lo, uint32_t s_hi, uint64_t step, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const DBox b = *box;
+  float4 p = posq[i];
+  float4 v = vel[i];
+  prev[i] = p;
+  const float hdt = 0.5f * dt;
+  p.x += v.x * hdt;
+  p.y += v.y * hdt;
+  p.z += v.z * hdt;
+  const float sig = sqrtf((1.0f - a * a) * kt * v.w);
+  v.x = a * v.x + sig * gaussian(s_lo, s_hi, step, i, 0u);
+  v.y = a * v.y + sig * gaussian(s_lo, s_hi, step, i, 1u);
+  v.z = a * v.z + sig * gaussian(s_lo, s_hi, step, i, 2u);
+  p.x += v.x * hdt;
+  p.y += v.y * hdt;
+  p.z += v.z * hdt;
+  int ka, kb, kc;
+  hb_wrap(p.x, p.y, p.z, ka, kb, kc, b);
+  int4 im = image[i];
+  im.x += ka;
+  im.y += kb;
+  im.z += kc;
+  image[i] = im;
+  posq[i] = p;
+  vel[i] = v;
+}
+
+#define RED_BLOCKS 296
+// kinetic energy and momentum, FP64, fixed grid and fixed tree shape
+__global__ void k_kinetic_part(const float4 *__restrict__ vel, double *__restrict__ part,
+                               uint32_t n) {
+  __shared__ double s[4][256];
+  double ke = 0.0, px = 0.0, py = 0.0, pz = 0.0;
+  for (uint32_t i = blockIdx.x * 256u + threadIdx.x; i < n; i += gridDim.x * 256u) {
+    const float4 v = vel[i];
+    if (v.w > 0.0f) {
+      const double m = 1.0 / (double)v.w;
+      ke += 0.5 * m * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
+      px += m * v.x;
+      py += m * v.y;
+      pz += m * v.z;
+    }
+  }
+  s[0][threadIdx.x] = ke;
+  s[1][threadIdx.x] = px;
+  s[2][threadIdx.x] = py;
+  s[3][threadIdx.x] = pz;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st)
+      for (int q = 0; q < 4; ++q) s[q][threadIdx.x] += s[q][threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) part[4 * blockIdx.x + threadIdx.x] = s[threadIdx.x][0];
+}
+
+__global__ void k_kinetic_final(const double *__restrict__ part, int nb, double *__restrict__ out) {
+  __shared__ double s[4][256];
+  double a[4] = {0, 0, 0, 0};
+  for (int b = threadIdx.x; b < nb; b += 256)
+    for (int q = 0; q < 4; ++q) a[q] += part[4 * b + q];
+  for (int q = 0; q < 4; ++q) s[q][threadIdx.x] = a[q];
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st)
+      for (int q = 0; q < 4; ++q) s[q][threadIdx.x] += s[q][threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) out[threadIdx.x] = s[threadIdx.x][0];
+}
+
+}  // namespace
+
+int forces_finalize(hb_forcefield *ff, bool ev, cudaStream_t s) {
+  hb_system *sys = ff->sys;
+  const uint32_t n = sys->n;
+  const float4 *recip = ff->spme.on ? ff->spme.d_recip : nullptr;
+  const double *sums = ff->spme.on ? ff->spme.d_sums : nullptr;
+  if (n > 0) {
+    if (ev)
+      k_finalize<true><<<hb_div_up(n, 256), 256, 0, s>>>(ff->d_fp, recip, ff->d_sorted_ids,
+                                                         sys->d_force, ff->d_energy, ff->d_virial,
+                                                         sums, ff->d_acc, n, ff->n_pad);
+    else
+      k_finalize<false><<<hb_div_up(n, 256), 256, 0, s>>>(ff->d_fp, recip, ff->d_sorted_ids,
+                                                          sys->d_force, ff->d_energy,
+                                                          ff->d_virial, sums, ff->d_acc, n,
+                                                          ff->n_pad);
+  }
+  if (ev) {
+    double e_self = 0.0;
+    if (ff->spme.on) {
+      for (double q : sys->h_charge) e_self += q * q;
+      e_self *= (double)ff->spme.alpha / std::sqrt(M_PI);
+    }
+    k_scalars<<<1, 1, 0, s>>>(ff->d_acc, sums, e_self, nullptr, ff->d_scalars);
+  }
+  HB_CUDA(cudaGetLastError());
+  return HB_OK;
+}
+
+int integ_vv_kick_drift(hb_integrator *it, cudaStream_t s) {
+  hb_system *sys = it->sys;
+  if (sys->n == 0) return HB_OK;
+  if (it->kind == HB_INTEGRATOR_VV_LOSSLESS)
+    k_vvl_kick_drift<<<hb_div_up(sys->n, 256), 256, 0, s>>>(
+        sys->d_posq, sys->d_vel, sys->d_image, sys->d_force, sys->d_pos_prev, sys->d_xlo,
+        sys->d_vlo, sys->d_box, (float)it->dt, sys->n);
+  else
+    k_vv_kick_drift<<<hb_div_up(sys->n, 256), 256, 0, s>>>(sys->d_posq, sys->d_vel, sys->d_image,
+                                                           sys->d_force, sys->d_pos_prev,
+                                                           sys->d_box, (float)it->dt, sys->n);
+  HB_CUDA(cudaGetLastError());
+  return HB_OK;
+}
+
+int integ_vv_kick(hb_integrator *it, cudaStream_t s) {
+  hb_system *sys = it->sys;
+  if (sys->n == 0) return HB_OK;
+  if (it->kind == HB_INTEGRATOR_VV_LOSSLESS)
+    k_vvl_kick<<<hb_div_up(sys->n, 256), 256, 0, s>>>(sys->d_vel, sys->d_force, sys->d_vlo,
+                                                      (float)it->dt, sys->n);
+  else
+    k_vv_kick<<<hb_div_up(sys->n, 256), 256, 0, s>>>(sys->d_vel, sys->d_force, (float)it->dt,
+                                                     sys->n);
+  HB_CUDA(cudaGetLastError());
+  return HB_OK;
+}
+
+int integ_lang_kick(hb_integrator *it, cudaStream_t s) {
+  hb_system *sys = it->sys;
+  if (sys->n == 0) return HB_OK;
+  k_lang_kick<<<hb_div_up(sys->n, 256), 256, 0, s>>>(sys->d_vel, sys->d_force, (float)it->dt,
+                                                     sys->n);
+  HB_CUDA(cudaGetLastError());
+  return HB_OK;
+}
+
+int integ_lang_drift_ou(hb_integrator *it, cudaStream_t s) {
+  hb_system *sys = it->sys;
+  if (sys->n == 0) return HB_OK;
+  const float a = (float)std::exp(-it->friction * it->dt);
+  k_lang_drift_ou<<<hb_div_up(sys->n, 256), 256, 0, s>>>(
+      sys->d_posq, sys->d_vel, sys->d_image, sys->d_pos_prev, sys->d_box, (float)it->dt, a,
+      (float)it->temperature, (uint32_t)it->seed, (uint32_t)(it->seed >> 32), it->step, sys->n);
+  HB_CUDA(cudaGetLastError());
+  return HB_OK;
+}
+
+int reduce_kinetic(hb_system *sys, double out[4]) {
+  cudaStream_t s = sys->ctx->stream;
+  if (sys->n == 0) {
+    for (int q = 0; q < 4; ++q) out[q] = 0.0;
+    return HB_OK;
+  }
+  k_kinetic_part<<<RED_BLOCKS, 256, 0, s>>>(sys->d_vel, sys->d_red, sys->n);
+  k_kinetic_final<<<1, 256, 0, s>>>(sys->d_red, RED_BLOCKS, sys->d_red + 4 * RED_BLOCKS);
+  HB_CUDA(cudaGetLastError());
+  HB_CUDA(cudaMemcpyAsync(sys->h_red, sys->d_red + 4 * RED_BLOCKS, sizeof(double) * 4,
+                          cudaMemcpyDeviceToHost, s));
+  HB_CUDA(cudaStreamSynchronize(s));
+  for (int q = 0; q < 4; ++q) out[q] = sys->h_red[q];
+  return HB_OK;
+}

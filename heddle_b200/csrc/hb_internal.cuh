@@ -1,0 +1,286 @@
+// hb_internal.cuh -- shared types and device helpers of the B200-native
+// HeddleMD force-and-constraint path.  Everything here is internal to
+// libheddle_b200.so; the public surface is include/heddle_b200.h.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/heddle_b200.h"
+
+// ---------------------------------------------------------------------
+// error plumbing
+// ---------------------------------------------------------------------
+void hb_set_error(const std::string &msg);
+int hb_fail(int code, const std::string &msg);
+
+#define HB_CUDA(call)                                                       \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess) {                                                \
+      return hb_fail(HB_ERR_CUDA, std::string(#call) + ": " +               \
+                                      cudaGetErrorString(e_));              \
+    }                                                                       \
+  } while (0)
+
+#define HB_TRY(call)                                                        \
+  do {                                                                      \
+    int r_ = (call);                                                        \
+    if (r_ != HB_OK) return r_;                                             \
+  } while (0)
+
+// fixed-point scales: pair/recip force, energy and virial accumulate as
+// two's-complement int64 with 2^40 fractional bits (resolution 9.1e-13,
+// range +-8.4e6 in atomic units); the SPME charge grid uses 2^32 as the
+// reference's spread does (kernels/spme_spread_gather.cuh:31).
+#define HB_FP_SCALE 1099511627776.0f        /* 2^40 */
+#define HB_FP_INV_SCALE (1.0 / 1099511627776.0)
+#define HB_RHO_SCALE 4294967296.0f          /* 2^32 */
+
+#define HB_TILE 32
+#define HB_SENTINEL 0xFFFFFFFFu
+
+// status word bits (kernels/neighbor.cu:634-669 layout, plus build bits)
+#define HB_ST_DISPLACED 1u        /* an atom moved more than r_skin / 2 */
+#define HB_ST_ENTRY_OVERFLOW 8u   /* entry capacity exceeded on a rebuild */
+#define HB_ST_ENTRY_HIGHWATER 2u  /* entry count above 3/4 of capacity */
+
+// ---------------------------------------------------------------------
+// device box: lattice plus reciprocal helpers, kept in device memory so a
+// barostat can change it inside a captured graph
+// ---------------------------------------------------------------------
+struct DBox {
+  float lx, ly, lz, xy, xz, yz;
+  float ilx, ily, ilz;   // 1 / lx etc.
+  int ortho;             // xy == xz == yz == 0
+};
+
+// Operation-by-operation single-precision minimum image, no contraction:
+// the membership rule of the neighbour set (same operation order as the
+// reference's kernels/pbc.cuh:18-43).  Used only where exactness matters.
+__device__ __forceinline__ float hb_exact_r2(float dx, float dy, float dz,
+                                             const DBox &b) {
+  float sc = __fdiv_rn(dz, b.lz);
+  float sb = __fdiv_rn(__fsub_rn(dy, __fmul_rn(sc, b.yz)), b.ly);
+  float sa = __fdiv_rn(
+      __fsub_rn(__fsub_rn(dx, __fmul_rn(sb, b.xy)), __fmul_rn(sc, b.xz)), b.lx);
+  float ka = floorf(__fadd_rn(sa, 0.5f));
+  float kb = floorf(__fadd_rn(sb, 0.5f));
+  float kc = floorf(__fadd_rn(sc, 0.5f));
+  dx = __fsub_rn(dx, __fadd_rn(__fadd_rn(__fmul_rn(ka, b.lx), __fmul_rn(kb, b.xy)),
+                               __fmul_rn(kc, b.xz)));
+  dy = __fsub_rn(dy, __fadd_rn(__fmul_rn(kb, b.ly), __fmul_rn(kc, b.yz)));
+  dz = __fsub_rn(dz, __fmul_rn(kc, b.lz));
+  return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)),
+                   __fmul_rn(dz, dz));
+}
+
+// fast minimum image (contraction allowed) for force arithmetic
+__device__ __forceinline__ void hb_min_image(float &dx, float &dy, float &dz,
+                                             const DBox &b) {
+  float sc = dz * b.ilz;
+  float sb = (dy - sc * b.yz) * b.ily;
+  float sa = (dx - sb * b.xy - sc * b.xz) * b.ilx;
+  float ka = rintf(sa), kb = rintf(sb), kc = rintf(sc);
+  dx -= ka * b.lx + kb * b.xy + kc * b.xz;
+  dy -= kb * b.ly + kc * b.yz;
+  dz -= kc * b.lz;
+}
+
+// wrap into the primary cell [-1/2, 1/2)^3 (fractional) and return the
+// image triple (kernels/pbc.cuh:73-91 semantics)
+__device__ __forceinline__ void hb_wrap(float &x, float &y, float &z, int &ka,
+                                        int &kb, int &kc, const DBox &b) {
+  float sc = z / b.lz;
+  float sb = (y - sc * b.yz) / b.ly;
+  float sa = (x - sb * b.xy - sc * b.xz) / b.lx;
+  float fa = floorf(sa + 0.5f), fb = floorf(sb + 0.5f), fc = floorf(sc + 0.5f);
+  x -= fa * b.lx + fb * b.xy + fc * b.xz;
+  y -= fb * b.ly + fc * b.yz;
+  z -= fc * b.lz;
+  ka = (int)fa;
+  kb = (int)fb;
+  kc = (int)fc;
+}
+
+__device__ __forceinline__ void hb_frac(float x, float y, float z,
+                                        const DBox &b, float &sa, float &sb,
+                                        float &sc) {
+  sc = z / b.lz;
+  sb = (y - sc * b.yz) / b.ly;
+  sa = (x - sb * b.xy - sc * b.xz) / b.lx;
+}
+
+// ---------------------------------------------------------------------
+// host-side objects
+// ---------------------------------------------------------------------
+struct hb_context {
+  int device = 0;
+  int n_sm = 148;
+  cudaStream_t stream = nullptr;    // main stream
+  cudaStream_t stream2 = nullptr;   // SPME runs here, overlapping the pair kernel
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  bool timing = false;
+  // stage timers (accumulated over the last hb_integrator_step call)
+  std::vector<cudaEvent_t> tev;
+  double t_ms[8] = {0};
+};
+
+struct hb_system {
+  hb_context *ctx = nullptr;
+  uint32_t n = 0;
+  double box[6] = {0};
+  DBox *d_box = nullptr;
+  float4 *d_posq = nullptr;      // x, y, z, q (wrapped into the primary cell)
+  float4 *d_vel = nullptr;       // vx, vy, vz, 1/m
+  int4 *d_image = nullptr;       // image counts a, b, c, type
+  float4 *d_force = nullptr;     // fx, fy, fz, 0 (total force, atom order)
+  float4 *d_pos_prev = nullptr;  // pre-drift positions (constraint snapshot)
+  double *d_vlo = nullptr;       // lossless mode: low parts of v ([3n])
+  double *d_xlo = nullptr;       // lossless mode: low parts of x ([3n])
+  std::vector<double> h_mass;
+  std::vector<double> h_charge;
+  std::vector<uint32_t> h_type;
+  // FP64 reduction scratch
+  double *d_red = nullptr;       // partials
+  double *h_red = nullptr;       // pinned
+};
+
+// SPME reciprocal state
+struct SpmeState {
+  int on = 0;
+  int na = 0, nb = 0, nc = 0, nch = 0, order = 4;
+  float alpha = 0.f;
+  unsigned long long *d_rho_fixed = nullptr;  // [na*nb*nc] int64 grid
+  float2 *d_grid = nullptr;                   // [na*nb*nch] complex
+  float *d_v = nullptr;                       // [na*nb*nc] real potential
+  float *d_bfac = nullptr;                    // b-factors a | b | c
+  float2 *d_tw = nullptr;                     // twiddles a | b | c
+  double *d_part = nullptr;                   // energy / virial partials
+  int n_part = 0;
+  double *d_sums = nullptr;                   // [2] E_recip, W_recip
+  float4 *d_recip = nullptr;                  // per sorted atom fx, fy, fz, e
+  float self_pref = 0.f;                      // alpha / sqrt(pi)
+};
+
+struct hb_forcefield {
+  hb_system *sys = nullptr;
+  // ---- parameters
+  int lj_on = 0, coul_on = 0;
+  uint32_t n_types = 0;
+  std::vector<float4> h_lj;        // per type pair: sigma^2, 24 eps, cut^2, r_switch^2
+  float4 *d_lj = nullptr;
+  float alpha = 0.f, coul_rc2 = 0.f;
+  float rc_max = 0.f, r_skin = 0.f, r_search = 0.f;
+  int any_switch = 0;
+  int excl_scaled = 0;             // some exclusion has a non-zero scale
+  uint32_t *d_excl_off = nullptr;  // CSR over original ids
+  uint32_t *d_excl_partner = nullptr;
+  float2 *d_excl_scale = nullptr;  // (lj, coulomb)
+  uint32_t n_excl = 0;
+  // ---- neighbour list (sorted-index space)
+  uint32_t n_tiles = 0, n_pad = 0;
+  int nv_log2 = 5;                 // voxel grid 2^nv_log2 per axis
+  uint32_t *d_vox_key = nullptr;   // per atom
+  uint32_t *d_vox_count = nullptr; // per voxel (+1)
+  uint32_t *d_vox_off = nullptr;
+  uint32_t *d_scan_tmp = nullptr;
+  uint32_t *d_sorted_ids = nullptr;  // sorted slot -> atom id (pad = sentinel)
+  uint32_t *d_inv_perm = nullptr;    // atom id -> sorted slot
+  float4 *d_tile_posq = nullptr;     // positions in sorted order
+  int *d_tile_type = nullptr;
+  float4 *d_tile_center = nullptr;   // per tile: centre xyz, spc flag in w
+  float4 *d_tile_half = nullptr;     // per tile: half extents
+  uint32_t *d_tile_nent = nullptr;   // entries per tile (count pass)
+  uint32_t *d_entry_off = nullptr;   // [n_tiles + 1]
+  uint32_t *d_entry_j = nullptr;     // [cap * 32] sorted j slots
+  uint32_t *d_entry_excl = nullptr;  // [cap * 32] exclusion masks
+  uint64_t entry_cap = 0;
+  float4 *d_ref_pos = nullptr;       // positions at the last rebuild
+  uint32_t *d_status = nullptr;      // status word
+  uint32_t *d_counters = nullptr;    // [0] rebuilds, [1] entries of last build
+  uint32_t *h_status = nullptr;      // pinned mirror
+  uint64_t rebuilds_host = 0;
+  bool built = false;
+  // ---- accumulators (sorted-slot space)
+  unsigned long long *d_fp = nullptr;  // [5][n_pad]: fx fy fz e w
+  // ---- SPME
+  SpmeState spme;
+  // ---- scalars
+  double *d_scalars = nullptr;       // [8]
+  unsigned long long *d_acc = nullptr;  // int64 totals: [0] LJ energy, [1] pair
+                                        // energy, [2] pair virial
+  double h_scalars[8] = {0};
+  float *d_energy = nullptr;         // per atom (atom order)
+  float *d_virial = nullptr;
+};
+
+struct hb_constraints {
+  hb_system *sys = nullptr;
+  uint32_t n_settle = 0, n_shake = 0;
+  // SETTLE: per group (O, H1, H2) atom ids and geometry
+  uint4 *d_settle_atoms = nullptr;   // o, h1, h2, 0
+  float4 *d_settle_geom = nullptr;   // ra, rb, rc, 0
+  float2 *d_settle_mass = nullptr;   // m_o, m_h
+  // SHAKE: per group CSR
+  uint32_t *d_shake_aoff = nullptr, *d_shake_atoms = nullptr;
+  uint32_t *d_shake_coff = nullptr;
+  uint2 *d_shake_pairs = nullptr;    // local i, j
+  double *d_shake_d2 = nullptr;
+  double shake_tol = 3.57e-6;
+  uint32_t shake_max_iter = 32;
+  uint32_t n_slots = 0;
+  float *d_virial = nullptr;         // per atom
+  uint32_t *d_iters = nullptr;       // max sweeps of the last SHAKE call
+};
+
+struct hb_integrator {
+  hb_system *sys = nullptr;
+  int kind = HB_INTEGRATOR_VV;
+  double dt = 0.0, friction = 0.0, temperature = 0.0;
+  uint64_t seed = 0, step = 0;
+  bool forces_valid = false;
+  // graph mode
+  cudaGraphExec_t graph_exec = nullptr;
+  hb_forcefield *graph_ff = nullptr;
+  hb_constraints *graph_cons = nullptr;
+};
+
+// ---------------------------------------------------------------------
+// internal entry points implemented across the translation units
+// ---------------------------------------------------------------------
+// neighbour list (hb_nlist.cu)
+int nl_setup(hb_forcefield *ff);
+int nl_free(hb_forcefield *ff);
+// Rebuild the list.  gated: kernels run only when the status word has the
+// displacement bit set (a device-side decision, no host read).
+int nl_rebuild(hb_forcefield *ff, bool gated, cudaStream_t s);
+int nl_displacement_check(hb_forcefield *ff, cudaStream_t s);
+int nl_gather_positions(hb_forcefield *ff, cudaStream_t s);
+int nl_first_build(hb_forcefield *ff);
+int nl_pairs(hb_forcefield *ff, std::vector<uint32_t> &pairs, uint64_t &dups);
+// pair kernel (hb_pair.cu)
+int pair_launch(hb_forcefield *ff, bool ev, cudaStream_t s);
+// SPME (hb_spme.cu)
+int spme_setup(hb_forcefield *ff, const hb_forcefield_desc *d);
+int spme_free(hb_forcefield *ff);
+int spme_launch(hb_forcefield *ff, bool ev, cudaStream_t s);
+// combine (hb_integ.cu): fixed-point + reciprocal -> force (atom order)
+int forces_finalize(hb_forcefield *ff, bool ev, cudaStream_t s);
+int scalars_reduce(hb_forcefield *ff, cudaStream_t s);
+// integrators (hb_integ.cu)
+int integ_vv_kick_drift(hb_integrator *it, cudaStream_t s);
+int integ_vv_kick(hb_integrator *it, cudaStream_t s);
+int integ_lang_kick(hb_integrator *it, cudaStream_t s);
+int integ_lang_drift_ou(hb_integrator *it, cudaStream_t s);
+int reduce_kinetic(hb_system *sys, double out[4]);
+// constraints (hb_cons.cu)
+int cons_positions(hb_constraints *c, double dt, cudaStream_t s);
+int cons_velocities(hb_constraints *c, double dt, bool virial, cudaStream_t s);
+
+static inline unsigned int hb_div_up(uint64_t a, uint64_t b) {
+  return (unsigned int)((a + b - 1) / b);
+}

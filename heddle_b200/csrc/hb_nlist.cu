@@ -1,0 +1,706 @@
+// hb_nlist.cu -- packed neighbour list for the B200 force path.
+//
+// Replaces the reference's cell list + packed-neighbour construction
+// (kernels/neighbor.cu:95-724, src/forces/neighbor_list.rs:945-1354) with a
+// design of its own:
+//   * atoms are counting-sorted into a 2^k-per-axis voxel grid walked in
+//     Morton order, ties broken by atom id, so every 32 consecutive sorted
+//     atoms form a compact tile and the order is deterministic;
+//   * all per-step force work runs in this sorted-slot space (positions are
+//     gathered once per step, forces are scattered back once);
+//   * one warp per i-tile sweeps j-tiles J > I through an AABB prune, keeps
+//     every j-atom within r_search of any i-atom, and packs 32 of them per
+//     entry together with a 32-bit exclusion mask per j-atom (bit m: the
+//     pair with i-atom m is in the exclusion list), so the pair kernel never
+//     scans exclusion lists for ordinary pairs;
+//   * the self tile is entry 0 of each i-tile and is evaluated with a half
+//     rotation (each unordered pair once);
+//   * entries are laid out per i-tile by a count pass, a scan and a fill
+//     pass, so the layout is identical run to run;
+//   * every rebuild kernel is gated on the device status word, so a rebuild
+//     is decided on the device each step with no host read.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "hb_internal.cuh"
+
+namespace {
+
+__device__ __forceinline__ bool gate_off(const uint32_t *gate) {
+  return gate != nullptr && ((*(volatile const uint32_t *)gate) & HB_ST_DISPLACED) == 0u;
+}
+
+__device__ __forceinline__ uint32_t spread_bits(uint32_t v) {
+  // 10-bit value -> bits at positions 0, 3, 6, ...
+  v &= 0x3FFu;
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+__global__ void k_vox_hist(const uint32_t *gate, const float4 *__restrict__ posq,
+                           const DBox *__restrict__ box, int nv_log2,
+                           uint32_t *__restrict__ key, uint32_t *__restrict__ count,
+                           uint32_t n) {
+  if (gate_off(gate)) return;
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  DBox b = *box;
+  float4 p = posq[i];
+  float sa, sb, sc;
+  hb_frac(p.x, p.y, p.z, b, sa, sb, sc);
+  const int nv = 1 << nv_log2;
+  int v[3];
+  float s[3] = {sa, sb, sc};
+  for (int d = 0; d < 3; ++d) {
+    float u = s[d] + 0.5f;
+    u -= floorf(u);
+    int c = (int)(u * (float)nv);
+    v[d] = c < 0 ? 0 : (c >= nv ? nv - 1 : c);
+  }
+  uint32_t k = (spread_bits((uint32_t)v[0]) << 2) | (spread_bits((uint32_t)v[1]) << 1) |
+               spread_bits((uint32_t)v[2]);
+  key[i] = k;
+  atomicAdd(&count[k], 1u);
+}
+
+// ---- three-phase exclusive scan (integer, deterministic) ----
+__global__ void __launch_bounds__(1024) k_scan_block(const uint32_t *gate, const uint32_t *in,
+                                                     uint32_t *out, uint32_t *bsum,
+                                                     uint32_t len) {
+  if (gate_off(gate)) return;
+  __shared__ uint32_t ws[32];
+  uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t i = blockIdx.x * 1024u + threadIdx.x;
+  uint32_t v = i < len ? in[i] : 0u;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+    if ((int)lane >= o) x += y;
+  }
+  if (lane == 31u) ws[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = ws[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+      if ((int)lane >= o) w += y;
+    }
+    ws[lane] = w;
+  }
+  __syncthreads();
+  if (warp > 0) x += ws[warp - 1];
+  if (i < len) out[i] = x - v;
+  if (threadIdx.x == 1023u) bsum[blockIdx.x] = x;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_top(const uint32_t *gate, uint32_t *bsum,
+                                                   uint32_t nb) {
+  if (gate_off(gate)) return;
+  __shared__ uint32_t ws[32];
+  __shared__ uint32_t carry;
+  uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry = 0u;
+  __syncthreads();
+  for (uint32_t base = 0; base < nb; base += 1024u) {
+    uint32_t i = base + threadIdx.x;
+    uint32_t v = i < nb ? bsum[i] : 0u;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+      if ((int)lane >= o) x += y;
+    }
+    if (lane == 31u) ws[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t w = ws[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+        if ((int)lane >= o) w += y;
+      }
+      ws[lane] = w;
+    }
+    __syncthreads();
+    if (warp > 0) x += ws[warp - 1];
+    uint32_t c = carry;
+    if (i < nb) bsum[i] = c + x - v;
+    __syncthreads();
+    if (threadIdx.x == 1023u) carry = c + x;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_scan_add(const uint32_t *gate, uint32_t *out,
+                                                   const uint32_t *bsum, uint32_t len) {
+  if (gate_off(gate)) return;
+  uint32_t i = blockIdx.x * 1024u + threadIdx.x;
+  if (i < len && blockIdx.x > 0) out[i] += bsum[blockIdx.x];
+}
+
+// Scatter atoms to their voxel ranges.  atomicSub on the histogram hands
+// out slots (in an arbitrary order) and leaves the histogram at zero for
+// the next rebuild; k_vox_sort then orders each voxel by atom id.
+__global__ void k_vox_scatter(const uint32_t *gate, const uint32_t *__restrict__ key,
+                              const uint32_t *__restrict__ off, uint32_t *count,
+                              uint32_t *__restrict__ sorted_ids, uint32_t n) {
+  if (gate_off(gate)) return;
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t k = key[i];
+  uint32_t slot = atomicSub(&count[k], 1u) - 1u;
+  sorted_ids[off[k] + slot] = i;
+}
+
+__global__ void k_vox_sort(const uint32_t *gate, const uint32_t *__restrict__ off,
+                           uint32_t *sorted_ids, uint32_t n_vox) {
+  if (gate_off(gate)) return;
+  uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n_vox) return;
+  uint32_t s = off[v], e = off[v + 1];
+  for (uint32_t k = s + 1; k < e; ++k) {
+    uint32_t key = sorted_ids[k];
+    int p = (int)k - 1;
+    while (p >= (int)s && sorted_ids[p] > key) {
+      sorted_ids[p + 1] = sorted_ids[p];
+      --p;
+    }
+    sorted_ids[p + 1] = key;
+  }
+}
+
+// Fill the sorted-slot views and the displacement reference.
+__global__ void k_tile_fill(const uint32_t *gate, uint32_t *sorted_ids,
+                            const float4 *__restrict__ posq, const int4 *__restrict__ image,
+                            uint32_t *__restrict__ inv_perm, float4 *__restrict__ tile_posq,
+                            int *__restrict__ tile_type, float4 *__restrict__ ref_pos,
+                            uint32_t n, uint32_t n_pad) {
+  if (gate_off(gate)) return;
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_pad) return;
+  if (k < n) {
+    uint32_t id = sorted_ids[k];
+    inv_perm[id] = k;
+    float4 p = posq[id];
+    tile_posq[k] = p;
+    tile_type[k] = image[id].w;
+    ref_pos[id] = p;
+  } else {
+    sorted_ids[k] = HB_SENTINEL;
+    tile_posq[k] = make_float4(1.0e18f, 1.0e18f, 1.0e18f, 0.0f);
+    tile_type[k] = 0;
+  }
+}
+
+// Per-tile axis-aligned box (one warp per tile).  centre.w = 1 when the
+// single-periodic-copy shortcut is valid for the tile until the next
+// rebuild: half + r_skin / 2 + rc_max <= L / 2 on every axis of an
+// orthorhombic box (the condition of jit_composed.rs:1577-1607 with the
+// skin margin added, because atoms drift between rebuilds).
+__global__ void k_tile_bbox(const uint32_t *gate, const float4 *__restrict__ tile_posq,
+                            const DBox *__restrict__ box, float rc_max, float r_skin,
+                            float4 *__restrict__ center, float4 *__restrict__ half, uint32_t n,
+                            uint32_t n_tiles) {
+  if (gate_off(gate)) return;
+  uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint32_t lane = threadIdx.x & 31u;
+  if (warp >= n_tiles) return;
+  uint32_t k = warp * 32u + lane;
+  bool valid = k < n;
+  float4 p = tile_posq[k];
+  float lo[3] = {valid ? p.x : 3.0e38f, valid ? p.y : 3.0e38f, valid ? p.z : 3.0e38f};
+  float hi[3] = {valid ? p.x : -3.0e38f, valid ? p.y : -3.0e38f, valid ? p.z : -3.0e38f};
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = fminf(lo[d], __shfl_xor_sync(0xFFFFFFFFu, lo[d], o));
+      hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xFFFFFFFFu, hi[d], o));
+    }
+  }
+  if (lane == 0) {
+    DBox b = *box;
+    float c[3], h[3];
+    for (int d = 0; d < 3; ++d) {
+      c[d] = 0.5f * (lo[d] + hi[d]);
+      h[d] = 0.5f * (hi[d] - lo[d]);
+    }
+    float m = 0.5f * r_skin + rc_max;
+    bool spc = b.ortho && (h[0] + m <= 0.5f * b.lx) && (h[1] + m <= 0.5f * b.ly) &&
+               (h[2] + m <= 0.5f * b.lz);
+    center[warp] = make_float4(c[0], c[1], c[2], spc ? 1.0f : 0.0f);
+    half[warp] = make_float4(h[0], h[1], h[2], 0.0f);
+  }
+}
+
+// Exclusion mask of one j-atom against the 32 slots of i-tile I.
+__device__ __forceinline__ uint32_t excl_mask(uint32_t sj, uint32_t I,
+                                              const uint32_t *__restrict__ sorted_ids,
+                                              const uint32_t *__restrict__ inv_perm,
+                                              const uint32_t *__restrict__ eoff,
+                                              const uint32_t *__restrict__ epart) {
+  if (eoff == nullptr || sj == HB_SENTINEL) return 0u;
+  uint32_t oj = sorted_ids[sj];
+  uint32_t m = 0u;
+  uint32_t lo = I * 32u;
+  for (uint32_t q = eoff[oj]; q < eoff[oj + 1]; ++q) {
+    uint32_t sp = inv_perm[epart[q]];
+    if (sp >= lo && sp < lo + 32u) m |= 1u << (sp - lo);
+  }
+  return m;
+}
+
+#define NL_WARPS 4
+
+// Packed-entry construction.  WRITE = false counts entries per i-tile;
+// WRITE = true writes them at entry_off[I] (after an exclusive scan).
+template <bool WRITE>
+__global__ void __launch_bounds__(NL_WARPS * 32)
+    k_nl_build(const uint32_t *gate, const float4 *__restrict__ tile_posq,
+               const float4 *__restrict__ center, const float4 *__restrict__ half,
+               const DBox *__restrict__ box, float rs2, float rb2, float band_lo,
+               float band_hi, uint32_t n, uint32_t n_tiles, uint32_t *__restrict__ tile_nent,
+               const uint32_t *__restrict__ entry_off, uint32_t *__restrict__ entry_j,
+               uint32_t *__restrict__ entry_excl, uint64_t cap,
+               const uint32_t *__restrict__ sorted_ids, const uint32_t *__restrict__ inv_perm,
+               const uint32_t *__restrict__ eoff, const uint32_t *__restrict__ epart) {
+  if (gate_off(gate)) return;
+  __shared__ float sx[NL_WARPS][32], sy[NL_WARPS][32], sz[NL_WARPS][32];
+  __shared__ uint32_t jbuf[NL_WARPS][64];
+  const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t I = blockIdx.x * NL_WARPS + w;
+  if (I >= n_tiles) return;
+  const DBox b = *box;
+  const uint32_t ki = I * 32u + lane;
+  const float4 pi = tile_posq[ki];
+  sx[w][lane] = pi.x;
+  sy[w][lane] = pi.y;
+  sz[w][lane] = pi.z;
+  const uint32_t ivalid = __ballot_sync(0xFFFFFFFFu, ki < n);
+  __syncwarp();
+  const float4 ci = center[I], hi = half[I];
+  uint64_t base = WRITE ? (uint64_t)entry_off[I] : 0u;
+  uint32_t nent = 0;
+
+  // entry 0: the self tile (all pairs inside the tile, half rotation)
+  if (__popc(ivalid) >= 2) {
+    if (WRITE) {
+      uint64_t e = base;
+      if (e < cap) {
+        uint32_t sj = ki < n ? ki : HB_SENTINEL;
+        entry_j[e * 32u + lane] = sj;
+        entry_excl[e * 32u + lane] = excl_mask(sj, I, sorted_ids, inv_perm, eoff, epart);
+      }
+    }
+    nent = 1;
+  }
+
+  uint32_t blen = 0;
+  for (uint32_t j0 = I + 1; j0 < n_tiles; j0 += 32u) {
+    uint32_t J = j0 + lane;
+    bool pass = false;
+    if (J < n_tiles) {
+      float4 cj = center[J], hj = half[J];
+      float dx = ci.x - cj.x, dy = ci.y - cj.y, dz = ci.z - cj.z;
+      hb_min_image(dx, dy, dz, b);
+      float ex = fmaxf(fabsf(dx) - (hi.x + hj.x), 0.0f);
+      float ey = fmaxf(fabsf(dy) - (hi.y + hj.y), 0.0f);
+      float ez = fmaxf(fabsf(dz) - (hi.z + hj.z), 0.0f);
+      pass = ex * ex + ey * ey + ez * ez <= rb2;
+    }
+    uint32_t cand = __ballot_sync(0xFFFFFFFFu, pass);
+    while (cand) {
+      uint32_t bit = __ffs(cand) - 1u;
+      cand &= cand - 1u;
+      uint32_t Jt = j0 + bit;
+      uint32_t kj = Jt * 32u + lane;
+      bool jvalid = kj < n;
+      bool hit = false;
+      if (jvalid) {
+        float4 pj = tile_posq[kj];
+        uint32_t mm = ivalid;
+        while (mm) {
+          uint32_t m = __ffs(mm) - 1u;
+          mm &= mm - 1u;
+          float dx = sx[w][m] - pj.x, dy = sy[w][m] - pj.y, dz = sz[w][m] - pj.z;
+          // fast minimum image decides far from the boundary; the exact
+          // single-precision rule decides inside a 1e-5 relative band
+          float fx = dx, fy = dy, fz = dz;
+          hb_min_image(fx, fy, fz, b);
+          float r2 = fx * fx + fy * fy + fz * fz;
+          if (r2 < band_lo) {
+            hit = true;
+            break;
+          }
+          if (r2 <= band_hi && hb_exact_r2(dx, dy, dz, b) <= rs2) {
+            hit = true;
+            break;
+          }
+        }
+      }
+      uint32_t hits = __ballot_sync(0xFFFFFFFFu, hit);
+      if (hit) {
+        uint32_t pre = __popc(hits & ((1u << lane) - 1u));
+        jbuf[w][blen + pre] = kj;
+      }
+      blen += __popc(hits);
+      __syncwarp();
+      if (blen >= 32u) {
+        if (WRITE) {
+          uint64_t e = base + nent;
+          if (e < cap) {
+            uint32_t sj = jbuf[w][lane];
+            entry_j[e * 32u + lane] = sj;
+            entry_excl[e * 32u + lane] = excl_mask(sj, I, sorted_ids, inv_perm, eoff, epart);
+          }
+        }
+        nent++;
+        uint32_t rest = blen - 32u;
+        uint32_t v = lane < rest ? jbuf[w][32u + lane] : 0u;
+        __syncwarp();
+        if (lane < rest) jbuf[w][lane] = v;
+        blen = rest;
+        __syncwarp();
+      }
+    }
+  }
+  if (blen > 0u) {
+    if (WRITE) {
+      uint64_t e = base + nent;
+      if (e < cap) {
+        uint32_t sj = lane < blen ? jbuf[w][lane] : HB_SENTINEL;
+        entry_j[e * 32u + lane] = sj;
+        entry_excl[e * 32u + lane] = excl_mask(sj, I, sorted_ids, inv_perm, eoff, epart);
+      }
+    }
+    nent++;
+  }
+  if (!WRITE && lane == 0) tile_nent[I] = nent;
+}
+
+// Last kernel of a rebuild: capacity bits, counters, and clearing of the
+// displacement bit (which gates every kernel of the rebuild).
+__global__ void k_nl_finish(const uint32_t *gate, uint32_t *status, uint32_t *counters,
+                            const uint32_t *entry_off, uint32_t n_tiles, uint64_t cap) {
+  if (gate_off(gate)) return;
+  uint32_t total = entry_off[n_tiles];
+  uint32_t st = *status;
+  if ((uint64_t)total > cap) st |= HB_ST_ENTRY_OVERFLOW;
+  else if ((uint64_t)total * 4u > cap * 3u) st |= HB_ST_ENTRY_HIGHWATER;
+  st &= ~HB_ST_DISPLACED;
+  *status = st;
+  counters[0] += 1u;
+  counters[1] = total;
+}
+
+__global__ void k_disp_check(const float4 *__restrict__ posq, const float4 *__restrict__ ref,
+                             const DBox *__restrict__ box, float thr2, uint32_t *status,
+                             uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool moved = false;
+  if (i < n) {
+    DBox b = *box;
+    float4 p = posq[i], r = ref[i];
+    float dx = p.x - r.x, dy = p.y - r.y, dz = p.z - r.z;
+    hb_min_image(dx, dy, dz, b);
+    moved = dx * dx + dy * dy + dz * dz > thr2;
+  }
+  // one atomic per warp at most
+  if (__any_sync(0xFFFFFFFFu, moved) && (threadIdx.x & 31u) == 0u) atomicOr(status, HB_ST_DISPLACED);
+}
+
+__global__ void k_gather_pos(const uint32_t *__restrict__ sorted_ids,
+                             const float4 *__restrict__ posq, float4 *__restrict__ tile_posq,
+                             uint32_t n) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) tile_posq[k] = posq[sorted_ids[k]];
+}
+
+int scan_exclusive(const uint32_t *gate, const uint32_t *in, uint32_t *out, uint32_t *tmp,
+                   uint32_t len, cudaStream_t s) {
+  uint32_t nb = hb_div_up(len, 1024);
+  k_scan_block<<<nb, 1024, 0, s>>>(gate, in, out, tmp, len);
+  k_scan_top<<<1, 1024, 0, s>>>(gate, tmp, nb);
+  k_scan_add<<<nb, 1024, 0, s>>>(gate, out, tmp, len);
+  HB_CUDA(cudaGetLastError());
+  return HB_OK;
+}
+
+}  // namespace
+
+int nl_setup(hb_forcefield *ff) {
+  hb_system *sys = ff->sys;
+  const uint32_t n = sys->n;
+  ff->n_tiles = hb_div_up(n, 32);
+  ff->n_pad = ff->n_tiles * 32u;
+  // voxel grid: the smallest power of two per axis with nv^3 >= n
+  int l2 = 2;
+  while ((1u << (3 * l2)) < n && l2 < 9) ++l2;
+  ff->nv_log2 = l2;
+  const uint32_t n_vox = 1u << (3 * l2);
+  const uint32_t n_pad = ff->n_pad ? ff->n_pad : 32u;
+  HB_CUDA(cudaMalloc(&ff->d_vox_key, sizeof(uint32_t) * std::max(n, 1u)));
+  HB_CUDA(cudaMalloc(&ff->d_vox_count, sizeof(uint32_t) * (n_vox + 1)));
+  HB_CUDA(cudaMemset(ff->d_vox_count, 0, sizeof(uint32_t) * (n_vox + 1)));
+  HB_CUDA(cudaMalloc(&ff->d_vox_off, sizeof(uint32_t) * (n_vox + 1)));
+  uint32_t scan_len = std::max(n_vox + 1, ff->n_tiles + 1);
+  HB_CUDA(cudaMalloc(&ff->d_scan_tmp, sizeof(uint32_t) * (hb_div_up(scan_len, 1024) + 1)));
+  HB_CUDA(cudaMalloc(&ff->d_sorted_ids, sizeof(uint32_t) * n_pad));
+  HB_CUDA(cudaMalloc(&ff->d_inv_perm, sizeof(uint32_t) * std::max(n, 1u)));
+  HB_CUDA(cudaMalloc(&ff->d_tile_posq, sizeof(float4) * n_pad));
+  HB_CUDA(cudaMalloc(&ff->d_tile_type, sizeof(int) * n_pad));
+  HB_CUDA(cudaMalloc(&ff->d_tile_center, sizeof(float4) * std::max(ff->n_tiles, 1u)));
+  HB_CUDA(cudaMalloc(&ff->d_tile_half, sizeof(float4) * std::max(ff->n_tiles, 1u)));
+  HB_CUDA(cudaMalloc(&ff->d_tile_nent, sizeof(uint32_t) * (ff->n_tiles + 1)));
+  HB_CUDA(cudaMemset(ff->d_tile_nent, 0, sizeof(uint32_t) * (ff->n_tiles + 1)));
+  HB_CUDA(cudaMalloc(&ff->d_entry_off, sizeof(uint32_t) * (ff->n_tiles + 1)));
+  HB_CUDA(cudaMalloc(&ff->d_ref_pos, sizeof(float4) * std::max(n, 1u)));
+  HB_CUDA(cudaMalloc(&ff->d_status, sizeof(uint32_t)));
+  HB_CUDA(cudaMemset(ff->d_status, 0, sizeof(uint32_t)));
+  HB_CUDA(cudaMalloc(&ff->d_counters, sizeof(uint32_t) * 4));
+  HB_CUDA(cudaMemset(ff->d_counters, 0, sizeof(uint32_t) * 4));
+  HB_CUDA(cudaMallocHost(&ff->h_status, sizeof(uint32_t) * 8));
+  HB_CUDA(cudaMalloc(&ff->d_fp, sizeof(unsigned long long) * 5 * n_pad));
+  HB_CUDA(cudaMemset(ff->d_fp, 0, sizeof(unsigned long long) * 5 * n_pad));
+  return HB_OK;
+}
+
+int nl_free(hb_forcefield *ff) {
+  cudaFree(ff->d_vox_key);
+  cudaFree(ff->d_vox_count);
+  cudaFree(ff->d_vox_off);
+  cudaFree(ff->d_scan_tmp);
+  cudaFree(ff->d_sorted_ids);
+  cudaFree(ff->d_inv_perm);
+  cudaFree(ff->d_tile_posq);
+  cudaFree(ff->d_tile_type);
+  cudaFree(ff->d_tile_center);
+  cudaFree(ff->d_tile_half);
+  cudaFree(ff->d_tile_nent);
+  cudaFree(ff->d_entry_off);
+  cudaFree(ff->d_entry_j);
+  cudaFree(ff->d_entry_excl);
+  cudaFree(ff->d_ref_pos);
+  cudaFree(ff->d_status);
+  cudaFree(ff->d_counters);
+  cudaFreeHost(ff->h_status);
+  cudaFree(ff->d_fp);
+  return HB_OK;
+}
+
+// Launch the rebuild sequence.  stop_after_count: run through the count
+// pass and the entry scan only (the first build sizes the buffers there).
+static int nl_launch(hb_forcefield *ff, const uint32_t *gate, cudaStream_t s, int phase) {
+  hb_system *sys = ff->sys;
+  const uint32_t n = sys->n;
+  const uint32_t n_vox = 1u << (3 * ff->nv_log2);
+  const float rs = ff->r_search;
+  const float rs2 = rs * rs;
+  // AABB prune radius with a margin so rounding never drops a pair
+  const float rb = rs * (1.0f + 1.0e-5f) + 1.0e-4f;
+  const float band_lo = rs2 * (1.0f - 1.0e-5f), band_hi = rs2 * (1.0f + 1.0e-5f);
+  if (phase == 0) {
+    k_vox_hist<<<hb_div_up(n, 256), 256, 0, s>>>(gate, sys->d_posq, sys->d_box, ff->nv_log2,
+                                                  ff->d_vox_key, ff->d_vox_count, n);
+    HB_TRY(scan_exclusive(gate, ff->d_vox_count, ff->d_vox_off, ff->d_scan_tmp, n_vox + 1, s));
+    k_vox_scatter<<<hb_div_up(n, 256), 256, 0, s>>>(gate, ff->d_vox_key, ff->d_vox_off,
+                                                     ff->d_vox_count, ff->d_sorted_ids, n);
+    k_vox_sort<<<hb_div_up(n_vox, 256), 256, 0, s>>>(gate, ff->d_vox_off, ff->d_sorted_ids, n_vox);
+    k_tile_fill<<<hb_div_up(ff->n_pad, 256), 256, 0, s>>>(
+        gate, ff->d_sorted_ids, sys->d_posq, sys->d_image, ff->d_inv_perm, ff->d_tile_posq,
+        ff->d_tile_type, ff->d_ref_pos, n, ff->n_pad);
+    k_tile_bbox<<<hb_div_up((uint64_t)ff->n_tiles * 32u, 128), 128, 0, s>>>(
+        gate, ff->d_tile_posq, sys->d_box, ff->rc_max, ff->r_skin, ff->d_tile_center,
+        ff->d_tile_half, n, ff->n_tiles);
+    k_nl_build<false><<<hb_div_up(ff->n_tiles, NL_WARPS), NL_WARPS * 32, 0, s>>>(
+        gate, ff->d_tile_posq, ff->d_tile_center, ff->d_tile_half, sys->d_box, rs2, rb * rb,
+        band_lo, band_hi, n, ff->n_tiles, ff->d_tile_nent, ff->d_entry_off, ff->d_entry_j,
+        ff->d_entry_excl, ff->entry_cap, ff->d_sorted_ids, ff->d_inv_perm, ff->d_excl_off,
+        ff->d_excl_partner);
+    HB_TRY(scan_exclusive(gate, ff->d_tile_nent, ff->d_entry_off, ff->d_scan_tmp,
+                          ff->n_tiles + 1, s));
+  }
+  if (phase == 1) {
+    k_nl_build<true><<<hb_div_up(ff->n_tiles, NL_WARPS), NL_WARPS * 32, 0, s>>>(
+        gate, ff->d_tile_posq, ff->d_tile_center, ff->d_tile_half, sys->d_box, rs2, rb * rb,
+        band_lo, band_hi, n, ff->n_tiles, ff->d_tile_nent, ff->d_entry_off, ff->d_entry_j,
+        ff->d_entry_excl, ff->entry_cap, ff->d_sorted_ids, ff->d_inv_perm, ff->d_excl_off,
+        ff->d_excl_partner);
+    k_nl_finish<<<1, 1, 0, s>>>(gate, ff->d_status, ff->d_counters, ff->d_entry_off,
+                                ff->n_tiles, ff->entry_cap);
+  }
+  HB_CUDA(cudaGetLastError());
+  return HB_OK;
+}
+
+int nl_rebuild(hb_forcefield *ff, bool gated, cudaStream_t s) {
+  if (ff->sys->n == 0) return HB_OK;
+  const uint32_t *gate = gated ? ff->d_status : nullptr;
+  if (!gated) {
+    // an explicit rebuild: raise the displacement bit so k_nl_finish clears it
+    uint32_t one = HB_ST_DISPLACED;
+    HB_CUDA(cudaMemcpyAsync(ff->d_status, &one, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    HB_CUDA(cudaStreamSynchronize(s));
+  }
+  HB_TRY(nl_launch(ff, gate, s, 0));
+  HB_TRY(nl_launch(ff, gate, s, 1));
+  return HB_OK;
+}
+
+// First build: count, size the entry buffers from the count (x1.5 + slack),
+// then fill.  Host-synchronous; runs at force-field creation and when the
+// host grows the buffers after a high-water signal.
+int nl_first_build(hb_forcefield *ff) {
+  hb_system *sys = ff->sys;
+  if (sys->n == 0) {
+    ff->built = true;
+    return HB_OK;
+  }
+  cudaStream_t s = sys->ctx->stream;
+  uint32_t one = HB_ST_DISPLACED;
+  HB_CUDA(cudaMemcpyAsync(ff->d_status, &one, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  HB_TRY(nl_launch(ff, nullptr, s, 0));
+  uint32_t total = 0;
+  HB_CUDA(cudaMemcpyAsync(&total, ff->d_entry_off + ff->n_tiles, sizeof(uint32_t),
+                          cudaMemcpyDeviceToHost, s));
+  HB_CUDA(cudaStreamSynchronize(s));
+  uint64_t want = (uint64_t)total + total / 2 + 64;
+  if (want > ff->entry_cap) {
+    cudaFree(ff->d_entry_j);
+    cudaFree(ff->d_entry_excl);
+    ff->d_entry_j = nullptr;
+    ff->d_entry_excl = nullptr;
+    HB_CUDA(cudaMalloc(&ff->d_entry_j, sizeof(uint32_t) * 32 * want));
+    HB_CUDA(cudaMalloc(&ff->d_entry_excl, sizeof(uint32_t) * 32 * want));
+    ff->entry_cap = want;
+  }
+  HB_TRY(nl_launch(ff, nullptr, s, 1));
+  uint32_t st = 0;
+  HB_CUDA(cudaMemcpyAsync(&st, ff->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  HB_CUDA(cudaStreamSynchronize(s));
+  // clear the capacity bits of the sizing build
+  st &= ~(HB_ST_ENTRY_HIGHWATER | HB_ST_ENTRY_OVERFLOW);
+  HB_CUDA(cudaMemcpyAsync(ff->d_status, &st, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  HB_CUDA(cudaStreamSynchronize(s));
+  ff->built = true;
+  return HB_OK;
+}
+
+int nl_displacement_check(hb_forcefield *ff, cudaStream_t s) {
+  hb_system *sys = ff->sys;
+  if (sys->n == 0) return HB_OK;
+  float thr = 0.5f * ff->r_skin;
+  k_disp_check<<<hb_div_up(sys->n, 256), 256, 0, s>>>(sys->d_posq, ff->d_ref_pos, sys->d_box,
+                                                       thr * thr, ff->d_status, sys->n);
+  HB_CUDA(cudaGetLastError());
+  return HB_OK;
+}
+
+int nl_gather_positions(hb_forcefield *ff, cudaStream_t s) {
+  hb_system *sys = ff->sys;
+  if (sys->n == 0) return HB_OK;
+  k_gather_pos<<<hb_div_up(sys->n, 256), 256, 0, s>>>(ff->d_sorted_ids, sys->d_posq,
+                                                       ff->d_tile_posq, sys->n);
+  HB_CUDA(cudaGetLastError());
+  return HB_OK;
+}
+
+// Host decode of the packed list (the pair_snapshot analogue): every pair
+// held by an entry whose exact single-precision distance is within
+// r_search, as canonical (min id, max id), plus a duplicate count.
+static float host_exact_r2(float dx, float dy, float dz, const float b[6]) {
+  volatile float sc = dz / b[2];
+  volatile float sb = (dy - sc * b[5]) / b[1];
+  volatile float t1 = sb * b[3];
+  volatile float t2 = sc * b[4];
+  volatile float t3 = dx - t1;
+  volatile float sa = (t3 - t2) / b[0];
+  float ka = std::floor(sa + 0.5f), kb = std::floor(sb + 0.5f), kc = std::floor(sc + 0.5f);
+  volatile float u1 = ka * b[0];
+  volatile float u2 = kb * b[3];
+  volatile float u3 = kc * b[4];
+  volatile float u4 = u1 + u2;
+  volatile float u5 = u4 + u3;
+  volatile float ddx = dx - u5;
+  volatile float v1 = kb * b[1];
+  volatile float v2 = kc * b[5];
+  volatile float v3 = v1 + v2;
+  volatile float ddy = dy - v3;
+  volatile float w1 = kc * b[2];
+  volatile float ddz = dz - w1;
+  volatile float q1 = ddx * ddx;
+  volatile float q2 = ddy * ddy;
+  volatile float q3 = ddz * ddz;
+  volatile float q4 = q1 + q2;
+  volatile float q5 = q4 + q3;
+  return q5;
+}
+
+int nl_pairs(hb_forcefield *ff, std::vector<uint32_t> &pairs, uint64_t &dups) {
+  hb_system *sys = ff->sys;
+  cudaStream_t s = sys->ctx->stream;
+  HB_CUDA(cudaStreamSynchronize(s));
+  HB_CUDA(cudaStreamSynchronize(sys->ctx->stream2));
+  const uint32_t n = sys->n;
+  pairs.clear();
+  dups = 0;
+  if (n == 0) return HB_OK;
+  std::vector<uint32_t> off(ff->n_tiles + 1), ids(ff->n_pad);
+  std::vector<float4> pos(ff->n_pad);
+  HB_CUDA(cudaMemcpy(off.data(), ff->d_entry_off, sizeof(uint32_t) * (ff->n_tiles + 1),
+                     cudaMemcpyDeviceToHost));
+  HB_CUDA(cudaMemcpy(ids.data(), ff->d_sorted_ids, sizeof(uint32_t) * ff->n_pad,
+                     cudaMemcpyDeviceToHost));
+  HB_CUDA(cudaMemcpy(pos.data(), ff->d_tile_posq, sizeof(float4) * ff->n_pad,
+                     cudaMemcpyDeviceToHost));
+  uint64_t total = off[ff->n_tiles];
+  if (total > ff->entry_cap) return hb_fail(HB_ERR_NL_OVERFLOW, "packed entries overflowed");
+  std::vector<uint32_t> ej(total * 32);
+  if (total)
+    HB_CUDA(cudaMemcpy(ej.data(), ff->d_entry_j, sizeof(uint32_t) * 32 * total,
+                       cudaMemcpyDeviceToHost));
+  float b[6];
+  for (int d = 0; d < 6; ++d) b[d] = (float)sys->box[d];
+  const float rs2 = ff->r_search * ff->r_search;
+  std::vector<uint64_t> keys;
+  for (uint32_t I = 0; I < ff->n_tiles; ++I) {
+    for (uint32_t e = off[I]; e < off[I + 1]; ++e) {
+      bool self = (e == off[I]) && ej[(uint64_t)e * 32] == I * 32u;
+      for (uint32_t l = 0; l < 32; ++l) {
+        uint32_t si = I * 32u + l;
+        if (si >= n) continue;
+        uint32_t tmax = self ? 16u : 31u;
+        for (uint32_t t = self ? 1u : 0u; t <= tmax; ++t) {
+          if (self && t == 16u && l >= 16u) continue;
+          uint32_t jl = self ? ((l + t) & 31u) : ((l + t) & 31u);
+          uint32_t sj = ej[(uint64_t)e * 32 + jl];
+          if (sj == HB_SENTINEL || sj >= n) continue;
+          float4 a = pos[si], c = pos[sj];
+          float r2 = host_exact_r2(a.x - c.x, a.y - c.y, a.z - c.z, b);
+          if (r2 <= rs2) {
+            uint32_t oi = ids[si], oj = ids[sj];
+            uint32_t lo = std::min(oi, oj), hi = std::max(oi, oj);
+            keys.push_back(((uint64_t)lo << 32) | hi);
+          }
+        }
+      }
+    }
+  }
+  std::sort(keys.begin(), keys.end());
+  pairs.reserve(keys.size() * 2);
+  for (size_t k = 0; k < keys.size(); ++k) {
+    if (k > 0 && keys[k] == keys[k - 1]) {
+      dups++;
+      continue;
+    }
+    pairs.push_back((uint32_t)(keys[k] >> 32));
+    pairs.push_back((uint32_t)(keys[k] & 0xFFFFFFFFu));
+  }
+  return HB_OK;
+}

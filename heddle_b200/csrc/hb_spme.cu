@@ -1,0 +1,623 @@
+// hb_spme.cu -- SPME reciprocal space: charge spread, 3-D FFT with the
+// influence-function convolution fused into the middle pass, force gather.
+//
+// Physics follows the reference (src/forces/spme.rs:228-503, :815-822;
+// kernels/spme_recip.cu:34-402; kernels/spme_spread_gather.cuh:36-334):
+// cardinal B-splines of order p on the fractional grid u = (s + 1/2) n,
+// grid points floor(u) - d with weight M_p(d + t); the influence function
+// G(k) = (1/V)(4 pi / K^2) exp(-K^2 / 4 alpha^2) |b_a b_b b_c|^2 with
+// Essmann's near-zero averaging of the b-factors; tinfoil k = 0; energy
+// 1/2 sum_k G |rho_hat|^2, virial 1/2 sum_k G (1 - K^2 / 2 alpha^2)
+// |rho_hat|^2; per-atom energy share 1/2 q phi - alpha / sqrt(pi) q^2;
+// uniform per-atom virial share W_recip / N.
+//
+// Device pipeline (own design):
+//   spread   : 4 threads per atom (sorted, spatially coherent order), each
+//              adds its p^2 contributions to an int64 grid with scale 2^32
+//              (order-independent, byte-identical repeat runs);
+//   fft_c    : per row, int64 -> f32, clears the int64 grid for the next
+//              step, length-n_c transform, keeps n_c / 2 + 1 modes;
+//   fft_b    : batches of 16 lines along b, transform in shared memory;
+//   fft_a    : batches along a: forward transform, multiply by G computed
+//              on the fly (no influence buffers, so a box change needs no
+//              refresh pass), FP64 energy / virial partials, inverse
+//              transform -- the convolution costs no extra grid pass;
+//   ifft_b, ifft_c (Hermitian extension, real part) -> V;
+//   gather   : one thread per atom, p^3 reads of V, force, energy share.
+// The FFT is a Stockham autosort transform with radix 4, 2, 3, 5, 7
+// butterflies, twiddles from an FP64-built table, lines held in shared
+// memory with a padded stride.  It is deterministic by construction.
+#include <cmath>
+#include <vector>
+
+#include "hb_internal.cuh"
+
+namespace {
+
+struct FftPlan {
+  int n;
+  int nst;
+  int r[16];
+};
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // a * conj(b)
+  return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+// In-shared-memory transform of L lines of length n, line-major with
+// stride S = n + 1.  Returns the buffer holding the result.
+template <bool INV>
+__device__ float2 *fft_lines(float2 *A, float2 *B, const float2 *__restrict__ tw, int n,
+                             int L, const FftPlan &pl) {
+  const int S = n + 1;
+  int Ns = 1;
+  for (int st = 0; st < pl.nst; ++st) {
+    const int p = pl.r[st];
+    const int m = n / p;
+    const int tstep = n / (Ns * p);
+    const int np = n / p;
+    for (int idx = threadIdx.x; idx < m * L; idx += blockDim.x) {
+      const int l = idx / m, j = idx - (idx / m) * m;
+      const int k = j % Ns;
+      const float2 *src = A + l * S;
+      float2 v[7];
+      for (int q = 0; q < p; ++q) v[q] = src[j + q * m];
+      if (Ns > 1) {
+        for (int q = 1; q < p; ++q) {
+          const float2 w = tw[q * k * tstep];
+          v[q] = INV ? cmulc(v[q], w) : cmul(v[q], w);
+        }
+      }
+      if (p == 2) {
+        float2 a = v[0], b = v[1];
+        v[0] = make_float2(a.x + b.x, a.y + b.y);
+        v[1] = make_float2(a.x - b.x, a.y - b.y);
+      } else if (p == 4) {
+        float2 a0 = make_float2(v[0].x + v[2].x, v[0].y + v[2].y);
+        float2 a1 = make_float2(v[0].x - v[2].x, v[0].y - v[2].y);
+        float2 a2 = make_float2(v[1].x + v[3].x, v[1].y + v[3].y);
+        float2 a3 = make_float2(v[1].x - v[3].x, v[1].y - v[3].y);
+        // forward: X1 = a1 - i a3, X3 = a1 + i a3 (inverse swaps the sign)
+        float2 ia3 = INV ? make_float2(-a3.y, a3.x) : make_float2(a3.y, -a3.x);
+        v[0] = make_float2(a0.x + a2.x, a0.y + a2.y);
+        v[2] = make_float2(a0.x - a2.x, a0.y - a2.y);
+        v[1] = make_float2(a1.x + ia3.x, a1.y + ia3.y);
+        v[3] = make_float2(a1.x - ia3.x, a1.y - ia3.y);
+      } else {
+        float2 o[7];
+        for (int r = 0; r < p; ++r) {
+          float2 acc = v[0];
+          for (int q = 1; q < p; ++q) {
+            const float2 w = tw[((q * r) % p) * np];
+            const float2 t = INV ? cmulc(v[q], w) : cmul(v[q], w);
+            acc.x += t.x;
+            acc.y += t.y;
+          }
+          o[r] = acc;
+        }
+        for (int r = 0; r < p; ++r) v[r] = o[r];
+      }
+      float2 *dst = B + l * S;
+      const int base = (j / Ns) * Ns * p + k;
+      for (int q = 0; q < p; ++q) dst[base + q * Ns] = v[q];
+    }
+    __syncthreads();
+    float2 *t = A;
+    A = B;
+    B = t;
+    Ns *= p;
+  }
+  return A;
+}
+
+// B-spline weights w[d] = M_P(d + t), d = 0..P-1, and optionally their
+// derivatives, by the Cox-de Boor recursion raised one order at a time.
+template <int P, bool DERIV>
+__device__ __forceinline__ void bspline(float t, float *w, float *dw) {
+  float c[P];
+  c[0] = 1.0f;
+#pragma unroll
+  for (int d = 1; d < P; ++d) c[d] = 0.0f;
+#pragma unroll
+  for (int k = 2; k <= P; ++k) {
+    if (DERIV && k == P) {
+#pragma unroll
+      for (int d = 0; d < P; ++d) dw[d] = (d < P - 1 ? c[d] : 0.0f) - (d >= 1 ? c[d - 1] : 0.0f);
+    }
+    const float inv = 1.0f / (float)(k - 1);
+#pragma unroll
+    for (int d = k - 1; d >= 0; --d) {
+      float a = (d <= k - 2) ? (t + (float)d) * c[d] : 0.0f;
+      float b = (d >= 1) ? ((float)k - t - (float)d) * c[d - 1] : 0.0f;
+      c[d] = (a + b) * inv;
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < P; ++d) w[d] = c[d];
+}
+
+__device__ __forceinline__ void grid_setup(float x, float y, float z, const DBox &b, int na,
+                                           int nb, int nc, float t[3], int g0[3]) {
+  int ka, kb, kc;
+  hb_wrap(x, y, z, ka, kb, kc, b);
+  float s[3];
+  hb_frac(x, y, z, b, s[0], s[1], s[2]);
+  const int n[3] = {na, nb, nc};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    float u = (s[d] + 0.5f) * (float)n[d];
+    float f = floorf(u);
+    t[d] = u - f;
+    int fi = (int)f;
+    fi %= n[d];
+    if (fi < 0) fi += n[d];
+    g0[d] = fi;
+  }
+}
+
+template <int P>
+__global__ void k_spread(const float4 *__restrict__ tile_posq, const DBox *__restrict__ box,
+                         int na, int nb, int nc, unsigned long long *__restrict__ rho,
+                         uint32_t n) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t k = g / P;
+  const int da = (int)(g - k * P);
+  if (k >= n) return;
+  const float4 p = tile_posq[k];
+  if (p.w == 0.0f) return;
+  const DBox b = *box;
+  float t[3];
+  int g0[3];
+  grid_setup(p.x, p.y, p.z, b, na, nb, nc, t, g0);
+  float wa[P], wb[P], wc[P];
+  bspline<P, false>(t[0], wa, nullptr);
+  bspline<P, false>(t[1], wb, nullptr);
+  bspline<P, false>(t[2], wc, nullptr);
+  int ga = g0[0] - da;
+  if (ga < 0) ga += na;
+  const float qa = p.w * wa[da];
+#pragma unroll
+  for (int db = 0; db < P; ++db) {
+    int gb = g0[1] - db;
+    if (gb < 0) gb += nb;
+    const float qab = qa * wb[db];
+    const size_t rowbase = ((size_t)ga * nb + gb) * nc;
+#pragma unroll
+    for (int dc = 0; dc < P; ++dc) {
+      int gc = g0[2] - dc;
+      if (gc < 0) gc += nc;
+      const long long v = __float2ll_rn(qab * wc[dc] * HB_RHO_SCALE);
+      if (v != 0) atomicAdd(&rho[rowbase + gc], (unsigned long long)v);
+    }
+  }
+}
+
+// forward transform along c, one CTA per L rows; clears the int64 grid
+__global__ void k_fft_c_fwd(unsigned long long *__restrict__ rho, float2 *__restrict__ grid,
+                            const float2 *__restrict__ tw_g, FftPlan pl, int nrows, int nch,
+                            int L) {
+  extern __shared__ float2 sm[];
+  const int n = pl.n, S = n + 1;
+  float2 *tw = sm;
+  float2 *A = sm + n;
+  float2 *B = A + L * S;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = tw_g[i];
+  const int row0 = blockIdx.x * L;
+  const int nr = min(L, nrows - row0);
+  for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
+    const int r = idx / n, c = idx - (idx / n) * n;
+    float v = 0.0f;
+    if (r < nr) {
+      const size_t gi = (size_t)(row0 + r) * n + c;
+      v = (float)(long long)rho[gi] * (1.0f / HB_RHO_SCALE);
+      rho[gi] = 0ull;
+    }
+    A[r * S + c] = make_float2(v, 0.0f);
+  }
+  __syncthreads();
+  float2 *R = fft_lines<false>(A, B, tw, n, L, pl);
+  for (int idx = threadIdx.x; idx < L * nch; idx += blockDim.x) {
+    const int r = idx / nch, c = idx - (idx / nch) * nch;
+    if (r < nr) grid[(size_t)(row0 + r) * nch + c] = R[r * S + c];
+  }
+}
+
+// transform along b for L consecutive kc of one a-plane
+template <bool INV>
+__global__ void k_fft_b(float2 *__restrict__ grid, const float2 *__restrict__ tw_g, FftPlan pl,
+                        int nb, int nch, int L) {
+  extern __shared__ float2 sm[];
+  const int n = pl.n, S = n + 1;
+  float2 *tw = sm;
+  float2 *A = sm + n;
+  float2 *B = A + L * S;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = tw_g[i];
+  const int nchunk = (nch + L - 1) / L;
+  const int a = blockIdx.x / nchunk;
+  const int kc0 = (blockIdx.x - a * nchunk) * L;
+  for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
+    const int l = idx % L, bp = idx / L;
+    const int kc = kc0 + l;
+    A[l * S + bp] = kc < nch ? grid[((size_t)a * nb + bp) * nch + kc] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  float2 *R = fft_lines<INV>(A, B, tw, n, L, pl);
+  for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
+    const int l = idx % L, bp = idx / L;
+    const int kc = kc0 + l;
+    if (kc < nch) grid[((size_t)a * nb + bp) * nch + kc] = R[l * S + bp];
+  }
+}
+
+// transform along a, influence multiply with FP64 energy / virial
+// partials, inverse transform along a
+__global__ void k_fft_a_conv(float2 *__restrict__ grid, const float2 *__restrict__ tw_g,
+                             FftPlan pl, int na, int nb, int nc, int nch, int L,
+                             const DBox *__restrict__ box, const float *__restrict__ bfac,
+                             float alpha, double *__restrict__ part) {
+  extern __shared__ float2 sm[];
+  __shared__ double red_e[256], red_w[256];
+  const int n = pl.n, S = n + 1;
+  float2 *tw = sm;
+  float2 *A = sm + n;
+  float2 *B = A + L * S;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = tw_g[i];
+  const int nchunk = (nch + L - 1) / L;
+  const int bq = blockIdx.x / nchunk;
+  const int kc0 = (blockIdx.x - bq * nchunk) * L;
+  for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
+    const int l = idx % L, ap = idx / L;
+    const int kc = kc0 + l;
+    A[l * S + ap] = kc < nch ? grid[((size_t)ap * nb + bq) * nch + kc] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  float2 *R = fft_lines<false>(A, B, tw, n, L, pl);
+  float2 *O = (R == A) ? B : A;
+  const DBox bx = *box;
+  const float ilx = bx.ilx, ily = bx.ily, ilz = bx.ilz;
+  const float bax = ilx, bay = -bx.xy * ilx * ily, baz = (bx.xy * bx.yz - bx.xz * bx.ly) * ilx * ily * ilz;
+  const float bby = ily, bbz = -bx.yz * ily * ilz, bcz = ilz;
+  const float two_pi = 6.283185307179586f;
+  const float inv_vol = ilx * ily * ilz;
+  const float inv4a2 = 1.0f / (4.0f * alpha * alpha);
+  const float inv2a2 = 1.0f / (2.0f * alpha * alpha);
+  const float mb = (bq <= nb / 2) ? (float)bq : (float)(bq - nb);
+  const float bfb = bfac[na + bq];
+  double e_acc = 0.0, w_acc = 0.0;
+  for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
+    const int l = idx / n, ka = idx - (idx / n) * n;
+    const int kc = kc0 + l;
+    float2 X = R[l * S + ka];
+    float G = 0.0f, vf = 0.0f;
+    if (kc < nch) {
+      const float ma = (ka <= na / 2) ? (float)ka : (float)(ka - na);
+      const float mc = (float)kc;
+      const float kx = two_pi * (ma * bax);
+      const float ky = two_pi * (ma * bay + mb * bby);
+      const float kz = two_pi * (ma * baz + mb * bbz + mc * bcz);
+      const float k2 = kx * kx + ky * ky + kz * kz;
+      if (k2 > 0.0f) {
+        G = inv_vol * (12.566370614359172f / k2) * expf(-k2 * inv4a2) * bfac[ka] * bfb *
+            bfac[na + nb + kc];
+        vf = G * (1.0f - k2 * inv2a2);
+      }
+      const double hw = (kc == 0 || ((nc & 1) == 0 && 2 * kc == nc)) ? 1.0 : 2.0;
+      const double x2 = (double)X.x * X.x + (double)X.y * X.y;
+      e_acc += hw * (double)G * x2;
+      w_acc += hw * (double)vf * x2;
+    }
+    R[l * S + ka] = make_float2(G * X.x, G * X.y);
+  }
+  red_e[threadIdx.x] = e_acc;
+  red_w[threadIdx.x] = w_acc;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st) {
+      red_e[threadIdx.x] += red_e[threadIdx.x + st];
+      red_w[threadIdx.x] += red_w[threadIdx.x + st];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = red_e[0];
+    part[2 * blockIdx.x + 1] = red_w[0];
+  }
+  float2 *R2 = fft_lines<true>(R, O, tw, n, L, pl);
+  for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
+    const int l = idx % L, ap = idx / L;
+    const int kc = kc0 + l;
+    if (kc < nch) grid[((size_t)ap * nb + bq) * nch + kc] = R2[l * S + ap];
+  }
+}
+
+// inverse transform along c with Hermitian extension; writes V (real)
+__global__ void k_fft_c_inv(const float2 *__restrict__ grid, float *__restrict__ v,
+                            const float2 *__restrict__ tw_g, FftPlan pl, int nrows, int nch,
+                            int L) {
+  extern __shared__ float2 sm[];
+  const int n = pl.n, S = n + 1;
+  float2 *tw = sm;
+  float2 *A = sm + n;
+  float2 *B = A + L * S;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = tw_g[i];
+  const int row0 = blockIdx.x * L;
+  const int nr = min(L, nrows - row0);
+  for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
+    const int r = idx / n, c = idx - (idx / n) * n;
+    float2 x = make_float2(0.f, 0.f);
+    if (r < nr) {
+      if (c < nch) {
+        x = grid[(size_t)(row0 + r) * nch + c];
+      } else {
+        float2 y = grid[(size_t)(row0 + r) * nch + (n - c)];
+        x = make_float2(y.x, -y.y);
+      }
+    }
+    A[r * S + c] = x;
+  }
+  __syncthreads();
+  float2 *R = fft_lines<true>(A, B, tw, n, L, pl);
+  for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
+    const int r = idx / n, c = idx - (idx / n) * n;
+    if (r < nr) v[(size_t)(row0 + r) * n + c] = R[r * S + c].x;
+  }
+}
+
+template <int P>
+__global__ void k_gather(const float4 *__restrict__ tile_posq, const float *__restrict__ V,
+                         const DBox *__restrict__ box, int na, int nb, int nc, float self_pref,
+                         float4 *__restrict__ out, uint32_t n) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const float4 p = tile_posq[k];
+  const DBox b = *box;
+  float t[3];
+  int g0[3];
+  grid_setup(p.x, p.y, p.z, b, na, nb, nc, t, g0);
+  float wa[P], wb[P], wc[P], dwa[P], dwb[P], dwc[P];
+  bspline<P, true>(t[0], wa, dwa);
+  bspline<P, true>(t[1], wb, dwb);
+  bspline<P, true>(t[2], wc, dwc);
+  int gc[P];
+#pragma unroll
+  for (int d = 0; d < P; ++d) {
+    int x = g0[2] - d;
+    gc[d] = x < 0 ? x + nc : x;
+  }
+  float phi = 0.f, ga = 0.f, gb = 0.f, gcc = 0.f;
+#pragma unroll
+  for (int da = 0; da < P; ++da) {
+    int ia = g0[0] - da;
+    if (ia < 0) ia += na;
+#pragma unroll
+    for (int db = 0; db < P; ++db) {
+      int ib = g0[1] - db;
+      if (ib < 0) ib += nb;
+      const float *row = V + ((size_t)ia * nb + ib) * nc;
+      float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+      for (int dc = 0; dc < P; ++dc) {
+        const float v = __ldg(row + gc[dc]);
+        s0 += v * wc[dc];
+        s1 += v * dwc[dc];
+      }
+      phi += wa[da] * wb[db] * s0;
+      ga += dwa[da] * wb[db] * s0;
+      gb += wa[da] * dwb[db] * s0;
+      gcc += wa[da] * wb[db] * s1;
+    }
+  }
+  ga *= (float)na;
+  gb *= (float)nb;
+  gcc *= (float)nc;
+  // rows of H^{-T} (spme_spread_gather.cuh:128-148)
+  const float bax = b.ilx, bay = -b.xy * b.ilx * b.ily,
+              baz = (b.xy * b.yz - b.xz * b.ly) * b.ilx * b.ily * b.ilz;
+  const float bby = b.ily, bbz = -b.yz * b.ily * b.ilz, bcz = b.ilz;
+  const float q = p.w;
+  float4 o;
+  o.x = -q * (ga * bax);
+  o.y = -q * (ga * bay + gb * bby);
+  o.z = -q * (ga * baz + gb * bbz + gcc * bcz);
+  o.w = 0.5f * q * phi - self_pref * q * q;
+  out[k] = o;
+}
+
+__global__ void k_spme_sums(const double *__restrict__ part, int n_part,
+                            double *__restrict__ sums) {
+  __shared__ double se[256], sw[256];
+  double e = 0.0, w = 0.0;
+  for (int i = threadIdx.x; i < n_part; i += 256) {
+    e += part[2 * i];
+    w += part[2 * i + 1];
+  }
+  se[threadIdx.x] = e;
+  sw[threadIdx.x] = w;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st) {
+      se[threadIdx.x] += se[threadIdx.x + st];
+      sw[threadIdx.x] += sw[threadIdx.x + st];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    sums[0] = 0.5 * se[0];
+    sums[1] = 0.5 * sw[0];
+  }
+}
+
+bool make_plan(int n, FftPlan &pl) {
+  pl.n = n;
+  pl.nst = 0;
+  int m = n;
+  while (m % 4 == 0 && m > 4 && pl.nst < 16) {
+    pl.r[pl.nst++] = 4;
+    m /= 4;
+  }
+  const int primes[5] = {4, 2, 3, 5, 7};
+  for (int pi = 0; pi < 5; ++pi) {
+    while (m % primes[pi] == 0 && pl.nst < 16) {
+      pl.r[pl.nst++] = primes[pi];
+      m /= primes[pi];
+    }
+  }
+  return m == 1;
+}
+
+int lines_per_cta(int n) {
+  int L = 2048 / n;
+  if (L > 16) L = 16;
+  if (L < 2) L = 2;
+  return L;
+}
+
+// host restatement of the b-factors (src/forces/spme.rs:524-585)
+double bspline_host(int p, double x) {
+  double v[16];
+  for (int i = 0; i < p; ++i) {
+    double xi = x - i;
+    v[i] = (xi >= 0.0 && xi < 1.0) ? 1.0 : 0.0;
+  }
+  for (int k = 2; k <= p; ++k)
+    for (int i = 0; i <= p - k; ++i) {
+      double xi = x - i;
+      v[i] = (xi * v[i] + ((double)k - xi) * v[i + 1]) / (double)(k - 1);
+    }
+  return v[0];
+}
+
+void b_factors(int n, int p, std::vector<float> &out) {
+  std::vector<double> mod(n);
+  for (int k = 0; k < n; ++k) {
+    double th = 2.0 * M_PI * k / n, re = 0.0, im = 0.0;
+    for (int j = 0; j < p - 1; ++j) {
+      double m = bspline_host(p, (double)(j + 1));
+      re += m * std::cos(th * j);
+      im += m * std::sin(th * j);
+    }
+    mod[k] = re * re + im * im;
+  }
+  for (int k = 0; k < n; ++k)
+    if (mod[k] < 1.0e-7) mod[k] = 0.5 * (mod[(k + n - 1) % n] + mod[(k + 1) % n]);
+  for (int k = 0; k < n; ++k) out.push_back(mod[k] > 0.0 ? (float)(1.0 / mod[k]) : 0.0f);
+}
+
+void twiddles(int n, std::vector<float2> &out) {
+  for (int t = 0; t < n; ++t) {
+    double a = -2.0 * M_PI * (double)t / (double)n;
+    out.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+  }
+}
+
+size_t fft_smem(int n, int L) { return sizeof(float2) * ((size_t)n + 2 * (size_t)L * (n + 1)); }
+
+}  // namespace
+
+int spme_setup(hb_forcefield *ff, const hb_forcefield_desc *d) {
+  SpmeState &S = ff->spme;
+  S.on = 1;
+  S.na = (int)d->grid[0];
+  S.nb = (int)d->grid[1];
+  S.nc = (int)d->grid[2];
+  S.nch = S.nc / 2 + 1;
+  S.order = (int)d->spline_order;
+  S.alpha = (float)d->alpha;
+  S.self_pref = (float)(d->alpha / std::sqrt(M_PI));
+  FftPlan p;
+  for (int ax = 0; ax < 3; ++ax) {
+    int n = (int)d->grid[ax];
+    if (n < 2 * S.order)
+      return hb_fail(HB_ERR_INVALID_GRID, "SPME grid[" + std::string(1, "abc"[ax]) + "] = " +
+                                              std::to_string(n) + " is less than 2 * spline_order = " +
+                                              std::to_string(2 * S.order));
+    if (!make_plan(n, p) || n > 1024)
+      return hb_fail(HB_ERR_INVALID_GRID, "SPME grid sizes must factor into 2, 3, 5, 7 and be <= 1024");
+  }
+  const size_t m = (size_t)S.na * S.nb * S.nc;
+  const size_t mc = (size_t)S.na * S.nb * S.nch;
+  HB_CUDA(cudaMalloc(&S.d_rho_fixed, sizeof(unsigned long long) * m));
+  HB_CUDA(cudaMemset(S.d_rho_fixed, 0, sizeof(unsigned long long) * m));
+  HB_CUDA(cudaMalloc(&S.d_grid, sizeof(float2) * mc));
+  HB_CUDA(cudaMalloc(&S.d_v, sizeof(float) * m));
+  std::vector<float> bf;
+  b_factors(S.na, S.order, bf);
+  b_factors(S.nb, S.order, bf);
+  b_factors(S.nc, S.order, bf);
+  HB_CUDA(cudaMalloc(&S.d_bfac, sizeof(float) * bf.size()));
+  HB_CUDA(cudaMemcpy(S.d_bfac, bf.data(), sizeof(float) * bf.size(), cudaMemcpyHostToDevice));
+  std::vector<float2> tw;
+  twiddles(S.na, tw);
+  twiddles(S.nb, tw);
+  twiddles(S.nc, tw);
+  HB_CUDA(cudaMalloc(&S.d_tw, sizeof(float2) * tw.size()));
+  HB_CUDA(cudaMemcpy(S.d_tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice));
+  const int La = lines_per_cta(S.na);
+  S.n_part = S.nb * ((S.nch + La - 1) / La);
+  HB_CUDA(cudaMalloc(&S.d_part, sizeof(double) * 2 * S.n_part));
+  HB_CUDA(cudaMalloc(&S.d_sums, sizeof(double) * 2));
+  HB_CUDA(cudaMemset(S.d_sums, 0, sizeof(double) * 2));
+  HB_CUDA(cudaMalloc(&S.d_recip, sizeof(float4) * std::max(ff->n_pad, 32u)));
+  HB_CUDA(cudaMemset(S.d_recip, 0, sizeof(float4) * std::max(ff->n_pad, 32u)));
+  return HB_OK;
+}
+
+int spme_free(hb_forcefield *ff) {
+  SpmeState &S = ff->spme;
+  cudaFree(S.d_rho_fixed);
+  cudaFree(S.d_grid);
+  cudaFree(S.d_v);
+  cudaFree(S.d_bfac);
+  cudaFree(S.d_tw);
+  cudaFree(S.d_part);
+  cudaFree(S.d_sums);
+  cudaFree(S.d_recip);
+  return HB_OK;
+}
+
+int spme_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
+  SpmeState &S = ff->spme;
+  if (!S.on) return HB_OK;
+  hb_system *sys = ff->sys;
+  const uint32_t n = sys->n;
+  const int na = S.na, nb = S.nb, nc = S.nc, nch = S.nch;
+  FftPlan pa, pb, pc;
+  make_plan(na, pa);
+  make_plan(nb, pb);
+  make_plan(nc, pc);
+  const float2 *twa = S.d_tw, *twb = S.d_tw + na, *twc = S.d_tw + na + nb;
+  if (n > 0) {
+    const uint64_t th = (uint64_t)n * S.order;
+    switch (S.order) {
+      case 4: k_spread<4><<<hb_div_up(th, 256), 256, 0, s>>>(ff->d_tile_posq, sys->d_box, na, nb, nc, S.d_rho_fixed, n); break;
+      case 5: k_spread<5><<<hb_div_up(th, 256), 256, 0, s>>>(ff->d_tile_posq, sys->d_box, na, nb, nc, S.d_rho_fixed, n); break;
+      case 6: k_spread<6><<<hb_div_up(th, 256), 256, 0, s>>>(ff->d_tile_posq, sys->d_box, na, nb, nc, S.d_rho_fixed, n); break;
+      case 7: k_spread<7><<<hb_div_up(th, 256), 256, 0, s>>>(ff->d_tile_posq, sys->d_box, na, nb, nc, S.d_rho_fixed, n); break;
+      case 8: k_spread<8><<<hb_div_up(th, 256), 256, 0, s>>>(ff->d_tile_posq, sys->d_box, na, nb, nc, S.d_rho_fixed, n); break;
+      default: return hb_fail(HB_ERR_INVALID_ARGUMENT, "spline order must be 4..8");
+    }
+  }
+  const int Lc = lines_per_cta(nc), Lb = lines_per_cta(nb), La = lines_per_cta(na);
+  const int nrows = na * nb;
+  k_fft_c_fwd<<<hb_div_up(nrows, Lc), 256, fft_smem(nc, Lc), s>>>(S.d_rho_fixed, S.d_grid, twc, pc, nrows, nch, Lc);
+  k_fft_b<false><<<na * ((nch + Lb - 1) / Lb), 256, fft_smem(nb, Lb), s>>>(S.d_grid, twb, pb, nb, nch, Lb);
+  k_fft_a_conv<<<nb * ((nch + La - 1) / La), 256, fft_smem(na, La), s>>>(
+      S.d_grid, twa, pa, na, nb, nc, nch, La, sys->d_box, S.d_bfac, S.alpha, S.d_part);
+  k_fft_b<true><<<na * ((nch + Lb - 1) / Lb), 256, fft_smem(nb, Lb), s>>>(S.d_grid, twb, pb, nb, nch, Lb);
+  k_fft_c_inv<<<hb_div_up(nrows, Lc), 256, fft_smem(nc, Lc), s>>>(S.d_grid, S.d_v, twc, pc, nrows, nch, Lc);
+  if (n > 0) {
+    switch (S.order) {
+      case 4: k_gather<4><<<hb_div_up(n, 128), 128, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
+      case 5: k_gather<5><<<hb_div_up(n, 128), 128, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
+      case 6: k_gather<6><<<hb_div_up(n, 128), 128, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
+      case 7: k_gather<7><<<hb_div_up(n, 128), 128, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
+      case 8: k_gather<8><<<hb_div_up(n, 128), 128, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
+    }
+  }
+  if (ev) k_spme_sums<<<1, 256, 0, s>>>(S.d_part, S.n_part, S.d_sums);
+  HB_CUDA(cudaGetLastError());
+  return HB_OK;
+}

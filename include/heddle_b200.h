@@ -1,0 +1,240 @@
+/*
+ * heddle_b200.h -- C ABI of the B200-native HeddleMD force-and-constraint
+ * path.
+ *
+ * Every entry point takes plain pointers and sizes, returns an int status
+ * (HB_OK or an HB_ERR_* code) and leaves a thread-local message readable
+ * through hb_last_error().  Units are Hartree atomic units (bohr, hartree,
+ * electron mass, elementary charge, atomic time; k_Coulomb = k_B = 1), the
+ * reference's internal units (src/units/atomic_constants.rs:11-35).
+ * The box is the lower-triangular lattice (lx, ly, lz, xy, xz, yz) of
+ * src/pbc.rs:11-60.
+ *
+ * Threading: a context and everything created from it is single-threaded
+ * and runs on the context's stream(s), as the reference runs on one default
+ * stream (src/runner.rs:2441-2447).
+ *
+ * Each declaration names the reference interface it replaces (paths are
+ * relative to the HeddleMD project root).
+ */
+#ifndef HEDDLE_B200_H
+#define HEDDLE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (errors of rqm/error-handling.md:13-115) ---- */
+enum {
+  HB_OK = 0,
+  HB_ERR_INVALID_ARGUMENT = 1,   /* malformed descriptor / null pointer */
+  HB_ERR_CUDA = 2,               /* CUDA runtime failure (GpuError) */
+  HB_ERR_NL_OVERFLOW = 3,        /* NeighborListError::PackedNeighborOverflow */
+  HB_ERR_BOX_TOO_SMALL = 4,      /* NeighborListError::BoxTooSmallForCells */
+  HB_ERR_INVALID_GRID = 5,       /* SpmeError::InvalidGrid */
+  HB_ERR_CONSTRAINT_SHAPE = 6,   /* ConstraintError (group too large, bad kind) */
+  HB_ERR_DEVICE_TIMEOUT = 7,     /* a bounded device-side wait gave up */
+  HB_ERR_UNSUPPORTED = 8,        /* combination the reference rejects
+                                    (e.g. all-pairs + SPME, src/io/config.rs:85-88) */
+  HB_ERR_NOT_FINITE = 9          /* non-finite position / box value */
+};
+
+/* aggregate level of ForceField::step (src/forces/mod.rs:662-717) */
+enum { HB_FORCES_ONLY = 0, HB_FORCES_AND_SCALARS = 1 };
+
+/* integrator kinds (registry names of src/integrator/mod.rs:627-677) */
+enum {
+  HB_INTEGRATOR_VV = 0,          /* "velocity-verlet" */
+  HB_INTEGRATOR_VV_LOSSLESS = 1, /* velocity Verlet, lossless (f32 + f64) mode */
+  HB_INTEGRATOR_LANGEVIN = 2     /* "langevin-baoab" (middle scheme) */
+};
+
+/* constraint kinds (src/integrator/constraint.rs:205-212) */
+enum { HB_CONSTRAINT_SETTLE = 0, HB_CONSTRAINT_SHAKE = 1 };
+
+typedef struct hb_context hb_context;
+typedef struct hb_system hb_system;
+typedef struct hb_forcefield hb_forcefield;
+typedef struct hb_constraints hb_constraints;
+typedef struct hb_integrator hb_integrator;
+
+/* Message of the last failing call on this thread ("" when none). */
+const char *hb_last_error(void);
+
+/* Library version string. */
+const char *hb_version(void);
+
+/* ---- context: replaces init_device (src/gpu/device.rs:67-74) ---- */
+int hb_context_create(int device_ordinal, hb_context **out);
+int hb_context_destroy(hb_context *ctx);
+int hb_context_synchronize(hb_context *ctx);
+
+/* ---- system state: replaces ParticleBuffers::new (src/gpu/buffers.rs:11-38)
+ * and SimulationBox::new (src/pbc.rs:142-170).  The library copies the host
+ * arrays into device structure-of-arrays and owns them. */
+typedef struct {
+  uint32_t n_atoms;
+  const double *positions;   /* [3n] */
+  const double *velocities;  /* [3n] or NULL (zero) */
+  const double *masses;      /* [n] */
+  const double *charges;     /* [n] */
+  const uint32_t *types;     /* [n] particle-type indices */
+  const int32_t *images;     /* [3n] or NULL (zero) */
+  double box[6];             /* lx, ly, lz, xy, xz, yz */
+} hb_system_desc;
+
+int hb_system_create(hb_context *ctx, const hb_system_desc *desc,
+                     hb_system **out);
+int hb_system_destroy(hb_system *sys);
+/* Overwrite positions / velocities from host ([3n] each, NULL = keep). */
+int hb_system_set_state(hb_system *sys, const double *positions,
+                        const double *velocities);
+/* Download positions, velocities, images, forces (any may be NULL). */
+int hb_system_get_state(hb_system *sys, double *positions, double *velocities,
+                        int32_t *images, double *forces);
+int hb_system_set_box(hb_system *sys, const double box[6]);
+int hb_system_get_box(hb_system *sys, double box[6]);
+
+/* ---- force field: replaces ForceField::new (src/forces/mod.rs:355-621)
+ * with the LJ slot (src/forces/lj.rs), SPME real (src/forces/spme.rs:620-781)
+ * and SPME reciprocal (src/forces/spme.rs:228-503, :862-917). */
+typedef struct {
+  /* Lennard-Jones: tables [n_types * n_types], row-major (ti * n + tj). */
+  int lj_enabled;
+  uint32_t n_types;
+  const double *lj_sigma;
+  const double *lj_epsilon;
+  const double *lj_cutoff;
+  const double *lj_switch;
+  /* erfc-screened real-space Coulomb */
+  int coulomb_enabled;
+  double alpha;
+  double r_cut_coulomb;
+  /* SPME reciprocal */
+  int recip_enabled;
+  uint32_t grid[3];
+  uint32_t spline_order;     /* 4..8 */
+  /* exclusions: CSR over atoms (offsets [n+1]), partner ids, scales */
+  const uint32_t *excl_offsets;  /* NULL = none */
+  const uint32_t *excl_partners;
+  const double *excl_lj_scale;
+  const double *excl_coulomb_scale;
+  /* neighbour list */
+  double r_skin;
+} hb_forcefield_desc;
+
+int hb_forcefield_create(hb_system *sys, const hb_forcefield_desc *desc,
+                         hb_forcefield **out);
+int hb_forcefield_destroy(hb_forcefield *ff);
+/* ForceField::step (src/forces/mod.rs:662-670): neighbour pre-step (rebuild
+ * when any atom moved more than r_skin / 2), pair forces, SPME, combine.
+ * Forces land in the system's force buffer; level HB_FORCES_AND_SCALARS
+ * also produces per-atom energies / virials and the FP64 scalars. */
+int hb_forcefield_step(hb_forcefield *ff, int level);
+/* NeighborListState::pre_step (src/forces/neighbor_list.rs:1265-1354):
+ * rebuild if needed (force != 0 forces a rebuild); *rebuilt = 1 if so. */
+int hb_forcefield_pre_step(hb_forcefield *ff, int force, int *rebuilt);
+/* FP64 scalars of the last HB_FORCES_AND_SCALARS step:
+ * out[0] LJ energy, [1] real-space Coulomb, [2] reciprocal (k-space sum),
+ * [3] self energy (subtracted), [4] total potential, [5] pair virial,
+ * [6] reciprocal virial, [7] total virial. */
+int hb_forcefield_scalars(hb_forcefield *ff, double out[8]);
+/* per-atom energy and virial shares of the last scalar step ([n] each). */
+int hb_forcefield_get_per_atom(hb_forcefield *ff, double *energy,
+                               double *virial);
+/* Canonical neighbour pairs (i < j) held by the packed list whose f32
+ * minimum-image distance is within r_cut + r_skin: the analogue of
+ * NeighborListState::pair_snapshot (src/forces/neighbor_list.rs:1366-1560).
+ * Writes min(count, cap) pairs (i, j) sorted; *count = total;
+ * *duplicates = pairs represented more than once (must be 0). */
+int hb_neighbor_pairs(hb_forcefield *ff, uint32_t *pairs, uint64_t cap,
+                      uint64_t *count, uint64_t *duplicates);
+/* Neighbour-list statistics: out[0] tiles, [1] entries, [2] entry capacity,
+ * [3] rebuild count, [4] status word, [5] pair slots per step. */
+int hb_neighbor_stats(hb_forcefield *ff, uint64_t out[6]);
+
+/* ---- constraints: replaces the Constraint hooks
+ * (src/integrator/constraint.rs:43-122) of SETTLE (src/integrator/settle.rs)
+ * and SHAKE/RATTLE (src/integrator/shake.rs).  Groups are CSR lists of atom
+ * ids; SETTLE groups are (O, H1, H2) with geometry (ra, rb, rc); SHAKE groups
+ * carry local constraint pairs with target distances. */
+typedef struct {
+  uint32_t n_groups;
+  const uint32_t *group_offsets;   /* [n_groups + 1] into group_atoms */
+  const uint32_t *group_atoms;
+  const uint32_t *group_kind;      /* HB_CONSTRAINT_* per group */
+  /* SETTLE geometry per group (ignored for SHAKE groups) */
+  const double *settle_ra;
+  const double *settle_rb;
+  const double *settle_rc;
+  /* SHAKE constraints: CSR per group into (local i, local j, distance) */
+  const uint32_t *con_offsets;     /* [n_groups + 1] */
+  const uint32_t *con_i;
+  const uint32_t *con_j;
+  const double *con_dist;
+  double shake_tol;                /* absolute tolerance on |r|^2 - d^2 */
+  uint32_t shake_max_iter;
+} hb_constraints_desc;
+
+int hb_constraints_create(hb_system *sys, const hb_constraints_desc *desc,
+                          hb_constraints **out);
+int hb_constraints_destroy(hb_constraints *c);
+/* Constraint::apply_before_drift: snapshot pre-drift positions. */
+int hb_constraints_before_drift(hb_constraints *c);
+/* Constraint::apply_after_drift: position reset + velocity correction. */
+int hb_constraints_after_drift(hb_constraints *c, double dt);
+/* Constraint::apply_after_kick: velocity projection (+ virial when dt > 0). */
+int hb_constraints_after_kick(hb_constraints *c, double dt);
+/* per-atom constraint virial of the last step ([n]) */
+int hb_constraints_get_virial(hb_constraints *c, double *virial);
+
+/* ---- integrator: replaces integrator::run_step (src/integrator/mod.rs:344)
+ * for velocity Verlet (src/integrator/velocity_verlet.rs) and Langevin
+ * (src/integrator/langevin_baoab.rs). */
+typedef struct {
+  int kind;                 /* HB_INTEGRATOR_* */
+  double dt;
+  double friction;          /* Langevin gamma (1 / time) */
+  double temperature;       /* k_B T in hartree */
+  uint64_t seed;
+  uint64_t step0;           /* first Philox draw counter */
+} hb_integrator_desc;
+
+int hb_integrator_create(hb_system *sys, const hb_integrator_desc *desc,
+                         hb_integrator **out);
+int hb_integrator_destroy(hb_integrator *it);
+/* Advance n_steps steps.  cons may be NULL.  scalar_every > 0 evaluates
+ * forces with scalars on every scalar_every-th step (0 = never). */
+int hb_integrator_step(hb_integrator *it, hb_forcefield *ff,
+                       hb_constraints *cons, uint32_t n_steps,
+                       uint32_t scalar_every);
+/* Same as hb_integrator_step, launched as CUDA graphs of one step each
+ * (captured on first use; the neighbour rebuild runs as a device-side
+ * conditional node). */
+int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
+                             hb_constraints *cons, uint32_t n_steps);
+
+/* Kernel launches of one step: the step is captured into a throwaway CUDA
+ * graph (nothing runs) and its kernel nodes are counted (*kernels). */
+int hb_integrator_count_launches(hb_integrator *it, hb_forcefield *ff,
+                                 hb_constraints *cons, uint64_t *kernels);
+
+/* ---- FP64 deterministic scalar reductions (kernels/nose_hoover.cu:22-103,
+ * kernels/barostat.cu:11-78): kinetic energy and the mass-weighted
+ * velocity sum. out[0] = KE, out[1..3] = total momentum. */
+int hb_reduce_kinetic(hb_system *sys, double out[4]);
+
+/* ---- device timing of the last hb_integrator_step call, in ms:
+ * out[0] total, out[1] pair kernel (sum), out[2] SPME (sum), out[3]
+ * neighbour rebuilds (sum), out[4] integrator + constraints (sum);
+ * instrumentation is on when enable != 0. */
+int hb_timing_enable(hb_context *ctx, int enable);
+int hb_timing_get(hb_context *ctx, double out[8]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HEDDLE_B200_H */

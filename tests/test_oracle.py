@@ -1,0 +1,155 @@
+"""The FP64 oracle pinned against the reference's known answers (CPU only).
+
+The reference stores no golden numbers for this path; its tests check the
+SPME pipeline against an explicit Ewald sum (tests/spme_pipeline.rs:101-190),
+the spread against B-spline weights and charge conservation (:192-383), and
+rely on Philox-4x32-10 (kernels/philox.cuh).  Those cases live in
+tests/golden/reference_kat.json (regenerated by tests/golden/make_golden.py).
+"""
+
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle as O
+from heddle_b200 import systems as S
+
+GOLD = Path(__file__).resolve().parent / "golden"
+KAT = json.loads((GOLD / "reference_kat.json").read_text())
+
+
+class _Spec:
+    def __init__(self, pos, q, L, alpha, grid, order):
+        self.positions = np.asarray(pos, dtype=float)
+        self.charges = np.asarray(q, dtype=float)
+        self.types = np.zeros(len(q), dtype=np.int32)
+        self.box = [L, L, L, 0.0, 0.0, 0.0]
+        self.lj_sigma = None
+        self.alpha = alpha
+        self.r_cut_coul = 0.3 * L
+        self.grid = tuple(grid)
+        self.order = order
+        self.excl_offsets = None
+
+
+@pytest.mark.parametrize("case", KAT["spme_vs_ewald"], ids=lambda c: c["name"])
+def test_spme_matches_explicit_ewald(case):
+    # tests/spme_pipeline.rs:101-190 and :880-924 (orders 4-8), bound 5e-3
+    L = case["box"]
+    ref = case["ewald_energy_mmax8"]
+    e_c = O.ewald_recip_energy(case["positions"], case["charges"], [L, L, L, 0, 0, 0], case["alpha"], 8)
+    assert abs(e_c - ref) / abs(ref) < 1e-12
+    for order in case["orders"]:
+        sp = _Spec(case["positions"], case["charges"], L, case["alpha"], case["grid"], order)
+        _, _, _, T = O.forces(sp)
+        assert abs(T["recip"] - ref) / abs(ref) < case["rel_bound"], order
+
+
+def test_spread_conserves_charge_and_single_particle_is_bspline():
+    # tests/spme_pipeline.rs:192-232 and :320-383
+    rng = np.random.default_rng(1)
+    L = 1.0
+    pos = rng.uniform(-0.5, 0.5, size=(5, 3))
+    q = np.array([1.0, -0.5, 0.25, 0.75, -1.5])
+    rho = O.spme_spread(pos, q, [L, L, L, 0, 0, 0], (12, 12, 12), 4)
+    assert abs(rho.sum() - q.sum()) < 1e-12
+    one = O.spme_spread(np.array([[0.013, -0.21, 0.37]]), np.array([1.0]), [L, L, L, 0, 0, 0], (16, 16, 16), 4)
+    nz = one[one != 0]
+    assert nz.size == 64
+    u = (np.array([0.013, -0.21, 0.37]) + 0.5) * 16
+    t = u - np.floor(u)
+    w = [O.bspline_weights(4, x)[0] for x in t]
+    expect = np.einsum("i,j,k->ijk", w[0], w[1], w[2])
+    assert np.allclose(np.sort(nz), np.sort(expect.reshape(-1)), rtol=1e-13, atol=0)
+
+
+@pytest.mark.parametrize("order", [4, 5, 6, 7, 8])
+def test_bspline_partition_of_unity(order):
+    for t in (0.0, 0.2, 0.5, 0.99):
+        w, dw = O.bspline_weights(order, t)
+        assert abs(w.sum() - 1.0) < 1e-14
+        assert abs(dw.sum()) < 1e-13
+        assert (w >= 0).all()
+
+
+def test_b_factors_finite_and_even_orders_positive():
+    # src/forces/spme.rs:1011-1033 (finite b-factors)
+    for order in (4, 5, 6, 7, 8):
+        for n in (16, 25, 64):
+            b = O.b_factors(n, order)
+            assert np.isfinite(b).all() and (b > 0).all()
+
+
+@pytest.mark.parametrize("vec", KAT["philox4x32_10"], ids=["zeros", "ones", "pi"])
+def test_philox_known_answers(vec):
+    key = [int(x, 16) for x in vec["key"]]
+    out = O.philox(key[0], key[1], [int(x, 16) for x in vec["ctr"]])
+    assert [int(x, 16) for x in vec["out"]] == out.tolist()
+
+
+def test_philox_gaussian_moments():
+    g = np.array([O.philox_gaussian(7, s, p, a) for s in range(20) for p in range(50) for a in range(3)])
+    assert abs(g.mean()) < 0.06 and abs(g.std() - 1.0) < 0.05
+
+
+def test_water_forces_match_golden_and_finite_differences():
+    gold = np.load(GOLD / "water_216.npz")
+    spec = S.spc_water(216, r_cut_A=7.0, skin_A=1.0, seed=3, velocity_seed=4)
+    assert np.array_equal(spec.positions, gold["positions"])
+    F, E, W, T = O.forces(spec)
+    assert np.allclose(F, gold["forces"], rtol=0, atol=1e-12)
+    assert np.allclose(E, gold["energies"], rtol=0, atol=1e-12)
+    # force = -dE/dx (central differences) for a few coordinates
+    rng = np.random.default_rng(0)
+    for _ in range(3):
+        i, d, h = int(rng.integers(spec.n)), int(rng.integers(3)), 1e-5
+        p1, p2 = spec.positions.copy(), spec.positions.copy()
+        p1[i, d] += h
+        p2[i, d] -= h
+        fd = -(O.forces(spec, p1)[1].sum() - O.forces(spec, p2)[1].sum()) / (2 * h)
+        assert abs(fd - F[i, d]) < 1e-6 * max(1.0, abs(F[i, d])) + 1e-7
+
+
+def test_neighbor_rule_matches_bruteforce():
+    spec = S.spc_water(64, r_cut_A=5.0, skin_A=0.5)
+    x = spec.positions.astype(np.float32)
+    box = spec.box.astype(np.float32)
+    rs = np.float32(spec.r_cut_coul + spec.r_skin)
+    pairs = O.neighbor_pairs_f32(x, box, rs)
+    # independent float32 evaluation of the same rule
+    d = x[:, None, :] - x[None, :, :]
+    L = box[0]
+    s = (d / L).astype(np.float32)
+    k = np.floor((s + np.float32(0.5)).astype(np.float32)).astype(np.float32)
+    d = (d - (k * L).astype(np.float32)).astype(np.float32)
+    r2 = ((d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1]).astype(np.float32) + d[..., 2] * d[..., 2]).astype(np.float32)
+    i, j = np.nonzero(np.triu(r2 <= rs * rs, 1))
+    assert np.array_equal(pairs, np.stack([i, j], axis=1).astype(np.uint32))
+
+
+def test_settle_projection_restores_geometry():
+    spec = S.spc_water(27, r_cut_A=3.0, skin_A=0.5)
+    rng = np.random.default_rng(2)
+    ref = spec.positions.copy()
+    pos = ref + rng.normal(scale=0.02, size=ref.shape)
+    vel = np.zeros_like(pos)
+    p, v, vir, used = O.constrain_positions(spec, ref, pos, vel, spec.dt)
+    assert used >= 0
+    for m in range(27):
+        o, h1, h2 = p[3 * m], p[3 * m + 1], p[3 * m + 2]
+        assert abs(np.linalg.norm(o - h1) - spec.meta["r_oh"]) < 1e-10
+        assert abs(np.linalg.norm(o - h2) - spec.meta["r_oh"]) < 1e-10
+        assert abs(np.linalg.norm(h1 - h2) - spec.meta["d_hh"]) < 1e-10
+    # the projection preserves each molecule's centre of mass
+    m3 = spec.masses.reshape(-1, 3)
+    c0 = (m3[..., None] * pos.reshape(-1, 3, 3)).sum(1) / m3.sum(1)[:, None]
+    c1 = (m3[..., None] * p.reshape(-1, 3, 3)).sum(1) / m3.sum(1)[:, None]
+    assert np.abs(c0 - c1).max() < 1e-12
+    vv, _ = O.constrain_velocities(spec, p, rng.normal(size=pos.shape), spec.dt)
+    for m in range(27):
+        x = p[3 * m: 3 * m + 3]
+        u = vv[3 * m: 3 * m + 3]
+        for a, b in ((0, 1), (0, 2), (1, 2)):
+            assert abs(np.dot(x[a] - x[b], u[a] - u[b])) < 1e-10
