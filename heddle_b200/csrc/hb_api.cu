@@ -605,11 +605,8 @@ extern "C" int hb_neighbor_stats(hb_forcefield *ff, uint64_t out[6]) {
   uint32_t cnt[4] = {0, 0, 0, 0}, st = 0;
   HB_CUDA(cudaMemcpyAsync(cnt, ff->d_counters, sizeof(uint32_t) * 4, cudaMemcpyDeviceToHost, s));
   HB_CUDA(cudaMemcpyAsync(&st, ff->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  uint32_t total = 0;
-  if (ff->n_tiles)
-    HB_CUDA(cudaMemcpyAsync(&total, ff->d_entry_off + ff->n_tiles, sizeof(uint32_t),
-                            cudaMemcpyDeviceToHost, s));
   HB_CUDA(cudaStreamSynchronize(s));
+  const uint32_t total = cnt[1];
   out[0] = ff->n_tiles;
   out[1] = total;
   out[2] = ff->entry_cap;

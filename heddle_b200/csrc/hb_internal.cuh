@@ -194,14 +194,15 @@ struct hb_forcefield {
   int *d_tile_type = nullptr;
   float4 *d_tile_center = nullptr;   // per tile: centre xyz, spc flag in w
   float4 *d_tile_half = nullptr;     // per tile: half extents
-  uint32_t *d_tile_nent = nullptr;   // entries per tile (count pass)
-  uint32_t *d_entry_off = nullptr;   // [n_tiles + 1]
-  uint32_t *d_entry_j = nullptr;     // [cap * 32] sorted j slots
-  uint32_t *d_entry_excl = nullptr;  // [cap * 32] exclusion masks
-  uint64_t entry_cap = 0;
+  uint32_t *d_tile_nent = nullptr;   // entries held by each tile
+  uint32_t slab = 0;                 // entry capacity per tile
+  uint32_t *d_entry_j = nullptr;     // [n_tiles * slab * 32] sorted j slots
+  uint32_t *d_entry_excl = nullptr;  // [n_tiles * slab * 32] exclusion masks
+  uint64_t entry_cap = 0;            // n_tiles * slab
   float4 *d_ref_pos = nullptr;       // positions at the last rebuild
   uint32_t *d_status = nullptr;      // status word
-  uint32_t *d_counters = nullptr;    // [0] rebuilds, [1] entries of last build
+  uint32_t *d_counters = nullptr;    // [0] rebuilds, [1] entries of the last
+                                     // build, [2] running count of a build
   uint32_t *h_status = nullptr;      // pinned mirror
   uint64_t rebuilds_host = 0;
   bool built = false;

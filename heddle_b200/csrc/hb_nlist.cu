@@ -15,8 +15,11 @@
 //     scans exclusion lists for ordinary pairs;
 //   * the self tile is entry 0 of each i-tile and is evaluated with a half
 //     rotation (each unordered pair once);
-//   * entries are laid out per i-tile by a count pass, a scan and a fill
-//     pass, so the layout is identical run to run;
+//   * entries live in a fixed-size slab per i-tile (sized from a counting
+//     pass at the first build), so a rebuild is one pass and the layout is
+//     identical run to run;
+//   * a j-atom is refined against the 32 i-atoms only when it lies within
+//     r_search of the i-tile's box (one test prunes most far atoms);
 //   * every rebuild kernel is gated on the device status word, so a rebuild
 //     is decided on the device each step with no host read.
 #include <algorithm>
@@ -234,7 +237,10 @@ __global__ void k_tile_bbox(const uint32_t *gate, const float4 *__restrict__ til
     float m = 0.5f * r_skin + rc_max;
     bool spc = b.ortho && (h[0] + m <= 0.5f * b.lx) && (h[1] + m <= 0.5f * b.ly) &&
                (h[2] + m <= 0.5f * b.lz);
-    center[warp] = make_float4(c[0], c[1], c[2], spc ? 1.0f : 0.0f);
+    // bit 0: single periodic copy; bit 1: per-axis minimum-image box tests
+    // are exact (orthorhombic cell)
+    const int flags = (spc ? 1 : 0) | (b.ortho ? 2 : 0);
+    center[warp] = make_float4(c[0], c[1], c[2], (float)flags);
     half[warp] = make_float4(h[0], h[1], h[2], 0.0f);
   }
 }
@@ -258,16 +264,19 @@ __device__ __forceinline__ uint32_t excl_mask(uint32_t sj, uint32_t I,
 
 #define NL_WARPS 4
 
-// Packed-entry construction.  WRITE = false counts entries per i-tile;
-// WRITE = true writes them at entry_off[I] (after an exclusive scan).
+// Packed-entry construction, one warp per i-tile.  WRITE = false counts
+// the tile's entries (sizing pass of the first build); WRITE = true writes
+// them into the tile's slab and flags slabs that filled past 3/4 or
+// overflowed.
 template <bool WRITE>
 __global__ void __launch_bounds__(NL_WARPS * 32)
     k_nl_build(const uint32_t *gate, const float4 *__restrict__ tile_posq,
                const float4 *__restrict__ center, const float4 *__restrict__ half,
                const DBox *__restrict__ box, float rs2, float rb2, float band_lo,
                float band_hi, uint32_t n, uint32_t n_tiles, uint32_t *__restrict__ tile_nent,
-               const uint32_t *__restrict__ entry_off, uint32_t *__restrict__ entry_j,
-               uint32_t *__restrict__ entry_excl, uint64_t cap,
+               uint32_t slab, uint32_t *__restrict__ entry_j,
+               uint32_t *__restrict__ entry_excl, uint32_t *__restrict__ status,
+               uint32_t *__restrict__ counters,
                const uint32_t *__restrict__ sorted_ids, const uint32_t *__restrict__ inv_perm,
                const uint32_t *__restrict__ eoff, const uint32_t *__restrict__ epart) {
   if (gate_off(gate)) return;
@@ -285,14 +294,15 @@ __global__ void __launch_bounds__(NL_WARPS * 32)
   const uint32_t ivalid = __ballot_sync(0xFFFFFFFFu, ki < n);
   __syncwarp();
   const float4 ci = center[I], hi = half[I];
-  uint64_t base = WRITE ? (uint64_t)entry_off[I] : 0u;
+  const bool ortho_tests = ((int)ci.w & 2) != 0;
+  const uint64_t base = (uint64_t)I * slab;
   uint32_t nent = 0;
 
   // entry 0: the self tile (all pairs inside the tile, half rotation)
   if (__popc(ivalid) >= 2) {
     if (WRITE) {
       uint64_t e = base;
-      if (e < cap) {
+      if (slab > 0u) {
         uint32_t sj = ki < n ? ki : HB_SENTINEL;
         entry_j[e * 32u + lane] = sj;
         entry_excl[e * 32u + lane] = excl_mask(sj, I, sorted_ids, inv_perm, eoff, epart);
@@ -305,7 +315,9 @@ __global__ void __launch_bounds__(NL_WARPS * 32)
   for (uint32_t j0 = I + 1; j0 < n_tiles; j0 += 32u) {
     uint32_t J = j0 + lane;
     bool pass = false;
-    if (J < n_tiles) {
+    if (J < n_tiles && !ortho_tests) {
+      pass = true;
+    } else if (J < n_tiles) {
       float4 cj = center[J], hj = half[J];
       float dx = ci.x - cj.x, dy = ci.y - cj.y, dz = ci.z - cj.z;
       hb_min_image(dx, dy, dz, b);
@@ -322,8 +334,22 @@ __global__ void __launch_bounds__(NL_WARPS * 32)
       uint32_t kj = Jt * 32u + lane;
       bool jvalid = kj < n;
       bool hit = false;
+      bool near = jvalid;
+      float4 pj;
       if (jvalid) {
-        float4 pj = tile_posq[kj];
+        pj = tile_posq[kj];
+        if (ortho_tests) {
+          // distance from the j-atom to the i-tile box bounds its distance
+          // to every i-atom from below
+          float dx = pj.x - ci.x, dy = pj.y - ci.y, dz = pj.z - ci.z;
+          hb_min_image(dx, dy, dz, b);
+          float ex = fmaxf(fabsf(dx) - hi.x, 0.0f);
+          float ey = fmaxf(fabsf(dy) - hi.y, 0.0f);
+          float ez = fmaxf(fabsf(dz) - hi.z, 0.0f);
+          near = ex * ex + ey * ey + ez * ez <= rb2;
+        }
+      }
+      if (near) {
         uint32_t mm = ivalid;
         while (mm) {
           uint32_t m = __ffs(mm) - 1u;
@@ -354,7 +380,7 @@ __global__ void __launch_bounds__(NL_WARPS * 32)
       if (blen >= 32u) {
         if (WRITE) {
           uint64_t e = base + nent;
-          if (e < cap) {
+          if (nent < slab) {
             uint32_t sj = jbuf[w][lane];
             entry_j[e * 32u + lane] = sj;
             entry_excl[e * 32u + lane] = excl_mask(sj, I, sorted_ids, inv_perm, eoff, epart);
@@ -373,7 +399,7 @@ __global__ void __launch_bounds__(NL_WARPS * 32)
   if (blen > 0u) {
     if (WRITE) {
       uint64_t e = base + nent;
-      if (e < cap) {
+      if (nent < slab) {
         uint32_t sj = lane < blen ? jbuf[w][lane] : HB_SENTINEL;
         entry_j[e * 32u + lane] = sj;
         entry_excl[e * 32u + lane] = excl_mask(sj, I, sorted_ids, inv_perm, eoff, epart);
@@ -381,22 +407,24 @@ __global__ void __launch_bounds__(NL_WARPS * 32)
     }
     nent++;
   }
-  if (!WRITE && lane == 0) tile_nent[I] = nent;
+  if (lane == 0) {
+    tile_nent[I] = nent;
+    if (WRITE) {
+      atomicAdd(&counters[2], nent);
+      if (nent > slab) atomicOr(status, HB_ST_ENTRY_OVERFLOW);
+      else if (4u * nent > 3u * slab) atomicOr(status, HB_ST_ENTRY_HIGHWATER);
+    }
+  }
 }
 
-// Last kernel of a rebuild: capacity bits, counters, and clearing of the
-// displacement bit (which gates every kernel of the rebuild).
-__global__ void k_nl_finish(const uint32_t *gate, uint32_t *status, uint32_t *counters,
-                            const uint32_t *entry_off, uint32_t n_tiles, uint64_t cap) {
+// Last kernel of a rebuild: counters, and clearing of the displacement bit
+// (which gates every kernel of the rebuild).
+__global__ void k_nl_finish(const uint32_t *gate, uint32_t *status, uint32_t *counters) {
   if (gate_off(gate)) return;
-  uint32_t total = entry_off[n_tiles];
-  uint32_t st = *status;
-  if ((uint64_t)total > cap) st |= HB_ST_ENTRY_OVERFLOW;
-  else if ((uint64_t)total * 4u > cap * 3u) st |= HB_ST_ENTRY_HIGHWATER;
-  st &= ~HB_ST_DISPLACED;
-  *status = st;
+  *status &= ~HB_ST_DISPLACED;
   counters[0] += 1u;
-  counters[1] = total;
+  counters[1] = counters[2];
+  counters[2] = 0u;
 }
 
 __global__ void k_disp_check(const float4 *__restrict__ posq, const float4 *__restrict__ ref,
@@ -459,7 +487,6 @@ int nl_setup(hb_forcefield *ff) {
   HB_CUDA(cudaMalloc(&ff->d_tile_half, sizeof(float4) * std::max(ff->n_tiles, 1u)));
   HB_CUDA(cudaMalloc(&ff->d_tile_nent, sizeof(uint32_t) * (ff->n_tiles + 1)));
   HB_CUDA(cudaMemset(ff->d_tile_nent, 0, sizeof(uint32_t) * (ff->n_tiles + 1)));
-  HB_CUDA(cudaMalloc(&ff->d_entry_off, sizeof(uint32_t) * (ff->n_tiles + 1)));
   HB_CUDA(cudaMalloc(&ff->d_ref_pos, sizeof(float4) * std::max(n, 1u)));
   HB_CUDA(cudaMalloc(&ff->d_status, sizeof(uint32_t)));
   HB_CUDA(cudaMemset(ff->d_status, 0, sizeof(uint32_t)));
@@ -483,7 +510,6 @@ int nl_free(hb_forcefield *ff) {
   cudaFree(ff->d_tile_center);
   cudaFree(ff->d_tile_half);
   cudaFree(ff->d_tile_nent);
-  cudaFree(ff->d_entry_off);
   cudaFree(ff->d_entry_j);
   cudaFree(ff->d_entry_excl);
   cudaFree(ff->d_ref_pos);
@@ -494,18 +520,20 @@ int nl_free(hb_forcefield *ff) {
   return HB_OK;
 }
 
-// Launch the rebuild sequence.  stop_after_count: run through the count
-// pass and the entry scan only (the first build sizes the buffers there).
-static int nl_launch(hb_forcefield *ff, const uint32_t *gate, cudaStream_t s, int phase) {
+// The rebuild sequence: voxel sort, sorted-slot views and tile boxes
+// (sort), then either the counting pass of the first build (count_only)
+// or the single fill pass plus the finishing kernel.
+static int nl_launch(hb_forcefield *ff, const uint32_t *gate, cudaStream_t s, bool sort,
+                     bool count_only) {
   hb_system *sys = ff->sys;
   const uint32_t n = sys->n;
   const uint32_t n_vox = 1u << (3 * ff->nv_log2);
   const float rs = ff->r_search;
   const float rs2 = rs * rs;
-  // AABB prune radius with a margin so rounding never drops a pair
+  // box-prune radius with a margin so rounding never drops a pair
   const float rb = rs * (1.0f + 1.0e-5f) + 1.0e-4f;
   const float band_lo = rs2 * (1.0f - 1.0e-5f), band_hi = rs2 * (1.0f + 1.0e-5f);
-  if (phase == 0) {
+  if (sort) {
     k_vox_hist<<<hb_div_up(n, 256), 256, 0, s>>>(gate, sys->d_posq, sys->d_box, ff->nv_log2,
                                                   ff->d_vox_key, ff->d_vox_count, n);
     HB_TRY(scan_exclusive(gate, ff->d_vox_count, ff->d_vox_off, ff->d_scan_tmp, n_vox + 1, s));
@@ -518,22 +546,19 @@ static int nl_launch(hb_forcefield *ff, const uint32_t *gate, cudaStream_t s, in
     k_tile_bbox<<<hb_div_up((uint64_t)ff->n_tiles * 32u, 128), 128, 0, s>>>(
         gate, ff->d_tile_posq, sys->d_box, ff->rc_max, ff->r_skin, ff->d_tile_center,
         ff->d_tile_half, n, ff->n_tiles);
+  }
+  if (count_only) {
     k_nl_build<false><<<hb_div_up(ff->n_tiles, NL_WARPS), NL_WARPS * 32, 0, s>>>(
         gate, ff->d_tile_posq, ff->d_tile_center, ff->d_tile_half, sys->d_box, rs2, rb * rb,
-        band_lo, band_hi, n, ff->n_tiles, ff->d_tile_nent, ff->d_entry_off, ff->d_entry_j,
-        ff->d_entry_excl, ff->entry_cap, ff->d_sorted_ids, ff->d_inv_perm, ff->d_excl_off,
-        ff->d_excl_partner);
-    HB_TRY(scan_exclusive(gate, ff->d_tile_nent, ff->d_entry_off, ff->d_scan_tmp,
-                          ff->n_tiles + 1, s));
-  }
-  if (phase == 1) {
+        band_lo, band_hi, n, ff->n_tiles, ff->d_tile_nent, 0u, nullptr, nullptr, ff->d_status,
+        ff->d_counters, ff->d_sorted_ids, ff->d_inv_perm, ff->d_excl_off, ff->d_excl_partner);
+  } else {
     k_nl_build<true><<<hb_div_up(ff->n_tiles, NL_WARPS), NL_WARPS * 32, 0, s>>>(
         gate, ff->d_tile_posq, ff->d_tile_center, ff->d_tile_half, sys->d_box, rs2, rb * rb,
-        band_lo, band_hi, n, ff->n_tiles, ff->d_tile_nent, ff->d_entry_off, ff->d_entry_j,
-        ff->d_entry_excl, ff->entry_cap, ff->d_sorted_ids, ff->d_inv_perm, ff->d_excl_off,
-        ff->d_excl_partner);
-    k_nl_finish<<<1, 1, 0, s>>>(gate, ff->d_status, ff->d_counters, ff->d_entry_off,
-                                ff->n_tiles, ff->entry_cap);
+        band_lo, band_hi, n, ff->n_tiles, ff->d_tile_nent, ff->slab, ff->d_entry_j,
+        ff->d_entry_excl, ff->d_status, ff->d_counters, ff->d_sorted_ids, ff->d_inv_perm,
+        ff->d_excl_off, ff->d_excl_partner);
+    k_nl_finish<<<1, 1, 0, s>>>(gate, ff->d_status, ff->d_counters);
   }
   HB_CUDA(cudaGetLastError());
   return HB_OK;
@@ -548,14 +573,12 @@ int nl_rebuild(hb_forcefield *ff, bool gated, cudaStream_t s) {
     HB_CUDA(cudaMemcpyAsync(ff->d_status, &one, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
     HB_CUDA(cudaStreamSynchronize(s));
   }
-  HB_TRY(nl_launch(ff, gate, s, 0));
-  HB_TRY(nl_launch(ff, gate, s, 1));
-  return HB_OK;
+  return nl_launch(ff, gate, s, true, false);
 }
 
-// First build: count, size the entry buffers from the count (x1.5 + slack),
-// then fill.  Host-synchronous; runs at force-field creation and when the
-// host grows the buffers after a high-water signal.
+// First build: counting pass, slab size = 1.5 x the largest tile count + 4,
+// then the fill pass.  Host-synchronous; runs at force-field creation and
+// when the host grows the slabs after a high-water signal.
 int nl_first_build(hb_forcefield *ff) {
   hb_system *sys = ff->sys;
   if (sys->n == 0) {
@@ -565,26 +588,30 @@ int nl_first_build(hb_forcefield *ff) {
   cudaStream_t s = sys->ctx->stream;
   uint32_t one = HB_ST_DISPLACED;
   HB_CUDA(cudaMemcpyAsync(ff->d_status, &one, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-  HB_TRY(nl_launch(ff, nullptr, s, 0));
-  uint32_t total = 0;
-  HB_CUDA(cudaMemcpyAsync(&total, ff->d_entry_off + ff->n_tiles, sizeof(uint32_t),
+  HB_TRY(nl_launch(ff, nullptr, s, true, true));
+  std::vector<uint32_t> nent(ff->n_tiles);
+  HB_CUDA(cudaMemcpyAsync(nent.data(), ff->d_tile_nent, sizeof(uint32_t) * ff->n_tiles,
                           cudaMemcpyDeviceToHost, s));
   HB_CUDA(cudaStreamSynchronize(s));
-  uint64_t want = (uint64_t)total + total / 2 + 64;
-  if (want > ff->entry_cap) {
+  uint32_t mx = 0;
+  for (uint32_t v : nent) mx = std::max(mx, v);
+  const uint32_t want = mx + mx / 2 + 4;
+  if (want > ff->slab) {
     cudaFree(ff->d_entry_j);
     cudaFree(ff->d_entry_excl);
     ff->d_entry_j = nullptr;
     ff->d_entry_excl = nullptr;
-    HB_CUDA(cudaMalloc(&ff->d_entry_j, sizeof(uint32_t) * 32 * want));
-    HB_CUDA(cudaMalloc(&ff->d_entry_excl, sizeof(uint32_t) * 32 * want));
-    ff->entry_cap = want;
+    const size_t cap = (size_t)ff->n_tiles * want;
+    HB_CUDA(cudaMalloc(&ff->d_entry_j, sizeof(uint32_t) * 32 * cap));
+    HB_CUDA(cudaMalloc(&ff->d_entry_excl, sizeof(uint32_t) * 32 * cap));
+    ff->slab = want;
+    ff->entry_cap = cap;
   }
-  HB_TRY(nl_launch(ff, nullptr, s, 1));
+  HB_TRY(nl_launch(ff, nullptr, s, false, false));
   uint32_t st = 0;
   HB_CUDA(cudaMemcpyAsync(&st, ff->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   HB_CUDA(cudaStreamSynchronize(s));
-  // clear the capacity bits of the sizing build
+  if (st & HB_ST_ENTRY_OVERFLOW) return hb_fail(HB_ERR_NL_OVERFLOW, "slab sizing failed");
   st &= ~(HB_ST_ENTRY_HIGHWATER | HB_ST_ENTRY_OVERFLOW);
   HB_CUDA(cudaMemcpyAsync(ff->d_status, &st, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
   HB_CUDA(cudaStreamSynchronize(s));
@@ -651,35 +678,35 @@ int nl_pairs(hb_forcefield *ff, std::vector<uint32_t> &pairs, uint64_t &dups) {
   pairs.clear();
   dups = 0;
   if (n == 0) return HB_OK;
-  std::vector<uint32_t> off(ff->n_tiles + 1), ids(ff->n_pad);
+  std::vector<uint32_t> nent(ff->n_tiles), ids(ff->n_pad);
   std::vector<float4> pos(ff->n_pad);
-  HB_CUDA(cudaMemcpy(off.data(), ff->d_entry_off, sizeof(uint32_t) * (ff->n_tiles + 1),
+  HB_CUDA(cudaMemcpy(nent.data(), ff->d_tile_nent, sizeof(uint32_t) * ff->n_tiles,
                      cudaMemcpyDeviceToHost));
   HB_CUDA(cudaMemcpy(ids.data(), ff->d_sorted_ids, sizeof(uint32_t) * ff->n_pad,
                      cudaMemcpyDeviceToHost));
   HB_CUDA(cudaMemcpy(pos.data(), ff->d_tile_posq, sizeof(float4) * ff->n_pad,
                      cudaMemcpyDeviceToHost));
-  uint64_t total = off[ff->n_tiles];
-  if (total > ff->entry_cap) return hb_fail(HB_ERR_NL_OVERFLOW, "packed entries overflowed");
-  std::vector<uint32_t> ej(total * 32);
-  if (total)
-    HB_CUDA(cudaMemcpy(ej.data(), ff->d_entry_j, sizeof(uint32_t) * 32 * total,
+  std::vector<uint32_t> ej((size_t)ff->entry_cap * 32);
+  if (ff->entry_cap)
+    HB_CUDA(cudaMemcpy(ej.data(), ff->d_entry_j, sizeof(uint32_t) * 32 * ff->entry_cap,
                        cudaMemcpyDeviceToHost));
   float b[6];
   for (int d = 0; d < 6; ++d) b[d] = (float)sys->box[d];
   const float rs2 = ff->r_search * ff->r_search;
   std::vector<uint64_t> keys;
   for (uint32_t I = 0; I < ff->n_tiles; ++I) {
-    for (uint32_t e = off[I]; e < off[I + 1]; ++e) {
-      bool self = (e == off[I]) && ej[(uint64_t)e * 32] == I * 32u;
+    if (nent[I] > ff->slab) return hb_fail(HB_ERR_NL_OVERFLOW, "packed entries overflowed");
+    const bool has_self = n - I * 32u >= 2u;
+    for (uint32_t q = 0; q < nent[I]; ++q) {
+      const uint64_t e = (uint64_t)I * ff->slab + q;
+      const bool self = has_self && q == 0;
       for (uint32_t l = 0; l < 32; ++l) {
         uint32_t si = I * 32u + l;
         if (si >= n) continue;
-        uint32_t tmax = self ? 16u : 31u;
-        for (uint32_t t = self ? 1u : 0u; t <= tmax; ++t) {
+        const uint32_t t0 = self ? 1u : 0u, t1 = self ? 16u : 31u;
+        for (uint32_t t = t0; t <= t1; ++t) {
           if (self && t == 16u && l >= 16u) continue;
-          uint32_t jl = self ? ((l + t) & 31u) : ((l + t) & 31u);
-          uint32_t sj = ej[(uint64_t)e * 32 + jl];
+          uint32_t sj = ej[e * 32 + ((l + t) & 31u)];
           if (sj == HB_SENTINEL || sj >= n) continue;
           float4 a = pos[si], c = pos[sj];
           float r2 = host_exact_r2(a.x - c.x, a.y - c.y, a.z - c.z, b);

@@ -34,7 +34,7 @@ struct PairParams {
   float alpha;
   float c2a;  // 2 alpha / sqrt(pi)
   uint32_t n, n_tiles;
-  uint64_t cap;
+  uint32_t slab;
 };
 
 __device__ __forceinline__ void shift_to(float &x, float &y, float &z, const float4 &c,
@@ -56,7 +56,7 @@ __device__ __forceinline__ void red_add(unsigned long long *p, long long v) {
 template <bool EV, bool SCALED, bool SWITCH>
 __global__ void __launch_bounds__(PAIR_WARPS * 32)
     k_pair(const float4 *__restrict__ tile_posq, const int *__restrict__ tile_type,
-           const float4 *__restrict__ center, const uint32_t *__restrict__ entry_off,
+           const float4 *__restrict__ center, const uint32_t *__restrict__ tile_nent,
            const uint32_t *__restrict__ entry_j, const uint32_t *__restrict__ entry_excl,
            const DBox *__restrict__ box, const float4 *__restrict__ lj_table, PairParams P,
            unsigned long long *__restrict__ fp, unsigned long long *__restrict__ e_lj_total,
@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32)
   if (I >= P.n_tiles) return;
   const DBox b = *box;
   const float4 c = center[I];
-  const bool spc = c.w != 0.0f;
+  const bool spc = ((int)c.w & 1) != 0;
   const uint32_t si = I * 32u + lane;
   const bool ivalid = si < P.n;
   float4 pi = tile_posq[si];
@@ -88,9 +88,8 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32)
   long long ax = 0, ay = 0, az = 0, ae = 0, aw = 0;
   float elj_warp = 0.0f;
 
-  uint32_t e0 = entry_off[I], e1 = entry_off[I + 1];
-  if ((uint64_t)e1 > P.cap) e1 = (uint32_t)P.cap;
-  if (e0 > e1) e0 = e1;
+  const uint32_t e0 = I * P.slab;
+  const uint32_t e1 = e0 + min(tile_nent[I], P.slab);
   const uint32_t nvalid_i = P.n - I * 32u;
   const bool has_self = nvalid_i >= 2u;
 
@@ -184,7 +183,7 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32)
             fac += s_lj * f;
             if (EV) {
               en += s_lj * u;
-              elj += 0.5f * s_lj * u;
+              elj += s_lj * u;
             }
           }
         }
@@ -283,7 +282,7 @@ template <bool EV, bool SCALED, bool SWITCH>
 int launch_t(hb_forcefield *ff, cudaStream_t s, const PairParams &P) {
   size_t smem = sizeof(float4) * (size_t)P.n_types * P.n_types;
   k_pair<EV, SCALED, SWITCH><<<hb_div_up(P.n_tiles, PAIR_WARPS), PAIR_WARPS * 32, smem, s>>>(
-      ff->d_tile_posq, ff->d_tile_type, ff->d_tile_center, ff->d_entry_off, ff->d_entry_j,
+      ff->d_tile_posq, ff->d_tile_type, ff->d_tile_center, ff->d_tile_nent, ff->d_entry_j,
       ff->d_entry_excl, ff->sys->d_box, ff->d_lj, P, ff->d_fp,
       ff->d_acc,
       ff->d_sorted_ids, ff->d_excl_off, ff->d_excl_partner, ff->d_excl_scale);
@@ -306,7 +305,7 @@ int pair_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
   P.c2a = 2.0f * ff->alpha / 1.7724538509055160273f;
   P.n = ff->sys->n;
   P.n_tiles = ff->n_tiles;
-  P.cap = ff->entry_cap;
+  P.slab = ff->slab;
   const bool sc = ff->excl_scaled != 0, sw = ff->any_switch != 0;
   if (ev) {
     if (sc) return sw ? launch_t<true, true, true>(ff, s, P) : launch_t<true, true, false>(ff, s, P);

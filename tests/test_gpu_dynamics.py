@@ -33,10 +33,18 @@ def close(*objs):
 
 
 def geometry_error(pos, spec):
+    # atoms are wrapped one by one, so bond vectors take the minimum image
     p = pos.reshape(-1, 3, 3)
-    d1 = np.linalg.norm(p[:, 0] - p[:, 1], axis=1) - spec.meta["r_oh"]
-    d2 = np.linalg.norm(p[:, 0] - p[:, 2], axis=1) - spec.meta["r_oh"]
-    d3 = np.linalg.norm(p[:, 1] - p[:, 2], axis=1) - spec.meta["d_hh"]
+    L = spec.box[:3]
+
+    def dist(a, b):
+        d = p[:, a] - p[:, b]
+        d -= L * np.round(d / L)
+        return np.linalg.norm(d, axis=1)
+
+    d1 = dist(0, 1) - spec.meta["r_oh"]
+    d2 = dist(0, 2) - spec.meta["r_oh"]
+    d3 = dist(1, 2) - spec.meta["d_hh"]
     return float(np.abs(np.concatenate([d1, d2, d3])).max())
 
 
