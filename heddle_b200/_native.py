@@ -138,6 +138,8 @@ SIGNATURES = {
     "hb_integrator_step_graph": (C.c_int, [VP, VP, VP, C.c_uint32]),
     "hb_integrator_count_launches": (C.c_int, [VP, VP, VP, PU64]),
     "hb_reduce_kinetic": (C.c_int, [VP, PD]),
+    "hb_spme_recip_noalloc": (C.c_int, [C.c_void_p, C.c_uint32, PD, PU32, C.c_uint32, C.c_double,
+                                        C.c_void_p, PD, C.c_void_p]),
     "hb_timing_enable": (C.c_int, [VP, C.c_int]),
     "hb_timing_get": (C.c_int, [VP, PD]),
 }

@@ -621,3 +621,192 @@ int spme_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
   HB_CUDA(cudaGetLastError());
   return HB_OK;
 }
+
+// ---------------------------------------------------------------------
+// Allocation-free SPME reciprocal evaluation (hb_spme_recip_noalloc).
+//
+// For callers that must not allocate device memory -- code running while a
+// stream is being captured into a CUDA graph (cudaMalloc is not allowed
+// then), or a host process whose device memory is owned by another
+// allocator (a framework's caching pool, a fixed-budget serving process)
+// -- this entry point runs the same spread / FFT / convolution / gather
+// kernels as the force field on grids of at most HB_NOALLOC_MAX_POINTS
+// points, with all scratch in one file-scope device array.  Every GPU that
+// loads the library holds that array until the process exits.
+// ---------------------------------------------------------------------
+#include <mutex>
+
+#define HB_NOALLOC_MAX_DIM 64           // grid points per axis
+#define HB_NOALLOC_MAX_POINTS 32768     // grid points in total (e.g. 32^3)
+#define HB_NOALLOC_MAX_PART 2048        // energy / virial partial slots
+
+namespace {
+
+// byte offsets of the scratch regions (each 256-byte aligned)
+constexpr size_t kNaRho = 0;                                                  // int64 grid
+constexpr size_t kNaGrid = kNaRho + 8u * HB_NOALLOC_MAX_POINTS;               // complex grid
+constexpr size_t kNaV = kNaGrid + 8u * HB_NOALLOC_MAX_POINTS;                 // real potential
+constexpr size_t kNaBfac = kNaV + 4u * HB_NOALLOC_MAX_POINTS;                 // b-factors
+constexpr size_t kNaTw = kNaBfac + 4u * 3u * HB_NOALLOC_MAX_DIM + 256u;       // twiddles
+constexpr size_t kNaPart = kNaTw + 8u * 3u * HB_NOALLOC_MAX_DIM + 256u;       // partials
+constexpr size_t kNaSums = kNaPart + 16u * HB_NOALLOC_MAX_PART;               // E, W
+constexpr size_t kNaBox = kNaSums + 256u;                                     // DBox
+constexpr size_t kNaBytes = kNaBox + 256u;
+
+// The scratch of hb_spme_recip_noalloc.  In host code this name is only a
+// host-side stand-in for the symbol; its device address comes from
+// cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+std::mutex g_noalloc_mutex;
+void *g_noalloc_ptr[64] = {nullptr};
+
+// host b-factors on the stack (same restatement as b_factors above)
+void b_factors_fixed(int n, int p, float *out) {
+  double mod[HB_NOALLOC_MAX_DIM];
+  for (int k = 0; k < n; ++k) {
+    double th = 2.0 * M_PI * k / n, re = 0.0, im = 0.0;
+    for (int j = 0; j < p - 1; ++j) {
+      double m = bspline_host(p, (double)(j + 1));
+      re += m * std::cos(th * j);
+      im += m * std::sin(th * j);
+    }
+    mod[k] = re * re + im * im;
+  }
+  for (int k = 0; k < n; ++k)
+    if (mod[k] < 1.0e-7) mod[k] = 0.5 * (mod[(k + n - 1) % n] + mod[(k + 1) % n]);
+  for (int k = 0; k < n; ++k) out[k] = mod[k] > 0.0 ? (float)(1.0 / mod[k]) : 0.0f;
+}
+
+}  // namespace
+
+extern "C" int hb_spme_recip_noalloc(const float *posq, uint32_t n, const double box[6],
+                                     const uint32_t grid[3], uint32_t order, double alpha,
+                                     float *out, double *energy, void *stream) {
+  if (!box || !grid || (n > 0 && (!posq || !out)))
+    return hb_fail(HB_ERR_INVALID_ARGUMENT, "null argument");
+  if (order < 4 || order > 8) return hb_fail(HB_ERR_INVALID_ARGUMENT, "spline order must be 4..8");
+  if (!(std::isfinite(alpha) && alpha > 0.0)) return hb_fail(HB_ERR_INVALID_ARGUMENT, "alpha must be > 0");
+  for (int d = 0; d < 6; ++d)
+    if (!std::isfinite(box[d])) return hb_fail(HB_ERR_NOT_FINITE, "box must be finite");
+  if (!(box[0] > 0.0 && box[1] > 0.0 && box[2] > 0.0))
+    return hb_fail(HB_ERR_INVALID_ARGUMENT, "box diagonal must be positive");
+  const int na = (int)grid[0], nb = (int)grid[1], nc = (int)grid[2];
+  FftPlan pa, pb, pc;
+  for (int d = 0; d < 3; ++d) {
+    const int g = (int)grid[d];
+    if (g < 2 * (int)order)
+      return hb_fail(HB_ERR_INVALID_GRID, "grid[" + std::to_string(d) + "] = " + std::to_string(g) +
+                                              " is less than 2 * spline_order");
+    if (g > HB_NOALLOC_MAX_DIM)
+      return hb_fail(HB_ERR_INVALID_GRID, "allocation-free SPME supports at most " +
+                                              std::to_string(HB_NOALLOC_MAX_DIM) + " points per axis");
+  }
+  if ((uint64_t)na * nb * nc > HB_NOALLOC_MAX_POINTS)
+    return hb_fail(HB_ERR_INVALID_GRID, "allocation-free SPME supports at most " +
+                                            std::to_string(HB_NOALLOC_MAX_POINTS) + " grid points");
+  if (!make_plan(na, pa) || !make_plan(nb, pb) || !make_plan(nc, pc))
+    return hb_fail(HB_ERR_INVALID_GRID, "SPME grid sizes must factor into 2, 3, 5, 7");
+  const int nch = nc / 2 + 1;
+  const int La = lines_per_cta(na), Lb = lines_per_cta(nb), Lc = lines_per_cta(nc);
+  const int n_part = nb * ((nch + La - 1) / La);
+  if (n_part > HB_NOALLOC_MAX_PART) return hb_fail(HB_ERR_INVALID_GRID, "grid too large");
+
+  // once per device: the device address of the scratch array
+  int dev = 0;
+  HB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return hb_fail(HB_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+  unsigned char *base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+      void *p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess)
+        return hb_fail(HB_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      g_noalloc_ptr[dev] = p;
+    }
+    base = (unsigned char *)g_noalloc_ptr[dev];
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned long long *rho = (unsigned long long *)(base + kNaRho);
+  float2 *cgrid = (float2 *)(base + kNaGrid);
+  float *v = (float *)(base + kNaV);
+  float *bfac = (float *)(base + kNaBfac);
+  float2 *tw = (float2 *)(base + kNaTw);
+  double *part = (double *)(base + kNaPart);
+  double *sums = (double *)(base + kNaSums);
+  DBox *dbox = (DBox *)(base + kNaBox);
+
+  // per-call constants (host stack -> scratch); the array keeps the last
+  // call's contents, so everything the kernels read is written here
+  float h_bfac[3 * HB_NOALLOC_MAX_DIM];
+  float2 h_tw[3 * HB_NOALLOC_MAX_DIM];
+  b_factors_fixed(na, (int)order, h_bfac);
+  b_factors_fixed(nb, (int)order, h_bfac + na);
+  b_factors_fixed(nc, (int)order, h_bfac + na + nb);
+  int off = 0;
+  for (int ax = 0; ax < 3; ++ax) {
+    const int g = (int)grid[ax];
+    for (int t = 0; t < g; ++t) {
+      double a = -2.0 * M_PI * (double)t / (double)g;
+      h_tw[off + t] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    off += g;
+  }
+  DBox h_box;
+  h_box.lx = (float)box[0];
+  h_box.ly = (float)box[1];
+  h_box.lz = (float)box[2];
+  h_box.xy = (float)box[3];
+  h_box.xz = (float)box[4];
+  h_box.yz = (float)box[5];
+  h_box.ilx = (float)(1.0 / box[0]);
+  h_box.ily = (float)(1.0 / box[1]);
+  h_box.ilz = (float)(1.0 / box[2]);
+  h_box.ortho = (box[3] == 0.0 && box[4] == 0.0 && box[5] == 0.0) ? 1 : 0;
+  HB_CUDA(cudaMemcpyAsync(bfac, h_bfac, sizeof(float) * (na + nb + nc), cudaMemcpyHostToDevice, s));
+  HB_CUDA(cudaMemcpyAsync(tw, h_tw, sizeof(float2) * (na + nb + nc), cudaMemcpyHostToDevice, s));
+  HB_CUDA(cudaMemcpyAsync(dbox, &h_box, sizeof(DBox), cudaMemcpyHostToDevice, s));
+  // the charge grid must start at zero
+  HB_CUDA(cudaMemsetAsync(rho, 0, sizeof(unsigned long long) * (size_t)na * nb * nc, s));
+
+  const float4 *pq = (const float4 *)posq;
+  float4 *o = (float4 *)out;
+  const float self_pref = (float)(alpha / std::sqrt(M_PI));
+  if (n > 0) {
+    const uint64_t th = (uint64_t)n * order;
+    switch (order) {
+      case 4: k_spread<4><<<hb_div_up(th, 256), 256, 0, s>>>(pq, dbox, na, nb, nc, rho, n); break;
+      case 5: k_spread<5><<<hb_div_up(th, 256), 256, 0, s>>>(pq, dbox, na, nb, nc, rho, n); break;
+      case 6: k_spread<6><<<hb_div_up(th, 256), 256, 0, s>>>(pq, dbox, na, nb, nc, rho, n); break;
+      case 7: k_spread<7><<<hb_div_up(th, 256), 256, 0, s>>>(pq, dbox, na, nb, nc, rho, n); break;
+      default: k_spread<8><<<hb_div_up(th, 256), 256, 0, s>>>(pq, dbox, na, nb, nc, rho, n); break;
+    }
+  }
+  const int nrows = na * nb;
+  k_fft_c_fwd<<<hb_div_up(nrows, Lc), 256, fft_smem(nc, Lc), s>>>(rho, cgrid, tw + na + nb, pc, nrows, nch, Lc);
+  k_fft_b<false><<<na * ((nch + Lb - 1) / Lb), 256, fft_smem(nb, Lb), s>>>(cgrid, tw + na, pb, nb, nch, Lb);
+  k_fft_a_conv<<<n_part, 256, fft_smem(na, La), s>>>(cgrid, tw, pa, na, nb, nc, nch, La, dbox, bfac,
+                                                     (float)alpha, part);
+  k_fft_b<true><<<na * ((nch + Lb - 1) / Lb), 256, fft_smem(nb, Lb), s>>>(cgrid, tw + na, pb, nb, nch, Lb);
+  k_fft_c_inv<<<hb_div_up(nrows, Lc), 256, fft_smem(nc, Lc), s>>>(cgrid, v, tw + na + nb, pc, nrows, nch, Lc);
+  if (n > 0) {
+    switch (order) {
+      case 4: k_gather<4><<<hb_div_up(n, 128), 128, 0, s>>>(pq, v, dbox, na, nb, nc, self_pref, o, n); break;
+      case 5: k_gather<5><<<hb_div_up(n, 128), 128, 0, s>>>(pq, v, dbox, na, nb, nc, self_pref, o, n); break;
+      case 6: k_gather<6><<<hb_div_up(n, 128), 128, 0, s>>>(pq, v, dbox, na, nb, nc, self_pref, o, n); break;
+      case 7: k_gather<7><<<hb_div_up(n, 128), 128, 0, s>>>(pq, v, dbox, na, nb, nc, self_pref, o, n); break;
+      default: k_gather<8><<<hb_div_up(n, 128), 128, 0, s>>>(pq, v, dbox, na, nb, nc, self_pref, o, n); break;
+    }
+  }
+  k_spme_sums<<<1, 256, 0, s>>>(part, n_part, sums);
+  HB_CUDA(cudaGetLastError());
+  if (energy) {
+    double h_sums[2];
+    HB_CUDA(cudaMemcpyAsync(h_sums, sums, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+    HB_CUDA(cudaStreamSynchronize(s));
+    *energy = h_sums[0];
+  }
+  return HB_OK;
+}

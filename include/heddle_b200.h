@@ -227,6 +227,30 @@ int hb_integrator_count_launches(hb_integrator *it, hb_forcefield *ff,
  * velocity sum. out[0] = KE, out[1..3] = total momentum. */
 int hb_reduce_kinetic(hb_system *sys, double out[4]);
 
+/* ---- allocation-free SPME reciprocal evaluation.  No counterpart in the
+ * reference: it exists for callers that must not allocate device memory --
+ * code that runs while a stream is captured into a CUDA graph (cudaMalloc
+ * is not allowed then) or a process whose device memory belongs to another
+ * allocator (a framework's caching pool, a fixed-budget serving process).
+ *
+ * posq: device [4n] floats (x, y, z, q) in any atom order; out: device
+ * [4n] floats receiving (fx, fy, fz, per-atom energy share 1/2 q phi -
+ * alpha/sqrt(pi) q^2) of the reciprocal part; energy: host pointer for the
+ * FP64 reciprocal energy, or NULL (non-NULL synchronises the stream);
+ * stream: a cudaStream_t, or NULL for the legacy default stream.
+ *
+ * Limits: at most 64 grid points per axis and 32768 in total (e.g. 32^3);
+ * larger grids are rejected with HB_ERR_INVALID_GRID.  All scratch lives in
+ * one file-scope device array (about 0.7 MB) that every GPU loading the
+ * library holds until the process exits; the call allocates nothing.  The
+ * first call on a device looks up that array's address (cudaGetSymbolAddress)
+ * and caches it: make that first call before any stream capture.  Every call
+ * shares the one array, so calls whose GPU work overlaps (different streams
+ * or threads) race; serialise them. */
+int hb_spme_recip_noalloc(const float *posq, uint32_t n, const double box[6],
+                          const uint32_t grid[3], uint32_t order, double alpha,
+                          float *out, double *energy, void *stream);
+
 /* ---- device timing of the last hb_integrator_step call, in ms:
  * out[0] total, out[1] pair kernel (sum), out[2] SPME (sum), out[3]
  * neighbour rebuilds (sum), out[4] integrator + constraints (sum);
