@@ -196,13 +196,15 @@ struct hb_forcefield {
   float4 *d_tile_half = nullptr;     // per tile: half extents
   uint32_t *d_tile_nent = nullptr;   // entries held by each tile
   uint32_t slab = 0;                 // entry capacity per tile
+  uint32_t maxc = 1024;              // candidate j-tiles per i-tile (shared memory)
   uint32_t *d_entry_j = nullptr;     // [n_tiles * slab * 32] sorted j slots
   uint32_t *d_entry_excl = nullptr;  // [n_tiles * slab * 32] exclusion masks
   uint64_t entry_cap = 0;            // n_tiles * slab
   float4 *d_ref_pos = nullptr;       // positions at the last rebuild
   uint32_t *d_status = nullptr;      // status word
   uint32_t *d_counters = nullptr;    // [0] rebuilds, [1] entries of the last
-                                     // build, [2] running count of a build
+                                     // build, [2] running count of a build,
+                                     // [3] largest candidate count seen
   uint32_t *h_status = nullptr;      // pinned mirror
   uint64_t rebuilds_host = 0;
   bool built = false;

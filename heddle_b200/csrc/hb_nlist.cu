@@ -262,156 +262,198 @@ __device__ __forceinline__ uint32_t excl_mask(uint32_t sj, uint32_t I,
   return m;
 }
 
-#define NL_WARPS 4
+#define NLT_WARPS 8
 
-// Packed-entry construction, one warp per i-tile.  WRITE = false counts
-// the tile's entries (sizing pass of the first build); WRITE = true writes
-// them into the tile's slab and flags slabs that filled past 3/4 or
-// overflowed.
+// k-th set bit (0-based) of a 32-bit mask
+__device__ __forceinline__ uint32_t select_bit(uint32_t m, uint32_t k) {
+  for (uint32_t i = 0; i < k; ++i) m &= m - 1u;
+  return (uint32_t)__ffs(m) - 1u;
+}
+
+// Packed-entry construction, one 256-thread block per i-tile I:
+//  1. the block sweeps j-tiles J > I in order, keeping those whose box lies
+//     within r_search of I's box (candidate list in shared memory);
+//  2. each warp takes candidates and computes a 32-bit hit mask: bit l is
+//     set when j-atom l of the candidate lies within r_search of any i-atom.
+//     Far from the r_search boundary a j-atom shifted once to the image
+//     nearest I's centre decides with plain differences; inside a 1e-4
+//     relative band the exact single-precision rule decides;
+//  3. a prefix sum of the masks' popcounts fixes where every hit goes;
+//  4. the warps write the entries (self tile first) into I's slab, each
+//     with the exclusion masks of its 32 j-atoms.
+// WRITE = false only counts entries and candidates (first-build sizing).
 template <bool WRITE>
-__global__ void __launch_bounds__(NL_WARPS * 32)
-    k_nl_build(const uint32_t *gate, const float4 *__restrict__ tile_posq,
-               const float4 *__restrict__ center, const float4 *__restrict__ half,
-               const DBox *__restrict__ box, float rs2, float rb2, float band_lo,
-               float band_hi, uint32_t n, uint32_t n_tiles, uint32_t *__restrict__ tile_nent,
-               uint32_t slab, uint32_t *__restrict__ entry_j,
-               uint32_t *__restrict__ entry_excl, uint32_t *__restrict__ status,
-               uint32_t *__restrict__ counters,
-               const uint32_t *__restrict__ sorted_ids, const uint32_t *__restrict__ inv_perm,
-               const uint32_t *__restrict__ eoff, const uint32_t *__restrict__ epart) {
+__global__ void __launch_bounds__(NLT_WARPS * 32)
+    k_nl_tile(const uint32_t *gate, const float4 *__restrict__ tile_posq,
+              const float4 *__restrict__ center, const float4 *__restrict__ half,
+              const DBox *__restrict__ box, float rs2, float rb, float band_lo, float band_hi,
+              uint32_t n, uint32_t n_tiles, uint32_t maxc, uint32_t *__restrict__ tile_nent,
+              uint32_t slab, uint32_t *__restrict__ entry_j, uint32_t *__restrict__ entry_excl,
+              uint32_t *__restrict__ status, uint32_t *__restrict__ counters,
+              const uint32_t *__restrict__ sorted_ids, const uint32_t *__restrict__ inv_perm,
+              const uint32_t *__restrict__ eoff, const uint32_t *__restrict__ epart) {
   if (gate_off(gate)) return;
-  __shared__ float sx[NL_WARPS][32], sy[NL_WARPS][32], sz[NL_WARPS][32];
-  __shared__ uint32_t jbuf[NL_WARPS][64];
+  extern __shared__ uint32_t sm_nl[];
+  uint32_t *cand = sm_nl;             // [maxc] candidate j-tiles
+  uint32_t *hmask = sm_nl + maxc;     // [maxc] hit masks
+  uint32_t *pre = hmask + maxc;       // [maxc + 1] exclusive prefix of hits
+  __shared__ uint32_t s_cnt[NLT_WARPS];
+  __shared__ uint32_t s_ncand;
   const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  const uint32_t I = blockIdx.x * NL_WARPS + w;
-  if (I >= n_tiles) return;
+  const uint32_t I = blockIdx.x;
   const DBox b = *box;
-  const uint32_t ki = I * 32u + lane;
-  const float4 pi = tile_posq[ki];
-  sx[w][lane] = pi.x;
-  sy[w][lane] = pi.y;
-  sz[w][lane] = pi.z;
-  const uint32_t ivalid = __ballot_sync(0xFFFFFFFFu, ki < n);
-  __syncwarp();
   const float4 ci = center[I], hi = half[I];
-  const bool ortho_tests = ((int)ci.w & 2) != 0;
-  const uint64_t base = (uint64_t)I * slab;
-  uint32_t nent = 0;
+  const bool ortho = ((int)ci.w & 2) != 0;
+  const float rb2 = rb * rb;
+  if (threadIdx.x == 0) s_ncand = 0u;
+  __syncthreads();
 
-  // entry 0: the self tile (all pairs inside the tile, half rotation)
-  if (__popc(ivalid) >= 2) {
-    if (WRITE) {
-      uint64_t e = base;
-      if (slab > 0u) {
-        uint32_t sj = ki < n ? ki : HB_SENTINEL;
-        entry_j[e * 32u + lane] = sj;
-        entry_excl[e * 32u + lane] = excl_mask(sj, I, sorted_ids, inv_perm, eoff, epart);
-      }
-    }
-    nent = 1;
-  }
-
-  uint32_t blen = 0;
-  for (uint32_t j0 = I + 1; j0 < n_tiles; j0 += 32u) {
-    uint32_t J = j0 + lane;
+  // 1. ordered candidate sweep
+  for (uint32_t base = I + 1u; base < n_tiles; base += 32u * NLT_WARPS) {
+    const uint32_t J = base + w * 32u + lane;
     bool pass = false;
-    if (J < n_tiles && !ortho_tests) {
-      pass = true;
-    } else if (J < n_tiles) {
-      float4 cj = center[J], hj = half[J];
-      float dx = ci.x - cj.x, dy = ci.y - cj.y, dz = ci.z - cj.z;
-      hb_min_image(dx, dy, dz, b);
-      float ex = fmaxf(fabsf(dx) - (hi.x + hj.x), 0.0f);
-      float ey = fmaxf(fabsf(dy) - (hi.y + hj.y), 0.0f);
-      float ez = fmaxf(fabsf(dz) - (hi.z + hj.z), 0.0f);
-      pass = ex * ex + ey * ey + ez * ez <= rb2;
+    if (J < n_tiles) {
+      if (!ortho) {
+        pass = true;
+      } else {
+        const float4 cj = center[J], hj = half[J];
+        float dx = ci.x - cj.x, dy = ci.y - cj.y, dz = ci.z - cj.z;
+        hb_min_image(dx, dy, dz, b);
+        const float ex = fmaxf(fabsf(dx) - (hi.x + hj.x), 0.0f);
+        const float ey = fmaxf(fabsf(dy) - (hi.y + hj.y), 0.0f);
+        const float ez = fmaxf(fabsf(dz) - (hi.z + hj.z), 0.0f);
+        pass = ex * ex + ey * ey + ez * ez <= rb2;
+      }
     }
-    uint32_t cand = __ballot_sync(0xFFFFFFFFu, pass);
-    while (cand) {
-      uint32_t bit = __ffs(cand) - 1u;
-      cand &= cand - 1u;
-      uint32_t Jt = j0 + bit;
-      uint32_t kj = Jt * 32u + lane;
-      bool jvalid = kj < n;
-      bool hit = false;
-      bool near = jvalid;
-      float4 pj;
-      if (jvalid) {
-        pj = tile_posq[kj];
-        if (ortho_tests) {
-          // distance from the j-atom to the i-tile box bounds its distance
-          // to every i-atom from below
-          float dx = pj.x - ci.x, dy = pj.y - ci.y, dz = pj.z - ci.z;
-          hb_min_image(dx, dy, dz, b);
-          float ex = fmaxf(fabsf(dx) - hi.x, 0.0f);
-          float ey = fmaxf(fabsf(dy) - hi.y, 0.0f);
-          float ez = fmaxf(fabsf(dz) - hi.z, 0.0f);
-          near = ex * ex + ey * ey + ez * ez <= rb2;
+    const uint32_t bal = __ballot_sync(0xFFFFFFFFu, pass);
+    if (lane == 0) s_cnt[w] = __popc(bal);
+    __syncthreads();
+    uint32_t off = s_ncand;
+    for (uint32_t k = 0; k < w; ++k) off += s_cnt[k];
+    if (pass) {
+      const uint32_t pos = off + __popc(bal & ((1u << lane) - 1u));
+      if (pos < maxc) cand[pos] = J;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t t = s_ncand;
+      for (uint32_t k = 0; k < NLT_WARPS; ++k) t += s_cnt[k];
+      s_ncand = t;
+    }
+    __syncthreads();
+  }
+  const uint32_t ncand_all = s_ncand;
+  const uint32_t ncand = ncand_all < maxc ? ncand_all : maxc;
+
+  // 2. hit masks; i-atoms stay in registers and are broadcast by shuffles
+  const uint32_t ki = I * 32u + lane;
+  const float4 pim = tile_posq[ki];
+  const uint32_t ivalid = __ballot_sync(0xFFFFFFFFu, ki < n);
+  const bool shift_ok = ortho && (hi.x + rb <= 0.5f * b.lx) && (hi.y + rb <= 0.5f * b.ly) &&
+                        (hi.z + rb <= 0.5f * b.lz);
+  for (uint32_t c = w; c < ncand; c += NLT_WARPS) {
+    const uint32_t kj = cand[c] * 32u + lane;
+    const bool jvalid = kj < n;
+    const float4 pj = tile_posq[kj];
+    float sx = pj.x, sy = pj.y, sz = pj.z;
+    if (shift_ok) {
+      sx -= b.lx * rintf((sx - ci.x) * b.ilx);
+      sy -= b.ly * rintf((sy - ci.y) * b.ily);
+      sz -= b.lz * rintf((sz - ci.z) * b.ilz);
+    }
+    bool near = jvalid;
+    if (near && ortho) {
+      float dx = sx - ci.x, dy = sy - ci.y, dz = sz - ci.z;
+      if (!shift_ok) hb_min_image(dx, dy, dz, b);
+      const float ex = fmaxf(fabsf(dx) - hi.x, 0.0f);
+      const float ey = fmaxf(fabsf(dy) - hi.y, 0.0f);
+      const float ez = fmaxf(fabsf(dz) - hi.z, 0.0f);
+      near = ex * ex + ey * ey + ez * ez <= rb2;
+    }
+    bool hit = false;
+    uint32_t open = __ballot_sync(0xFFFFFFFFu, near);
+    for (uint32_t m = 0; m < 32u && open != 0u; ++m) {
+      const float xi = __shfl_sync(0xFFFFFFFFu, pim.x, m);
+      const float yi = __shfl_sync(0xFFFFFFFFu, pim.y, m);
+      const float zi = __shfl_sync(0xFFFFFFFFu, pim.z, m);
+      if (near && !hit && ((ivalid >> m) & 1u)) {
+        float dx = xi - sx, dy = yi - sy, dz = zi - sz;
+        if (!shift_ok) hb_min_image(dx, dy, dz, b);
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 < band_lo) {
+          hit = true;
+        } else if (r2 <= band_hi && hb_exact_r2(xi - pj.x, yi - pj.y, zi - pj.z, b) <= rs2) {
+          hit = true;
         }
       }
-      if (near) {
-        uint32_t mm = ivalid;
-        while (mm) {
-          uint32_t m = __ffs(mm) - 1u;
-          mm &= mm - 1u;
-          float dx = sx[w][m] - pj.x, dy = sy[w][m] - pj.y, dz = sz[w][m] - pj.z;
-          // fast minimum image decides far from the boundary; the exact
-          // single-precision rule decides inside a 1e-5 relative band
-          float fx = dx, fy = dy, fz = dz;
-          hb_min_image(fx, fy, fz, b);
-          float r2 = fx * fx + fy * fy + fz * fz;
-          if (r2 < band_lo) {
-            hit = true;
-            break;
+      open = __ballot_sync(0xFFFFFFFFu, near && !hit);
+    }
+    const uint32_t hm = __ballot_sync(0xFFFFFFFFu, hit);
+    if (lane == 0) hmask[c] = hm;
+  }
+  __syncthreads();
+
+  // 3. exclusive prefix of the hit counts (one warp)
+  if (w == 0) {
+    uint32_t carry = 0;
+    for (uint32_t c0 = 0; c0 < ncand; c0 += 32u) {
+      const uint32_t c = c0 + lane;
+      const uint32_t v = c < ncand ? __popc(hmask[c]) : 0u;
+      uint32_t x = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if ((int)lane >= o) x += y;
+      }
+      if (c < ncand) pre[c] = carry + x - v;
+      carry += __shfl_sync(0xFFFFFFFFu, x, 31);
+    }
+    if (lane == 0) pre[ncand] = carry;
+  }
+  __syncthreads();
+  const uint32_t H = pre[ncand];
+  const uint32_t has_self = (n - I * 32u >= 2u) ? 1u : 0u;
+  const uint32_t nent = has_self + (H + 31u) / 32u;
+
+  // 4. entries
+  if (WRITE) {
+    for (uint32_t e = w; e < nent && e < slab; e += NLT_WARPS) {
+      uint32_t sj = HB_SENTINEL;
+      if (has_self && e == 0) {
+        if (ki < n) sj = ki;
+      } else {
+        const uint32_t h = (e - has_self) * 32u + lane;
+        if (h < H) {
+          uint32_t lo = 0, hiidx = ncand;  // largest c with pre[c] <= h
+          while (hiidx - lo > 1u) {
+            const uint32_t mid = (lo + hiidx) >> 1;
+            if (pre[mid] <= h) lo = mid;
+            else hiidx = mid;
           }
-          if (r2 <= band_hi && hb_exact_r2(dx, dy, dz, b) <= rs2) {
-            hit = true;
-            break;
-          }
+          sj = cand[lo] * 32u + select_bit(hmask[lo], h - pre[lo]);
         }
       }
-      uint32_t hits = __ballot_sync(0xFFFFFFFFu, hit);
-      if (hit) {
-        uint32_t pre = __popc(hits & ((1u << lane) - 1u));
-        jbuf[w][blen + pre] = kj;
-      }
-      blen += __popc(hits);
-      __syncwarp();
-      if (blen >= 32u) {
-        if (WRITE) {
-          uint64_t e = base + nent;
-          if (nent < slab) {
-            uint32_t sj = jbuf[w][lane];
-            entry_j[e * 32u + lane] = sj;
-            entry_excl[e * 32u + lane] = excl_mask(sj, I, sorted_ids, inv_perm, eoff, epart);
-          }
+      const uint64_t slot = ((uint64_t)I * slab + e) * 32u + lane;
+      entry_j[slot] = sj;
+      // stored in the i-lane's rotation order: bit t of lane l's word says
+      // whether i-atom l and the j-atom of lane (l + t) mod 32 are excluded
+      const uint32_t jm = excl_mask(sj, I, sorted_ids, inv_perm, eoff, epart);
+      uint32_t im = 0u;
+      if (__any_sync(0xFFFFFFFFu, jm != 0u)) {
+        for (uint32_t t = 0; t < 32u; ++t) {
+          const uint32_t m = __shfl_sync(0xFFFFFFFFu, jm, (lane + t) & 31u);
+          im |= ((m >> lane) & 1u) << t;
         }
-        nent++;
-        uint32_t rest = blen - 32u;
-        uint32_t v = lane < rest ? jbuf[w][32u + lane] : 0u;
-        __syncwarp();
-        if (lane < rest) jbuf[w][lane] = v;
-        blen = rest;
-        __syncwarp();
       }
+      entry_excl[slot] = im;
     }
   }
-  if (blen > 0u) {
-    if (WRITE) {
-      uint64_t e = base + nent;
-      if (nent < slab) {
-        uint32_t sj = lane < blen ? jbuf[w][lane] : HB_SENTINEL;
-        entry_j[e * 32u + lane] = sj;
-        entry_excl[e * 32u + lane] = excl_mask(sj, I, sorted_ids, inv_perm, eoff, epart);
-      }
-    }
-    nent++;
-  }
-  if (lane == 0) {
+  if (threadIdx.x == 0) {
     tile_nent[I] = nent;
+    atomicMax(&counters[3], ncand_all);
     if (WRITE) {
       atomicAdd(&counters[2], nent);
-      if (nent > slab) atomicOr(status, HB_ST_ENTRY_OVERFLOW);
+      if (nent > slab || ncand_all > maxc) atomicOr(status, HB_ST_ENTRY_OVERFLOW);
       else if (4u * nent > 3u * slab) atomicOr(status, HB_ST_ENTRY_HIGHWATER);
     }
   }
@@ -530,9 +572,11 @@ static int nl_launch(hb_forcefield *ff, const uint32_t *gate, cudaStream_t s, bo
   const uint32_t n_vox = 1u << (3 * ff->nv_log2);
   const float rs = ff->r_search;
   const float rs2 = rs * rs;
-  // box-prune radius with a margin so rounding never drops a pair
-  const float rb = rs * (1.0f + 1.0e-5f) + 1.0e-4f;
-  const float band_lo = rs2 * (1.0f - 1.0e-5f), band_hi = rs2 * (1.0f + 1.0e-5f);
+  // box-prune radius with a margin so rounding never drops a pair, and the
+  // relative band inside which the exact rule decides
+  const float rb = rs * (1.0f + 1.0e-4f) + 1.0e-4f;
+  const float band_lo = rs2 * (1.0f - 1.0e-4f), band_hi = rs2 * (1.0f + 1.0e-4f);
+  const size_t smem = sizeof(uint32_t) * (3u * ff->maxc + 1u);
   if (sort) {
     k_vox_hist<<<hb_div_up(n, 256), 256, 0, s>>>(gate, sys->d_posq, sys->d_box, ff->nv_log2,
                                                   ff->d_vox_key, ff->d_vox_count, n);
@@ -548,14 +592,14 @@ static int nl_launch(hb_forcefield *ff, const uint32_t *gate, cudaStream_t s, bo
         ff->d_tile_half, n, ff->n_tiles);
   }
   if (count_only) {
-    k_nl_build<false><<<hb_div_up(ff->n_tiles, NL_WARPS), NL_WARPS * 32, 0, s>>>(
-        gate, ff->d_tile_posq, ff->d_tile_center, ff->d_tile_half, sys->d_box, rs2, rb * rb,
-        band_lo, band_hi, n, ff->n_tiles, ff->d_tile_nent, 0u, nullptr, nullptr, ff->d_status,
+    k_nl_tile<false><<<ff->n_tiles, NLT_WARPS * 32, smem, s>>>(
+        gate, ff->d_tile_posq, ff->d_tile_center, ff->d_tile_half, sys->d_box, rs2, rb, band_lo,
+        band_hi, n, ff->n_tiles, ff->maxc, ff->d_tile_nent, 0u, nullptr, nullptr, ff->d_status,
         ff->d_counters, ff->d_sorted_ids, ff->d_inv_perm, ff->d_excl_off, ff->d_excl_partner);
   } else {
-    k_nl_build<true><<<hb_div_up(ff->n_tiles, NL_WARPS), NL_WARPS * 32, 0, s>>>(
-        gate, ff->d_tile_posq, ff->d_tile_center, ff->d_tile_half, sys->d_box, rs2, rb * rb,
-        band_lo, band_hi, n, ff->n_tiles, ff->d_tile_nent, ff->slab, ff->d_entry_j,
+    k_nl_tile<true><<<ff->n_tiles, NLT_WARPS * 32, smem, s>>>(
+        gate, ff->d_tile_posq, ff->d_tile_center, ff->d_tile_half, sys->d_box, rs2, rb, band_lo,
+        band_hi, n, ff->n_tiles, ff->maxc, ff->d_tile_nent, ff->slab, ff->d_entry_j,
         ff->d_entry_excl, ff->d_status, ff->d_counters, ff->d_sorted_ids, ff->d_inv_perm,
         ff->d_excl_off, ff->d_excl_partner);
     k_nl_finish<<<1, 1, 0, s>>>(gate, ff->d_status, ff->d_counters);
@@ -588,7 +632,20 @@ int nl_first_build(hb_forcefield *ff) {
   cudaStream_t s = sys->ctx->stream;
   uint32_t one = HB_ST_DISPLACED;
   HB_CUDA(cudaMemcpyAsync(ff->d_status, &one, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-  HB_TRY(nl_launch(ff, nullptr, s, true, true));
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    HB_CUDA(cudaMemsetAsync(ff->d_counters + 3, 0, sizeof(uint32_t), s));
+    HB_TRY(nl_launch(ff, nullptr, s, attempt == 0, true));
+    uint32_t mc = 0;
+    HB_CUDA(cudaMemcpyAsync(&mc, ff->d_counters + 3, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    HB_CUDA(cudaStreamSynchronize(s));
+    const uint32_t want_c = mc + mc / 2 + 64;
+    if (mc <= ff->maxc && ff->maxc >= want_c) break;
+    ff->maxc = std::max(want_c, ff->maxc);
+    HB_CUDA(cudaFuncSetAttribute(k_nl_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(uint32_t) * (3u * ff->maxc + 1u))));
+    HB_CUDA(cudaFuncSetAttribute(k_nl_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(uint32_t) * (3u * ff->maxc + 1u))));
+  }
   std::vector<uint32_t> nent(ff->n_tiles);
   HB_CUDA(cudaMemcpyAsync(nent.data(), ff->d_tile_nent, sizeof(uint32_t) * ff->n_tiles,
                           cudaMemcpyDeviceToHost, s));

@@ -54,7 +54,7 @@ __device__ __forceinline__ void red_add(unsigned long long *p, long long v) {
 }
 
 template <bool EV, bool SCALED, bool SWITCH>
-__global__ void __launch_bounds__(PAIR_WARPS * 32)
+__global__ void __launch_bounds__(PAIR_WARPS * 32, 8)
     k_pair(const float4 *__restrict__ tile_posq, const int *__restrict__ tile_type,
            const float4 *__restrict__ center, const uint32_t *__restrict__ tile_nent,
            const uint32_t *__restrict__ entry_j, const uint32_t *__restrict__ entry_excl,
@@ -96,7 +96,8 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32)
   for (uint32_t e = e0; e < e1; ++e) {
     const bool self = has_self && (e == e0);
     uint32_t sj = entry_j[(uint64_t)e * 32u + lane];
-    uint32_t jm = entry_excl[(uint64_t)e * 32u + lane];
+    // exclusions in this lane's rotation order: bit t <-> j of lane (lane+t)
+    const uint32_t xm = entry_excl[(uint64_t)e * 32u + lane];
     const bool jvalid = sj != HB_SENTINEL;
     float4 pj;
     int tj = 0;
@@ -121,7 +122,6 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32)
     pj.z = __shfl_sync(0xFFFFFFFFu, pj.z, src);                       \
     pj.w = __shfl_sync(0xFFFFFFFFu, pj.w, src);                       \
     tj = __shfl_sync(0xFFFFFFFFu, tj, src);                           \
-    jm = __shfl_sync(0xFFFFFFFFu, jm, src);                           \
     fjx = __shfl_sync(0xFFFFFFFFu, fjx, src);                         \
     fjy = __shfl_sync(0xFFFFFFFFu, fjy, src);                         \
     fjz = __shfl_sync(0xFFFFFFFFu, fjz, src);                         \
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32)
       float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
       if (!spc) hb_min_image(dx, dy, dz, b);
       const float r2 = dx * dx + dy * dy + dz * dz;
-      const bool excl = (jm >> lane) & 1u;
+      const bool excl = (xm >> t) & 1u;
       bool active = r2 < P.rc2_max && (SCALED || !excl);
       if (self && t == 16u && lane >= 16u) active = false;
       if (active) {

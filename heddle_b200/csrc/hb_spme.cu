@@ -47,62 +47,101 @@ __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // a * conj(b)
   return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
 
-// In-shared-memory transform of L lines of length n, line-major with
-// stride S = n + 1.  Returns the buffer holding the result.
+// p-point DFT of v (forward: exp(-2 pi i qr / p)), p in {2, 3, 4, 5, 7};
+// the twiddle constants are cos / sin of 2 pi k / p.
+template <int P, bool INV>
+__device__ __forceinline__ void butterfly(float2 *v) {
+  if constexpr (P == 2) {
+    const float2 a = v[0], b = v[1];
+    v[0] = make_float2(a.x + b.x, a.y + b.y);
+    v[1] = make_float2(a.x - b.x, a.y - b.y);
+  } else if constexpr (P == 4) {
+    const float2 a0 = make_float2(v[0].x + v[2].x, v[0].y + v[2].y);
+    const float2 a1 = make_float2(v[0].x - v[2].x, v[0].y - v[2].y);
+    const float2 a2 = make_float2(v[1].x + v[3].x, v[1].y + v[3].y);
+    const float2 a3 = make_float2(v[1].x - v[3].x, v[1].y - v[3].y);
+    // forward: X1 = a1 - i a3, X3 = a1 + i a3 (inverse swaps the sign)
+    const float2 ia3 = INV ? make_float2(-a3.y, a3.x) : make_float2(a3.y, -a3.x);
+    v[0] = make_float2(a0.x + a2.x, a0.y + a2.y);
+    v[2] = make_float2(a0.x - a2.x, a0.y - a2.y);
+    v[1] = make_float2(a1.x + ia3.x, a1.y + ia3.y);
+    v[3] = make_float2(a1.x - ia3.x, a1.y - ia3.y);
+  } else {
+    constexpr float c3[3] = {1.0f, -0.5f, -0.5f};
+    constexpr float s3[3] = {0.0f, 0.86602540378443865f, -0.86602540378443865f};
+    constexpr float c5[5] = {1.0f, 0.30901699437494742f, -0.80901699437494742f,
+                             -0.80901699437494742f, 0.30901699437494742f};
+    constexpr float s5[5] = {0.0f, 0.95105651629515357f, 0.58778525229247313f,
+                             -0.58778525229247313f, -0.95105651629515357f};
+    constexpr float c7[7] = {1.0f, 0.62348980185873353f, -0.22252093395631440f,
+                             -0.90096886790241913f, -0.90096886790241913f,
+                             -0.22252093395631440f, 0.62348980185873353f};
+    constexpr float s7[7] = {0.0f, 0.78183148246802981f, 0.97492791218182361f,
+                             0.43388373911755812f, -0.43388373911755812f,
+                             -0.97492791218182361f, -0.78183148246802981f};
+    const float *cs = P == 3 ? c3 : (P == 5 ? c5 : c7);
+    const float *sn = P == 3 ? s3 : (P == 5 ? s5 : s7);
+    float2 o[P];
+#pragma unroll
+    for (int r = 0; r < P; ++r) {
+      float2 acc = v[0];
+#pragma unroll
+      for (int q = 1; q < P; ++q) {
+        const int e = (q * r) % P;
+        const float c = cs[e], sgn = INV ? sn[e] : -sn[e];
+        acc.x += v[q].x * c - v[q].y * sgn;
+        acc.y += v[q].x * sgn + v[q].y * c;
+      }
+      o[r] = acc;
+    }
+#pragma unroll
+    for (int r = 0; r < P; ++r) v[r] = o[r];
+  }
+}
+
+// One Stockham radix-P stage over L lines (line-major, stride n + 1):
+// butterfly j of a line reads elements j + q m, twiddles them by
+// w^(q (j mod Ns)), and writes (j / Ns) Ns P + (j mod Ns) + q Ns.
+template <int P, bool INV>
+__device__ __forceinline__ void stage_dyn(const float2 *A, float2 *B, const float2 *tw, int n,
+                                          int L, int Ns) {
+  const int S = n + 1, m = n / P, tstep = n / (Ns * P);
+  for (int idx = threadIdx.x; idx < m * L; idx += blockDim.x) {
+    const int l = idx / m, j = idx - l * m;
+    const int k = j % Ns;
+    const float2 *src = A + l * S;
+    float2 v[P];
+#pragma unroll
+    for (int q = 0; q < P; ++q) v[q] = src[j + q * m];
+    if (Ns > 1) {
+#pragma unroll
+      for (int q = 1; q < P; ++q) {
+        const float2 w = tw[q * k * tstep];
+        v[q] = INV ? cmulc(v[q], w) : cmul(v[q], w);
+      }
+    }
+    butterfly<P, INV>(v);
+    float2 *dst = B + l * S;
+    const int base = (j / Ns) * Ns * P + k;
+#pragma unroll
+    for (int q = 0; q < P; ++q) dst[base + q * Ns] = v[q];
+  }
+}
+
+// Runtime-planned transform of L lines of length n (fallback for sizes
+// without a compile-time specialisation).  Returns the result buffer.
 template <bool INV>
 __device__ float2 *fft_lines(float2 *A, float2 *B, const float2 *__restrict__ tw, int n,
                              int L, const FftPlan &pl) {
-  const int S = n + 1;
   int Ns = 1;
   for (int st = 0; st < pl.nst; ++st) {
     const int p = pl.r[st];
-    const int m = n / p;
-    const int tstep = n / (Ns * p);
-    const int np = n / p;
-    for (int idx = threadIdx.x; idx < m * L; idx += blockDim.x) {
-      const int l = idx / m, j = idx - (idx / m) * m;
-      const int k = j % Ns;
-      const float2 *src = A + l * S;
-      float2 v[7];
-      for (int q = 0; q < p; ++q) v[q] = src[j + q * m];
-      if (Ns > 1) {
-        for (int q = 1; q < p; ++q) {
-          const float2 w = tw[q * k * tstep];
-          v[q] = INV ? cmulc(v[q], w) : cmul(v[q], w);
-        }
-      }
-      if (p == 2) {
-        float2 a = v[0], b = v[1];
-        v[0] = make_float2(a.x + b.x, a.y + b.y);
-        v[1] = make_float2(a.x - b.x, a.y - b.y);
-      } else if (p == 4) {
-        float2 a0 = make_float2(v[0].x + v[2].x, v[0].y + v[2].y);
-        float2 a1 = make_float2(v[0].x - v[2].x, v[0].y - v[2].y);
-        float2 a2 = make_float2(v[1].x + v[3].x, v[1].y + v[3].y);
-        float2 a3 = make_float2(v[1].x - v[3].x, v[1].y - v[3].y);
-        // forward: X1 = a1 - i a3, X3 = a1 + i a3 (inverse swaps the sign)
-        float2 ia3 = INV ? make_float2(-a3.y, a3.x) : make_float2(a3.y, -a3.x);
-        v[0] = make_float2(a0.x + a2.x, a0.y + a2.y);
-        v[2] = make_float2(a0.x - a2.x, a0.y - a2.y);
-        v[1] = make_float2(a1.x + ia3.x, a1.y + ia3.y);
-        v[3] = make_float2(a1.x - ia3.x, a1.y - ia3.y);
-      } else {
-        float2 o[7];
-        for (int r = 0; r < p; ++r) {
-          float2 acc = v[0];
-          for (int q = 1; q < p; ++q) {
-            const float2 w = tw[((q * r) % p) * np];
-            const float2 t = INV ? cmulc(v[q], w) : cmul(v[q], w);
-            acc.x += t.x;
-            acc.y += t.y;
-          }
-          o[r] = acc;
-        }
-        for (int r = 0; r < p; ++r) v[r] = o[r];
-      }
-      float2 *dst = B + l * S;
-      const int base = (j / Ns) * Ns * p + k;
-      for (int q = 0; q < p; ++q) dst[base + q * Ns] = v[q];
+    switch (p) {
+      case 2: stage_dyn<2, INV>(A, B, tw, n, L, Ns); break;
+      case 3: stage_dyn<3, INV>(A, B, tw, n, L, Ns); break;
+      case 4: stage_dyn<4, INV>(A, B, tw, n, L, Ns); break;
+      case 5: stage_dyn<5, INV>(A, B, tw, n, L, Ns); break;
+      default: stage_dyn<7, INV>(A, B, tw, n, L, Ns); break;
     }
     __syncthreads();
     float2 *t = A;
@@ -111,6 +150,72 @@ __device__ float2 *fft_lines(float2 *A, float2 *B, const float2 *__restrict__ tw
     Ns *= p;
   }
   return A;
+}
+
+// ---- compile-time transforms: radix order 4, 2, 3, 5, 7 (as make_plan) ----
+__host__ __device__ constexpr int radix_first(int n) {
+  return n % 4 == 0 ? 4 : (n % 2 == 0 ? 2 : (n % 3 == 0 ? 3 : (n % 5 == 0 ? 5 : 7)));
+}
+__host__ __device__ constexpr int stage_radix(int n, int s) {
+  int p = radix_first(n);
+  while (s > 0) {
+    n /= p;
+    p = radix_first(n);
+    --s;
+  }
+  return p;
+}
+__host__ __device__ constexpr int n_stages(int n) {
+  int c = 0;
+  while (n > 1) {
+    n /= radix_first(n);
+    ++c;
+  }
+  return c;
+}
+__host__ __device__ constexpr int lines_of(int n) { return 2048 / n > 16 ? 16 : (2048 / n < 2 ? 2 : 2048 / n); }
+constexpr int FFT_THREADS = 256;
+
+template <int N, int L, bool INV, int S, int NS>
+__device__ __forceinline__ float2 *fft_stages(float2 *A, float2 *B, const float2 *__restrict__ tw) {
+  if constexpr (S == n_stages(N)) {
+    return A;
+  } else {
+    constexpr int P = stage_radix(N, S), M = N / P, TSTEP = N / (NS * P), STR = N + 1;
+    for (int idx = threadIdx.x; idx < M * L; idx += FFT_THREADS) {
+      const int l = idx / M, j = idx % M;
+      const int k = j % NS;
+      const float2 *src = A + l * STR;
+      float2 v[P];
+#pragma unroll
+      for (int q = 0; q < P; ++q) v[q] = src[j + q * M];
+      if constexpr (NS > 1) {
+#pragma unroll
+        for (int q = 1; q < P; ++q) {
+          const float2 w = tw[q * k * TSTEP];
+          v[q] = INV ? cmulc(v[q], w) : cmul(v[q], w);
+        }
+      }
+      butterfly<P, INV>(v);
+      float2 *dst = B + l * STR;
+      const int base = (j / NS) * NS * P + k;
+#pragma unroll
+      for (int q = 0; q < P; ++q) dst[base + q * NS] = v[q];
+    }
+    __syncthreads();
+    return fft_stages<N, L, INV, S + 1, NS * P>(B, A, tw);
+  }
+}
+
+// N > 0: compile-time transform of lines_of(N) lines; N == 0: runtime plan
+template <int N, bool INV>
+__device__ __forceinline__ float2 *fft_run(float2 *A, float2 *B, const float2 *__restrict__ tw,
+                                           int n, int L, const FftPlan &pl) {
+  if constexpr (N == 0) {
+    return fft_lines<INV>(A, B, tw, n, L, pl);
+  } else {
+    return fft_stages<N, lines_of(N), INV, 0, 1>(A, B, tw);
+  }
 }
 
 // B-spline weights w[d] = M_P(d + t), d = 0..P-1, and optionally their
@@ -178,7 +283,11 @@ __global__ void k_spread(const float4 *__restrict__ tile_posq, const DBox *__res
   bspline<P, false>(t[2], wc, nullptr);
   int ga = g0[0] - da;
   if (ga < 0) ga += na;
-  const float qa = p.w * wa[da];
+  float wda = 0.0f;
+#pragma unroll
+  for (int d = 0; d < P; ++d)
+    if (d == da) wda = wa[d];
+  const float qa = p.w * wda;
 #pragma unroll
   for (int db = 0; db < P; ++db) {
     int gb = g0[1] - db;
@@ -196,11 +305,14 @@ __global__ void k_spread(const float4 *__restrict__ tile_posq, const DBox *__res
 }
 
 // forward transform along c, one CTA per L rows; clears the int64 grid
-__global__ void k_fft_c_fwd(unsigned long long *__restrict__ rho, float2 *__restrict__ grid,
-                            const float2 *__restrict__ tw_g, FftPlan pl, int nrows, int nch,
-                            int L) {
+template <int N>
+__global__ void __launch_bounds__(256) k_fft_c_fwd(unsigned long long *__restrict__ rho,
+                                                   float2 *__restrict__ grid,
+                                                   const float2 *__restrict__ tw_g, FftPlan pl,
+                                                   int nrows, int nch, int L_rt) {
   extern __shared__ float2 sm[];
-  const int n = pl.n, S = n + 1;
+  const int n = N ? N : pl.n, S = n + 1;
+  const int L = N ? lines_of(N) : L_rt;
   float2 *tw = sm;
   float2 *A = sm + n;
   float2 *B = A + L * S;
@@ -218,7 +330,7 @@ __global__ void k_fft_c_fwd(unsigned long long *__restrict__ rho, float2 *__rest
     A[r * S + c] = make_float2(v, 0.0f);
   }
   __syncthreads();
-  float2 *R = fft_lines<false>(A, B, tw, n, L, pl);
+  float2 *R = fft_run<N, false>(A, B, tw, n, L, pl);
   for (int idx = threadIdx.x; idx < L * nch; idx += blockDim.x) {
     const int r = idx / nch, c = idx - (idx / nch) * nch;
     if (r < nr) grid[(size_t)(row0 + r) * nch + c] = R[r * S + c];
@@ -226,11 +338,15 @@ __global__ void k_fft_c_fwd(unsigned long long *__restrict__ rho, float2 *__rest
 }
 
 // transform along b for L consecutive kc of one a-plane
-template <bool INV>
-__global__ void k_fft_b(float2 *__restrict__ grid, const float2 *__restrict__ tw_g, FftPlan pl,
-                        int nb, int nch, int L) {
+template <int N, bool INV>
+__global__ void __launch_bounds__(256) k_fft_b(float2 *__restrict__ grid,
+                                               const float2 *__restrict__ tw_g, FftPlan pl,
+                                               int nb_rt, int nch, int L_rt) {
   extern __shared__ float2 sm[];
-  const int n = pl.n, S = n + 1;
+  const int n = N ? N : pl.n, S = n + 1;
+  const int nb = n;
+  const int L = N ? lines_of(N) : L_rt;
+  (void)nb_rt;
   float2 *tw = sm;
   float2 *A = sm + n;
   float2 *B = A + L * S;
@@ -244,7 +360,7 @@ __global__ void k_fft_b(float2 *__restrict__ grid, const float2 *__restrict__ tw
     A[l * S + bp] = kc < nch ? grid[((size_t)a * nb + bp) * nch + kc] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  float2 *R = fft_lines<INV>(A, B, tw, n, L, pl);
+  float2 *R = fft_run<N, INV>(A, B, tw, n, L, pl);
   for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
     const int l = idx % L, bp = idx / L;
     const int kc = kc0 + l;
@@ -254,13 +370,19 @@ __global__ void k_fft_b(float2 *__restrict__ grid, const float2 *__restrict__ tw
 
 // transform along a, influence multiply with FP64 energy / virial
 // partials, inverse transform along a
-__global__ void k_fft_a_conv(float2 *__restrict__ grid, const float2 *__restrict__ tw_g,
-                             FftPlan pl, int na, int nb, int nc, int nch, int L,
-                             const DBox *__restrict__ box, const float *__restrict__ bfac,
-                             float alpha, double *__restrict__ part) {
+template <int N>
+__global__ void __launch_bounds__(256) k_fft_a_conv(float2 *__restrict__ grid,
+                                                    const float2 *__restrict__ tw_g, FftPlan pl,
+                                                    int na_rt, int nb, int nc, int nch, int L_rt,
+                                                    const DBox *__restrict__ box,
+                                                    const float *__restrict__ bfac, float alpha,
+                                                    double *__restrict__ part) {
   extern __shared__ float2 sm[];
   __shared__ double red_e[256], red_w[256];
-  const int n = pl.n, S = n + 1;
+  const int n = N ? N : pl.n, S = n + 1;
+  const int na = n;
+  const int L = N ? lines_of(N) : L_rt;
+  (void)na_rt;
   float2 *tw = sm;
   float2 *A = sm + n;
   float2 *B = A + L * S;
@@ -274,7 +396,7 @@ __global__ void k_fft_a_conv(float2 *__restrict__ grid, const float2 *__restrict
     A[l * S + ap] = kc < nch ? grid[((size_t)ap * nb + bq) * nch + kc] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  float2 *R = fft_lines<false>(A, B, tw, n, L, pl);
+  float2 *R = fft_run<N, false>(A, B, tw, n, L, pl);
   float2 *O = (R == A) ? B : A;
   const DBox bx = *box;
   const float ilx = bx.ilx, ily = bx.ily, ilz = bx.ilz;
@@ -325,7 +447,7 @@ __global__ void k_fft_a_conv(float2 *__restrict__ grid, const float2 *__restrict
     part[2 * blockIdx.x] = red_e[0];
     part[2 * blockIdx.x + 1] = red_w[0];
   }
-  float2 *R2 = fft_lines<true>(R, O, tw, n, L, pl);
+  float2 *R2 = fft_run<N, true>(R, O, tw, n, L, pl);
   for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
     const int l = idx % L, ap = idx / L;
     const int kc = kc0 + l;
@@ -334,11 +456,14 @@ __global__ void k_fft_a_conv(float2 *__restrict__ grid, const float2 *__restrict
 }
 
 // inverse transform along c with Hermitian extension; writes V (real)
-__global__ void k_fft_c_inv(const float2 *__restrict__ grid, float *__restrict__ v,
-                            const float2 *__restrict__ tw_g, FftPlan pl, int nrows, int nch,
-                            int L) {
+template <int N>
+__global__ void __launch_bounds__(256) k_fft_c_inv(const float2 *__restrict__ grid,
+                                                   float *__restrict__ v,
+                                                   const float2 *__restrict__ tw_g, FftPlan pl,
+                                                   int nrows, int nch, int L_rt) {
   extern __shared__ float2 sm[];
-  const int n = pl.n, S = n + 1;
+  const int n = N ? N : pl.n, S = n + 1;
+  const int L = N ? lines_of(N) : L_rt;
   float2 *tw = sm;
   float2 *A = sm + n;
   float2 *B = A + L * S;
@@ -359,7 +484,7 @@ __global__ void k_fft_c_inv(const float2 *__restrict__ grid, float *__restrict__
     A[r * S + c] = x;
   }
   __syncthreads();
-  float2 *R = fft_lines<true>(A, B, tw, n, L, pl);
+  float2 *R = fft_run<N, true>(A, B, tw, n, L, pl);
   for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
     const int r = idx / n, c = idx - (idx / n) * n;
     if (r < nr) v[(size_t)(row0 + r) * n + c] = R[r * S + c].x;
@@ -515,6 +640,72 @@ void twiddles(int n, std::vector<float2> &out) {
 
 size_t fft_smem(int n, int L) { return sizeof(float2) * ((size_t)n + 2 * (size_t)L * (n + 1)); }
 
+#define HB_FFT_SIZES(X) X(16) X(20) X(24) X(25) X(32) X(40) X(48) X(64) X(80) X(96) X(128) X(160) X(192) X(256)
+
+struct SpmeLaunch {
+  int na, nb, nc, nch, La, Lb, Lc;
+  FftPlan pa, pb, pc;
+};
+
+SpmeLaunch spme_plan(int na, int nb, int nc) {
+  SpmeLaunch q;
+  q.na = na;
+  q.nb = nb;
+  q.nc = nc;
+  q.nch = nc / 2 + 1;
+  q.La = lines_per_cta(na);
+  q.Lb = lines_per_cta(nb);
+  q.Lc = lines_per_cta(nc);
+  make_plan(na, q.pa);
+  make_plan(nb, q.pb);
+  make_plan(nc, q.pc);
+  return q;
+}
+
+// the five transform passes of one step: c forward (+ int64 -> f32 and
+// clearing), b forward, a forward + influence + a inverse, b inverse,
+// c inverse -> V
+void fft_passes(const SpmeLaunch &q, unsigned long long *rho, float2 *grid, float *v,
+                const float2 *tw, const DBox *box, const float *bfac, float alpha, double *part,
+                cudaStream_t s) {
+  const int nrows = q.na * q.nb;
+  const float2 *twa = tw, *twb = tw + q.na, *twc = tw + q.na + q.nb;
+  const int gc = hb_div_up(nrows, q.Lc);
+  const int gb = q.na * ((q.nch + q.Lb - 1) / q.Lb);
+  const int ga = q.nb * ((q.nch + q.La - 1) / q.La);
+  const size_t sc = fft_smem(q.nc, q.Lc), sb = fft_smem(q.nb, q.Lb), sa = fft_smem(q.na, q.La);
+  switch (q.nc) {
+#define HB_C(NN) case NN: k_fft_c_fwd<NN><<<gc, 256, sc, s>>>(rho, grid, twc, q.pc, nrows, q.nch, q.Lc); break;
+    HB_FFT_SIZES(HB_C)
+#undef HB_C
+    default: k_fft_c_fwd<0><<<gc, 256, sc, s>>>(rho, grid, twc, q.pc, nrows, q.nch, q.Lc);
+  }
+  switch (q.nb) {
+#define HB_B(NN) case NN: k_fft_b<NN, false><<<gb, 256, sb, s>>>(grid, twb, q.pb, q.nb, q.nch, q.Lb); break;
+    HB_FFT_SIZES(HB_B)
+#undef HB_B
+    default: k_fft_b<0, false><<<gb, 256, sb, s>>>(grid, twb, q.pb, q.nb, q.nch, q.Lb);
+  }
+  switch (q.na) {
+#define HB_A(NN) case NN: k_fft_a_conv<NN><<<ga, 256, sa, s>>>(grid, twa, q.pa, q.na, q.nb, q.nc, q.nch, q.La, box, bfac, alpha, part); break;
+    HB_FFT_SIZES(HB_A)
+#undef HB_A
+    default: k_fft_a_conv<0><<<ga, 256, sa, s>>>(grid, twa, q.pa, q.na, q.nb, q.nc, q.nch, q.La, box, bfac, alpha, part);
+  }
+  switch (q.nb) {
+#define HB_B(NN) case NN: k_fft_b<NN, true><<<gb, 256, sb, s>>>(grid, twb, q.pb, q.nb, q.nch, q.Lb); break;
+    HB_FFT_SIZES(HB_B)
+#undef HB_B
+    default: k_fft_b<0, true><<<gb, 256, sb, s>>>(grid, twb, q.pb, q.nb, q.nch, q.Lb);
+  }
+  switch (q.nc) {
+#define HB_C(NN) case NN: k_fft_c_inv<NN><<<gc, 256, sc, s>>>(grid, v, twc, q.pc, nrows, q.nch, q.Lc); break;
+    HB_FFT_SIZES(HB_C)
+#undef HB_C
+    default: k_fft_c_inv<0><<<gc, 256, sc, s>>>(grid, v, twc, q.pc, nrows, q.nch, q.Lc);
+  }
+}
+
 }  // namespace
 
 int spme_setup(hb_forcefield *ff, const hb_forcefield_desc *d) {
@@ -583,12 +774,7 @@ int spme_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
   if (!S.on) return HB_OK;
   hb_system *sys = ff->sys;
   const uint32_t n = sys->n;
-  const int na = S.na, nb = S.nb, nc = S.nc, nch = S.nch;
-  FftPlan pa, pb, pc;
-  make_plan(na, pa);
-  make_plan(nb, pb);
-  make_plan(nc, pc);
-  const float2 *twa = S.d_tw, *twb = S.d_tw + na, *twc = S.d_tw + na + nb;
+  const int na = S.na, nb = S.nb, nc = S.nc;
   if (n > 0) {
     const uint64_t th = (uint64_t)n * S.order;
     switch (S.order) {
@@ -600,14 +786,8 @@ int spme_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
       default: return hb_fail(HB_ERR_INVALID_ARGUMENT, "spline order must be 4..8");
     }
   }
-  const int Lc = lines_per_cta(nc), Lb = lines_per_cta(nb), La = lines_per_cta(na);
-  const int nrows = na * nb;
-  k_fft_c_fwd<<<hb_div_up(nrows, Lc), 256, fft_smem(nc, Lc), s>>>(S.d_rho_fixed, S.d_grid, twc, pc, nrows, nch, Lc);
-  k_fft_b<false><<<na * ((nch + Lb - 1) / Lb), 256, fft_smem(nb, Lb), s>>>(S.d_grid, twb, pb, nb, nch, Lb);
-  k_fft_a_conv<<<nb * ((nch + La - 1) / La), 256, fft_smem(na, La), s>>>(
-      S.d_grid, twa, pa, na, nb, nc, nch, La, sys->d_box, S.d_bfac, S.alpha, S.d_part);
-  k_fft_b<true><<<na * ((nch + Lb - 1) / Lb), 256, fft_smem(nb, Lb), s>>>(S.d_grid, twb, pb, nb, nch, Lb);
-  k_fft_c_inv<<<hb_div_up(nrows, Lc), 256, fft_smem(nc, Lc), s>>>(S.d_grid, S.d_v, twc, pc, nrows, nch, Lc);
+  fft_passes(spme_plan(na, nb, nc), S.d_rho_fixed, S.d_grid, S.d_v, S.d_tw, sys->d_box, S.d_bfac,
+             S.alpha, S.d_part, s);
   if (n > 0) {
     switch (S.order) {
       case 4: k_gather<4><<<hb_div_up(n, 128), 128, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
@@ -784,13 +964,7 @@ extern "C" int hb_spme_recip_noalloc(const float *posq, uint32_t n, const double
       default: k_spread<8><<<hb_div_up(th, 256), 256, 0, s>>>(pq, dbox, na, nb, nc, rho, n); break;
     }
   }
-  const int nrows = na * nb;
-  k_fft_c_fwd<<<hb_div_up(nrows, Lc), 256, fft_smem(nc, Lc), s>>>(rho, cgrid, tw + na + nb, pc, nrows, nch, Lc);
-  k_fft_b<false><<<na * ((nch + Lb - 1) / Lb), 256, fft_smem(nb, Lb), s>>>(cgrid, tw + na, pb, nb, nch, Lb);
-  k_fft_a_conv<<<n_part, 256, fft_smem(na, La), s>>>(cgrid, tw, pa, na, nb, nc, nch, La, dbox, bfac,
-                                                     (float)alpha, part);
-  k_fft_b<true><<<na * ((nch + Lb - 1) / Lb), 256, fft_smem(nb, Lb), s>>>(cgrid, tw + na, pb, nb, nch, Lb);
-  k_fft_c_inv<<<hb_div_up(nrows, Lc), 256, fft_smem(nc, Lc), s>>>(cgrid, v, tw + na + nb, pc, nrows, nch, Lc);
+  fft_passes(spme_plan(na, nb, nc), rho, cgrid, v, tw, dbox, bfac, (float)alpha, part, s);
   if (n > 0) {
     switch (order) {
       case 4: k_gather<4><<<hb_div_up(n, 128), 128, 0, s>>>(pq, v, dbox, na, nb, nc, self_pref, o, n); break;
