@@ -395,10 +395,12 @@ class Integrator:
     def step_graph(self, ff: ForceField, cons: Constraints | None = None, n_steps: int = 1) -> None:
         N.check(self.lib.hb_integrator_step_graph(self.h, ff.h, cons.h if cons else None, int(n_steps)))
 
-    def count_launches(self, ff: ForceField, cons: Constraints | None = None) -> int:
-        out = C.c_uint64(0)
-        N.check(self.lib.hb_integrator_count_launches(self.h, ff.h, cons.h if cons else None, C.byref(out)))
-        return int(out.value)
+    def count_launches(self, ff: ForceField, cons: Constraints | None = None) -> tuple:
+        """(kernels every step, kernels of one neighbour rebuild)."""
+        out = np.zeros(2, dtype=np.uint64)
+        N.check(self.lib.hb_integrator_count_launches(self.h, ff.h, cons.h if cons else None,
+                                                      out.ctypes.data_as(N.PU64)))
+        return int(out[0]), int(out[1])
 
     def close(self) -> None:
         if getattr(self, "h", None):

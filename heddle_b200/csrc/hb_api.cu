@@ -49,6 +49,7 @@ extern "C" int hb_context_create(int device_ordinal, hb_context **out) {
   c->n_sm = prop.multiProcessorCount;
   HB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   HB_CUDA(cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking));
+  HB_CUDA(cudaStreamCreateWithFlags(&c->stream3, cudaStreamNonBlocking));
   HB_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
   HB_CUDA(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
   *out = c;
@@ -65,6 +66,7 @@ extern "C" int hb_context_destroy(hb_context *ctx) {
   cudaEventDestroy(ctx->ev_join);
   cudaStreamDestroy(ctx->stream);
   cudaStreamDestroy(ctx->stream2);
+  cudaStreamDestroy(ctx->stream3);
   delete ctx;
   return HB_OK;
 }
@@ -501,12 +503,13 @@ extern "C" int hb_forcefield_create(hb_system *sys, const hb_forcefield_desc *d,
 
 // ForceField::step body: gated neighbour rebuild, pair kernel on the main
 // stream overlapped with the SPME chain on the second stream, combine.
-static int force_eval(hb_forcefield *ff, bool ev) {
+static int force_eval(hb_forcefield *ff, bool ev, bool capturing = false) {
   hb_context *ctx = ff->sys->ctx;
   cudaStream_t s = ctx->stream, s2 = ctx->stream2;
   cudaEvent_t t0 = stage_begin(s);
   HB_TRY(nl_displacement_check(ff, s));
-  HB_TRY(nl_rebuild(ff, true, s));
+  if (capturing) HB_TRY(nl_rebuild_conditional(ff, s));
+  else HB_TRY(nl_rebuild(ff, true, s));
   HB_TRY(nl_gather_positions(ff, s));
   stage_end(3, t0, s);
   if (ff->spme.on) {
@@ -779,13 +782,23 @@ extern "C" int hb_integrator_create(hb_system *sys, const hb_integrator_desc *d,
   it->temperature = d->temperature;
   it->seed = d->seed;
   it->step = d->step0;
+  if (cudaMalloc(&it->d_step, sizeof(uint64_t)) != cudaSuccess ||
+      cudaMemcpy(it->d_step, &it->step, sizeof(uint64_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaEventCreate(&it->g_ev0) != cudaSuccess || cudaEventCreate(&it->g_ev1) != cudaSuccess) {
+    hb_integrator_destroy(it);
+    return hb_fail(HB_ERR_CUDA, "integrator state allocation failed");
+  }
   *out = it;
   return HB_OK;
 }
 
 extern "C" int hb_integrator_destroy(hb_integrator *it) {
   if (!it) return HB_OK;
+  cudaStreamSynchronize(it->sys->ctx->stream);
   if (it->graph_exec) cudaGraphExecDestroy(it->graph_exec);
+  cudaFree(it->d_step);
+  if (it->g_ev0) cudaEventDestroy(it->g_ev0);
+  if (it->g_ev1) cudaEventDestroy(it->g_ev1);
   delete it;
   return HB_OK;
 }
@@ -796,7 +809,8 @@ extern "C" int hb_integrator_destroy(hb_integrator *it) {
 // forces, velocity projection, final half kick.  Langevin (middle scheme):
 // full kick, velocity projection, half drift, O, half drift, position
 // constraint, forces.
-static int one_step(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons, bool ev) {
+static int one_step(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons, bool ev,
+                    bool capturing = false) {
   cudaStream_t s = it->sys->ctx->stream;
   cudaEvent_t t4 = stage_begin(s);
   if (it->kind == HB_INTEGRATOR_LANGEVIN) {
@@ -805,12 +819,12 @@ static int one_step(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons, 
     HB_TRY(integ_lang_drift_ou(it, s));
     if (cons) HB_TRY(cons_positions(cons, it->dt, s));
     stage_end(4, t4, s);
-    HB_TRY(force_eval(ff, ev));
+    HB_TRY(force_eval(ff, ev, capturing));
   } else {
     HB_TRY(integ_vv_kick_drift(it, s));
     if (cons) HB_TRY(cons_positions(cons, it->dt, s));
     stage_end(4, t4, s);
-    HB_TRY(force_eval(ff, ev));
+    HB_TRY(force_eval(ff, ev, capturing));
     cudaEvent_t t5 = stage_begin(s);
     if (cons) HB_TRY(cons_velocities(cons, it->dt, true, s));
     HB_TRY(integ_vv_kick(it, s));
@@ -858,16 +872,13 @@ extern "C" int hb_integrator_step(hb_integrator *it, hb_forcefield *ff, hb_const
 extern "C" int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
                                         hb_constraints *cons, uint32_t n_steps) {
   HB_REQUIRE(it && ff, HB_ERR_INVALID_ARGUMENT, "null argument");
+  HB_REQUIRE(ff->sys == it->sys && (!cons || cons->sys == it->sys), HB_ERR_INVALID_ARGUMENT,
+             "integrator, force field and constraints must share one system");
   hb_context *ctx = it->sys->ctx;
   cudaStream_t s = ctx->stream;
   if (!it->forces_valid) {
     HB_TRY(force_eval(ff, false));
     it->forces_valid = true;
-  }
-  if (it->kind == HB_INTEGRATOR_LANGEVIN) {
-    // the Philox step counter is a kernel argument; per-step graphs would
-    // freeze it, so the stochastic integrator runs eagerly
-    return hb_integrator_step(it, ff, cons, n_steps, 0);
   }
   if (!it->graph_exec || it->graph_ff != ff || it->graph_cons != cons) {
     if (it->graph_exec) cudaGraphExecDestroy(it->graph_exec);
@@ -875,8 +886,9 @@ extern "C" int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
     HB_CUDA(cudaStreamSynchronize(s));
     cudaGraph_t g;
     HB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    int rc = one_step(it, ff, cons, false);
-    it->step--;
+    const uint64_t step = it->step;
+    int rc = one_step(it, ff, cons, false, true);
+    it->step = step;
     cudaError_t ce = cudaStreamEndCapture(s, &g);
     if (rc != HB_OK) return rc;
     if (ce != cudaSuccess) return hb_fail(HB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
@@ -885,9 +897,18 @@ extern "C" int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
     it->graph_ff = ff;
     it->graph_cons = cons;
   }
+  if (ctx->timing) HB_CUDA(cudaEventRecord(it->g_ev0, s));
   for (uint32_t k = 0; k < n_steps; ++k) {
     HB_CUDA(cudaGraphLaunch(it->graph_exec, s));
     it->step++;
+  }
+  if (ctx->timing) {
+    HB_CUDA(cudaEventRecord(it->g_ev1, s));
+    HB_CUDA(cudaEventSynchronize(it->g_ev1));
+    float ms = 0.f;
+    HB_CUDA(cudaEventElapsedTime(&ms, it->g_ev0, it->g_ev1));
+    for (int q = 0; q < 8; ++q) ctx->t_ms[q] = 0.0;
+    ctx->t_ms[0] = ms;
   }
   const uint64_t cap_before = ff->entry_cap;
   HB_TRY(check_status(ff));
@@ -899,31 +920,43 @@ extern "C" int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
   return HB_OK;
 }
 
+static int count_kernel_nodes(cudaGraph_t g, uint64_t &kernels) {
+  size_t nn = 0;
+  HB_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  if (nn) HB_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    HB_CUDA(cudaGraphNodeGetType(nd, &t));
+    if (t == cudaGraphNodeTypeKernel) ++kernels;
+  }
+  return HB_OK;
+}
+
 extern "C" int hb_integrator_count_launches(hb_integrator *it, hb_forcefield *ff,
                                             hb_constraints *cons, uint64_t *kernels) {
   HB_REQUIRE(it && ff && kernels, HB_ERR_INVALID_ARGUMENT, "null argument");
   cudaStream_t s = it->sys->ctx->stream;
   HB_CUDA(cudaStreamSynchronize(s));
+  // capture the eager launch sequence (rebuild kernels gated, no
+  // conditional node) and count its kernel nodes
   cudaGraph_t g;
   HB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   const uint64_t step = it->step;
-  int rc = one_step(it, ff, cons, false);
+  int rc = one_step(it, ff, cons, false, false);
   it->step = step;
   cudaError_t ce = cudaStreamEndCapture(s, &g);
   if (rc != HB_OK) return rc;
   if (ce != cudaSuccess) return hb_fail(HB_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(ce));
-  size_t nn = 0;
-  HB_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
-  std::vector<cudaGraphNode_t> nodes(nn);
-  if (nn) HB_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
-  uint64_t k = 0;
-  for (auto nd : nodes) {
-    cudaGraphNodeType t;
-    HB_CUDA(cudaGraphNodeGetType(nd, &t));
-    if (t == cudaGraphNodeTypeKernel) ++k;
-  }
+  uint64_t eager = 0;
+  rc = count_kernel_nodes(g, eager);
   cudaGraphDestroy(g);
-  *kernels = k;
+  if (rc != HB_OK) return rc;
+  // in the graph form the gated rebuild kernels move into the IF node's
+  // body and one kernel sets the condition
+  const uint64_t body = ff->sys->n ? (uint64_t)nl_kernel_count() : 0u;
+  kernels[0] = eager - body + (body ? 1u : 0u);
+  kernels[1] = body;
   return HB_OK;
 }
 

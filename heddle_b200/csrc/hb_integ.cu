@@ -234,9 +234,11 @@ __global__ void k_lang_kick(float4 *__restrict__ vel, const float4 *__restrict__
 __global__ void k_lang_drift_ou(float4 *__restrict__ posq, float4 *__restrict__ vel,
                                 int4 *__restrict__ image, float4 *__restrict__ prev,
                                 const DBox *__restrict__ box, float dt, float a, float kt,
-                                uint32_t s_lo, uint32_t s_hi, uint64_t step, uint32_t n) {
+                                uint32_t s_lo, uint32_t s_hi, const uint64_t *__restrict__ step_ptr,
+                                uint32_t n) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const uint64_t step = *step_ptr;
   const DBox b = *box;
   float4 p = posq[i];
   float4 v = vel[i];
@@ -262,6 +264,10 @@ __global__ void k_lang_drift_ou(float4 *__restrict__ posq, float4 *__restrict__ 
   posq[i] = p;
   vel[i] = v;
 }
+
+// the Philox draw counter lives on the device so a captured step advances
+// it on every replay
+__global__ void k_step_inc(uint64_t *step) { *step += 1ull; }
 
 #define RED_BLOCKS 296
 // kinetic energy and momentum, FP64, fixed grid and fixed tree shape
@@ -380,7 +386,8 @@ int integ_lang_drift_ou(hb_integrator *it, cudaStream_t s) {
   const float a = (float)std::exp(-it->friction * it->dt);
   k_lang_drift_ou<<<hb_div_up(sys->n, 256), 256, 0, s>>>(
       sys->d_posq, sys->d_vel, sys->d_image, sys->d_pos_prev, sys->d_box, (float)it->dt, a,
-      (float)it->temperature, (uint32_t)it->seed, (uint32_t)(it->seed >> 32), it->step, sys->n);
+      (float)it->temperature, (uint32_t)it->seed, (uint32_t)(it->seed >> 32), it->d_step, sys->n);
+  k_step_inc<<<1, 1, 0, s>>>(it->d_step);
   HB_CUDA(cudaGetLastError());
   return HB_OK;
 }

@@ -122,6 +122,7 @@ struct hb_context {
   int n_sm = 148;
   cudaStream_t stream = nullptr;    // main stream
   cudaStream_t stream2 = nullptr;   // SPME runs here, overlapping the pair kernel
+  cudaStream_t stream3 = nullptr;   // captures the bodies of conditional graph nodes
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool timing = false;
   // stage timers (accumulated over the last hb_integrator_step call)
@@ -245,9 +246,11 @@ struct hb_integrator {
   int kind = HB_INTEGRATOR_VV;
   double dt = 0.0, friction = 0.0, temperature = 0.0;
   uint64_t seed = 0, step = 0;
+  uint64_t *d_step = nullptr;   // Philox draw counter read by the O step
   bool forces_valid = false;
   // graph mode
   cudaGraphExec_t graph_exec = nullptr;
+  cudaEvent_t g_ev0 = nullptr, g_ev1 = nullptr;
   hb_forcefield *graph_ff = nullptr;
   hb_constraints *graph_cons = nullptr;
 };
@@ -261,6 +264,9 @@ int nl_free(hb_forcefield *ff);
 // Rebuild the list.  gated: kernels run only when the status word has the
 // displacement bit set (a device-side decision, no host read).
 int nl_rebuild(hb_forcefield *ff, bool gated, cudaStream_t s);
+int nl_kernel_count();
+// During stream capture: the rebuild as a device-side conditional graph node.
+int nl_rebuild_conditional(hb_forcefield *ff, cudaStream_t s);
 int nl_displacement_check(hb_forcefield *ff, cudaStream_t s);
 int nl_gather_positions(hb_forcefield *ff, cudaStream_t s);
 int nl_first_build(hb_forcefield *ff);

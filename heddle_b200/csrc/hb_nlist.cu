@@ -608,6 +608,10 @@ static int nl_launch(hb_forcefield *ff, const uint32_t *gate, cudaStream_t s, bo
   return HB_OK;
 }
 
+// kernels launched by one rebuild: voxel histogram, three scan kernels,
+// scatter, voxel sort, tile fill, tile boxes, tile build, finish
+int nl_kernel_count() { return 10; }
+
 int nl_rebuild(hb_forcefield *ff, bool gated, cudaStream_t s) {
   if (ff->sys->n == 0) return HB_OK;
   const uint32_t *gate = gated ? ff->d_status : nullptr;
@@ -673,6 +677,49 @@ int nl_first_build(hb_forcefield *ff) {
   HB_CUDA(cudaMemcpyAsync(ff->d_status, &st, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
   HB_CUDA(cudaStreamSynchronize(s));
   ff->built = true;
+  return HB_OK;
+}
+
+namespace {
+__global__ void k_set_rebuild_condition(cudaGraphConditionalHandle h, const uint32_t *status) {
+  cudaGraphSetConditional(h, ((*status) & HB_ST_DISPLACED) ? 1u : 0u);
+}
+}  // namespace
+
+// Inside a stream capture: the rebuild becomes an IF node of the graph
+// being captured, taken when the displacement bit is set.  The body (the
+// ungated rebuild sequence) is captured on the context's side stream.
+int nl_rebuild_conditional(hb_forcefield *ff, cudaStream_t s) {
+  if (ff->sys->n == 0) return HB_OK;
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  HB_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd));
+  if (st != cudaStreamCaptureStatusActive)
+    return hb_fail(HB_ERR_INVALID_ARGUMENT, "conditional rebuild needs an active capture");
+  cudaGraphConditionalHandle h;
+  HB_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+  k_set_rebuild_condition<<<1, 1, 0, s>>>(h, ff->d_status);
+  HB_CUDA(cudaGetLastError());
+  HB_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  HB_CUDA(cudaGraphAddNode(&node, g, deps, nd, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  cudaStream_t side = ff->sys->ctx->stream3;
+  HB_CUDA(cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal));
+  int rc = nl_launch(ff, nullptr, side, true, false);
+  cudaGraph_t out;
+  cudaError_t ce = cudaStreamEndCapture(side, &out);
+  if (rc != HB_OK) return rc;
+  if (ce != cudaSuccess) return hb_fail(HB_ERR_CUDA, std::string("rebuild body capture: ") + cudaGetErrorString(ce));
+  HB_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
   return HB_OK;
 }
 

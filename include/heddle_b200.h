@@ -212,13 +212,16 @@ int hb_integrator_step(hb_integrator *it, hb_forcefield *ff,
                        hb_constraints *cons, uint32_t n_steps,
                        uint32_t scalar_every);
 /* Same as hb_integrator_step, launched as CUDA graphs of one step each
- * (captured on first use; the neighbour rebuild runs as a device-side
- * conditional node). */
+ * (captured on first use; the neighbour rebuild is a device-side IF node
+ * taken when an atom moved more than r_skin / 2; the Langevin draw counter
+ * lives on the device, so replays draw fresh noise). */
 int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
                              hb_constraints *cons, uint32_t n_steps);
 
 /* Kernel launches of one step: the step is captured into a throwaway CUDA
- * graph (nothing runs) and its kernel nodes are counted (*kernels). */
+ * graph (nothing runs) and its kernel nodes are counted: kernels[0] = the
+ * kernels every step launches, kernels[1] = the kernels of a neighbour
+ * rebuild (a conditional node taken only on rebuild steps). */
 int hb_integrator_count_launches(hb_integrator *it, hb_forcefield *ff,
                                  hb_constraints *cons, uint64_t *kernels);
 

@@ -135,6 +135,27 @@ def test_graph_replay_equals_eager(ctx):
     close(it_a, cons_a, ff_a, sys_a, it_b, cons_b, ff_b, sys_b)
 
 
+def test_langevin_graph_replay_equals_eager(ctx):
+    # the Philox draw counter lives on the device, so graph replays draw
+    # the same noise as eager launches, and the rebuild condition is the
+    # same device-side decision
+    spec = S.spc_water(512, skin_A=0.5)
+    sa, fa, ca, ia = make(ctx, spec, kind="langevin-baoab", seed=77)
+    ia.step(fa, ca, n_steps=15)
+    st_a = sa.state()
+    rb_a = fa.stats()["rebuilds"]
+    sb, fb, cb, ib = make(ctx, spec, kind="langevin-baoab", seed=77)
+    ib.step_graph(fb, cb, n_steps=15)
+    st_b = sb.state()
+    rb_b = fb.stats()["rebuilds"]
+    assert rb_a == rb_b and rb_a > 1
+    for a, b in zip(st_a, st_b):
+        assert np.array_equal(a, b)
+    top, body = ib.count_launches(fb, cb)
+    assert top > 10 and body > 5
+    close(ia, ca, fa, sa, ib, cb, fb, sb)
+
+
 def test_neighbor_rebuilds_happen_on_device(ctx):
     spec = S.spc_water(512, skin_A=0.5)
     sys_, ff, cons, it = make(ctx, spec)
