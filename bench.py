@@ -55,6 +55,9 @@ def parse():
                    help="untimed Langevin steps (friction 50/ps) that relax the lattice start")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--tune", type=int, default=1, help="autotune the neighbour-list skin (1/0)")
+    p.add_argument("--graphs", type=int, default=1,
+                   help="1: CUDA-graph steps (headline); 0: eager launches (for profilers, which "
+                        "cannot see kernels inside graphs with conditional nodes)")
     return p.parse_args()
 
 
@@ -217,12 +220,12 @@ def run_ours(args):
     ff0 = hb.ForceField.from_spec(sys_, spec)
     eq = hb.Integrator(sys_, "langevin-baoab", spec.dt, friction=50.0 / (1.0e-12 / U.AUT_S),
                        temperature=spec.temperature, seed=99 + rank)
-    eq.step_graph(ff0, cons, n_steps=args.equilibrate)
+    (eq.step_graph if args.graphs else eq.step)(ff0, cons, n_steps=args.equilibrate)
     eq.close()
     ff0.close()
     # skin autotuning on the relaxed system (untimed)
     tune = None
-    if args.tune:
+    if args.tune and args.graphs:
         from heddle_b200.autotune import tune_skin
 
         tune = tune_skin(ctx, sys_, spec, cons, lang)
@@ -231,7 +234,8 @@ def run_ours(args):
     ff = hb.ForceField.from_spec(sys_, spec)
     it = hb.Integrator(sys_, **lang)
     per_step_kernels, rebuild_kernels = it.count_launches(ff, cons)
-    it.step_graph(ff, cons, n_steps=max(3, args.warmup))
+    run = it.step_graph if args.graphs else it.step
+    run(ff, cons, n_steps=max(3, args.warmup))
     ctx.synchronize()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
 
@@ -253,7 +257,7 @@ def run_ours(args):
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
-            it.step_graph(ff, cons, n_steps=1)
+            run(ff, cons, n_steps=1)
             t_ms += float(ctx.timings()[0])
     ctx.synchronize()
     torch.cuda.synchronize()
@@ -276,7 +280,7 @@ def run_ours(args):
     t0 = time.perf_counter()
     for _ in range(k2):
         sys_.set_state(pos_h, vel_h)
-        it.step_graph(ff, cons, n_steps=1)
+        run(ff, cons, n_steps=1)
         pos_h, vel_h, _, _ = sys_.state()
     t_e2e = time.perf_counter() - t0
     if dist is not None:
@@ -315,7 +319,8 @@ def run_ours(args):
             "neighbour": {"tiles": stats["tiles"], "entries": stats["entries"],
                           "rebuilds_in_timed_steps": rebuilds, "skin_A": args.skin,
                           "skin_autotune": tune},
-            "launch_mode": "CUDA graph per step; neighbour rebuild = device-side conditional node",
+            "launch_mode": ("CUDA graph per step; neighbour rebuild = device-side conditional node"
+                            if args.graphs else "eager launches"),
             "roofline": {"bound": "hbm", "kernel": "k_pair (LJ + erfc pair kernel)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,

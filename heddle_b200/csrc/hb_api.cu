@@ -5,6 +5,7 @@
 // stream, force combine).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <set>
 #include <string>
@@ -464,6 +465,11 @@ extern "C" int hb_forcefield_create(hb_system *sys, const hb_forcefield_desc *d,
   hb_forcefield *ff = new hb_forcefield();
   *ff = tmp;
   ff->sys = sys;
+  // pair kernel: the rotation sweep by default; HB_PAIR_KERNEL=compact selects
+  // the compacted pair-list form (shared-memory int64 atomics)
+  ff->pair_variant = 1;
+  if (const char *pk = std::getenv("HB_PAIR_KERNEL"))
+    ff->pair_variant = std::string(pk) == "compact" ? 0 : 1;
   HB_CUDA(cudaSetDevice(sys->ctx->device));
   HB_CUDA(cudaMalloc(&ff->d_lj, sizeof(float4) * ff->h_lj.size()));
   HB_CUDA(cudaMemcpy(ff->d_lj, ff->h_lj.data(), sizeof(float4) * ff->h_lj.size(),

@@ -63,6 +63,10 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, 8)
            const uint32_t *__restrict__ sorted_ids, const uint32_t *__restrict__ eoff,
            const uint32_t *__restrict__ epart, const float2 *__restrict__ escale) {
   extern __shared__ float4 sm_lj[];
+  // per warp: the current entry's j positions / charges and types, read by
+  // lane l at rotation t from slot (l + t) mod 32 (conflict-free)
+  __shared__ float4 sm_jp[PAIR_WARPS][32];
+  __shared__ int sm_jt[PAIR_WARPS][32];
   const int nt2 = P.n_types * P.n_types;
   for (int k = threadIdx.x; k < nt2; k += blockDim.x) sm_lj[k] = lj_table[k];
   __syncthreads();
@@ -101,27 +105,26 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, 8)
     const bool jvalid = sj != HB_SENTINEL;
     float4 pj;
     int tj = 0;
-    uint32_t oj = 0u;
+    uint32_t oj = 0u, oj_home = 0u;
     if (jvalid) {
       pj = tile_posq[sj];
       tj = tile_type[sj];
       if (spc) shift_to(pj.x, pj.y, pj.z, c, b);
-      if (SCALED) oj = sorted_ids[sj];
+      if (SCALED) oj_home = sorted_ids[sj];
     } else {
       pj = make_float4(1.0e18f, 1.0e18f, 1.0e18f, 0.0f);
     }
     float fix = 0.f, fiy = 0.f, fiz = 0.f, fie = 0.f, fiw = 0.f;
     float fjx = 0.f, fjy = 0.f, fjz = 0.f, fje = 0.f, fjw = 0.f;
     float elj = 0.0f;
+    __syncwarp();
+    sm_jp[w][lane] = pj;
+    sm_jt[w][lane] = tj;
+    __syncwarp();
 
 #define HB_ROTATE()                                                   \
   {                                                                   \
     const int src = (lane + 1u) & 31u;                                \
-    pj.x = __shfl_sync(0xFFFFFFFFu, pj.x, src);                       \
-    pj.y = __shfl_sync(0xFFFFFFFFu, pj.y, src);                       \
-    pj.z = __shfl_sync(0xFFFFFFFFu, pj.z, src);                       \
-    pj.w = __shfl_sync(0xFFFFFFFFu, pj.w, src);                       \
-    tj = __shfl_sync(0xFFFFFFFFu, tj, src);                           \
     fjx = __shfl_sync(0xFFFFFFFFu, fjx, src);                         \
     fjy = __shfl_sync(0xFFFFFFFFu, fjy, src);                         \
     fjz = __shfl_sync(0xFFFFFFFFu, fjz, src);                         \
@@ -129,7 +132,6 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, 8)
       fje = __shfl_sync(0xFFFFFFFFu, fje, src);                       \
       fjw = __shfl_sync(0xFFFFFFFFu, fjw, src);                       \
     }                                                                 \
-    if (SCALED) oj = __shfl_sync(0xFFFFFFFFu, oj, src);               \
   }
 
     uint32_t t0 = 0u, t1 = 32u;
@@ -139,6 +141,12 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, 8)
       t1 = 17u;
     }
     for (uint32_t t = t0; t < t1; ++t) {
+      {
+        const uint32_t jl = (lane + t) & 31u;
+        pj = sm_jp[w][jl];
+        tj = sm_jt[w][jl];
+        if (SCALED) oj = __shfl_sync(0xFFFFFFFFu, oj_home, jl);
+      }
       float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
       if (!spc) hb_min_image(dx, dy, dz, b);
       const float r2 = dx * dx + dy * dy + dz * dz;
@@ -278,6 +286,232 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, 8)
 #undef HB_ROTATE
 }
 
+// ---------------------------------------------------------------------
+// Compacted form.  Per entry: (1) a distance pass, one lane per i-atom over
+// the 32 rotations, leaves a 32-bit mask of rotations whose pair is within
+// the cutoff; (2) the active pairs are listed in shared memory slot-major
+// (every lane's first active pair, then every lane's second, ...) so that
+// consecutive pairs belong to different i-atoms; (3) a math pass evaluates
+// only listed pairs with all 32 lanes busy, and adds the pair force to the
+// i and j accumulators in shared memory as int64 fixed point (atomic,
+// order-independent, so repeat runs stay byte-identical).
+// ---------------------------------------------------------------------
+#define P2_WARPS 4
+
+struct P2Warp {
+  float4 ipos[32];
+  float4 jpos[32];
+  int itype[32];
+  int jtype[32];
+  uint32_t oi[32];
+  uint32_t oj[32];
+  uint32_t xm[32];
+  unsigned long long fi[5][32];
+  unsigned long long fj[5][32];
+  uint16_t pairs[1024];
+};
+
+template <bool EV, bool SCALED, bool SWITCH>
+__global__ void __launch_bounds__(P2_WARPS * 32)
+    k_pair2(const float4 *__restrict__ tile_posq, const int *__restrict__ tile_type,
+            const float4 *__restrict__ center, const uint32_t *__restrict__ tile_nent,
+            const uint32_t *__restrict__ entry_j, const uint32_t *__restrict__ entry_excl,
+            const DBox *__restrict__ box, const float4 *__restrict__ lj_table, PairParams P,
+            unsigned long long *__restrict__ fp, unsigned long long *__restrict__ e_lj_total,
+            const uint32_t *__restrict__ sorted_ids, const uint32_t *__restrict__ eoff,
+            const uint32_t *__restrict__ epart, const float2 *__restrict__ escale) {
+  extern __shared__ float4 sm_lj2[];
+  __shared__ P2Warp smw[P2_WARPS];
+  const int nt2 = P.n_types * P.n_types;
+  for (int k = threadIdx.x; k < nt2; k += blockDim.x) sm_lj2[k] = lj_table[k];
+  __syncthreads();
+  const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t I = blockIdx.x * P2_WARPS + w;
+  if (I >= P.n_tiles) return;
+  P2Warp &S = smw[w];
+  constexpr int NC = EV ? 5 : 3;
+  const DBox b = *box;
+  const float4 c = center[I];
+  const bool spc = ((int)c.w & 1) != 0;
+  const uint32_t si = I * 32u + lane;
+  const bool ivalid = si < P.n;
+  float4 pi = tile_posq[si];
+  if (ivalid) {
+    if (spc) shift_to(pi.x, pi.y, pi.z, c, b);
+  } else {
+    pi = make_float4(-1.0e18f, -1.0e18f, -1.0e18f, 0.0f);
+  }
+  S.ipos[lane] = pi;
+  S.itype[lane] = ivalid ? tile_type[si] : 0;
+  if (SCALED) S.oi[lane] = ivalid ? sorted_ids[si] : HB_SENTINEL;
+#pragma unroll
+  for (int q = 0; q < NC; ++q) S.fi[q][lane] = 0ull;
+  float elj = 0.0f;
+  const uint32_t e0 = I * P.slab;
+  const uint32_t e1 = e0 + min(tile_nent[I], P.slab);
+  const bool has_self = P.n - I * 32u >= 2u;
+  const uint32_t lt = (1u << lane) - 1u;
+
+  for (uint32_t e = e0; e < e1; ++e) {
+    const bool self = has_self && (e == e0);
+    const uint32_t sj = entry_j[(uint64_t)e * 32u + lane];
+    const uint32_t xm = entry_excl[(uint64_t)e * 32u + lane];
+    const bool jvalid = sj != HB_SENTINEL;
+    float4 pj;
+    if (jvalid) {
+      pj = tile_posq[sj];
+      if (spc) shift_to(pj.x, pj.y, pj.z, c, b);
+    } else {
+      pj = make_float4(1.0e18f, 1.0e18f, 1.0e18f, 0.0f);
+    }
+    S.jpos[lane] = pj;
+    S.jtype[lane] = jvalid ? tile_type[sj] : 0;
+    if (SCALED) {
+      S.oj[lane] = jvalid ? sorted_ids[sj] : HB_SENTINEL;
+      S.xm[lane] = xm;
+    }
+#pragma unroll
+    for (int q = 0; q < NC; ++q) S.fj[q][lane] = 0ull;
+    __syncwarp();
+
+    // (1) distance pass
+    uint32_t mask = 0u;
+    const int t0 = self ? 1 : 0, t1 = self ? 16 : 31;
+    for (int t = t0; t <= t1; ++t) {
+      const float4 q = S.jpos[(lane + t) & 31u];
+      float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
+      if (!spc) hb_min_image(dx, dy, dz, b);
+      const float r2 = dx * dx + dy * dy + dz * dz;
+      bool act = r2 < P.rc2_max && (SCALED || !((xm >> t) & 1u));
+      if (self && t == 16 && lane >= 16u) act = false;
+      mask |= (act ? 1u : 0u) << t;
+    }
+    // (2) slot-major pair list
+    const uint32_t maxcnt = __reduce_max_sync(0xFFFFFFFFu, (uint32_t)__popc(mask));
+    uint32_t np = 0, m = mask;
+    for (uint32_t slot = 0; slot < maxcnt; ++slot) {
+      const bool has = m != 0u;
+      const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
+      if (has) {
+        const uint32_t t = (uint32_t)__ffs(m) - 1u;
+        m &= m - 1u;
+        S.pairs[np + __popc(bal & lt)] = (uint16_t)((lane << 8) | t);
+      }
+      np += __popc(bal);
+    }
+    __syncwarp();
+    // (3) math pass over the listed pairs
+    for (uint32_t k = lane; k < np; k += 32u) {
+      const uint32_t pr = S.pairs[k];
+      const uint32_t i = pr >> 8, t = pr & 255u, j = (i + t) & 31u;
+      const float4 a = S.ipos[i], q = S.jpos[j];
+      float dx = a.x - q.x, dy = a.y - q.y, dz = a.z - q.z;
+      if (!spc) hb_min_image(dx, dy, dz, b);
+      const float r2 = dx * dx + dy * dy + dz * dz;
+      float s_lj = 1.0f, s_c = 1.0f;
+      if (SCALED && ((S.xm[i] >> t) & 1u)) {
+        s_lj = 0.0f;
+        s_c = 0.0f;
+        const uint32_t oi = S.oi[i], oj = S.oj[j];
+        for (uint32_t z = eoff[oj]; z < eoff[oj + 1]; ++z) {
+          if (epart[z] == oi) {
+            const float2 sc = escale[z];
+            s_lj = sc.x;
+            s_c = sc.y;
+            break;
+          }
+        }
+      }
+      const float inv_r = rsqrtf(r2);
+      const float inv_r2 = inv_r * inv_r;
+      float fac = 0.0f, en = 0.0f;
+      if (P.lj_on) {
+        const float4 L = sm_lj2[S.itype[i] * P.n_types + S.jtype[j]];
+        if (r2 <= L.z && L.y != 0.0f && s_lj != 0.0f) {
+          const float sr2 = L.x * inv_r2;
+          const float sr6 = sr2 * sr2 * sr2;
+          const float sr12 = sr6 * sr6;
+          float f = L.y * inv_r2 * (2.0f * sr12 - sr6);
+          float u = (L.y * (1.0f / 6.0f)) * (sr12 - sr6);
+          if (SWITCH && r2 > L.w && L.z > L.w) {
+            const float inv_d = 1.0f / (L.z - L.w);
+            const float tau = (r2 - L.w) * inv_d;
+            const float omt = 1.0f - tau;
+            const float sw = omt * omt * (1.0f + 2.0f * tau);
+            const float chain = 12.0f * tau * omt * inv_d;
+            f = sw * f + chain * u;
+            u = sw * u;
+          }
+          fac += s_lj * f;
+          if (EV) {
+            en += s_lj * u;
+            elj += s_lj * u;
+          }
+        }
+      }
+      if (P.coul_on && r2 <= P.coul_rc2 && s_c != 0.0f) {
+        const float r = r2 * inv_r;
+        const float ar = P.alpha * r;
+        const float g = __expf(-ar * ar);
+        const float tt = __fdividef(1.0f, 1.0f + 0.3275911f * ar);
+        const float poly =
+            0.254829592f +
+            (-0.284496736f + (1.421413741f + (-1.453152027f + 1.061405429f * tt) * tt) * tt) * tt;
+        const float erfc_ar = poly * tt * g;
+        const float qq = a.w * q.w;
+        fac += s_c * qq * inv_r2 * (erfc_ar * inv_r + P.c2a * g);
+        if (EV) en += s_c * qq * erfc_ar * inv_r;
+      }
+      const long long fx = to_fixed(fac * dx), fy = to_fixed(fac * dy), fz = to_fixed(fac * dz);
+      atomicAdd(&S.fi[0][i], (unsigned long long)fx);
+      atomicAdd(&S.fi[1][i], (unsigned long long)fy);
+      atomicAdd(&S.fi[2][i], (unsigned long long)fz);
+      atomicAdd(&S.fj[0][j], (unsigned long long)(-fx));
+      atomicAdd(&S.fj[1][j], (unsigned long long)(-fy));
+      atomicAdd(&S.fj[2][j], (unsigned long long)(-fz));
+      if (EV) {
+        const long long he = to_fixed(0.5f * en), hw = to_fixed(0.5f * fac * r2);
+        atomicAdd(&S.fi[3][i], (unsigned long long)he);
+        atomicAdd(&S.fi[4][i], (unsigned long long)hw);
+        atomicAdd(&S.fj[3][j], (unsigned long long)he);
+        atomicAdd(&S.fj[4][j], (unsigned long long)hw);
+      }
+    }
+    __syncwarp();
+    if (self) {
+#pragma unroll
+      for (int q = 0; q < NC; ++q) S.fi[q][lane] += S.fj[q][lane];
+    } else if (jvalid) {
+      const size_t np_all = (size_t)P.n_tiles * 32u;
+#pragma unroll
+      for (int q = 0; q < NC; ++q) red_add(&fp[q * np_all + sj], (long long)S.fj[q][lane]);
+    }
+    __syncwarp();
+  }
+  if (ivalid) {
+    const size_t np_all = (size_t)P.n_tiles * 32u;
+#pragma unroll
+    for (int q = 0; q < NC; ++q) red_add(&fp[q * np_all + si], (long long)S.fi[q][lane]);
+  }
+  if (EV) {
+    long long v = to_fixed(elj);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    if (lane == 0) red_add(e_lj_total, v);
+  }
+}
+
+template <bool EV, bool SCALED, bool SWITCH>
+int launch2_t(hb_forcefield *ff, cudaStream_t s, const PairParams &P) {
+  size_t smem = sizeof(float4) * (size_t)P.n_types * P.n_types;
+  k_pair2<EV, SCALED, SWITCH><<<hb_div_up(P.n_tiles, P2_WARPS), P2_WARPS * 32, smem, s>>>(
+      ff->d_tile_posq, ff->d_tile_type, ff->d_tile_center, ff->d_tile_nent, ff->d_entry_j,
+      ff->d_entry_excl, ff->sys->d_box, ff->d_lj, P, ff->d_fp, ff->d_acc, ff->d_sorted_ids,
+      ff->d_excl_off, ff->d_excl_partner, ff->d_excl_scale);
+  HB_CUDA(cudaGetLastError());
+  return HB_OK;
+}
+
 template <bool EV, bool SCALED, bool SWITCH>
 int launch_t(hb_forcefield *ff, cudaStream_t s, const PairParams &P) {
   size_t smem = sizeof(float4) * (size_t)P.n_types * P.n_types;
@@ -307,6 +541,14 @@ int pair_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
   P.n_tiles = ff->n_tiles;
   P.slab = ff->slab;
   const bool sc = ff->excl_scaled != 0, sw = ff->any_switch != 0;
+  if (ff->pair_variant == 0) {
+    if (ev) {
+      if (sc) return sw ? launch2_t<true, true, true>(ff, s, P) : launch2_t<true, true, false>(ff, s, P);
+      return sw ? launch2_t<true, false, true>(ff, s, P) : launch2_t<true, false, false>(ff, s, P);
+    }
+    if (sc) return sw ? launch2_t<false, true, true>(ff, s, P) : launch2_t<false, true, false>(ff, s, P);
+    return sw ? launch2_t<false, false, true>(ff, s, P) : launch2_t<false, false, false>(ff, s, P);
+  }
   if (ev) {
     if (sc) return sw ? launch_t<true, true, true>(ff, s, P) : launch_t<true, true, false>(ff, s, P);
     return sw ? launch_t<true, false, true>(ff, s, P) : launch_t<true, false, false>(ff, s, P);
