@@ -54,6 +54,8 @@ def parse():
     p.add_argument("--equilibrate", type=int, default=300,
                    help="untimed Langevin steps (friction 50/ps) that relax the lattice start")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--barostat", type=int, default=1,
+                   help="1: NPT with the Monte-Carlo barostat at 1 bar (move every 25 steps); 0: NVT")
     p.add_argument("--tune", type=int, default=1, help="autotune the neighbour-list skin (1/0)")
     p.add_argument("--graphs", type=int, default=1,
                    help="1: CUDA-graph steps (headline); 0: eager launches (for profilers, which "
@@ -68,7 +70,8 @@ def workload_config(args, spec, world):
         "atoms": spec.n,
         "grid": list(spec.grid),
         "r_skin_A": args.skin,
-        "barostat": "none (the MC barostat of the NPT configuration is not built yet)",
+        "barostat": ("Monte-Carlo, 1 bar, a volume move every 25 steps (device-side, inside the "
+                     "step graphs)" if args.barostat else "none (NVT)"),
         "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
         "l2": "flushed between timed steps (256 MiB write, outside the timed region)",
         "start": f"lattice, relaxed by {args.equilibrate} untimed Langevin steps (50/ps)",
@@ -233,7 +236,12 @@ def run_ours(args):
     spec.r_skin = U.angstrom_au(args.skin)
     ff = hb.ForceField.from_spec(sys_, spec)
     it = hb.Integrator(sys_, **lang)
-    per_step_kernels, rebuild_kernels = it.count_launches(ff, cons)
+    baro = None
+    if args.barostat:
+        baro = hb.Barostat(sys_, U.pressure_au_bar(1.0), spec.temperature, seed=4321 + rank,
+                           frequency=25, molecules=(spec.mol_offsets, spec.mol_atoms))
+        it.set_barostat(baro)
+    per_step_kernels, rebuild_kernels, move_kernels = it.count_launches(ff, cons)
     run = it.step_graph if args.graphs else it.step
     run(ff, cons, n_steps=max(3, args.warmup))
     ctx.synchronize()
@@ -249,6 +257,7 @@ def run_ours(args):
 
     # headline: CUDA-graph steps, one step per launch, L2 flushed in between
     rebuilds0 = ff.stats()["rebuilds"]
+    moves0 = baro.stats()["attempted"] if baro else 0
     t_ms = 0.0
     if dist is not None:
         dist.barrier()
@@ -265,6 +274,8 @@ def run_ours(args):
         dist.barrier()
     ctx.timing(False)
     rebuilds = ff.stats()["rebuilds"] - rebuilds0
+    baro_stats = baro.stats() if baro else None
+    moves = int(baro_stats["attempted"] - moves0) if baro else 0
     if dist is not None:
         tt = torch.tensor([t_ms], device=f"cuda:{local}")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -335,12 +346,18 @@ def run_ours(args):
                     "d2h_bytes_per_step": 4 * 3 * 8 * spec.n,
                     "note": "per step: positions + velocities (f64) in; positions, velocities, "
                             "forces, images out; wall clock"},
-            "gpu_launches": per_step_kernels * args.steps + rebuild_kernels * rebuilds,
+            "gpu_launches": (per_step_kernels * args.steps + rebuild_kernels * rebuilds +
+                             move_kernels * moves),
+            "barostat": ({"moves_in_timed_steps": moves, "volume_A3": baro_stats["volume"] *
+                          (U.BOHR_M / U.ANGSTROM_M) ** 3, "acceptance": baro_stats["acceptance"]}
+                         if baro else None),
         }
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(spec)
         print(json.dumps(line), flush=True)
     it.close()
+    if baro:
+        baro.close()
     cons.close()
     ff.close()
     sys_.close()

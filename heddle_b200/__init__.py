@@ -5,6 +5,7 @@ fixed-point and FP64 reductions, behind a C ABI (include/heddle_b200.h)."""
 
 from ._native import HeddleError, load  # noqa: F401
 from .api import (  # noqa: F401
+    Barostat,
     Constraints,
     Context,
     ForceField,
@@ -16,6 +17,6 @@ from .api import (  # noqa: F401
 )
 
 __all__ = [
-    "Context", "System", "ForceField", "Constraints", "Integrator",
+    "Context", "System", "ForceField", "Constraints", "Integrator", "Barostat",
     "PotentialRegistry", "LennardJonesParams", "SpmeParams", "HeddleError", "load",
 ]

@@ -51,6 +51,19 @@ class SystemDesc(C.Structure):
     ]
 
 
+class BarostatDesc(C.Structure):
+    _fields_ = [
+        ("pressure", C.c_double),
+        ("temperature", C.c_double),
+        ("frequency", C.c_uint32),
+        ("volume_step", C.c_double),
+        ("seed", C.c_uint64),
+        ("n_molecules", C.c_uint32),
+        ("mol_offsets", PU32),
+        ("mol_atoms", PU32),
+    ]
+
+
 class ForceFieldDesc(C.Structure):
     _fields_ = [
         ("lj_enabled", C.c_int),
@@ -137,6 +150,11 @@ SIGNATURES = {
     "hb_integrator_step": (C.c_int, [VP, VP, VP, C.c_uint32, C.c_uint32]),
     "hb_integrator_step_graph": (C.c_int, [VP, VP, VP, C.c_uint32]),
     "hb_integrator_count_launches": (C.c_int, [VP, VP, VP, PU64]),
+    "hb_barostat_create": (C.c_int, [VP, C.POINTER(BarostatDesc), PVP]),
+    "hb_barostat_destroy": (C.c_int, [VP]),
+    "hb_barostat_mc_move": (C.c_int, [VP, VP]),
+    "hb_barostat_stats": (C.c_int, [VP, PD]),
+    "hb_integrator_set_barostat": (C.c_int, [VP, VP]),
     "hb_reduce_kinetic": (C.c_int, [VP, PD]),
     "hb_spme_recip_noalloc": (C.c_int, [C.c_void_p, C.c_uint32, PD, PU32, C.c_uint32, C.c_double,
                                         C.c_void_p, PD, C.c_void_p]),

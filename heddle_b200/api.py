@@ -120,6 +120,11 @@ class System:
         b = _f64(box)
         N.check(self.lib.hb_system_set_box(self.h, N.dptr(b)))
 
+    def box(self) -> np.ndarray:
+        b = np.zeros(6)
+        N.check(self.lib.hb_system_get_box(self.h, N.dptr(b)))
+        return b
+
     def kinetic(self) -> np.ndarray:
         out = np.zeros(4)
         N.check(self.lib.hb_reduce_kinetic(self.h, N.dptr(out)))
@@ -396,13 +401,72 @@ class Integrator:
         N.check(self.lib.hb_integrator_step_graph(self.h, ff.h, cons.h if cons else None, int(n_steps)))
 
     def count_launches(self, ff: ForceField, cons: Constraints | None = None) -> tuple:
-        """(kernels every step, kernels of one neighbour rebuild)."""
-        out = np.zeros(2, dtype=np.uint64)
+        """(kernels every step, kernels of one neighbour rebuild, kernels of
+        one barostat move or 0)."""
+        out = np.zeros(3, dtype=np.uint64)
         N.check(self.lib.hb_integrator_count_launches(self.h, ff.h, cons.h if cons else None,
                                                       out.ctypes.data_as(N.PU64)))
-        return int(out[0]), int(out[1])
+        return int(out[0]), int(out[1]), int(out[2])
+
+    def set_barostat(self, baro: "Barostat | None") -> None:
+        N.check(self.lib.hb_integrator_set_barostat(self.h, baro.h if baro else None))
+        self._baro = baro
 
     def close(self) -> None:
         if getattr(self, "h", None):
             self.lib.hb_integrator_destroy(self.h)
+            self.h = None
+
+
+# ---------------------------------------------------------------------------
+# barostats (registry kind names of src/integrator/mc_barostat.rs:371-379)
+# ---------------------------------------------------------------------------
+BAROSTAT_STATS = ("volume", "acceptance", "max_volume_step", "conserved_term", "attempted",
+                  "accepted", "last_dv", "last_w", "last_u_old", "last_u_new", "last_scale",
+                  "last_accepted", "last_trial", "last_u2", "draws")
+
+
+class Barostat:
+    """Monte-Carlo barostat ("monte-carlo"): a device-side Metropolis volume
+    move on molecular centres of mass every `frequency` steps.  pressure in
+    hartree/bohr^3, temperature as k_B T in hartree, volume_step in bohr^3
+    (None: 1 % of the initial volume).  molecules = (offsets, atoms) CSR
+    covering every atom once; None makes every atom its own molecule."""
+
+    kind = "monte-carlo"
+
+    def __init__(self, system: System, pressure: float, temperature: float, seed: int,
+                 frequency: int = 25, volume_step: float | None = None, molecules=None):
+        self.system = system
+        self.lib = system.lib
+        d = N.BarostatDesc()
+        d.pressure = float(pressure)
+        d.temperature = float(temperature)
+        d.frequency = int(frequency)
+        d.volume_step = float(volume_step) if volume_step is not None else 0.0
+        d.seed = int(seed)
+        self._keep = []
+        if molecules is not None:
+            off = np.ascontiguousarray(molecules[0], dtype=np.uint32)
+            atoms = np.ascontiguousarray(molecules[1], dtype=np.uint32)
+            self._keep += [off, atoms]
+            d.n_molecules = len(off) - 1
+            d.mol_offsets = N.u32ptr(off)
+            d.mol_atoms = N.u32ptr(atoms)
+        h = C.c_void_p()
+        N.check(self.lib.hb_barostat_create(system.h, C.byref(d), C.byref(h)))
+        self.h = h
+
+    def move(self, ff: ForceField) -> None:
+        """One Barostat::apply_move; ff's last evaluation must carry scalars."""
+        N.check(self.lib.hb_barostat_mc_move(self.h, ff.h))
+
+    def stats(self) -> dict:
+        out = np.zeros(len(BAROSTAT_STATS))
+        N.check(self.lib.hb_barostat_stats(self.h, N.dptr(out)))
+        return dict(zip(BAROSTAT_STATS, out.tolist()))
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.hb_barostat_destroy(self.h)
             self.h = None

@@ -21,7 +21,8 @@ BUILD = PKG / "_build"
 LIB = PKG / "libheddle_b200.so"
 INCLUDE = PKG.parent / "include"
 
-SOURCES = ["hb_api.cu", "hb_nlist.cu", "hb_pair.cu", "hb_spme.cu", "hb_integ.cu", "hb_cons.cu"]
+SOURCES = ["hb_api.cu", "hb_nlist.cu", "hb_pair.cu", "hb_spme.cu", "hb_integ.cu", "hb_cons.cu",
+           "hb_baro.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [

@@ -24,10 +24,6 @@ int hb_fail(int code, const std::string &msg) {
 extern "C" const char *hb_last_error(void) { return g_err.c_str(); }
 extern "C" const char *hb_version(void) { return "heddle_b200 0.1 (sm_100a)"; }
 
-#define HB_REQUIRE(cond, code, msg) \
-  do {                              \
-    if (!(cond)) return hb_fail((code), (msg)); \
-  } while (0)
 
 // ---------------------------------------------------------------------
 // context
@@ -113,20 +109,7 @@ static void stage_end(int stage, cudaEvent_t b, cudaStream_t s) {
 // ---------------------------------------------------------------------
 // system
 // ---------------------------------------------------------------------
-static DBox make_dbox(const double b[6]) {
-  DBox d;
-  d.lx = (float)b[0];
-  d.ly = (float)b[1];
-  d.lz = (float)b[2];
-  d.xy = (float)b[3];
-  d.xz = (float)b[4];
-  d.yz = (float)b[5];
-  d.ilx = (float)(1.0 / b[0]);
-  d.ily = (float)(1.0 / b[1]);
-  d.ilz = (float)(1.0 / b[2]);
-  d.ortho = (b[3] == 0.0 && b[4] == 0.0 && b[5] == 0.0) ? 1 : 0;
-  return d;
-}
+static DBox make_dbox(const double b[6]) { return hb_make_dbox(b); }
 
 static bool finite6(const double b[6]) {
   for (int d = 0; d < 6; ++d)
@@ -134,22 +117,7 @@ static bool finite6(const double b[6]) {
   return b[0] > 0.0 && b[1] > 0.0 && b[2] > 0.0;
 }
 
-static void perp_widths(const double b[6], double w[3]) {
-  const double a[3] = {b[0], 0.0, 0.0}, bb[3] = {b[3], b[1], 0.0}, c[3] = {b[4], b[5], b[2]};
-  const double vol = b[0] * b[1] * b[2];
-  auto cr = [](const double *x, const double *y, double *o) {
-    o[0] = x[1] * y[2] - x[2] * y[1];
-    o[1] = x[2] * y[0] - x[0] * y[2];
-    o[2] = x[0] * y[1] - x[1] * y[0];
-  };
-  double t[3];
-  cr(bb, c, t);
-  w[0] = vol / std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
-  cr(c, a, t);
-  w[1] = vol / std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
-  cr(a, bb, t);
-  w[2] = vol / std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
-}
+static void perp_widths(const double b[6], double w[3]) { hb_perp_widths(b, w); }
 
 // wrap a position into the primary cell in FP64 (kernels/pbc.cuh:73-91)
 static void wrap_host(const double b[6], double &x, double &y, double &z, int &ka, int &kb,
@@ -166,9 +134,18 @@ static void wrap_host(const double b[6], double &x, double &y, double &z, int &k
   kc = (int)fc;
 }
 
+// The FP64 lattice lives on the device (a barostat move changes it there);
+// host code that needs the box reads it back first.
+int sys_refresh_box(hb_system *sys) {
+  HB_CUDA(cudaStreamSynchronize(sys->ctx->stream));
+  HB_CUDA(cudaMemcpy(sys->box, sys->d_box64, sizeof(double) * 6, cudaMemcpyDeviceToHost));
+  return HB_OK;
+}
+
 static int upload_state(hb_system *sys, const double *pos, const double *vel,
                         const int32_t *images_in, bool keep_images) {
   const uint32_t n = sys->n;
+  if (keep_images) HB_TRY(sys_refresh_box(sys));
   std::vector<float4> posq(n), v(n);
   std::vector<int4> img(n);
   std::vector<int4> old_img;
@@ -236,6 +213,8 @@ extern "C" int hb_system_create(hb_context *ctx, const hb_system_desc *d, hb_sys
   HB_CUDA(cudaMalloc(&s->d_box, sizeof(DBox)));
   DBox db = make_dbox(d->box);
   HB_CUDA(cudaMemcpy(s->d_box, &db, sizeof(DBox), cudaMemcpyHostToDevice));
+  HB_CUDA(cudaMalloc(&s->d_box64, sizeof(double) * 6));
+  HB_CUDA(cudaMemcpy(s->d_box64, d->box, sizeof(double) * 6, cudaMemcpyHostToDevice));
   HB_CUDA(cudaMalloc(&s->d_posq, sizeof(float4) * nn));
   HB_CUDA(cudaMalloc(&s->d_vel, sizeof(float4) * nn));
   HB_CUDA(cudaMalloc(&s->d_image, sizeof(int4) * nn));
@@ -262,6 +241,7 @@ extern "C" int hb_system_destroy(hb_system *s) {
   cudaSetDevice(s->ctx->device);
   cudaStreamSynchronize(s->ctx->stream);
   cudaFree(s->d_box);
+  cudaFree(s->d_box64);
   cudaFree(s->d_posq);
   cudaFree(s->d_vel);
   cudaFree(s->d_image);
@@ -341,13 +321,15 @@ extern "C" int hb_system_set_box(hb_system *sys, const double box[6]) {
   HB_REQUIRE(finite6(box), HB_ERR_NOT_FINITE, "box must be finite with positive diagonal");
   std::memcpy(sys->box, box, sizeof(double) * 6);
   DBox db = make_dbox(box);
-  HB_CUDA(cudaMemcpyAsync(sys->d_box, &db, sizeof(DBox), cudaMemcpyHostToDevice, sys->ctx->stream));
   HB_CUDA(cudaStreamSynchronize(sys->ctx->stream));
+  HB_CUDA(cudaMemcpy(sys->d_box, &db, sizeof(DBox), cudaMemcpyHostToDevice));
+  HB_CUDA(cudaMemcpy(sys->d_box64, box, sizeof(double) * 6, cudaMemcpyHostToDevice));
   return HB_OK;
 }
 
 extern "C" int hb_system_get_box(hb_system *sys, double box[6]) {
   HB_REQUIRE(sys && box, HB_ERR_INVALID_ARGUMENT, "null argument");
+  HB_TRY(sys_refresh_box(sys));
   std::memcpy(box, sys->box, sizeof(double) * 6);
   return HB_OK;
 }
@@ -428,6 +410,7 @@ extern "C" int hb_forcefield_create(hb_system *sys, const hb_forcefield_desc *d,
   // minimum image is well defined only for r_search <= half the smallest
   // perpendicular width (src/integrator/mc_barostat.rs:290-297)
   double w[3];
+  HB_TRY(sys_refresh_box(sys));
   perp_widths(sys->box, w);
   const double wmin = std::min(w[0], std::min(w[1], w[2]));
   if ((tmp.lj_on || tmp.coul_on) && n > 1 && wmin < 2.0 * (rc_max + d->r_skin) * (1.0 + 1e-4))
@@ -802,6 +785,7 @@ extern "C" int hb_integrator_destroy(hb_integrator *it) {
   if (!it) return HB_OK;
   cudaStreamSynchronize(it->sys->ctx->stream);
   if (it->graph_exec) cudaGraphExecDestroy(it->graph_exec);
+  if (it->graph_exec_move) cudaGraphExecDestroy(it->graph_exec_move);
   cudaFree(it->d_step);
   if (it->g_ev0) cudaEventDestroy(it->g_ev0);
   if (it->g_ev1) cudaEventDestroy(it->g_ev1);
@@ -840,6 +824,39 @@ static int one_step(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons, 
   return HB_OK;
 }
 
+// Barostat::apply_move on the device: propose + scale, a forces + scalars
+// evaluation against the trial box, Metropolis test + revert.
+static int baro_move(hb_barostat *b, hb_forcefield *ff, bool capturing) {
+  cudaStream_t s = ff->sys->ctx->stream;
+  HB_TRY(baro_propose(b, ff, s));
+  HB_TRY(force_eval(ff, true, capturing));
+  HB_TRY(baro_decide(b, ff, s));
+  return HB_OK;
+}
+
+extern "C" int hb_barostat_mc_move(hb_barostat *b, hb_forcefield *ff) {
+  HB_REQUIRE(b && ff, HB_ERR_INVALID_ARGUMENT, "null argument");
+  HB_REQUIRE(ff->sys == b->sys, HB_ERR_INVALID_ARGUMENT,
+             "barostat and force field must share one system");
+  if (b->sys->n == 0) return HB_OK;
+  HB_TRY(baro_move(b, ff, false));
+  return check_status(ff);
+}
+
+extern "C" int hb_integrator_set_barostat(hb_integrator *it, hb_barostat *b) {
+  HB_REQUIRE(it, HB_ERR_INVALID_ARGUMENT, "null integrator");
+  HB_REQUIRE(!b || b->sys == it->sys, HB_ERR_INVALID_ARGUMENT,
+             "integrator and barostat must share one system");
+  it->baro = b;
+  return HB_OK;
+}
+
+// a move follows the step whose number (counted from 1) is a multiple of
+// the barostat's frequency (src/runner.rs:2606-2607, 2693-2708)
+static bool move_due(const hb_integrator *it, uint64_t step_number) {
+  return it->baro && it->sys->n && step_number % it->baro->frequency == 0;
+}
+
 extern "C" int hb_integrator_step(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons,
                                   uint32_t n_steps, uint32_t scalar_every) {
   HB_REQUIRE(it && ff, HB_ERR_INVALID_ARGUMENT, "null argument");
@@ -855,8 +872,10 @@ extern "C" int hb_integrator_step(hb_integrator *it, hb_forcefield *ff, hb_const
     it->forces_valid = rc == HB_OK;
   }
   for (uint32_t k = 0; k < n_steps && rc == HB_OK; ++k) {
-    const bool ev = scalar_every > 0 && ((k + 1) % scalar_every == 0);
+    const bool move = move_due(it, it->step + 1);
+    const bool ev = (scalar_every > 0 && ((k + 1) % scalar_every == 0)) || move;
     rc = one_step(it, ff, cons, ev);
+    if (rc == HB_OK && move) rc = baro_move(it->baro, ff, false);
   }
   stage_end(0, t_all, ctx->stream);
   g_timer = nullptr;
@@ -875,6 +894,32 @@ extern "C" int hb_integrator_step(hb_integrator *it, hb_forcefield *ff, hb_const
   return HB_OK;
 }
 
+// capture one step (and, for the move graph, the volume move after it)
+static int capture_step(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons, bool move,
+                        cudaGraphExec_t *exec) {
+  cudaStream_t s = it->sys->ctx->stream;
+  cudaGraph_t g;
+  HB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  const uint64_t step = it->step;
+  int rc = one_step(it, ff, cons, move, true);
+  if (rc == HB_OK && move) rc = baro_move(it->baro, ff, true);
+  it->step = step;
+  cudaError_t ce = cudaStreamEndCapture(s, &g);
+  if (rc != HB_OK) return rc;
+  if (ce != cudaSuccess) return hb_fail(HB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+  cudaError_t ie = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  if (ie != cudaSuccess) return hb_fail(HB_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+  return HB_OK;
+}
+
+static void drop_graphs(hb_integrator *it) {
+  if (it->graph_exec) cudaGraphExecDestroy(it->graph_exec);
+  if (it->graph_exec_move) cudaGraphExecDestroy(it->graph_exec_move);
+  it->graph_exec = nullptr;
+  it->graph_exec_move = nullptr;
+}
+
 extern "C" int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
                                         hb_constraints *cons, uint32_t n_steps) {
   HB_REQUIRE(it && ff, HB_ERR_INVALID_ARGUMENT, "null argument");
@@ -886,26 +931,20 @@ extern "C" int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
     HB_TRY(force_eval(ff, false));
     it->forces_valid = true;
   }
-  if (!it->graph_exec || it->graph_ff != ff || it->graph_cons != cons) {
-    if (it->graph_exec) cudaGraphExecDestroy(it->graph_exec);
-    it->graph_exec = nullptr;
+  if (!it->graph_exec || it->graph_ff != ff || it->graph_cons != cons ||
+      it->graph_baro != it->baro) {
+    drop_graphs(it);
     HB_CUDA(cudaStreamSynchronize(s));
-    cudaGraph_t g;
-    HB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    const uint64_t step = it->step;
-    int rc = one_step(it, ff, cons, false, true);
-    it->step = step;
-    cudaError_t ce = cudaStreamEndCapture(s, &g);
-    if (rc != HB_OK) return rc;
-    if (ce != cudaSuccess) return hb_fail(HB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
-    HB_CUDA(cudaGraphInstantiate(&it->graph_exec, g, 0));
-    cudaGraphDestroy(g);
+    HB_TRY(capture_step(it, ff, cons, false, &it->graph_exec));
+    if (it->baro) HB_TRY(capture_step(it, ff, cons, true, &it->graph_exec_move));
     it->graph_ff = ff;
     it->graph_cons = cons;
+    it->graph_baro = it->baro;
   }
   if (ctx->timing) HB_CUDA(cudaEventRecord(it->g_ev0, s));
   for (uint32_t k = 0; k < n_steps; ++k) {
-    HB_CUDA(cudaGraphLaunch(it->graph_exec, s));
+    const bool move = move_due(it, it->step + 1);
+    HB_CUDA(cudaGraphLaunch(move ? it->graph_exec_move : it->graph_exec, s));
     it->step++;
   }
   if (ctx->timing) {
@@ -918,11 +957,8 @@ extern "C" int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
   }
   const uint64_t cap_before = ff->entry_cap;
   HB_TRY(check_status(ff));
-  if (ff->entry_cap != cap_before) {
-    // buffers moved: the captured graph holds stale pointers
-    cudaGraphExecDestroy(it->graph_exec);
-    it->graph_exec = nullptr;
-  }
+  // buffers moved: the captured graphs hold stale pointers
+  if (ff->entry_cap != cap_before) drop_graphs(it);
   return HB_OK;
 }
 
@@ -939,30 +975,39 @@ static int count_kernel_nodes(cudaGraph_t g, uint64_t &kernels) {
   return HB_OK;
 }
 
-extern "C" int hb_integrator_count_launches(hb_integrator *it, hb_forcefield *ff,
-                                            hb_constraints *cons, uint64_t *kernels) {
-  HB_REQUIRE(it && ff && kernels, HB_ERR_INVALID_ARGUMENT, "null argument");
+static int count_captured(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons, bool step,
+                          bool move, uint64_t &kernels) {
   cudaStream_t s = it->sys->ctx->stream;
-  HB_CUDA(cudaStreamSynchronize(s));
-  // capture the eager launch sequence (rebuild kernels gated, no
-  // conditional node) and count its kernel nodes
   cudaGraph_t g;
   HB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-  const uint64_t step = it->step;
-  int rc = one_step(it, ff, cons, false, false);
-  it->step = step;
+  const uint64_t st = it->step;
+  int rc = step ? one_step(it, ff, cons, false, false) : HB_OK;
+  if (rc == HB_OK && move) rc = baro_move(it->baro, ff, false);
+  it->step = st;
   cudaError_t ce = cudaStreamEndCapture(s, &g);
   if (rc != HB_OK) return rc;
   if (ce != cudaSuccess) return hb_fail(HB_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(ce));
-  uint64_t eager = 0;
-  rc = count_kernel_nodes(g, eager);
+  kernels = 0;
+  rc = count_kernel_nodes(g, kernels);
   cudaGraphDestroy(g);
-  if (rc != HB_OK) return rc;
+  return rc;
+}
+
+extern "C" int hb_integrator_count_launches(hb_integrator *it, hb_forcefield *ff,
+                                            hb_constraints *cons, uint64_t *kernels) {
+  HB_REQUIRE(it && ff && kernels, HB_ERR_INVALID_ARGUMENT, "null argument");
+  HB_CUDA(cudaStreamSynchronize(it->sys->ctx->stream));
+  // capture the eager launch sequence (rebuild kernels gated, no
+  // conditional node) and count its kernel nodes; nothing runs
+  uint64_t eager = 0, eager_move = 0;
+  HB_TRY(count_captured(it, ff, cons, true, false, eager));
+  if (it->baro && it->sys->n) HB_TRY(count_captured(it, ff, cons, false, true, eager_move));
   // in the graph form the gated rebuild kernels move into the IF node's
   // body and one kernel sets the condition
   const uint64_t body = ff->sys->n ? (uint64_t)nl_kernel_count() : 0u;
   kernels[0] = eager - body + (body ? 1u : 0u);
   kernels[1] = body;
+  kernels[2] = eager_move ? eager_move - body + 1u : 0u;
   return HB_OK;
 }
 

@@ -87,32 +87,12 @@ __global__ void k_scalars(unsigned long long *__restrict__ acc,
   acc[2] = 0ull;
 }
 
-// ---- Philox-4x32-10 (Salmon et al. 2011), counter (step_lo, step_hi,
-// atom, axis), key = seed, as kernels/philox.cuh uses it
-__device__ __forceinline__ void philox(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1,
-                                       uint32_t c2, uint32_t c3, uint32_t &o0, uint32_t &o1) {
-#pragma unroll
-  for (int r = 0; r < 10; ++r) {
-    const uint32_t hi0 = __umulhi(c0, 0xD2511F53u), lo0 = c0 * 0xD2511F53u;
-    const uint32_t hi2 = __umulhi(c2, 0xCD9E8D57u), lo2 = c2 * 0xCD9E8D57u;
-    const uint32_t n0 = hi2 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
-    c0 = n0;
-    c1 = lo2;
-    c2 = n2;
-    c3 = lo0;
-    k0 += 0x9E3779B9u;
-    k1 += 0xBB67AE85u;
-  }
-  o0 = c0;
-  o1 = c1;
-}
-
 // Box-Muller cosine branch on the first two words, u = (x + 1/2) 2^-32
 // (kernels/philox.cuh:135-150), evaluated in single precision.
 __device__ __forceinline__ float gaussian(uint32_t s_lo, uint32_t s_hi, uint64_t step,
                                           uint32_t atom, uint32_t axis) {
   uint32_t o0, o1;
-  philox(s_lo, s_hi, (uint32_t)step, (uint32_t)(step >> 32), atom, axis, o0, o1);
+  hb_philox(s_lo, s_hi, (uint32_t)step, (uint32_t)(step >> 32), atom, axis, o0, o1);
   const float u1 = ((float)(o0 >> 8) + 0.5f) * (1.0f / 16777216.0f);
   const float u2 = ((float)(o1 >> 8) + 0.5f) * (1.0f / 16777216.0f);
   return sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);

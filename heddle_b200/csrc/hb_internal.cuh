@@ -26,6 +26,11 @@ int hb_fail(int code, const std::string &msg);
     }                                                                       \
   } while (0)
 
+#define HB_REQUIRE(cond, code, msg)               \
+  do {                                            \
+    if (!(cond)) return hb_fail((code), (msg));   \
+  } while (0)
+
 #define HB_TRY(call)                                                        \
   do {                                                                      \
     int r_ = (call);                                                        \
@@ -106,6 +111,59 @@ __device__ __forceinline__ void hb_wrap(float &x, float &y, float &z, int &ka,
   kc = (int)fc;
 }
 
+// Philox-4x32-10 (Salmon et al. 2011) as kernels/philox.cuh and
+// src/integrator/philox.rs:21-50 use it: key (k0, k1), counter (c0..c3);
+// returns the first two output words.
+__host__ __device__ inline void hb_philox(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1,
+                                          uint32_t c2, uint32_t c3, uint32_t &o0,
+                                          uint32_t &o1) {
+  for (int r = 0; r < 10; ++r) {
+    const uint64_t p0 = (uint64_t)c0 * 0xD2511F53u, p2 = (uint64_t)c2 * 0xCD9E8D57u;
+    const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    const uint32_t hi2 = (uint32_t)(p2 >> 32), lo2 = (uint32_t)p2;
+    const uint32_t n0 = hi2 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0;
+    c1 = lo2;
+    c2 = n2;
+    c3 = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  o0 = c0;
+  o1 = c1;
+}
+
+// lower-triangular lattice (lx, ly, lz, xy, xz, yz) -> the single-precision
+// box the kernels read
+__host__ __device__ inline DBox hb_make_dbox(const double b[6]) {
+  DBox d;
+  d.lx = (float)b[0];
+  d.ly = (float)b[1];
+  d.lz = (float)b[2];
+  d.xy = (float)b[3];
+  d.xz = (float)b[4];
+  d.yz = (float)b[5];
+  d.ilx = (float)(1.0 / b[0]);
+  d.ily = (float)(1.0 / b[1]);
+  d.ilz = (float)(1.0 / b[2]);
+  d.ortho = (b[3] == 0.0 && b[4] == 0.0 && b[5] == 0.0) ? 1 : 0;
+  return d;
+}
+
+// perpendicular widths of the cell spanned by a = (lx,0,0), b = (xy,ly,0),
+// c = (xz,yz,lz): volume / |b x c|, volume / |c x a|, volume / |a x b|
+__host__ __device__ inline void hb_perp_widths(const double b[6], double w[3]) {
+  const double ax = b[0], bx = b[3], by = b[1], cx = b[4], cy = b[5], cz = b[2];
+  const double vol = ax * by * cz;
+  // b x c, c x a, a x b with a = (ax,0,0), b = (bx,by,0), c = (cx,cy,cz)
+  const double bc0 = by * cz, bc1 = -bx * cz, bc2 = bx * cy - by * cx;
+  const double ca1 = cz * ax, ca2 = -cy * ax;
+  const double ab2 = ax * by;
+  w[0] = vol / sqrt(bc0 * bc0 + bc1 * bc1 + bc2 * bc2);
+  w[1] = vol / sqrt(ca1 * ca1 + ca2 * ca2);
+  w[2] = vol / sqrt(ab2 * ab2);
+}
+
 __device__ __forceinline__ void hb_frac(float x, float y, float z,
                                         const DBox &b, float &sa, float &sb,
                                         float &sc) {
@@ -133,8 +191,9 @@ struct hb_context {
 struct hb_system {
   hb_context *ctx = nullptr;
   uint32_t n = 0;
-  double box[6] = {0};
-  DBox *d_box = nullptr;
+  double box[6] = {0};            // host mirror of d_box64 (refresh before use)
+  double *d_box64 = nullptr;       // [6] FP64 lattice, the authoritative box
+  DBox *d_box = nullptr;           // single-precision view of d_box64
   float4 *d_posq = nullptr;      // x, y, z, q (wrapped into the primary cell)
   float4 *d_vel = nullptr;       // vx, vy, vz, 1/m
   int4 *d_image = nullptr;       // image counts a, b, c, type
@@ -203,6 +262,7 @@ struct hb_forcefield {
   uint32_t *d_entry_excl = nullptr;  // [n_tiles * slab * 32] exclusion masks
   uint64_t entry_cap = 0;            // n_tiles * slab
   float4 *d_ref_pos = nullptr;       // positions at the last rebuild
+  DBox *d_ref_box = nullptr;         // box at the last rebuild
   uint32_t *d_status = nullptr;      // status word
   uint32_t *d_counters = nullptr;    // [0] rebuilds, [1] entries of the last
                                      // build, [2] running count of a build,
@@ -254,6 +314,41 @@ struct hb_integrator {
   cudaEvent_t g_ev0 = nullptr, g_ev1 = nullptr;
   hb_forcefield *graph_ff = nullptr;
   hb_constraints *graph_cons = nullptr;
+  // Monte-Carlo barostat attached to the step loop (may be null) and the
+  // graph of a step that ends with a volume move
+  hb_barostat *baro = nullptr;
+  cudaGraphExec_t graph_exec_move = nullptr;
+  hb_barostat *graph_baro = nullptr;
+};
+
+// Device-resident state of the Monte-Carlo barostat (FP64).  The whole move
+// -- draw, proposal, trial force evaluation, Metropolis test, revert and
+// step-size adaptation -- runs on the device with no host read.
+struct BaroState {
+  double lattice_pre[6];   // lattice before the trial
+  double scalars_pre[8];   // force-field scalars before the trial
+  double max_dv;           // current maximum volume displacement
+  double u_old, u_new, dv, v_old, v_new, scale, u1, u2, w;
+  double injection;        // sum of P dV over accepted moves
+  double volume;           // volume after the last move
+  unsigned long long draw, attempted, accepted;
+  unsigned int win_attempted, win_accepted;
+  int trial, last_accepted;
+};
+
+struct hb_barostat {
+  hb_system *sys = nullptr;
+  double pressure = 0.0, kt = 0.0;
+  uint32_t frequency = 25;
+  uint64_t seed = 0;
+  uint32_t n_mol = 0;
+  uint32_t *d_mol_off = nullptr;     // [n_mol + 1]
+  uint32_t *d_mol_atoms = nullptr;   // [n]
+  double *d_mass = nullptr;          // [n] FP64 masses
+  BaroState *d_state = nullptr;
+  float4 *d_snap_pos = nullptr;      // pre-move positions, images, forces
+  int4 *d_snap_img = nullptr;
+  float4 *d_snap_force = nullptr;
 };
 
 // ---------------------------------------------------------------------
@@ -287,6 +382,12 @@ int integ_vv_kick(hb_integrator *it, cudaStream_t s);
 int integ_lang_kick(hb_integrator *it, cudaStream_t s);
 int integ_lang_drift_ou(hb_integrator *it, cudaStream_t s);
 int reduce_kinetic(hb_system *sys, double out[4]);
+// system (hb_api.cu): copy the device FP64 lattice into the host mirror
+int sys_refresh_box(hb_system *sys);
+// Monte-Carlo barostat (hb_baro.cu): propose + scale, then (after a force
+// evaluation with scalars) decide + revert
+int baro_propose(hb_barostat *b, hb_forcefield *ff, cudaStream_t s);
+int baro_decide(hb_barostat *b, hb_forcefield *ff, cudaStream_t s);
 // constraints (hb_cons.cu)
 int cons_positions(hb_constraints *c, double dt, cudaStream_t s);
 int cons_velocities(hb_constraints *c, double dt, bool virial, cudaStream_t s);

@@ -461,8 +461,10 @@ __global__ void __launch_bounds__(NLT_WARPS * 32)
 
 // Last kernel of a rebuild: counters, and clearing of the displacement bit
 // (which gates every kernel of the rebuild).
-__global__ void k_nl_finish(const uint32_t *gate, uint32_t *status, uint32_t *counters) {
+__global__ void k_nl_finish(const uint32_t *gate, uint32_t *status, uint32_t *counters,
+                            const DBox *__restrict__ box, DBox *__restrict__ ref_box) {
   if (gate_off(gate)) return;
+  *ref_box = *box;
   *status &= ~HB_ST_DISPLACED;
   counters[0] += 1u;
   counters[1] = counters[2];
@@ -470,16 +472,23 @@ __global__ void k_nl_finish(const uint32_t *gate, uint32_t *status, uint32_t *co
 }
 
 __global__ void k_disp_check(const float4 *__restrict__ posq, const float4 *__restrict__ ref,
-                             const DBox *__restrict__ box, float thr2, uint32_t *status,
-                             uint32_t n) {
+                             const DBox *__restrict__ box, const DBox *__restrict__ ref_box,
+                             float thr2, uint32_t *status, uint32_t n) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   bool moved = false;
+  // a box that changed since the last rebuild (set_box, a barostat move)
+  // invalidates the list as well
+  if (i == 0u) {
+    const DBox a = *box, r = *ref_box;
+    moved = a.lx != r.lx || a.ly != r.ly || a.lz != r.lz || a.xy != r.xy || a.xz != r.xz ||
+            a.yz != r.yz;
+  }
   if (i < n) {
     DBox b = *box;
     float4 p = posq[i], r = ref[i];
     float dx = p.x - r.x, dy = p.y - r.y, dz = p.z - r.z;
     hb_min_image(dx, dy, dz, b);
-    moved = dx * dx + dy * dy + dz * dz > thr2;
+    moved = moved || dx * dx + dy * dy + dz * dz > thr2;
   }
   // one atomic per warp at most
   if (__any_sync(0xFFFFFFFFu, moved) && (threadIdx.x & 31u) == 0u) atomicOr(status, HB_ST_DISPLACED);
@@ -530,6 +539,8 @@ int nl_setup(hb_forcefield *ff) {
   HB_CUDA(cudaMalloc(&ff->d_tile_nent, sizeof(uint32_t) * (ff->n_tiles + 1)));
   HB_CUDA(cudaMemset(ff->d_tile_nent, 0, sizeof(uint32_t) * (ff->n_tiles + 1)));
   HB_CUDA(cudaMalloc(&ff->d_ref_pos, sizeof(float4) * std::max(n, 1u)));
+  HB_CUDA(cudaMalloc(&ff->d_ref_box, sizeof(DBox)));
+  HB_CUDA(cudaMemset(ff->d_ref_box, 0, sizeof(DBox)));
   HB_CUDA(cudaMalloc(&ff->d_status, sizeof(uint32_t)));
   HB_CUDA(cudaMemset(ff->d_status, 0, sizeof(uint32_t)));
   HB_CUDA(cudaMalloc(&ff->d_counters, sizeof(uint32_t) * 4));
@@ -555,6 +566,7 @@ int nl_free(hb_forcefield *ff) {
   cudaFree(ff->d_entry_j);
   cudaFree(ff->d_entry_excl);
   cudaFree(ff->d_ref_pos);
+  cudaFree(ff->d_ref_box);
   cudaFree(ff->d_status);
   cudaFree(ff->d_counters);
   cudaFreeHost(ff->h_status);
@@ -602,7 +614,7 @@ static int nl_launch(hb_forcefield *ff, const uint32_t *gate, cudaStream_t s, bo
         band_hi, n, ff->n_tiles, ff->maxc, ff->d_tile_nent, ff->slab, ff->d_entry_j,
         ff->d_entry_excl, ff->d_status, ff->d_counters, ff->d_sorted_ids, ff->d_inv_perm,
         ff->d_excl_off, ff->d_excl_partner);
-    k_nl_finish<<<1, 1, 0, s>>>(gate, ff->d_status, ff->d_counters);
+    k_nl_finish<<<1, 1, 0, s>>>(gate, ff->d_status, ff->d_counters, sys->d_box, ff->d_ref_box);
   }
   HB_CUDA(cudaGetLastError());
   return HB_OK;
@@ -728,7 +740,8 @@ int nl_displacement_check(hb_forcefield *ff, cudaStream_t s) {
   if (sys->n == 0) return HB_OK;
   float thr = 0.5f * ff->r_skin;
   k_disp_check<<<hb_div_up(sys->n, 256), 256, 0, s>>>(sys->d_posq, ff->d_ref_pos, sys->d_box,
-                                                       thr * thr, ff->d_status, sys->n);
+                                                       ff->d_ref_box, thr * thr, ff->d_status,
+                                                       sys->n);
   HB_CUDA(cudaGetLastError());
   return HB_OK;
 }
@@ -794,6 +807,7 @@ int nl_pairs(hb_forcefield *ff, std::vector<uint32_t> &pairs, uint64_t &dups) {
   if (ff->entry_cap)
     HB_CUDA(cudaMemcpy(ej.data(), ff->d_entry_j, sizeof(uint32_t) * 32 * ff->entry_cap,
                        cudaMemcpyDeviceToHost));
+  HB_TRY(sys_refresh_box(sys));
   float b[6];
   for (int d = 0; d < 6; ++d) b[d] = (float)sys->box[d];
   const float rs2 = ff->r_search * ff->r_search;

@@ -60,6 +60,9 @@ class SystemSpec:
     con_i: np.ndarray | None = None
     con_j: np.ndarray | None = None
     con_dist: np.ndarray | None = None
+    # molecules (CSR over atom ids; the barostat scales their centres)
+    mol_offsets: np.ndarray | None = None
+    mol_atoms: np.ndarray | None = None
     # dynamics
     dt: float = 0.0
     temperature: float = 0.0
@@ -222,6 +225,8 @@ def spc_water(n_mol: int, seed: int = 11, density: float = 997.0, r_cut_A: float
         group_kind=np.zeros(n_mol, dtype=np.uint32),
         settle_ra=np.full(n_mol, ra), settle_rb=np.full(n_mol, rb),
         settle_rc=np.full(n_mol, rcs),
+        mol_offsets=(3 * np.arange(n_mol + 1)).astype(np.uint32),
+        mol_atoms=np.arange(n, dtype=np.uint32),
         dt=U.time_au_fs(dt_fs), dt_fs=dt_fs, temperature=kt,
         friction=friction_per_ps / (1.0e-12 / U.AUT_S),
         meta={"L_A": L_m / U.ANGSTROM_M, "r_oh": r_oh, "hoh_deg": SPC["hoh_deg"],

@@ -60,6 +60,7 @@ typedef struct hb_system hb_system;
 typedef struct hb_forcefield hb_forcefield;
 typedef struct hb_constraints hb_constraints;
 typedef struct hb_integrator hb_integrator;
+typedef struct hb_barostat hb_barostat;
 
 /* Message of the last failing call on this thread ("" when none). */
 const char *hb_last_error(void);
@@ -221,9 +222,51 @@ int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
 /* Kernel launches of one step: the step is captured into a throwaway CUDA
  * graph (nothing runs) and its kernel nodes are counted: kernels[0] = the
  * kernels every step launches, kernels[1] = the kernels of a neighbour
- * rebuild (a conditional node taken only on rebuild steps). */
+ * rebuild (a conditional node taken only on rebuild steps), kernels[2] =
+ * the kernels of one barostat volume move (0 without a barostat). */
 int hb_integrator_count_launches(hb_integrator *it, hb_forcefield *ff,
                                  hb_constraints *cons, uint64_t *kernels);
+
+/* ---- Monte-Carlo barostat: replaces McBarostat
+ * (src/integrator/mc_barostat.rs:218-360, "monte-carlo" in the barostat
+ * registry) and mc_barostat_scale_molecule_com (kernels/mc_barostat.cu:19-74).
+ * A move: draw (Philox-4x32-10, key = seed, counter = move number),
+ * dV = max_dV (2 u1 - 1), isotropic lattice scale (V'/V)^(1/3) in FP64,
+ * molecule centres of mass scaled about the origin with every molecule kept
+ * rigid, a forces + scalars evaluation, Metropolis test on
+ * w = dU + P dV - n_mol kT ln(V'/V), and on rejection the box, positions,
+ * images, forces and scalars of the pre-move state restored.  A contraction
+ * that would take the narrowest perpendicular width below 2 (r_cut + r_skin)
+ * is rejected before any work.  Every 10 attempts max_dV is divided by 1.1
+ * (acceptance < 25 %) or multiplied by 1.1 up to 0.3 V (> 75 %).  The whole
+ * move runs on the device (no host read), so it also runs inside a graph. */
+typedef struct {
+  double pressure;           /* hartree / bohr^3 */
+  double temperature;        /* k_B T in hartree */
+  uint32_t frequency;        /* a move after every frequency-th step (>= 1) */
+  double volume_step;        /* initial max |dV| in bohr^3; <= 0: 1 % of V */
+  uint64_t seed;
+  uint32_t n_molecules;      /* 0: every atom is its own molecule */
+  const uint32_t *mol_offsets;   /* [n_molecules + 1] */
+  const uint32_t *mol_atoms;     /* [n_atoms]: each atom exactly once */
+} hb_barostat_desc;
+
+int hb_barostat_create(hb_system *sys, const hb_barostat_desc *desc, hb_barostat **out);
+int hb_barostat_destroy(hb_barostat *b);
+/* Barostat::apply_move.  The force field's last evaluation must have been
+ * HB_FORCES_AND_SCALARS at the current configuration (its potential energy
+ * is U_old), as the reference's runner arranges on the step before a move. */
+int hb_barostat_mc_move(hb_barostat *b, hb_forcefield *ff);
+/* out[0] volume, [1] acceptance ratio, [2] max_dV, [3] P V - cumulative
+ * P dV (the barostat's term of the conserved quantity), [4] attempted,
+ * [5] accepted, [6] last dV, [7] last w, [8] last U_old, [9] last U_new,
+ * [10] last scale, [11] last move accepted (0/1), [12] last trial applied
+ * (0/1), [13] last u2, [14] move counter. */
+int hb_barostat_stats(hb_barostat *b, double out[15]);
+/* Attach (or detach with NULL) a barostat to an integrator: the step whose
+ * number is a multiple of the barostat's frequency evaluates scalars and is
+ * followed by a move (src/runner.rs:2693-2708). */
+int hb_integrator_set_barostat(hb_integrator *it, hb_barostat *b);
 
 /* ---- FP64 deterministic scalar reductions (kernels/nose_hoover.cu:22-103,
  * kernels/barostat.cu:11-78): kinetic energy and the mass-weighted

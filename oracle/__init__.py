@@ -73,6 +73,8 @@ def lib() -> C.CDLL:
         L.or_philox4x32_10.argtypes = [C.c_uint32, C.c_uint32, PU, PU]
         L.or_philox_gaussian.restype = C.c_double
         L.or_philox_gaussian.argtypes = [C.c_uint32] * 6
+        L.or_mc_scale_com.argtypes = [C.c_int32, PI, PI, PD, C.POINTER(OrBox), C.POINTER(OrBox), C.c_double,
+                                      PD, PI]
         L.or_md_run.restype = C.c_int
         L.or_md_run.argtypes = [C.c_int32, PD, PD, PD, PD, PI, C.POINTER(OrBox), C.POINTER(OrFF),
                                 C.c_int32, PI, PI, PI, PI, PI, PD, C.c_int, C.c_double, C.c_double,
@@ -261,6 +263,20 @@ def philox(key_lo: int, key_hi: int, ctr) -> np.ndarray:
 def philox_gaussian(seed: int, step: int, particle: int, axis: int) -> float:
     return lib().or_philox_gaussian(seed & 0xFFFFFFFF, seed >> 32, step & 0xFFFFFFFF, step >> 32,
                                     particle, axis)
+
+
+def mc_scale_com(mol_offsets, mol_atoms, masses, box_old, box_new, scale: float, positions, images):
+    """Monte-Carlo barostat centre-of-mass scaling (kernels/mc_barostat.cu:19-74,
+    molecule translated as its contiguous image); returns (positions, images)."""
+    off, po = _i(mol_offsets)
+    at, pa = _i(mol_atoms)
+    m, pm = _d(masses)
+    pos, pp = _d(np.array(positions, dtype=np.float64).reshape(-1))
+    img, pi = _i(np.array(images, dtype=np.int32).reshape(-1))
+    b0 = box_of(box_old)
+    b1 = box_of(box_new)
+    lib().or_mc_scale_com(len(off) - 1, po, pa, pm, C.byref(b0), C.byref(b1), float(scale), pp, pi)
+    return pos.reshape(-1, 3), img.reshape(-1, 3)
 
 
 def md_run(spec, n_steps: int, integrator: str = "vv", positions=None, velocities=None,

@@ -1052,3 +1052,49 @@ done:
   free(ref);
   return rc;
 }
+
+/* ---------------------------------------------------------------------
+ * Monte-Carlo barostat centre-of-mass scaling
+ * (kernels/mc_barostat.cu:19-74; the molecule is translated as its
+ * contiguous image, see the header)
+ * ------------------------------------------------------------------- */
+void or_mc_scale_com(int32_t n_mol, const int32_t *off, const int32_t *atoms,
+                     const double *mass, const or_box *box_old, const or_box *box_new,
+                     double scale, double *pos, int32_t *img) {
+  for (int32_t m = 0; m < n_mol; ++m) {
+    const int32_t lo = off[m], hi = off[m + 1];
+    if (hi <= lo) continue;
+    const int32_t r = atoms[lo];
+    const double rx = pos[3 * r], ry = pos[3 * r + 1], rz = pos[3 * r + 2];
+    double mt = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
+    for (int32_t k = lo; k < hi; ++k) {
+      const int32_t a = atoms[k];
+      double dx = pos[3 * a] - rx, dy = pos[3 * a + 1] - ry, dz = pos[3 * a + 2] - rz;
+      or_min_image(box_old, &dx, &dy, &dz);
+      cx += mass[a] * dx;
+      cy += mass[a] * dy;
+      cz += mass[a] * dz;
+      mt += mass[a];
+    }
+    const double f = scale - 1.0;
+    const double sx = f * (rx + cx / mt), sy = f * (ry + cy / mt), sz = f * (rz + cz / mt);
+    for (int32_t k = lo; k < hi; ++k) {
+      const int32_t a = atoms[k];
+      const double ox = pos[3 * a] - rx, oy = pos[3 * a + 1] - ry, oz = pos[3 * a + 2] - rz;
+      double dx = ox, dy = oy, dz = oz;
+      or_min_image(box_old, &dx, &dy, &dz);
+      /* lattice counts of the minimum-image shift (ox - dx = K L) */
+      double sa, sb, sc;
+      cart_to_frac(box_old, ox - dx, oy - dy, oz - dz, &sa, &sb, &sc);
+      double x = rx + dx + sx, y = ry + dy + sy, z = rz + dz + sz;
+      int wa, wb, wc;
+      or_wrap_with_image(box_new, &x, &y, &z, &wa, &wb, &wc);
+      pos[3 * a] = x;
+      pos[3 * a + 1] = y;
+      pos[3 * a + 2] = z;
+      img[3 * a] += (int32_t)lrint(sa) + wa;
+      img[3 * a + 1] += (int32_t)lrint(sb) + wb;
+      img[3 * a + 2] += (int32_t)lrint(sc) + wc;
+    }
+  }
+}

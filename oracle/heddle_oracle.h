@@ -139,6 +139,19 @@ void or_philox4x32_10(uint32_t key_lo, uint32_t key_hi, const uint32_t ctr[4],
 double or_philox_gaussian(uint32_t seed_lo, uint32_t seed_hi, uint32_t step_lo,
                           uint32_t step_hi, uint32_t particle, uint32_t axis);
 
+/* ---- Monte-Carlo barostat centre-of-mass scaling
+ * (kernels/mc_barostat.cu:19-74, src/integrator/mc_barostat.rs:300-318) ----
+ * Each molecule (CSR off/atoms) is rebuilt as its contiguous image about its
+ * first atom (minimum-image displacements in box_old, the cell the positions
+ * live in), its mass-weighted centre c is computed, every atom is translated
+ * by (scale - 1) c and wrapped into box_new; img[3n] keeps each atom's
+ * integer offset from its molecule's contiguous image.  (The reference translates the stored, per-atom wrapped
+ * positions instead, which agrees for molecules that do not straddle the
+ * cell boundary.) */
+void or_mc_scale_com(int32_t n_mol, const int32_t *off, const int32_t *atoms,
+                     const double *mass, const or_box *box_old, const or_box *box_new,
+                     double scale, double *pos, int32_t *img);
+
 /* ---- CPU MD driver used as the timed CPU baseline ----
  * One velocity-Verlet or Langevin-middle step per iteration with SETTLE/SHAKE
  * groups, forces from or_forces.  integrator: 0 = velocity Verlet,

@@ -151,7 +151,7 @@ def test_langevin_graph_replay_equals_eager(ctx):
     assert rb_a == rb_b and rb_a > 1
     for a, b in zip(st_a, st_b):
         assert np.array_equal(a, b)
-    top, body = ib.count_launches(fb, cb)
+    top, body, _ = ib.count_launches(fb, cb)
     assert top > 10 and body > 5
     close(ia, ca, fa, sa, ib, cb, fb, sb)
 

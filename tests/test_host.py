@@ -143,3 +143,16 @@ def test_synthetic_systems_match_their_definitions():
 
 def test_fft_friendly_sizes():
     assert S.fft_friendly(63) == 64 and S.fft_friendly(126) == 128 and S.fft_friendly(25) == 25
+
+
+def test_package_exports_every_name_the_tests_use():
+    import re
+    from pathlib import Path
+
+    import heddle_b200 as hb
+
+    root = Path(__file__).resolve().parent.parent
+    names = set()
+    for f in list((root / "tests").glob("*.py")) + [root / "bench.py", root / "__graft_entry__.py"]:
+        names |= set(re.findall(r"\bhb\.([A-Za-z_]+)", f.read_text()))
+    assert sorted(n for n in names if not hasattr(hb, n)) == []

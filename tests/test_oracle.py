@@ -153,3 +153,41 @@ def test_settle_projection_restores_geometry():
         u = vv[3 * m: 3 * m + 3]
         for a, b in ((0, 1), (0, 2), (1, 2)):
             assert abs(np.dot(x[a] - x[b], u[a] - u[b])) < 1e-10
+
+
+def test_mc_scale_com_keeps_molecules_rigid():
+    # kernels/mc_barostat.cu:19-74: molecule centres scale about the origin;
+    # a water split across the cell boundary stays rigid, and a molecule
+    # inside the cell moves by exactly (s - 1) x its centre of mass
+    L = 20.0
+    box = np.array([L, L, L, 0.0, 0.0, 0.0])
+    s = 1.01
+    box1 = box * s
+    inside = np.array([[1.0, 2.0, 3.0], [2.8, 2.0, 3.0], [0.5, 3.7, 3.0]])
+    split = np.array([[9.9, 0.0, 0.0], [-9.6, 0.5, 0.0], [9.2, 1.6, 0.0]])  # H1 wrapped
+    pos = np.vstack([inside, split])
+    m = np.array([16.0, 1.0, 1.0, 16.0, 1.0, 1.0])
+    off = np.array([0, 3, 6])
+    atoms = np.arange(6)
+    img = np.zeros((6, 3), dtype=np.int32)
+    p1, i1 = O.mc_scale_com(off, atoms, m, box, box1, s, pos, img)
+    com_in = (m[:3, None] * inside).sum(0) / m[:3].sum()
+    assert np.allclose(p1[:3], inside + (s - 1) * com_in, atol=1e-12)
+    contig = split.copy()
+    contig[1, 0] += L
+    com_sp = (m[3:, None] * contig).sum(0) / m[3:].sum()
+    # rigid: the contiguous image rebuilt in the new cell is the old one
+    # translated, and its centre of mass scaled by s
+    d = p1[3:] - p1[3]
+    d -= box1[:3] * np.round(d / box1[:3])
+    new_contig = p1[3] + d
+    assert np.allclose(new_contig - new_contig[0], contig - contig[0], atol=1e-12)
+    assert np.allclose((m[3:, None] * new_contig).sum(0) / m[3:].sum(), s * com_sp, atol=1e-12)
+    # image counts keep each atom's integer offset from its molecule's
+    # contiguous image: x + img L' = contiguous + (img0 + K) L', K = -1 for
+    # the wrapped H
+    unwrapped = p1[3:] + i1[3:] * box1[:3]
+    K = np.array([[0, 0, 0], [-1, 0, 0], [0, 0, 0]])
+    assert np.allclose(unwrapped, new_contig + K * box1[:3], atol=1e-12)
+    # every stored atom is inside the new cell
+    assert np.all(np.abs(p1) <= 0.5 * box1[:3] + 1e-12)
