@@ -31,6 +31,7 @@ ERROR_NAMES = {
 HB_FORCES_ONLY, HB_FORCES_AND_SCALARS = 0, 1
 HB_INTEGRATOR_VV, HB_INTEGRATOR_VV_LOSSLESS, HB_INTEGRATOR_LANGEVIN = 0, 1, 2
 HB_CONSTRAINT_SETTLE, HB_CONSTRAINT_SHAKE = 0, 1
+HB_PAIRS_FAST, HB_PAIRS_EXACT = 0, 1
 
 PD = C.POINTER(C.c_double)
 PU32 = C.POINTER(C.c_uint32)
@@ -83,6 +84,7 @@ class ForceFieldDesc(C.Structure):
         ("excl_lj_scale", PD),
         ("excl_coulomb_scale", PD),
         ("r_skin", C.c_double),
+        ("pair_mode", C.c_int),
     ]
 
 
@@ -131,6 +133,7 @@ SIGNATURES = {
     "hb_system_get_state": (C.c_int, [VP, PD, PD, PI32, PD]),
     "hb_system_set_box": (C.c_int, [VP, PD]),
     "hb_system_get_box": (C.c_int, [VP, PD]),
+    "hb_system_flip_velocities": (C.c_int, [VP]),
     "hb_forcefield_create": (C.c_int, [VP, C.POINTER(ForceFieldDesc), PVP]),
     "hb_forcefield_destroy": (C.c_int, [VP]),
     "hb_forcefield_step": (C.c_int, [VP, C.c_int]),

@@ -120,6 +120,9 @@ class System:
         b = _f64(box)
         N.check(self.lib.hb_system_set_box(self.h, N.dptr(b)))
 
+    def flip_velocities(self) -> None:
+        N.check(self.lib.hb_system_flip_velocities(self.h))
+
     def box(self) -> np.ndarray:
         b = np.zeros(6)
         N.check(self.lib.hb_system_get_box(self.h, N.dptr(b)))
@@ -222,7 +225,7 @@ class ForceField:
     """ForceField::new / step over the C ABI."""
 
     def __init__(self, system: System, config: dict, exclusions=None, r_skin: float = 0.0,
-                 registry: PotentialRegistry | None = None):
+                 registry: PotentialRegistry | None = None, exact_pairs: bool = False):
         self.system = system
         self.lib = system.lib
         reg = registry or DEFAULT_POTENTIALS
@@ -239,13 +242,14 @@ class ForceField:
             d.excl_offsets, d.excl_partners = N.u32ptr(arrs[0]), N.u32ptr(arrs[1])
             d.excl_lj_scale, d.excl_coulomb_scale = N.dptr(arrs[2]), N.dptr(arrs[3])
         d.r_skin = float(r_skin)
+        d.pair_mode = N.HB_PAIRS_EXACT if exact_pairs else N.HB_PAIRS_FAST
         h = C.c_void_p()
         N.check(self.lib.hb_forcefield_create(system.h, C.byref(d), C.byref(h)))
         self.h = h
 
     @classmethod
     def from_spec(cls, system: System, spec: SystemSpec, r_skin: float | None = None,
-                  reciprocal: bool = True) -> "ForceField":
+                  reciprocal: bool = True, exact_pairs: bool = False) -> "ForceField":
         cfg = {}
         if spec.lj_sigma is not None:
             cfg["lennard_jones"] = LennardJonesParams(spec.lj_sigma, spec.lj_epsilon,
@@ -256,7 +260,8 @@ class ForceField:
         excl = None
         if spec.excl_offsets is not None:
             excl = (spec.excl_offsets, spec.excl_partners, spec.excl_lj, spec.excl_coul)
-        return cls(system, cfg, excl, spec.r_skin if r_skin is None else r_skin)
+        return cls(system, cfg, excl, spec.r_skin if r_skin is None else r_skin,
+                   exact_pairs=exact_pairs)
 
     def step(self, scalars: bool = False) -> None:
         N.check(self.lib.hb_forcefield_step(

@@ -145,6 +145,7 @@ int sys_refresh_box(hb_system *sys) {
 static int upload_state(hb_system *sys, const double *pos, const double *vel,
                         const int32_t *images_in, bool keep_images) {
   const uint32_t n = sys->n;
+  sys->fix_valid = false;
   if (keep_images) HB_TRY(sys_refresh_box(sys));
   std::vector<float4> posq(n), v(n);
   std::vector<int4> img(n);
@@ -221,10 +222,10 @@ extern "C" int hb_system_create(hb_context *ctx, const hb_system_desc *d, hb_sys
   HB_CUDA(cudaMalloc(&s->d_force, sizeof(float4) * nn));
   HB_CUDA(cudaMemset(s->d_force, 0, sizeof(float4) * nn));
   HB_CUDA(cudaMalloc(&s->d_pos_prev, sizeof(float4) * nn));
-  HB_CUDA(cudaMalloc(&s->d_vlo, sizeof(double) * 3 * nn));
-  HB_CUDA(cudaMemset(s->d_vlo, 0, sizeof(double) * 3 * nn));
-  HB_CUDA(cudaMalloc(&s->d_xlo, sizeof(double) * 3 * nn));
-  HB_CUDA(cudaMemset(s->d_xlo, 0, sizeof(double) * 3 * nn));
+  HB_CUDA(cudaMalloc(&s->d_vfix, sizeof(long long) * 3 * nn));
+  HB_CUDA(cudaMemset(s->d_vfix, 0, sizeof(long long) * 3 * nn));
+  HB_CUDA(cudaMalloc(&s->d_xfix, sizeof(long long) * 3 * nn));
+  HB_CUDA(cudaMemset(s->d_xfix, 0, sizeof(long long) * 3 * nn));
   HB_CUDA(cudaMalloc(&s->d_red, sizeof(double) * (4 * 296 + 8)));
   HB_CUDA(cudaMallocHost(&s->h_red, sizeof(double) * 8));
   int rc = upload_state(s, d->positions, d->velocities, d->images, false);
@@ -247,8 +248,8 @@ extern "C" int hb_system_destroy(hb_system *s) {
   cudaFree(s->d_image);
   cudaFree(s->d_force);
   cudaFree(s->d_pos_prev);
-  cudaFree(s->d_vlo);
-  cudaFree(s->d_xlo);
+  cudaFree(s->d_vfix);
+  cudaFree(s->d_xfix);
   cudaFree(s->d_red);
   cudaFreeHost(s->h_red);
   delete s;
@@ -263,6 +264,7 @@ extern "C" int hb_system_set_state(hb_system *sys, const double *positions,
   if (positions) {
     HB_TRY(upload_state(sys, positions, velocities, nullptr, true));
   } else if (velocities && n) {
+    sys->fix_valid = false;
     std::vector<float4> v(n);
     for (uint32_t i = 0; i < n; ++i)
       v[i] = make_float4((float)velocities[3 * i], (float)velocities[3 * i + 1],
@@ -325,6 +327,11 @@ extern "C" int hb_system_set_box(hb_system *sys, const double box[6]) {
   HB_CUDA(cudaMemcpy(sys->d_box, &db, sizeof(DBox), cudaMemcpyHostToDevice));
   HB_CUDA(cudaMemcpy(sys->d_box64, box, sizeof(double) * 6, cudaMemcpyHostToDevice));
   return HB_OK;
+}
+
+extern "C" int hb_system_flip_velocities(hb_system *sys) {
+  HB_REQUIRE(sys, HB_ERR_INVALID_ARGUMENT, "null system");
+  return integ_flip_velocities(sys, sys->ctx->stream);
 }
 
 extern "C" int hb_system_get_box(hb_system *sys, double box[6]) {
@@ -445,14 +452,18 @@ extern "C" int hb_forcefield_create(hb_system *sys, const hb_forcefield_desc *d,
                  "exclusion lists must be symmetric");
     epart.assign(d->excl_partners, d->excl_partners + ne);
   }
+  HB_REQUIRE(d->pair_mode == HB_PAIRS_FAST || d->pair_mode == HB_PAIRS_EXACT,
+             HB_ERR_INVALID_ARGUMENT, "unknown pair_mode");
   hb_forcefield *ff = new hb_forcefield();
   *ff = tmp;
   ff->sys = sys;
   // pair kernel: the rotation sweep by default; HB_PAIR_KERNEL=compact selects
-  // the compacted pair-list form (shared-memory int64 atomics)
+  // the compacted pair-list form (shared-memory int64 atomics); exact pairs
+  // use the compacted form with per-pair fixed point and minimum image
   ff->pair_variant = 1;
   if (const char *pk = std::getenv("HB_PAIR_KERNEL"))
     ff->pair_variant = std::string(pk) == "compact" ? 0 : 1;
+  if (d->pair_mode == HB_PAIRS_EXACT) ff->pair_variant = 2;
   HB_CUDA(cudaSetDevice(sys->ctx->device));
   HB_CUDA(cudaMalloc(&ff->d_lj, sizeof(float4) * ff->h_lj.size()));
   HB_CUDA(cudaMemcpy(ff->d_lj, ff->h_lj.data(), sizeof(float4) * ff->h_lj.size(),
@@ -722,6 +733,7 @@ extern "C" int hb_constraints_create(hb_system *sys, const hb_constraints_desc *
 
 extern "C" int hb_constraints_before_drift(hb_constraints *c) {
   HB_REQUIRE(c, HB_ERR_INVALID_ARGUMENT, "null constraints");
+  c->sys->fix_valid = false;
   hb_system *sys = c->sys;
   if (sys->n)
     HB_CUDA(cudaMemcpyAsync(sys->d_pos_prev, sys->d_posq, sizeof(float4) * sys->n,
@@ -731,11 +743,13 @@ extern "C" int hb_constraints_before_drift(hb_constraints *c) {
 
 extern "C" int hb_constraints_after_drift(hb_constraints *c, double dt) {
   HB_REQUIRE(c, HB_ERR_INVALID_ARGUMENT, "null constraints");
+  c->sys->fix_valid = false;
   return cons_positions(c, dt, c->sys->ctx->stream);
 }
 
 extern "C" int hb_constraints_after_kick(hb_constraints *c, double dt) {
   HB_REQUIRE(c, HB_ERR_INVALID_ARGUMENT, "null constraints");
+  c->sys->fix_valid = false;
   return cons_velocities(c, dt, dt > 0.0, c->sys->ctx->stream);
 }
 
@@ -776,6 +790,15 @@ extern "C" int hb_integrator_create(hb_system *sys, const hb_integrator_desc *d,
       cudaEventCreate(&it->g_ev0) != cudaSuccess || cudaEventCreate(&it->g_ev1) != cudaSuccess) {
     hb_integrator_destroy(it);
     return hb_fail(HB_ERR_CUDA, "integrator state allocation failed");
+  }
+  if (it->kind == HB_INTEGRATOR_VV_LOSSLESS) {
+    // the fixed-point state starts from the current f32 state (snapped to it)
+    int rc = integ_fix_derive(sys, sys->ctx->stream);
+    if (rc == HB_OK && cudaStreamSynchronize(sys->ctx->stream) != cudaSuccess) rc = HB_ERR_CUDA;
+    if (rc != HB_OK) {
+      hb_integrator_destroy(it);
+      return hb_fail(rc, "lossless state initialisation failed");
+    }
   }
   *out = it;
   return HB_OK;
@@ -839,6 +862,7 @@ extern "C" int hb_barostat_mc_move(hb_barostat *b, hb_forcefield *ff) {
   HB_REQUIRE(ff->sys == b->sys, HB_ERR_INVALID_ARGUMENT,
              "barostat and force field must share one system");
   if (b->sys->n == 0) return HB_OK;
+  b->sys->fix_valid = false;
   HB_TRY(baro_move(b, ff, false));
   return check_status(ff);
 }
@@ -857,11 +881,28 @@ static bool move_due(const hb_integrator *it, uint64_t step_number) {
   return it->baro && it->sys->n && step_number % it->baro->frequency == 0;
 }
 
+// Lossless mode keeps its own fixed-point state: it takes no constraints or
+// barostat (the reference's lossless integrator rejects constraints,
+// src/integrator/mod.rs:652) and re-derives the state when something else
+// wrote positions or velocities; any other integrator invalidates it.
+static int lossless_prologue(hb_integrator *it, hb_constraints *cons) {
+  hb_system *sys = it->sys;
+  if (it->kind != HB_INTEGRATOR_VV_LOSSLESS) {
+    sys->fix_valid = false;
+    return HB_OK;
+  }
+  HB_REQUIRE(!cons, HB_ERR_UNSUPPORTED, "the lossless integrator does not support constraints");
+  HB_REQUIRE(!it->baro, HB_ERR_UNSUPPORTED, "the lossless integrator does not support a barostat");
+  if (!sys->fix_valid) HB_TRY(integ_fix_derive(sys, sys->ctx->stream));
+  return HB_OK;
+}
+
 extern "C" int hb_integrator_step(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons,
                                   uint32_t n_steps, uint32_t scalar_every) {
   HB_REQUIRE(it && ff, HB_ERR_INVALID_ARGUMENT, "null argument");
   HB_REQUIRE(ff->sys == it->sys && (!cons || cons->sys == it->sys), HB_ERR_INVALID_ARGUMENT,
              "integrator, force field and constraints must share one system");
+  HB_TRY(lossless_prologue(it, cons));
   hb_context *ctx = it->sys->ctx;
   StageTimer timer{ctx, {}, 0};
   if (ctx->timing) g_timer = &timer;
@@ -925,6 +966,7 @@ extern "C" int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
   HB_REQUIRE(it && ff, HB_ERR_INVALID_ARGUMENT, "null argument");
   HB_REQUIRE(ff->sys == it->sys && (!cons || cons->sys == it->sys), HB_ERR_INVALID_ARGUMENT,
              "integrator, force field and constraints must share one system");
+  HB_TRY(lossless_prologue(it, cons));
   hb_context *ctx = it->sys->ctx;
   cudaStream_t s = ctx->stream;
   if (!it->forces_valid) {

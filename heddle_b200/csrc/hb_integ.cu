@@ -10,7 +10,7 @@
 //     fixed-shape trees -> byte-identical scalars run to run
 //     (kernels/nose_hoover.cu:22-103, kernels/barostat.cu:11-78);
 //   * velocity Verlet kick-drift / kick (kernels/integrate.cu:24-265) with
-//     the lossless (f32 value + f64 low part) variant, and the Langevin
+//     a lossless variant, and the Langevin
 //     middle scheme whose O step draws Philox-4x32-10 Gaussians keyed by
 //     (seed, step, atom, axis) (kernels/langevin.cu:13-80,
 //     kernels/philox.cuh).
@@ -140,62 +140,130 @@ __global__ void k_vv_kick(float4 *__restrict__ vel, const float4 *__restrict__ f
   vel[i] = v;
 }
 
-// lossless variant: (v_hi + v_lo) and (x_hi + x_lo) carried in f32 + f64
-// (kernels/integrate.cu:46-110)
-__global__ void k_vvl_kick_drift(float4 *__restrict__ posq, float4 *__restrict__ vel,
-                                 int4 *__restrict__ image, const float4 *__restrict__ force,
-                                 float4 *__restrict__ prev, double *__restrict__ xlo,
-                                 double *__restrict__ vlo, const DBox *__restrict__ box, float dt,
-                                 uint32_t n) {
+// Lossless variant.  The reference carries (f32 value, f64 low part) pairs
+// (kernels/integrate.cu:46-110); their round trip is exact only while no
+// f64 rounding error crosses an f32 rounding boundary.  Here the state is
+// 64-bit fixed point -- X in 2^-40 bohr, V in 2^-56 bohr/aut -- and one
+// step is
+//   V += K(X),  X += g(V),  wrap X by integer lattice vectors,  V += K(X)
+// with K(X) = rint(F(X) dt / 2m * 2^56) and g(V) = rint(V dt 2^-16), g odd.
+// Every update is an integer addition, so flipping V and stepping again
+// retraces the trajectory exactly (bit-exact time reversal by
+// construction, given forces that are a function of the positions alone).
+// posq / vel are the f32 images of X / V.
+__device__ __forceinline__ long long fix_kick(float f, double kc) {
+  return llrint((double)f * kc);
+}
+
+__global__ void k_fix_derive(float4 *__restrict__ posq, float4 *__restrict__ vel,
+                             long long *__restrict__ xfix, long long *__restrict__ vfix,
+                             uint32_t n) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const DBox b = *box;
+  float4 p = posq[i], v = vel[i];
+  const long long X[3] = {llrint((double)p.x * HB_XFIX_SCALE), llrint((double)p.y * HB_XFIX_SCALE),
+                          llrint((double)p.z * HB_XFIX_SCALE)};
+  const long long V[3] = {llrint((double)v.x * HB_VFIX_SCALE), llrint((double)v.y * HB_VFIX_SCALE),
+                          llrint((double)v.z * HB_VFIX_SCALE)};
+  for (int d = 0; d < 3; ++d) {
+    xfix[3 * i + d] = X[d];
+    vfix[3 * i + d] = V[d];
+  }
+  p.x = (float)((double)X[0] / HB_XFIX_SCALE);
+  p.y = (float)((double)X[1] / HB_XFIX_SCALE);
+  p.z = (float)((double)X[2] / HB_XFIX_SCALE);
+  v.x = (float)((double)V[0] / HB_VFIX_SCALE);
+  v.y = (float)((double)V[1] / HB_VFIX_SCALE);
+  v.z = (float)((double)V[2] / HB_VFIX_SCALE);
+  posq[i] = p;
+  vel[i] = v;
+}
+
+__global__ void k_vvl_kick_drift(float4 *__restrict__ posq, float4 *__restrict__ vel,
+                                 int4 *__restrict__ image, const float4 *__restrict__ force,
+                                 float4 *__restrict__ prev, long long *__restrict__ xfix,
+                                 long long *__restrict__ vfix, const double *__restrict__ lat,
+                                 double dt, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
   float4 p = posq[i];
   float4 v = vel[i];
   const float4 f = force[i];
   prev[i] = p;
-  const float h = 0.5f * dt * v.w;
-  float a[3] = {f.x * h, f.y * h, f.z * h};
-  float *vv[3] = {&v.x, &v.y, &v.z};
-  float *pp[3] = {&p.x, &p.y, &p.z};
+  const double kc = 0.5 * dt * (double)v.w * HB_VFIX_SCALE;
+  const double gc = dt * (HB_XFIX_SCALE / HB_VFIX_SCALE);
+  long long X[3], V[3];
+  const float fa3[3] = {f.x, f.y, f.z};
   for (int d = 0; d < 3; ++d) {
-    double ext = (double)*vv[d] + vlo[3 * i + d] + (double)a[d];
-    float hi = (float)ext;
-    vlo[3 * i + d] = ext - (double)hi;
-    *vv[d] = hi;
-    double dx = ((double)hi + vlo[3 * i + d]) * (double)dt;
-    double xe = (double)*pp[d] + xlo[3 * i + d] + dx;
-    float xh = (float)xe;
-    xlo[3 * i + d] = xe - (double)xh;
-    *pp[d] = xh;
+    V[d] = vfix[3 * i + d] + fix_kick(fa3[d], kc);
+    X[d] = xfix[3 * i + d] + llrint((double)V[d] * gc);
   }
-  int ka, kb, kc;
-  hb_wrap(p.x, p.y, p.z, ka, kb, kc, b);
-  int4 im = image[i];
-  im.x += ka;
-  im.y += kb;
-  im.z += kc;
-  image[i] = im;
+  // wrap by integer lattice vectors of the FP64 lattice
+  const double lx = lat[0], ly = lat[1], lz = lat[2], xy = lat[3], xz = lat[4], yz = lat[5];
+  const double x = (double)X[0] / HB_XFIX_SCALE, y = (double)X[1] / HB_XFIX_SCALE,
+               z = (double)X[2] / HB_XFIX_SCALE;
+  const double sc = z / lz, sb = (y - sc * yz) / ly, sa = (x - sb * xy - sc * xz) / lx;
+  const long long ka = (long long)floor(sa + 0.5), kb = (long long)floor(sb + 0.5),
+                  kcc = (long long)floor(sc + 0.5);
+  if (ka | kb | kcc) {
+    const long long LX = llrint(lx * HB_XFIX_SCALE), LY = llrint(ly * HB_XFIX_SCALE),
+                    LZ = llrint(lz * HB_XFIX_SCALE), XY = llrint(xy * HB_XFIX_SCALE),
+                    XZ = llrint(xz * HB_XFIX_SCALE), YZ = llrint(yz * HB_XFIX_SCALE);
+    X[0] -= ka * LX + kb * XY + kcc * XZ;
+    X[1] -= kb * LY + kcc * YZ;
+    X[2] -= kcc * LZ;
+    int4 im = image[i];
+    im.x += (int)ka;
+    im.y += (int)kb;
+    im.z += (int)kcc;
+    image[i] = im;
+  }
+  for (int d = 0; d < 3; ++d) {
+    xfix[3 * i + d] = X[d];
+    vfix[3 * i + d] = V[d];
+  }
+  p.x = (float)((double)X[0] / HB_XFIX_SCALE);
+  p.y = (float)((double)X[1] / HB_XFIX_SCALE);
+  p.z = (float)((double)X[2] / HB_XFIX_SCALE);
+  v.x = (float)((double)V[0] / HB_VFIX_SCALE);
+  v.y = (float)((double)V[1] / HB_VFIX_SCALE);
+  v.z = (float)((double)V[2] / HB_VFIX_SCALE);
   posq[i] = p;
   vel[i] = v;
 }
 
 __global__ void k_vvl_kick(float4 *__restrict__ vel, const float4 *__restrict__ force,
-                           double *__restrict__ vlo, float dt, uint32_t n) {
+                           long long *__restrict__ vfix, double dt, uint32_t n) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float4 v = vel[i];
   const float4 f = force[i];
-  const float h = 0.5f * dt * v.w;
-  float a[3] = {f.x * h, f.y * h, f.z * h};
-  float *vv[3] = {&v.x, &v.y, &v.z};
-  for (int d = 0; d < 3; ++d) {
-    double ext = (double)*vv[d] + vlo[3 * i + d] + (double)a[d];
-    float hi = (float)ext;
-    vlo[3 * i + d] = ext - (double)hi;
-    *vv[d] = hi;
-  }
+  const double kc = 0.5 * dt * (double)v.w * HB_VFIX_SCALE;
+  const long long V0 = vfix[3 * i] + fix_kick(f.x, kc);
+  const long long V1 = vfix[3 * i + 1] + fix_kick(f.y, kc);
+  const long long V2 = vfix[3 * i + 2] + fix_kick(f.z, kc);
+  vfix[3 * i] = V0;
+  vfix[3 * i + 1] = V1;
+  vfix[3 * i + 2] = V2;
+  v.x = (float)((double)V0 / HB_VFIX_SCALE);
+  v.y = (float)((double)V1 / HB_VFIX_SCALE);
+  v.z = (float)((double)V2 / HB_VFIX_SCALE);
   vel[i] = v;
+}
+
+// v <- -v on the f32 velocity and its fixed-point state
+__global__ void k_flip_velocities(float4 *__restrict__ vel, long long *__restrict__ vfix,
+                                  uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 v = vel[i];
+  v.x = -v.x;
+  v.y = -v.y;
+  v.z = -v.z;
+  vel[i] = v;
+  vfix[3 * i] = -vfix[3 * i];
+  vfix[3 * i + 1] = -vfix[3 * i + 1];
+  vfix[3 * i + 2] = -vfix[3 * i + 2];
 }
 
 __global__ void k_lang_kick(float4 *__restrict__ vel, const float4 *__restrict__ force, float dt,
@@ -328,8 +396,8 @@ int integ_vv_kick_drift(hb_integrator *it, cudaStream_t s) {
   if (sys->n == 0) return HB_OK;
   if (it->kind == HB_INTEGRATOR_VV_LOSSLESS)
     k_vvl_kick_drift<<<hb_div_up(sys->n, 256), 256, 0, s>>>(
-        sys->d_posq, sys->d_vel, sys->d_image, sys->d_force, sys->d_pos_prev, sys->d_xlo,
-        sys->d_vlo, sys->d_box, (float)it->dt, sys->n);
+        sys->d_posq, sys->d_vel, sys->d_image, sys->d_force, sys->d_pos_prev, sys->d_xfix,
+        sys->d_vfix, sys->d_box64, it->dt, sys->n);
   else
     k_vv_kick_drift<<<hb_div_up(sys->n, 256), 256, 0, s>>>(sys->d_posq, sys->d_vel, sys->d_image,
                                                            sys->d_force, sys->d_pos_prev,
@@ -338,12 +406,28 @@ int integ_vv_kick_drift(hb_integrator *it, cudaStream_t s) {
   return HB_OK;
 }
 
+int integ_flip_velocities(hb_system *sys, cudaStream_t s) {
+  if (sys->n == 0) return HB_OK;
+  k_flip_velocities<<<hb_div_up(sys->n, 256), 256, 0, s>>>(sys->d_vel, sys->d_vfix, sys->n);
+  HB_CUDA(cudaGetLastError());
+  return HB_OK;
+}
+
+int integ_fix_derive(hb_system *sys, cudaStream_t s) {
+  if (sys->n)
+    k_fix_derive<<<hb_div_up(sys->n, 256), 256, 0, s>>>(sys->d_posq, sys->d_vel, sys->d_xfix,
+                                                        sys->d_vfix, sys->n);
+  HB_CUDA(cudaGetLastError());
+  sys->fix_valid = true;
+  return HB_OK;
+}
+
 int integ_vv_kick(hb_integrator *it, cudaStream_t s) {
   hb_system *sys = it->sys;
   if (sys->n == 0) return HB_OK;
   if (it->kind == HB_INTEGRATOR_VV_LOSSLESS)
-    k_vvl_kick<<<hb_div_up(sys->n, 256), 256, 0, s>>>(sys->d_vel, sys->d_force, sys->d_vlo,
-                                                      (float)it->dt, sys->n);
+    k_vvl_kick<<<hb_div_up(sys->n, 256), 256, 0, s>>>(sys->d_vel, sys->d_force, sys->d_vfix,
+                                                      it->dt, sys->n);
   else
     k_vv_kick<<<hb_div_up(sys->n, 256), 256, 0, s>>>(sys->d_vel, sys->d_force, (float)it->dt,
                                                      sys->n);

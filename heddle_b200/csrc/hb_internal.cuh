@@ -44,6 +44,8 @@ int hb_fail(int code, const std::string &msg);
 #define HB_FP_SCALE 1099511627776.0f        /* 2^40 */
 #define HB_FP_INV_SCALE (1.0 / 1099511627776.0)
 #define HB_RHO_SCALE 4294967296.0f          /* 2^32 */
+#define HB_XFIX_SCALE 1099511627776.0       /* 2^40 per bohr */
+#define HB_VFIX_SCALE 72057594037927936.0   /* 2^56 per bohr / aut */
 
 #define HB_TILE 32
 #define HB_SENTINEL 0xFFFFFFFFu
@@ -199,8 +201,13 @@ struct hb_system {
   int4 *d_image = nullptr;       // image counts a, b, c, type
   float4 *d_force = nullptr;     // fx, fy, fz, 0 (total force, atom order)
   float4 *d_pos_prev = nullptr;  // pre-drift positions (constraint snapshot)
-  double *d_vlo = nullptr;       // lossless mode: low parts of v ([3n])
-  double *d_xlo = nullptr;       // lossless mode: low parts of x ([3n])
+  // lossless mode: the state as 64-bit fixed point ([3n] each), positions
+  // in 2^-40 bohr, velocities in 2^-56 bohr/aut; the f32 posq / vel are
+  // derived from it.  fix_valid: the fixed state mirrors posq / vel (any
+  // other writer of positions or velocities clears it).
+  long long *d_xfix = nullptr;
+  long long *d_vfix = nullptr;
+  bool fix_valid = false;
   std::vector<double> h_mass;
   std::vector<double> h_charge;
   std::vector<uint32_t> h_type;
@@ -234,7 +241,8 @@ struct hb_forcefield {
   std::vector<float4> h_lj;        // per type pair: sigma^2, 24 eps, cut^2, r_switch^2
   float4 *d_lj = nullptr;
   float alpha = 0.f, coul_rc2 = 0.f;
-  int pair_variant = 1;            // 0: compacted pair list, 1: full rotation sweep
+  int pair_variant = 1;            // 0: compacted pair list, 1: full rotation sweep,
+                                   // 2: compacted, per-pair fixed point + minimum image
   float rc_max = 0.f, r_skin = 0.f, r_search = 0.f;
   int any_switch = 0;
   int excl_scaled = 0;             // some exclusion has a non-zero scale
@@ -382,6 +390,9 @@ int integ_vv_kick(hb_integrator *it, cudaStream_t s);
 int integ_lang_kick(hb_integrator *it, cudaStream_t s);
 int integ_lang_drift_ou(hb_integrator *it, cudaStream_t s);
 int reduce_kinetic(hb_system *sys, double out[4]);
+int integ_flip_velocities(hb_system *sys, cudaStream_t s);
+// lossless mode: fixed-point state from posq / vel (and posq / vel snapped to it)
+int integ_fix_derive(hb_system *sys, cudaStream_t s);
 // system (hb_api.cu): copy the device FP64 lattice into the host mirror
 int sys_refresh_box(hb_system *sys);
 // Monte-Carlo barostat (hb_baro.cu): propose + scale, then (after a force

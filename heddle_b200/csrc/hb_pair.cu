@@ -311,7 +311,10 @@ struct P2Warp {
   uint16_t pairs[1024];
 };
 
-template <bool EV, bool SCALED, bool SWITCH>
+// EXACT: no single-periodic-copy shift (its rounding depends on the tile
+// the pair was packed into); every pair takes the minimum image of pi - pj,
+// so each pair force is a function of the two positions alone.
+template <bool EV, bool SCALED, bool SWITCH, bool EXACT>
 __global__ void __launch_bounds__(P2_WARPS * 32)
     k_pair2(const float4 *__restrict__ tile_posq, const int *__restrict__ tile_type,
             const float4 *__restrict__ center, const uint32_t *__restrict__ tile_nent,
@@ -332,7 +335,7 @@ __global__ void __launch_bounds__(P2_WARPS * 32)
   constexpr int NC = EV ? 5 : 3;
   const DBox b = *box;
   const float4 c = center[I];
-  const bool spc = ((int)c.w & 1) != 0;
+  const bool spc = !EXACT && ((int)c.w & 1) != 0;
   const uint32_t si = I * 32u + lane;
   const bool ivalid = si < P.n;
   float4 pi = tile_posq[si];
@@ -501,10 +504,10 @@ __global__ void __launch_bounds__(P2_WARPS * 32)
   }
 }
 
-template <bool EV, bool SCALED, bool SWITCH>
+template <bool EV, bool SCALED, bool SWITCH, bool EXACT>
 int launch2_t(hb_forcefield *ff, cudaStream_t s, const PairParams &P) {
   size_t smem = sizeof(float4) * (size_t)P.n_types * P.n_types;
-  k_pair2<EV, SCALED, SWITCH><<<hb_div_up(P.n_tiles, P2_WARPS), P2_WARPS * 32, smem, s>>>(
+  k_pair2<EV, SCALED, SWITCH, EXACT><<<hb_div_up(P.n_tiles, P2_WARPS), P2_WARPS * 32, smem, s>>>(
       ff->d_tile_posq, ff->d_tile_type, ff->d_tile_center, ff->d_tile_nent, ff->d_entry_j,
       ff->d_entry_excl, ff->sys->d_box, ff->d_lj, P, ff->d_fp, ff->d_acc, ff->d_sorted_ids,
       ff->d_excl_off, ff->d_excl_partner, ff->d_excl_scale);
@@ -543,11 +546,19 @@ int pair_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
   const bool sc = ff->excl_scaled != 0, sw = ff->any_switch != 0;
   if (ff->pair_variant == 0) {
     if (ev) {
-      if (sc) return sw ? launch2_t<true, true, true>(ff, s, P) : launch2_t<true, true, false>(ff, s, P);
-      return sw ? launch2_t<true, false, true>(ff, s, P) : launch2_t<true, false, false>(ff, s, P);
+      if (sc) return sw ? launch2_t<true, true, true, false>(ff, s, P) : launch2_t<true, true, false, false>(ff, s, P);
+      return sw ? launch2_t<true, false, true, false>(ff, s, P) : launch2_t<true, false, false, false>(ff, s, P);
     }
-    if (sc) return sw ? launch2_t<false, true, true>(ff, s, P) : launch2_t<false, true, false>(ff, s, P);
-    return sw ? launch2_t<false, false, true>(ff, s, P) : launch2_t<false, false, false>(ff, s, P);
+    if (sc) return sw ? launch2_t<false, true, true, false>(ff, s, P) : launch2_t<false, true, false, false>(ff, s, P);
+    return sw ? launch2_t<false, false, true, false>(ff, s, P) : launch2_t<false, false, false, false>(ff, s, P);
+  }
+  if (ff->pair_variant == 2) {
+    if (ev) {
+      if (sc) return sw ? launch2_t<true, true, true, true>(ff, s, P) : launch2_t<true, true, false, true>(ff, s, P);
+      return sw ? launch2_t<true, false, true, true>(ff, s, P) : launch2_t<true, false, false, true>(ff, s, P);
+    }
+    if (sc) return sw ? launch2_t<false, true, true, true>(ff, s, P) : launch2_t<false, true, false, true>(ff, s, P);
+    return sw ? launch2_t<false, false, true, true>(ff, s, P) : launch2_t<false, false, false, true>(ff, s, P);
   }
   if (ev) {
     if (sc) return sw ? launch_t<true, true, true>(ff, s, P) : launch_t<true, true, false>(ff, s, P);

@@ -125,6 +125,41 @@ def lj_argon(seed: int = 2024, n_atoms: int = 10_000, n_side: int = 22,
         meta={"sigma": sigma, "epsilon": eps, "r_cut": rc})
 
 
+def ionic_lattice(n_side: int = 32, spacing_A: float = 3.3, charge: float = 0.5,
+                  sigma_A: float = 3.0, eps_kj_mol: float = 0.5, mass_amu: float = 22.99,
+                  r_cut_A: float = 9.0, skin_A: float = 1.0, temperature_k: float = 300.0,
+                  seed: int = 3, velocity_seed: int = 13) -> SystemSpec:
+    """Rock-salt ordered +q/-q Lennard-Jones ions (one type, no constraints)
+    in a cubic box, with SPME at ~1 A grid spacing: an unconstrained system
+    that exercises the whole force path (pair kernel + reciprocal space)
+    under the plain and lossless velocity-Verlet integrators."""
+    n = n_side ** 3
+    a = U.angstrom_au(spacing_A)
+    L = n_side * a
+    rng = np.random.default_rng(seed)
+    idx = np.arange(n)
+    ijk = np.stack([idx // (n_side * n_side), (idx // n_side) % n_side, idx % n_side], axis=1)
+    pos = (ijk + 0.5) * a - 0.5 * L + rng.uniform(-0.02 * a, 0.02 * a, size=(n, 3))
+    charges = np.where(ijk.sum(1) % 2 == 0, charge, -charge).astype(np.float64)
+    mass = np.full(n, U.mass_au_amu(mass_amu))
+    from scipy.special import erfcinv
+
+    rc = U.angstrom_au(r_cut_A)
+    alpha = float(erfcinv(1e-5)) / rc
+    kt = U.temperature_au_k(temperature_k)
+    grid_n = fft_friendly(int(math.ceil(L / U.angstrom_au(1.0) - 1e-9)))
+    return SystemSpec(
+        name=f"ionic-lattice-{n}", positions=pos, velocities=generate_velocities(mass, kt, velocity_seed, 0),
+        masses=mass, charges=charges, types=np.zeros(n, dtype=np.uint32),
+        box=np.array([L, L, L, 0.0, 0.0, 0.0]), n_types=1,
+        lj_sigma=np.array([[U.angstrom_au(sigma_A)]]),
+        lj_epsilon=np.array([[U.energy_au_kj_per_mol(eps_kj_mol)]]),
+        lj_cutoff=np.array([[rc]]), lj_switch=np.array([[rc]]),
+        alpha=alpha, r_cut_coul=rc, grid=(grid_n, grid_n, grid_n), order=4,
+        r_skin=U.angstrom_au(skin_A), dt=U.time_au_fs(2.0), dt_fs=2.0, temperature=kt,
+        meta={"spacing_A": spacing_A})
+
+
 def _random_rotations(rng: np.random.Generator, n: int) -> np.ndarray:
     """Uniform rotations from uniform unit quaternions (Shoemake 1992)."""
     u1, u2, u3 = rng.random(n), rng.random(n), rng.random(n)

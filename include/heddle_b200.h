@@ -52,6 +52,9 @@ enum {
   HB_INTEGRATOR_LANGEVIN = 2     /* "langevin-baoab" (middle scheme) */
 };
 
+/* pair accumulation modes (hb_forcefield_desc.pair_mode) */
+enum { HB_PAIRS_FAST = 0, HB_PAIRS_EXACT = 1 };
+
 /* constraint kinds (src/integrator/constraint.rs:205-212) */
 enum { HB_CONSTRAINT_SETTLE = 0, HB_CONSTRAINT_SHAKE = 1 };
 
@@ -97,6 +100,10 @@ int hb_system_set_state(hb_system *sys, const double *positions,
 int hb_system_get_state(hb_system *sys, double *positions, double *velocities,
                         int32_t *images, double *forces);
 int hb_system_set_box(hb_system *sys, const double box[6]);
+/* Velocity flip v <- -v of both halves of the lossless (f32 + f64) state:
+ * step 3 of the reversal protocol (rqm/pipeline-reversibility.md,
+ * tests/integration_lossless.rs:302-395). */
+int hb_system_flip_velocities(hb_system *sys);
 int hb_system_get_box(hb_system *sys, double box[6]);
 
 /* ---- force field: replaces ForceField::new (src/forces/mod.rs:355-621)
@@ -125,6 +132,14 @@ typedef struct {
   const double *excl_coulomb_scale;
   /* neighbour list */
   double r_skin;
+  /* pair accumulation: HB_PAIRS_FAST sums each neighbour entry's 32 pair
+   * forces in f32 before the fixed-point add (the reference's scheme,
+   * src/forces/jit_composed.rs:1696-1786); HB_PAIRS_EXACT converts every
+   * pair force to fixed point and takes the minimum image per pair, so the
+   * forces are a function of the positions alone, independent of when the
+   * neighbour list was rebuilt and of how it packed the pairs -- what
+   * bit-exact time reversal of the lossless integrator needs. */
+  int pair_mode;
 } hb_forcefield_desc;
 
 int hb_forcefield_create(hb_system *sys, const hb_forcefield_desc *desc,
