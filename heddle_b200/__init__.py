@@ -6,6 +6,7 @@ fixed-point and FP64 reductions, behind a C ABI (include/heddle_b200.h)."""
 from ._native import HeddleError, load  # noqa: F401
 from .api import (  # noqa: F401
     Barostat,
+    Batch,
     Constraints,
     Context,
     ForceField,
@@ -17,6 +18,6 @@ from .api import (  # noqa: F401
 )
 
 __all__ = [
-    "Context", "System", "ForceField", "Constraints", "Integrator", "Barostat",
+    "Context", "System", "ForceField", "Constraints", "Integrator", "Barostat", "Batch",
     "PotentialRegistry", "LennardJonesParams", "SpmeParams", "HeddleError", "load",
 ]

@@ -158,6 +158,10 @@ SIGNATURES = {
     "hb_barostat_mc_move": (C.c_int, [VP, VP]),
     "hb_barostat_stats": (C.c_int, [VP, PD]),
     "hb_integrator_set_barostat": (C.c_int, [VP, VP]),
+    "hb_batch_create": (C.c_int, [VP, C.c_uint32, PVP, PVP, PVP, PVP]),
+    "hb_batch_destroy": (C.c_int, [VP]),
+    "hb_batch_step": (C.c_int, [VP, C.c_uint32]),
+    "hb_batch_count_launches": (C.c_int, [VP, PU64]),
     "hb_reduce_kinetic": (C.c_int, [VP, PD]),
     "hb_spme_recip_noalloc": (C.c_int, [C.c_void_p, C.c_uint32, PD, PU32, C.c_uint32, C.c_double,
                                         C.c_void_p, PD, C.c_void_p]),

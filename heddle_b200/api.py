@@ -475,3 +475,39 @@ class Barostat:
         if getattr(self, "h", None):
             self.lib.hb_barostat_destroy(self.h)
             self.h = None
+
+
+# ---------------------------------------------------------------------------
+# batched replicas
+# ---------------------------------------------------------------------------
+class Batch:
+    """Independent systems advanced together: every member's step in one
+    CUDA graph (one parallel branch per member context), one graph launch
+    per step.  members: list of (Integrator, ForceField, Constraints | None),
+    each on a Context of its own; ctx launches the graph."""
+
+    def __init__(self, ctx: Context, members):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self.members = list(members)
+        n = len(self.members)
+        arr = C.c_void_p * n
+        its = arr(*[m[0].h for m in self.members])
+        ffs = arr(*[m[1].h for m in self.members])
+        cons = arr(*[(m[2].h if m[2] is not None else None) for m in self.members])
+        h = C.c_void_p()
+        N.check(self.lib.hb_batch_create(ctx.h, n, its, ffs, cons, C.byref(h)))
+        self.h = h
+
+    def step(self, n_steps: int = 1) -> None:
+        N.check(self.lib.hb_batch_step(self.h, int(n_steps)))
+
+    def count_launches(self) -> tuple:
+        out = np.zeros(2, dtype=np.uint64)
+        N.check(self.lib.hb_batch_count_launches(self.h, out.ctypes.data_as(N.PU64)))
+        return int(out[0]), int(out[1])
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.hb_batch_destroy(self.h)
+            self.h = None

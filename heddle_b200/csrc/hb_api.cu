@@ -4,6 +4,7 @@
 // gated neighbour rebuild, pair kernel overlapped with SPME on a second
 // stream, force combine).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -14,6 +15,8 @@
 #include "hb_internal.cuh"
 
 static thread_local std::string g_err;
+static std::atomic<uint64_t> g_uid{1};
+uint64_t hb_next_uid() { return g_uid.fetch_add(1); }
 
 void hb_set_error(const std::string &msg) { g_err = msg; }
 int hb_fail(int code, const std::string &msg) {
@@ -973,15 +976,17 @@ extern "C" int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
     HB_TRY(force_eval(ff, false));
     it->forces_valid = true;
   }
-  if (!it->graph_exec || it->graph_ff != ff || it->graph_cons != cons ||
-      it->graph_baro != it->baro) {
+  const uint64_t cons_uid = cons ? cons->uid : 0, baro_uid = it->baro ? it->baro->uid : 0;
+  if (!it->graph_exec || it->graph_ff != ff->uid || it->graph_cons != cons_uid ||
+      it->graph_baro != baro_uid || it->graph_gen != ff->layout_gen) {
     drop_graphs(it);
     HB_CUDA(cudaStreamSynchronize(s));
     HB_TRY(capture_step(it, ff, cons, false, &it->graph_exec));
     if (it->baro) HB_TRY(capture_step(it, ff, cons, true, &it->graph_exec_move));
-    it->graph_ff = ff;
-    it->graph_cons = cons;
-    it->graph_baro = it->baro;
+    it->graph_ff = ff->uid;
+    it->graph_cons = cons_uid;
+    it->graph_baro = baro_uid;
+    it->graph_gen = ff->layout_gen;
   }
   if (ctx->timing) HB_CUDA(cudaEventRecord(it->g_ev0, s));
   for (uint32_t k = 0; k < n_steps; ++k) {
@@ -997,10 +1002,9 @@ extern "C" int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
     for (int q = 0; q < 8; ++q) ctx->t_ms[q] = 0.0;
     ctx->t_ms[0] = ms;
   }
-  const uint64_t cap_before = ff->entry_cap;
   HB_TRY(check_status(ff));
-  // buffers moved: the captured graphs hold stale pointers
-  if (ff->entry_cap != cap_before) drop_graphs(it);
+  // buffers or sizes changed: the captured graphs are stale
+  if (ff->layout_gen != it->graph_gen) drop_graphs(it);
   return HB_OK;
 }
 
@@ -1050,6 +1054,161 @@ extern "C" int hb_integrator_count_launches(hb_integrator *it, hb_forcefield *ff
   kernels[0] = eager - body + (body ? 1u : 0u);
   kernels[1] = body;
   kernels[2] = eager_move ? eager_move - body + 1u : 0u;
+  return HB_OK;
+}
+
+// ---------------------------------------------------------------------
+// batched replicas
+// ---------------------------------------------------------------------
+struct hb_batch {
+  hb_context *ctx = nullptr;                 // the graph launches on its stream
+  std::vector<hb_integrator *> its;
+  std::vector<hb_forcefield *> ffs;
+  std::vector<hb_constraints *> cons;
+  std::vector<cudaEvent_t> join;             // one per member
+  std::vector<uint64_t> gens;                // members' layout_gen at capture
+  cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+extern "C" int hb_batch_destroy(hb_batch *b) {
+  if (!b) return HB_OK;
+  cudaSetDevice(b->ctx->device);
+  cudaStreamSynchronize(b->ctx->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  for (auto e : b->join)
+    if (e) cudaEventDestroy(e);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->t0) cudaEventDestroy(b->t0);
+  if (b->t1) cudaEventDestroy(b->t1);
+  delete b;
+  return HB_OK;
+}
+
+extern "C" int hb_batch_create(hb_context *ctx, uint32_t n, hb_integrator *const *its,
+                               hb_forcefield *const *ffs, hb_constraints *const *cons,
+                               hb_batch **out) {
+  HB_REQUIRE(ctx && its && ffs && out && n > 0, HB_ERR_INVALID_ARGUMENT, "null argument");
+  for (uint32_t k = 0; k < n; ++k) {
+    HB_REQUIRE(its[k] && ffs[k], HB_ERR_INVALID_ARGUMENT, "null batch member");
+    HB_REQUIRE(ffs[k]->sys == its[k]->sys && (!cons || !cons[k] || cons[k]->sys == its[k]->sys),
+               HB_ERR_INVALID_ARGUMENT, "a member's integrator, force field and constraints "
+                                        "must share one system");
+    HB_REQUIRE(its[k]->sys->ctx->device == ctx->device, HB_ERR_INVALID_ARGUMENT,
+               "batch members must live on the batch's device");
+    HB_REQUIRE(its[k]->sys->ctx != ctx, HB_ERR_INVALID_ARGUMENT,
+               "batch members need contexts of their own (the batch context launches the graph)");
+    HB_REQUIRE(!its[k]->baro, HB_ERR_UNSUPPORTED, "batch members take no barostat");
+    for (uint32_t q = 0; q < k; ++q)
+      HB_REQUIRE(its[q]->sys != its[k]->sys, HB_ERR_INVALID_ARGUMENT,
+                 "a system may appear in one batch member only");
+  }
+  hb_batch *b = new hb_batch();
+  b->ctx = ctx;
+  b->its.assign(its, its + n);
+  b->ffs.assign(ffs, ffs + n);
+  b->cons.assign(n, nullptr);
+  if (cons)
+    for (uint32_t k = 0; k < n; ++k) b->cons[k] = cons[k];
+  b->join.assign(n, nullptr);
+  bool ok = cudaSetDevice(ctx->device) == cudaSuccess &&
+            cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreate(&b->t0) == cudaSuccess && cudaEventCreate(&b->t1) == cudaSuccess;
+  for (uint32_t k = 0; ok && k < n; ++k)
+    ok = cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    hb_batch_destroy(b);
+    return hb_fail(HB_ERR_CUDA, "batch event creation failed");
+  }
+  *out = b;
+  return HB_OK;
+}
+
+// one graph: fork from the batch stream to every member's stream, capture
+// the member's step there, join back
+static int batch_capture(hb_batch *b) {
+  cudaStream_t m = b->ctx->stream;
+  cudaGraph_t g;
+  HB_CUDA(cudaStreamBeginCapture(m, cudaStreamCaptureModeThreadLocal));
+  int rc = cudaEventRecord(b->fork, m) == cudaSuccess ? HB_OK : HB_ERR_CUDA;
+  std::vector<uint64_t> steps(b->its.size());
+  for (size_t k = 0; k < b->its.size() && rc == HB_OK; ++k) {
+    hb_integrator *it = b->its[k];
+    cudaStream_t s = it->sys->ctx->stream;
+    if (cudaStreamWaitEvent(s, b->fork, 0) != cudaSuccess) {
+      rc = hb_fail(HB_ERR_CUDA, "batch fork");
+      break;
+    }
+    steps[k] = it->step;
+    rc = one_step(it, b->ffs[k], b->cons[k], false, true);
+    it->step = steps[k];
+    if (rc == HB_OK && (cudaEventRecord(b->join[k], s) != cudaSuccess ||
+                        cudaStreamWaitEvent(m, b->join[k], 0) != cudaSuccess))
+      rc = hb_fail(HB_ERR_CUDA, "batch join");
+  }
+  cudaError_t ce = cudaStreamEndCapture(m, &g);
+  if (rc != HB_OK) return rc;
+  if (ce != cudaSuccess) return hb_fail(HB_ERR_CUDA, std::string("batch capture: ") + cudaGetErrorString(ce));
+  cudaError_t ie = cudaGraphInstantiate(&b->exec, g, 0);
+  cudaGraphDestroy(g);
+  if (ie != cudaSuccess) return hb_fail(HB_ERR_CUDA, std::string("batch instantiate: ") + cudaGetErrorString(ie));
+  return HB_OK;
+}
+
+extern "C" int hb_batch_step(hb_batch *b, uint32_t n_steps) {
+  HB_REQUIRE(b, HB_ERR_INVALID_ARGUMENT, "null batch");
+  hb_context *ctx = b->ctx;
+  const size_t n = b->its.size();
+  for (size_t k = 0; k < n; ++k) {
+    hb_integrator *it = b->its[k];
+    HB_REQUIRE(!it->baro, HB_ERR_UNSUPPORTED, "batch members take no barostat");
+    HB_TRY(lossless_prologue(it, b->cons[k]));
+    if (!it->forces_valid) {
+      HB_TRY(force_eval(b->ffs[k], false));
+      it->forces_valid = true;
+    }
+  }
+  // member streams before the batch stream: eager work above, then the graph
+  for (size_t k = 0; k < n; ++k) HB_CUDA(cudaStreamSynchronize(b->its[k]->sys->ctx->stream));
+  bool stale = b->gens.size() != n;
+  for (size_t k = 0; k < n && !stale; ++k) stale = b->gens[k] != b->ffs[k]->layout_gen;
+  if (stale && b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  if (!b->exec) {
+    HB_TRY(batch_capture(b));
+    b->gens.resize(n);
+    for (size_t k = 0; k < n; ++k) b->gens[k] = b->ffs[k]->layout_gen;
+  }
+  cudaStream_t m = ctx->stream;
+  if (ctx->timing) HB_CUDA(cudaEventRecord(b->t0, m));
+  for (uint32_t q = 0; q < n_steps; ++q) {
+    HB_CUDA(cudaGraphLaunch(b->exec, m));
+    for (size_t k = 0; k < n; ++k) b->its[k]->step++;
+  }
+  if (ctx->timing) HB_CUDA(cudaEventRecord(b->t1, m));
+  HB_CUDA(cudaStreamSynchronize(m));
+  if (ctx->timing) {
+    float ms = 0.f;
+    HB_CUDA(cudaEventElapsedTime(&ms, b->t0, b->t1));
+    for (int q = 0; q < 8; ++q) ctx->t_ms[q] = 0.0;
+    ctx->t_ms[0] = ms;
+  }
+  // a member whose list grows bumps its layout_gen: the next call recaptures
+  for (size_t k = 0; k < n; ++k) HB_TRY(check_status(b->ffs[k]));
+  return HB_OK;
+}
+
+extern "C" int hb_batch_count_launches(hb_batch *b, uint64_t kernels[2]) {
+  HB_REQUIRE(b && kernels, HB_ERR_INVALID_ARGUMENT, "null argument");
+  kernels[0] = kernels[1] = 0;
+  for (size_t k = 0; k < b->its.size(); ++k) {
+    uint64_t c[3] = {0, 0, 0};
+    HB_TRY(hb_integrator_count_launches(b->its[k], b->ffs[k], b->cons[k], c));
+    kernels[0] += c[0];
+    kernels[1] += c[1];
+  }
   return HB_OK;
 }
 

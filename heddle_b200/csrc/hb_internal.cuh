@@ -233,8 +233,14 @@ struct SpmeState {
   float self_pref = 0.f;                      // alpha / sqrt(pi)
 };
 
+// process-wide creation counter: objects that captured graphs refer to are
+// compared by this id, never by address (a freed object's address can be
+// reused by a new one)
+uint64_t hb_next_uid();
+
 struct hb_forcefield {
   hb_system *sys = nullptr;
+  uint64_t uid = hb_next_uid();
   // ---- parameters
   int lj_on = 0, coul_on = 0;
   uint32_t n_types = 0;
@@ -269,6 +275,8 @@ struct hb_forcefield {
   uint32_t *d_entry_j = nullptr;     // [n_tiles * slab * 32] sorted j slots
   uint32_t *d_entry_excl = nullptr;  // [n_tiles * slab * 32] exclusion masks
   uint64_t entry_cap = 0;            // n_tiles * slab
+  uint64_t layout_gen = 0;           // bumped when list buffers or sizes change:
+                                     // captured graphs older than it are stale
   float4 *d_ref_pos = nullptr;       // positions at the last rebuild
   DBox *d_ref_box = nullptr;         // box at the last rebuild
   uint32_t *d_status = nullptr;      // status word
@@ -293,6 +301,7 @@ struct hb_forcefield {
 
 struct hb_constraints {
   hb_system *sys = nullptr;
+  uint64_t uid = hb_next_uid();
   uint32_t n_settle = 0, n_shake = 0;
   // SETTLE: per group (O, H1, H2) atom ids and geometry
   uint4 *d_settle_atoms = nullptr;   // o, h1, h2, 0
@@ -320,13 +329,14 @@ struct hb_integrator {
   // graph mode
   cudaGraphExec_t graph_exec = nullptr;
   cudaEvent_t g_ev0 = nullptr, g_ev1 = nullptr;
-  hb_forcefield *graph_ff = nullptr;
-  hb_constraints *graph_cons = nullptr;
+  uint64_t graph_ff = 0;        // uids of the objects the graphs were captured with
+  uint64_t graph_cons = 0;
+  uint64_t graph_gen = 0;       // the force field's layout_gen at capture
   // Monte-Carlo barostat attached to the step loop (may be null) and the
   // graph of a step that ends with a volume move
   hb_barostat *baro = nullptr;
   cudaGraphExec_t graph_exec_move = nullptr;
-  hb_barostat *graph_baro = nullptr;
+  uint64_t graph_baro = 0;
 };
 
 // Device-resident state of the Monte-Carlo barostat (FP64).  The whole move
@@ -346,6 +356,7 @@ struct BaroState {
 
 struct hb_barostat {
   hb_system *sys = nullptr;
+  uint64_t uid = hb_next_uid();
   double pressure = 0.0, kt = 0.0;
   uint32_t frequency = 25;
   uint64_t seed = 0;

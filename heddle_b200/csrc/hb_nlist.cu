@@ -657,6 +657,7 @@ int nl_first_build(hb_forcefield *ff) {
     const uint32_t want_c = mc + mc / 2 + 64;
     if (mc <= ff->maxc && ff->maxc >= want_c) break;
     ff->maxc = std::max(want_c, ff->maxc);
+    ff->layout_gen++;
     HB_CUDA(cudaFuncSetAttribute(k_nl_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(sizeof(uint32_t) * (3u * ff->maxc + 1u))));
     HB_CUDA(cudaFuncSetAttribute(k_nl_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -679,6 +680,7 @@ int nl_first_build(hb_forcefield *ff) {
     HB_CUDA(cudaMalloc(&ff->d_entry_excl, sizeof(uint32_t) * 32 * cap));
     ff->slab = want;
     ff->entry_cap = cap;
+    ff->layout_gen++;
   }
   HB_TRY(nl_launch(ff, nullptr, s, false, false));
   uint32_t st = 0;

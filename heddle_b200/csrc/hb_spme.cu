@@ -640,7 +640,9 @@ void twiddles(int n, std::vector<float2> &out) {
 
 size_t fft_smem(int n, int L) { return sizeof(float2) * ((size_t)n + 2 * (size_t)L * (n + 1)); }
 
-#define HB_FFT_SIZES(X) X(16) X(20) X(24) X(25) X(32) X(40) X(48) X(64) X(80) X(96) X(128) X(160) X(192) X(256)
+#define HB_FFT_SIZES(X) \
+  X(16) X(20) X(24) X(25) X(27) X(30) X(32) X(36) X(40) X(45) X(48) X(50) X(54) X(60) X(64) \
+  X(80) X(96) X(128) X(160) X(192) X(256)
 
 struct SpmeLaunch {
   int na, nb, nc, nch, La, Lb, Lc;

@@ -280,3 +280,23 @@ def water_shake_groups(spec: SystemSpec) -> SystemSpec:
     spec.con_j = np.tile(np.array([1, 2, 2], dtype=np.uint32), n_mol)
     spec.con_dist = np.tile(np.array([r_oh, r_oh, d_hh]), n_mol)
     return spec
+
+
+def replica_batch(seed: int = 2025, n_boxes: int = 64, lo: int = 256, hi: int = 8192,
+                  r_cut_A: float = 9.0, skin_A: float = 1.2) -> list:
+    """The uneven replica batch: n_boxes SPC water boxes with N_mol drawn
+    log-uniform in [lo, hi] from `seed`, each built like the 8,192-molecule
+    NVT box (300 K, own seeds), grid ~1 A rounded to a 5-smooth size.  The
+    skin is capped per box so that 2 (r_cut + skin) fits the box width."""
+    rng = np.random.default_rng(seed)
+    n_mol = np.exp(rng.uniform(math.log(lo), math.log(hi), size=n_boxes)).astype(int)
+    specs = []
+    for k, nm in enumerate(n_mol):
+        probe = spc_water(int(nm), seed=1000 + k, velocity_seed=2000 + k, r_cut_A=r_cut_A,
+                          skin_A=skin_A)
+        width_A = probe.box[0] * U.BOHR_M / U.ANGSTROM_M
+        cap = 0.5 * width_A * (1.0 - 2e-4) - r_cut_A - 0.01
+        if cap < skin_A:
+            probe.r_skin = U.angstrom_au(max(cap, 0.2))
+        specs.append(probe)
+    return specs

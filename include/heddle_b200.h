@@ -64,6 +64,7 @@ typedef struct hb_forcefield hb_forcefield;
 typedef struct hb_constraints hb_constraints;
 typedef struct hb_integrator hb_integrator;
 typedef struct hb_barostat hb_barostat;
+typedef struct hb_batch hb_batch;
 
 /* Message of the last failing call on this thread ("" when none). */
 const char *hb_last_error(void);
@@ -282,6 +283,27 @@ int hb_barostat_stats(hb_barostat *b, double out[15]);
  * number is a multiple of the barostat's frequency evaluates scalars and is
  * followed by a move (src/runner.rs:2693-2708). */
 int hb_integrator_set_barostat(hb_integrator *it, hb_barostat *b);
+
+/* ---- batched replicas: the runner's captured-graph replay
+ * (src/runner.rs:2803-3000, src/gpu/graph.rs:222-242) extended to many
+ * independent systems of uneven sizes.  Every member's whole step is
+ * captured into ONE CUDA graph, each member on its own parallel branch
+ * (the streams of the member's context), so one graph launch advances every
+ * system by one step; each member keeps its device-side rebuild decision.
+ * Members keep their own force fields, constraints and integrators
+ * (velocity Verlet or Langevin; no barostat); members that share a context
+ * share its streams and run one after another inside the graph.  cons may
+ * be NULL or hold NULL entries.  Members must outlive the batch; a member's
+ * list growth (or any capacity change) makes the next call recapture. */
+int hb_batch_create(hb_context *ctx, uint32_t n_members, hb_integrator *const *its,
+                    hb_forcefield *const *ffs, hb_constraints *const *cons, hb_batch **out);
+int hb_batch_destroy(hb_batch *b);
+/* n_steps graph launches; the device time is reported by hb_timing_get on
+ * the batch's context (out[0]) when timing is enabled there. */
+int hb_batch_step(hb_batch *b, uint32_t n_steps);
+/* kernels[0] = kernels of one batch step (all members), kernels[1] = sum
+ * over members of the kernels of one neighbour rebuild. */
+int hb_batch_count_launches(hb_batch *b, uint64_t kernels[2]);
 
 /* ---- FP64 deterministic scalar reductions (kernels/nose_hoover.cu:22-103,
  * kernels/barostat.cu:11-78): kinetic energy and the mass-weighted

@@ -186,3 +186,17 @@ def test_tiny_systems(ctx):
     assert ff0.scalars()["potential"] == 0.0
     ff0.close()
     empty.close()
+
+
+@pytest.mark.parametrize("grid", [(27, 27, 27), (30, 36, 45), (50, 54, 60), (20, 24, 25)],
+                         ids=lambda g: "x".join(map(str, g)))
+def test_compiled_fft_sizes_match_oracle(ctx, grid):
+    # every compile-time specialised FFT length (radix 2/3/4/5 stage plans),
+    # also anisotropic grids: reciprocal energy and total forces vs FP64
+    spec = S.spc_water(216, r_cut_A=7.0, skin_A=1.0, seed=4)
+    spec.grid = grid
+    pos, F, sc, _, _ = gpu_forces(ctx, spec)
+    Fo, _, _, To = O.forces(spec, pos)
+    assert rms_rel(F, Fo) <= FORCE_RMS_TOL
+    _, _, _, Tp = O.forces(spec, pos, poly_erfc=True)
+    assert abs(sc["recip"] - Tp["recip"]) <= 1e-5 * abs(Tp["recip"])
