@@ -11,13 +11,18 @@ from .api import (  # noqa: F401
     Context,
     ForceField,
     Integrator,
+    HarmonicAngleParams,
+    HarmonicBondParams,
     LennardJonesParams,
+    PeriodicDihedralParams,
     PotentialRegistry,
+    ShakeMLP,
     SpmeParams,
     System,
 )
 
 __all__ = [
     "Context", "System", "ForceField", "Constraints", "Integrator", "Barostat", "Batch",
-    "PotentialRegistry", "LennardJonesParams", "SpmeParams", "HeddleError", "load",
+    "PotentialRegistry", "LennardJonesParams", "SpmeParams", "HarmonicBondParams",
+    "HarmonicAngleParams", "PeriodicDihedralParams", "ShakeMLP", "HeddleError", "load",
 ]

@@ -37,6 +37,7 @@ PD = C.POINTER(C.c_double)
 PU32 = C.POINTER(C.c_uint32)
 PI32 = C.POINTER(C.c_int32)
 PU64 = C.POINTER(C.c_uint64)
+PF32 = C.POINTER(C.c_float)
 
 
 class SystemDesc(C.Structure):
@@ -85,6 +86,19 @@ class ForceFieldDesc(C.Structure):
         ("excl_coulomb_scale", PD),
         ("r_skin", C.c_double),
         ("pair_mode", C.c_int),
+        ("n_bonds", C.c_uint32),
+        ("bond_atoms", PU32),
+        ("bond_k", PD),
+        ("bond_r0", PD),
+        ("n_angles", C.c_uint32),
+        ("angle_atoms", PU32),
+        ("angle_k", PD),
+        ("angle_theta0", PD),
+        ("n_dihedrals", C.c_uint32),
+        ("dihedral_atoms", PU32),
+        ("dihedral_k", PD),
+        ("dihedral_phi0", PD),
+        ("dihedral_n", PU32),
     ]
 
 
@@ -103,6 +117,7 @@ class ConstraintsDesc(C.Structure):
         ("con_dist", PD),
         ("shake_tol", C.c_double),
         ("shake_max_iter", C.c_uint32),
+        ("shake_tol_relative", C.c_int),
     ]
 
 
@@ -148,6 +163,20 @@ SIGNATURES = {
     "hb_constraints_after_drift": (C.c_int, [VP, C.c_double]),
     "hb_constraints_after_kick": (C.c_int, [VP, C.c_double]),
     "hb_constraints_get_virial": (C.c_int, [VP, PD]),
+    "hb_constraints_shake_stats": (C.c_int, [VP, PD, C.c_int]),
+    "hb_constraints_record": (C.c_int, [VP, C.c_int]),
+    "hb_constraints_get_record": (C.c_int, [VP, PF32, PD, PD, PD, PU32]),
+    "hb_constraints_set_warm_start": (C.c_int, [VP, VP]),
+    "hb_shake_mlp_create": (C.c_int, [VP, C.c_uint64, PVP]),
+    "hb_shake_mlp_destroy": (C.c_int, [VP]),
+    "hb_shake_mlp_param_count": (C.c_uint32, []),
+    "hb_shake_mlp_get_params": (C.c_int, [VP, PF32, C.c_uint32]),
+    "hb_shake_mlp_set_params": (C.c_int, [VP, PF32, C.c_uint32]),
+    "hb_shake_mlp_set_normalization": (C.c_int, [VP, PF32, PF32, C.c_float]),
+    "hb_shake_mlp_predict": (C.c_int, [VP, PF32, C.c_uint64, PF32]),
+    "hb_shake_mlp_gradients": (C.c_int, [VP, PF32, PF32, C.c_uint32, PF32, PD]),
+    "hb_shake_mlp_train": (C.c_int, [VP, PF32, PF32, C.c_uint64, C.c_uint32, C.c_uint32,
+                                     C.c_double, C.c_uint64, PD]),
     "hb_integrator_create": (C.c_int, [VP, C.POINTER(IntegratorDesc), PVP]),
     "hb_integrator_destroy": (C.c_int, [VP]),
     "hb_integrator_step": (C.c_int, [VP, VP, VP, C.c_uint32, C.c_uint32]),
@@ -218,6 +247,13 @@ def u32ptr(a: np.ndarray | None):
         return None
     assert a.dtype == np.uint32 and a.flags.c_contiguous
     return a.ctypes.data_as(PU32)
+
+
+def f32ptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(PF32)
 
 
 def i32ptr(a: np.ndarray | None):

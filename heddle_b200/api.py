@@ -159,6 +159,28 @@ class SpmeParams:
     reciprocal: bool = True
 
 
+@dataclass
+class HarmonicBondParams:
+    atoms: np.ndarray      # [n, 2]
+    k: np.ndarray          # hartree / bohr^2
+    r0: np.ndarray         # bohr
+
+
+@dataclass
+class HarmonicAngleParams:
+    atoms: np.ndarray      # [n, 3], vertex in the middle
+    k: np.ndarray          # hartree / rad^2
+    theta0: np.ndarray     # rad
+
+
+@dataclass
+class PeriodicDihedralParams:
+    atoms: np.ndarray      # [n, 4]
+    k: np.ndarray          # hartree
+    phi0: np.ndarray       # rad
+    n: np.ndarray          # multiplicity
+
+
 class PotentialBuilder:
     label = ""
 
@@ -202,12 +224,59 @@ class SpmeBuilder(PotentialBuilder):
         return True
 
 
+class HarmonicBondBuilder(PotentialBuilder):
+    label = "harmonic_bond"
+
+    def build(self, config, desc, keep):
+        p = config.get(self.label)
+        if p is None or len(p.k) == 0:
+            return False
+        arrs = [_u32(np.asarray(p.atoms).reshape(-1)), _f64(p.k), _f64(p.r0)]
+        keep.extend(arrs)
+        desc.n_bonds = len(arrs[1])
+        desc.bond_atoms, desc.bond_k, desc.bond_r0 = N.u32ptr(arrs[0]), N.dptr(arrs[1]), N.dptr(arrs[2])
+        return True
+
+
+class HarmonicAngleBuilder(PotentialBuilder):
+    label = "harmonic_angle"
+
+    def build(self, config, desc, keep):
+        p = config.get(self.label)
+        if p is None or len(p.k) == 0:
+            return False
+        arrs = [_u32(np.asarray(p.atoms).reshape(-1)), _f64(p.k), _f64(p.theta0)]
+        keep.extend(arrs)
+        desc.n_angles = len(arrs[1])
+        desc.angle_atoms, desc.angle_k, desc.angle_theta0 = (N.u32ptr(arrs[0]), N.dptr(arrs[1]),
+                                                             N.dptr(arrs[2]))
+        return True
+
+
+class PeriodicDihedralBuilder(PotentialBuilder):
+    label = "periodic_dihedral"
+
+    def build(self, config, desc, keep):
+        p = config.get(self.label)
+        if p is None or len(p.k) == 0:
+            return False
+        arrs = [_u32(np.asarray(p.atoms).reshape(-1)), _f64(p.k), _f64(p.phi0), _u32(p.n)]
+        keep.extend(arrs)
+        desc.n_dihedrals = len(arrs[1])
+        desc.dihedral_atoms, desc.dihedral_k = N.u32ptr(arrs[0]), N.dptr(arrs[1])
+        desc.dihedral_phi0, desc.dihedral_n = N.dptr(arrs[2]), N.u32ptr(arrs[3])
+        return True
+
+
 class PotentialRegistry:
-    """Builders in canonical order; a slot is active when its section is
-    present (compositional activation)."""
+    """Builders in canonical order (src/forces/mod.rs:277-289: LJ, SPME,
+    harmonic bond, harmonic angle, periodic dihedral); a slot is active when
+    its section is present (compositional activation)."""
 
     def __init__(self):
-        self.builders: list[PotentialBuilder] = [LennardJonesBuilder(), SpmeBuilder()]
+        self.builders: list[PotentialBuilder] = [
+            LennardJonesBuilder(), SpmeBuilder(), HarmonicBondBuilder(), HarmonicAngleBuilder(),
+            PeriodicDihedralBuilder()]
 
     def register(self, builder: PotentialBuilder) -> None:
         if any(b.label == builder.label for b in self.builders):
@@ -257,6 +326,11 @@ class ForceField:
         if spec.alpha is not None:
             cfg["spme"] = SpmeParams(spec.alpha, spec.r_cut_coul, spec.grid, spec.order,
                                      reciprocal=reciprocal and spec.grid is not None)
+        bonded = spec.meta.get("bonded") if spec.meta else None
+        if bonded:
+            for key in ("harmonic_bond", "harmonic_angle", "periodic_dihedral"):
+                if key in bonded:
+                    cfg[key] = bonded[key]
         excl = None
         if spec.excl_offsets is not None:
             excl = (spec.excl_offsets, spec.excl_partners, spec.excl_lj, spec.excl_coul)
@@ -273,10 +347,10 @@ class ForceField:
         return bool(r.value)
 
     def scalars(self) -> dict:
-        out = np.zeros(8)
+        out = np.zeros(10)
         N.check(self.lib.hb_forcefield_scalars(self.h, N.dptr(out)))
         keys = ["lj", "coulomb_real", "recip", "self", "potential", "virial_pair",
-                "virial_recip", "virial"]
+                "virial_recip", "virial", "bonded", "reserved"]
         return dict(zip(keys, out.tolist()))
 
     def per_atom(self):
@@ -317,7 +391,7 @@ class Constraints:
 
     def __init__(self, system: System, group_offsets, group_atoms, group_kind,
                  settle_geometry=None, shake=None, shake_tol: float = 3.57e-6,
-                 shake_max_iter: int = 32):
+                 shake_max_iter: int = 32, shake_tol_relative: bool = False):
         self.system = system
         self.lib = system.lib
         d = N.ConstraintsDesc()
@@ -335,9 +409,11 @@ class Constraints:
             d.con_offsets, d.con_i, d.con_j, d.con_dist = N.u32ptr(co), N.u32ptr(ci), N.u32ptr(cj), N.dptr(cd)
         d.shake_tol = float(shake_tol)
         d.shake_max_iter = int(shake_max_iter)
+        d.shake_tol_relative = 1 if shake_tol_relative else 0
         h = C.c_void_p()
         N.check(self.lib.hb_constraints_create(system.h, C.byref(d), C.byref(h)))
         self.h = h
+        self._mlp = None
 
     @classmethod
     def from_spec(cls, system: System, spec: SystemSpec, **kw) -> "Constraints":
@@ -347,6 +423,10 @@ class Constraints:
         shake = None
         if spec.con_offsets is not None:
             shake = (spec.con_offsets, spec.con_i, spec.con_j, spec.con_dist)
+        if "shake_rel_tol" in (spec.meta or {}) and "shake_tol" not in kw:
+            kw.setdefault("shake_tol", spec.meta["shake_rel_tol"])
+            kw.setdefault("shake_tol_relative", True)
+            kw.setdefault("shake_max_iter", 200)
         return cls(system, spec.group_offsets, spec.group_atoms, spec.group_kind, geo, shake, **kw)
 
     def before_drift(self):
@@ -362,6 +442,28 @@ class Constraints:
         out = np.zeros(self.system.n)
         N.check(self.lib.hb_constraints_get_virial(self.h, N.dptr(out)))
         return out
+
+    def shake_stats(self, reset: bool = False) -> dict:
+        out = np.zeros(3)
+        N.check(self.lib.hb_constraints_shake_stats(self.h, N.dptr(out), 1 if reset else 0))
+        return {"group_sweeps": out[0], "solves": out[1], "mean_sweeps": out[2]}
+
+    def record(self, enable: bool = True) -> None:
+        N.check(self.lib.hb_constraints_record(self.h, 1 if enable else 0))
+
+    def get_record(self) -> dict:
+        m = C.c_uint32(0)
+        N.check(self.lib.hb_constraints_get_record(self.h, None, None, None, None, C.byref(m)))
+        k = m.value
+        f = np.zeros(8 * max(k, 1), dtype=np.float32)
+        l1, ls, lam = np.zeros(max(k, 1)), np.zeros(max(k, 1)), np.zeros(max(k, 1))
+        N.check(self.lib.hb_constraints_get_record(self.h, N.f32ptr(f), N.dptr(l1), N.dptr(ls),
+                                                   N.dptr(lam), C.byref(m)))
+        return {"features": f[: 8 * k].reshape(k, 8), "lam1": l1[:k], "lscale": ls[:k], "lam": lam[:k]}
+
+    def set_warm_start(self, mlp: "ShakeMLP | None") -> None:
+        N.check(self.lib.hb_constraints_set_warm_start(self.h, mlp.h if mlp else None))
+        self._mlp = mlp
 
     def close(self) -> None:
         if getattr(self, "h", None):
@@ -510,4 +612,67 @@ class Batch:
     def close(self) -> None:
         if getattr(self, "h", None):
             self.lib.hb_batch_destroy(self.h)
+            self.h = None
+
+
+# ---------------------------------------------------------------------------
+# learned SHAKE warm start
+# ---------------------------------------------------------------------------
+class ShakeMLP:
+    """8 -> 64 -> 64 -> 1 tanh network whose hidden layers run as BF16
+    tensor-core GEMMs (forward, backward, Adam training on the device)."""
+
+    N_FEATURES = 8
+
+    def __init__(self, ctx: Context, seed: int = 0):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        h = C.c_void_p()
+        N.check(self.lib.hb_shake_mlp_create(ctx.h, int(seed), C.byref(h)))
+        self.h = h
+        self.n_params = int(self.lib.hb_shake_mlp_param_count())
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.n_params, dtype=np.float32)
+        N.check(self.lib.hb_shake_mlp_get_params(self.h, N.f32ptr(out), self.n_params))
+        return out
+
+    def set_params(self, p) -> None:
+        a = np.ascontiguousarray(p, dtype=np.float32)
+        N.check(self.lib.hb_shake_mlp_set_params(self.h, N.f32ptr(a), self.n_params))
+
+    def set_normalization(self, mean, inv_std, target_scale: float) -> None:
+        m = np.ascontiguousarray(mean, dtype=np.float32)
+        s = np.ascontiguousarray(inv_std, dtype=np.float32)
+        N.check(self.lib.hb_shake_mlp_set_normalization(self.h, N.f32ptr(m), N.f32ptr(s),
+                                                        float(target_scale)))
+
+    def predict(self, features) -> np.ndarray:
+        f = np.ascontiguousarray(features, dtype=np.float32).reshape(-1)
+        n = f.size // self.N_FEATURES
+        out = np.zeros(max(n, 1), dtype=np.float32)
+        N.check(self.lib.hb_shake_mlp_predict(self.h, N.f32ptr(f), n, N.f32ptr(out)))
+        return out[:n]
+
+    def gradients(self, features, targets):
+        f = np.ascontiguousarray(features, dtype=np.float32).reshape(-1)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        g = np.zeros(self.n_params, dtype=np.float32)
+        loss = C.c_double(0.0)
+        N.check(self.lib.hb_shake_mlp_gradients(self.h, N.f32ptr(f), N.f32ptr(t), t.size,
+                                                N.f32ptr(g), C.byref(loss)))
+        return g, loss.value
+
+    def train(self, features, targets, epochs: int, batch: int = 512, lr: float = 1e-3,
+              seed: int = 0) -> np.ndarray:
+        f = np.ascontiguousarray(features, dtype=np.float32).reshape(-1)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        losses = np.zeros(epochs)
+        N.check(self.lib.hb_shake_mlp_train(self.h, N.f32ptr(f), N.f32ptr(t), t.size, int(epochs),
+                                            int(batch), float(lr), int(seed), N.dptr(losses)))
+        return losses
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.hb_shake_mlp_destroy(self.h)
             self.h = None

@@ -352,6 +352,7 @@ extern "C" int hb_forcefield_destroy(hb_forcefield *ff) {
   cudaSetDevice(ff->sys->ctx->device);
   hb_context_synchronize(ff->sys->ctx);
   nl_free(ff);
+  bonded_free(ff);
   if (ff->spme.on) spme_free(ff);
   cudaFree(ff->d_lj);
   cudaFree(ff->d_excl_off);
@@ -483,8 +484,8 @@ extern "C" int hb_forcefield_create(hb_system *sys, const hb_forcefield_desc *d,
     }
     ff->n_excl = (uint32_t)epart.size();
   }
-  HB_CUDA(cudaMalloc(&ff->d_scalars, sizeof(double) * 8));
-  HB_CUDA(cudaMemset(ff->d_scalars, 0, sizeof(double) * 8));
+  HB_CUDA(cudaMalloc(&ff->d_scalars, sizeof(double) * HB_N_SCALARS));
+  HB_CUDA(cudaMemset(ff->d_scalars, 0, sizeof(double) * HB_N_SCALARS));
   HB_CUDA(cudaMalloc(&ff->d_acc, sizeof(unsigned long long) * 4));
   HB_CUDA(cudaMemset(ff->d_acc, 0, sizeof(unsigned long long) * 4));
   const size_t nn = std::max<size_t>(n, 1);
@@ -493,6 +494,7 @@ extern "C" int hb_forcefield_create(hb_system *sys, const hb_forcefield_desc *d,
   HB_CUDA(cudaMemset(ff->d_energy, 0, sizeof(float) * nn));
   HB_CUDA(cudaMemset(ff->d_virial, 0, sizeof(float) * nn));
   int rc = nl_setup(ff);
+  if (rc == HB_OK) rc = bonded_setup(ff, d);
   if (rc == HB_OK && d->recip_enabled) rc = spme_setup(ff, d);
   if (rc == HB_OK) rc = nl_first_build(ff);
   if (rc != HB_OK) {
@@ -515,6 +517,9 @@ static int force_eval(hb_forcefield *ff, bool ev, bool capturing = false) {
   else HB_TRY(nl_rebuild(ff, true, s));
   HB_TRY(nl_gather_positions(ff, s));
   stage_end(3, t0, s);
+  // bonded terms add into the same fixed-point accumulators (slots of the
+  // current list), before the pair kernel on the main stream
+  HB_TRY(bonded_launch(ff, ev, s));
   if (ff->spme.on) {
     HB_CUDA(cudaEventRecord(ctx->ev_fork, s));
     HB_CUDA(cudaStreamWaitEvent(s2, ctx->ev_fork, 0));
@@ -569,10 +574,10 @@ extern "C" int hb_forcefield_pre_step(hb_forcefield *ff, int force, int *rebuilt
   return check_status(ff);
 }
 
-extern "C" int hb_forcefield_scalars(hb_forcefield *ff, double out[8]) {
+extern "C" int hb_forcefield_scalars(hb_forcefield *ff, double out[HB_N_SCALARS]) {
   HB_REQUIRE(ff && out, HB_ERR_INVALID_ARGUMENT, "null argument");
   HB_CUDA(cudaStreamSynchronize(ff->sys->ctx->stream));
-  HB_CUDA(cudaMemcpy(out, ff->d_scalars, sizeof(double) * 8, cudaMemcpyDeviceToHost));
+  HB_CUDA(cudaMemcpy(out, ff->d_scalars, sizeof(double) * HB_N_SCALARS, cudaMemcpyDeviceToHost));
   return HB_OK;
 }
 
@@ -639,6 +644,12 @@ extern "C" int hb_constraints_destroy(hb_constraints *c) {
   cudaFree(c->d_shake_d2);
   cudaFree(c->d_virial);
   cudaFree(c->d_iters);
+  cudaFree(c->d_feat);
+  cudaFree(c->d_lam1);
+  cudaFree(c->d_lsc);
+  cudaFree(c->d_lam);
+  cudaFree(c->d_pred);
+  cudaFree(c->d_stats);
   delete c;
   return HB_OK;
 }
@@ -704,6 +715,8 @@ extern "C" int hb_constraints_create(hb_system *sys, const hb_constraints_desc *
   c->n_shake = (uint32_t)h_aoff.size() - 1;
   if (d->shake_tol > 0.0) c->shake_tol = d->shake_tol;
   if (d->shake_max_iter > 0) c->shake_max_iter = d->shake_max_iter;
+  c->shake_rel = d->shake_tol_relative ? 1 : 0;
+  c->n_shake_cons = (uint32_t)h_pairs.size();
   auto up = [](void **dst, const void *src, size_t bytes) -> int {
     HB_CUDA(cudaMalloc(dst, std::max<size_t>(bytes, 16)));
     if (bytes) HB_CUDA(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
@@ -723,7 +736,21 @@ extern "C" int hb_constraints_create(hb_system *sys, const hb_constraints_desc *
     if (cudaMalloc(&c->d_virial, sizeof(float) * nn) != cudaSuccess ||
         cudaMemset(c->d_virial, 0, sizeof(float) * nn) != cudaSuccess ||
         cudaMalloc(&c->d_iters, sizeof(uint32_t)) != cudaSuccess ||
-        cudaMemset(c->d_iters, 0, sizeof(uint32_t)) != cudaSuccess)
+        cudaMemset(c->d_iters, 0, sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc(&c->d_stats, sizeof(unsigned long long) * 2) != cudaSuccess ||
+        cudaMemset(c->d_stats, 0, sizeof(unsigned long long) * 2) != cudaSuccess)
+      rc = hb_fail(HB_ERR_CUDA, "constraint buffer allocation failed");
+    const size_t m = std::max<size_t>(c->n_shake_cons, 1);
+    if (rc == HB_OK &&
+        (cudaMalloc(&c->d_feat, sizeof(float) * 8 * m) != cudaSuccess ||
+         cudaMalloc(&c->d_lam1, sizeof(double) * m) != cudaSuccess ||
+         cudaMalloc(&c->d_lsc, sizeof(double) * m) != cudaSuccess ||
+         cudaMalloc(&c->d_lam, sizeof(double) * m) != cudaSuccess ||
+         cudaMalloc(&c->d_pred, sizeof(float) * m) != cudaSuccess ||
+         cudaMemset(c->d_feat, 0, sizeof(float) * 8 * m) != cudaSuccess ||
+         cudaMemset(c->d_lam1, 0, sizeof(double) * m) != cudaSuccess ||
+         cudaMemset(c->d_lsc, 0, sizeof(double) * m) != cudaSuccess ||
+         cudaMemset(c->d_lam, 0, sizeof(double) * m) != cudaSuccess))
       rc = hb_fail(HB_ERR_CUDA, "constraint buffer allocation failed");
   }
   if (rc != HB_OK) {
@@ -731,6 +758,44 @@ extern "C" int hb_constraints_create(hb_system *sys, const hb_constraints_desc *
     return rc;
   }
   *out = c;
+  return HB_OK;
+}
+
+extern "C" int hb_constraints_shake_stats(hb_constraints *c, double out[3], int reset) {
+  HB_REQUIRE(c && out, HB_ERR_INVALID_ARGUMENT, "null argument");
+  unsigned long long s[2] = {0, 0};
+  HB_CUDA(cudaStreamSynchronize(c->sys->ctx->stream));
+  HB_CUDA(cudaMemcpy(s, c->d_stats, sizeof(s), cudaMemcpyDeviceToHost));
+  out[0] = (double)s[0];
+  out[1] = (double)s[1];
+  out[2] = s[1] ? (double)s[0] / (double)s[1] : 0.0;
+  if (reset) HB_CUDA(cudaMemset(c->d_stats, 0, sizeof(s)));
+  return HB_OK;
+}
+
+extern "C" int hb_constraints_record(hb_constraints *c, int enable) {
+  HB_REQUIRE(c, HB_ERR_INVALID_ARGUMENT, "null constraints");
+  c->record = enable != 0;
+  return HB_OK;
+}
+
+extern "C" int hb_constraints_get_record(hb_constraints *c, float *features, double *lam1,
+                                         double *lscale, double *lam, uint32_t *m) {
+  HB_REQUIRE(c, HB_ERR_INVALID_ARGUMENT, "null constraints");
+  if (m) *m = c->n_shake_cons;
+  const size_t k = c->n_shake_cons;
+  if (!k) return HB_OK;
+  HB_CUDA(cudaStreamSynchronize(c->sys->ctx->stream));
+  if (features) HB_CUDA(cudaMemcpy(features, c->d_feat, sizeof(float) * 8 * k, cudaMemcpyDeviceToHost));
+  if (lam1) HB_CUDA(cudaMemcpy(lam1, c->d_lam1, sizeof(double) * k, cudaMemcpyDeviceToHost));
+  if (lscale) HB_CUDA(cudaMemcpy(lscale, c->d_lsc, sizeof(double) * k, cudaMemcpyDeviceToHost));
+  if (lam) HB_CUDA(cudaMemcpy(lam, c->d_lam, sizeof(double) * k, cudaMemcpyDeviceToHost));
+  return HB_OK;
+}
+
+extern "C" int hb_constraints_set_warm_start(hb_constraints *c, hb_shake_mlp *m) {
+  HB_REQUIRE(c, HB_ERR_INVALID_ARGUMENT, "null constraints");
+  c->mlp = m;
   return HB_OK;
 }
 

@@ -43,7 +43,7 @@ __global__ void k_baro_propose(BaroState *__restrict__ st, double *__restrict__ 
                                double r_search, uint32_t seed_lo, uint32_t seed_hi,
                                uint32_t *__restrict__ nl_status) {
   st->u_old = scalars[4];
-  for (int q = 0; q < 8; ++q) st->scalars_pre[q] = scalars[q];
+  for (int q = 0; q < HB_N_SCALARS; ++q) st->scalars_pre[q] = scalars[q];
   st->draw += 1ull;
   uint32_t o0, o1;
   hb_philox(seed_lo, seed_hi, (uint32_t)st->draw, (uint32_t)(st->draw >> 32), 0u, 0u, o0, o1);
@@ -172,7 +172,7 @@ __global__ void k_baro_decide(BaroState *__restrict__ st, double *__restrict__ l
     } else {
       for (int d = 0; d < 6; ++d) lat[d] = st->lattice_pre[d];
       *dbox = hb_make_dbox(lat);
-      for (int q = 0; q < 8; ++q) scalars[q] = st->scalars_pre[q];
+      for (int q = 0; q < HB_N_SCALARS; ++q) scalars[q] = st->scalars_pre[q];
       atomicOr(nl_status, HB_ST_DISPLACED);
     }
   }

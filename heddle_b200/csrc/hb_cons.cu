@@ -188,90 +188,204 @@ __global__ void k_settle_vel(const uint4 *__restrict__ atoms, const float2 *__re
 #define SHAKE_MAX_ATOMS 8
 #define SHAKE_MAX_CONS 12
 
+// Per-constraint inputs of the learned warm start (8 features), the first
+// Gauss-Seidel multiplier lam1 = sigma / (2 mu s.g) and the scale that
+// turns a multiplier difference into sigma units: ls = 2 mu s.g / d^2 * 1e3.
+// The network predicts (lam - lam1) * ls from the features; lam0 = lam1 +
+// prediction / ls warm-starts the sweeps.  Features: 1e3 sigma/d^2,
+// 1e3 (s.g/d^2 - 1), 1e3 (|g|^2/d^2 - 1), the first-order change of sigma
+// from the coupled constraints' first updates (1e3, in units of d^2), the
+// summed coupling strength, coupled count / 3, im_i / mu, 1e6 (sigma/d^2)^2.
+#define SHAKE_NF 8
+
+__device__ void shake_features(uint32_t nc, const uint32_t *ci, const uint32_t *cj,
+                               const double (*xc)[3], const double (*gdir)[3], const double *tgt,
+                               const double *im, float *feat, double *lam1, double *lsc) {
+  double sg[SHAKE_MAX_CONS], sig[SHAKE_MAX_CONS], mu[SHAKE_MAX_CONS];
+  for (uint32_t k = 0; k < nc; ++k) {
+    const uint32_t i = ci[k], j = cj[k];
+    double sx = xc[i][0] - xc[j][0], sy = xc[i][1] - xc[j][1], sz = xc[i][2] - xc[j][2];
+    sg[k] = sx * gdir[k][0] + sy * gdir[k][1] + sz * gdir[k][2];
+    sig[k] = sx * sx + sy * sy + sz * sz - tgt[k];
+    mu[k] = im[i] + im[j];
+  }
+  for (uint32_t k = 0; k < nc; ++k) {
+    const uint32_t i = ci[k], j = cj[k];
+    const double d2 = tgt[k];
+    const double sx = xc[i][0] - xc[j][0], sy = xc[i][1] - xc[j][1], sz = xc[i][2] - xc[j][2];
+    const double g2 = gdir[k][0] * gdir[k][0] + gdir[k][1] * gdir[k][1] + gdir[k][2] * gdir[k][2];
+    double cpl = 0.0, strength = 0.0;
+    int cnt = 0;
+    for (uint32_t l = 0; l < nc; ++l) {
+      if (l == k) continue;
+      const uint32_t il = ci[l], jl = cj[l];
+      uint32_t a;
+      double ek, el;
+      if (il == i || il == j) {
+        a = il;
+        el = 1.0;
+      } else if (jl == i || jl == j) {
+        a = jl;
+        el = -1.0;
+      } else {
+        continue;
+      }
+      ek = (a == i) ? 1.0 : -1.0;
+      const double skgl = sx * gdir[l][0] + sy * gdir[l][1] + sz * gdir[l][2];
+      const double w = (sg[l] != 0.0 && mu[l] != 0.0) ? -el * ek * (im[a] / mu[l]) * skgl / sg[l] : 0.0;
+      cpl += w * sig[l];
+      strength += fabs(w);
+      ++cnt;
+    }
+    const double l1 = (sg[k] != 0.0 && mu[k] != 0.0) ? sig[k] / (2.0 * mu[k] * sg[k]) : 0.0;
+    lam1[k] = l1;
+    lsc[k] = 2.0 * mu[k] * sg[k] / d2 * 1e3;
+    float *f = feat + (size_t)k * SHAKE_NF;
+    f[0] = (float)(1e3 * sig[k] / d2);
+    f[1] = (float)(1e3 * (sg[k] / d2 - 1.0));
+    f[2] = (float)(1e3 * (g2 / d2 - 1.0));
+    f[3] = (float)(1e3 * cpl / d2);
+    f[4] = (float)strength;
+    f[5] = (float)cnt / 3.0f;
+    f[6] = (float)(mu[k] > 0.0 ? im[i] / mu[k] : 0.0);
+    f[7] = (float)(1e6 * (sig[k] / d2) * (sig[k] / d2));
+  }
+}
+
+// Gauss-Seidel SHAKE on one group per thread (FP64).  rel: tolerance
+// relative to d^2 instead of absolute.  Optional: lam0 / lam1 / lsc warm
+// start from a predicted multiplier correction (pred), features out
+// (feat, lam1_out, lsc_out, computed before any update), converged total
+// multipliers out (lam_out), sweep statistics (stats[0] group-sweeps,
+// stats[1] groups), features_only (compute features, move nothing).
 __global__ void k_shake_pos(const uint32_t *__restrict__ aoff, const uint32_t *__restrict__ atoms,
                             const uint32_t *__restrict__ coff, const uint2 *__restrict__ pairs,
                             const double *__restrict__ d2, float4 *__restrict__ posq,
                             float4 *__restrict__ vel, const float4 *__restrict__ prev,
-                            const DBox *__restrict__ box, float dt, double tol, int max_iter,
-                            float *__restrict__ virial, uint32_t *__restrict__ iters,
-                            uint32_t ng) {
+                            const DBox *__restrict__ box, float dt, double tol, int rel,
+                            int max_iter, float *__restrict__ virial, uint32_t *__restrict__ iters,
+                            unsigned long long *__restrict__ stats, const float *__restrict__ pred,
+                            float *__restrict__ feat, double *__restrict__ lam1_io,
+                            double *__restrict__ lsc_io, double *__restrict__ lam_out,
+                            int features_only, uint32_t ng) {
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= ng) return;
-  const DBox bx = *box;
-  const uint32_t a0 = aoff[g], na = aoff[g + 1] - a0;
-  const uint32_t c0 = coff[g], nc = coff[g + 1] - c0;
-  double xr[SHAKE_MAX_ATOMS][3], xu[SHAKE_MAX_ATOMS][3], xc[SHAKE_MAX_ATOMS][3];
-  double im[SHAKE_MAX_ATOMS], ms[SHAKE_MAX_ATOMS];
-  const float4 r0 = prev[atoms[a0]], u0 = posq[atoms[a0]];
-  for (uint32_t a = 0; a < na; ++a) {
-    const uint32_t id = atoms[a0 + a];
-    const float4 r = prev[id], u = posq[id];
-    const float w = vel[id].w;
-    im[a] = (double)w;
-    ms[a] = w > 0.0f ? 1.0 / (double)w : 0.0;
-    V3 dr = mi(v3(r.x - r0.x, r.y - r0.y, r.z - r0.z), bx);
-    V3 du = mi(v3(u.x - u0.x, u.y - u0.y, u.z - u0.z), bx);
-    xr[a][0] = dr.x; xr[a][1] = dr.y; xr[a][2] = dr.z;
-    xu[a][0] = du.x; xu[a][1] = du.y; xu[a][2] = du.z;
-    for (int d = 0; d < 3; ++d) xc[a][d] = xu[a][d];
-  }
-  double gdir[SHAKE_MAX_CONS][3];
-  uint32_t ci[SHAKE_MAX_CONS], cj[SHAKE_MAX_CONS];
-  double tgt[SHAKE_MAX_CONS];
-  for (uint32_t k = 0; k < nc; ++k) {
-    const uint2 pr = pairs[c0 + k];
-    ci[k] = pr.x;
-    cj[k] = pr.y;
-    tgt[k] = d2[c0 + k];
-    for (int d = 0; d < 3; ++d) gdir[k][d] = xr[pr.x][d] - xr[pr.y][d];
-  }
-  int it = 0;
-  for (; it < max_iter; ++it) {
-    bool conv = true;
+  uint32_t it_used = 0;
+  if (g < ng) {
+    const DBox bx = *box;
+    const uint32_t a0 = aoff[g], na = aoff[g + 1] - a0;
+    const uint32_t c0 = coff[g], nc = coff[g + 1] - c0;
+    double xr[SHAKE_MAX_ATOMS][3], xu[SHAKE_MAX_ATOMS][3], xc[SHAKE_MAX_ATOMS][3];
+    double im[SHAKE_MAX_ATOMS], ms[SHAKE_MAX_ATOMS];
+    const float4 r0 = prev[atoms[a0]], u0 = posq[atoms[a0]];
+    for (uint32_t a = 0; a < na; ++a) {
+      const uint32_t id = atoms[a0 + a];
+      const float4 r = prev[id], u = posq[id];
+      const float w = vel[id].w;
+      im[a] = (double)w;
+      ms[a] = w > 0.0f ? 1.0 / (double)w : 0.0;
+      V3 dr = mi(v3(r.x - r0.x, r.y - r0.y, r.z - r0.z), bx);
+      V3 du = mi(v3(u.x - u0.x, u.y - u0.y, u.z - u0.z), bx);
+      xr[a][0] = dr.x; xr[a][1] = dr.y; xr[a][2] = dr.z;
+      xu[a][0] = du.x; xu[a][1] = du.y; xu[a][2] = du.z;
+      for (int d = 0; d < 3; ++d) xc[a][d] = xu[a][d];
+    }
+    double gdir[SHAKE_MAX_CONS][3];
+    uint32_t ci[SHAKE_MAX_CONS], cj[SHAKE_MAX_CONS];
+    double tgt[SHAKE_MAX_CONS], lam_tot[SHAKE_MAX_CONS];
     for (uint32_t k = 0; k < nc; ++k) {
-      const uint32_t i = ci[k], j = cj[k];
-      const double dx = xc[i][0] - xc[j][0], dy = xc[i][1] - xc[j][1], dz = xc[i][2] - xc[j][2];
-      const double sigma = dx * dx + dy * dy + dz * dz - tgt[k];
-      if (fabs(sigma) > tol) {
-        conv = false;
-        const double den = 2.0 * (dx * gdir[k][0] + dy * gdir[k][1] + dz * gdir[k][2]) * (im[i] + im[j]);
-        if (den == 0.0) continue;
-        const double lam = sigma / den;
-        for (int d = 0; d < 3; ++d) {
-          xc[i][d] -= lam * im[i] * gdir[k][d];
-          xc[j][d] += lam * im[j] * gdir[k][d];
+      const uint2 pr = pairs[c0 + k];
+      ci[k] = pr.x;
+      cj[k] = pr.y;
+      tgt[k] = d2[c0 + k];
+      lam_tot[k] = 0.0;
+      for (int d = 0; d < 3; ++d) gdir[k][d] = xr[pr.x][d] - xr[pr.y][d];
+    }
+    if (feat) {
+      shake_features(nc, ci, cj, xc, gdir, tgt, im, feat + (size_t)c0 * SHAKE_NF, lam1_io + c0,
+                     lsc_io + c0);
+    }
+    if (!features_only) {
+      if (pred) {
+        // warm start: every constraint's predicted multiplier applied at once
+        for (uint32_t k = 0; k < nc; ++k) {
+          const double ls = lsc_io[c0 + k];
+          const double l0 = lam1_io[c0 + k] + (ls != 0.0 ? (double)pred[c0 + k] / ls : 0.0);
+          if (!(fabs(l0) < 1e30)) continue;
+          const uint32_t i = ci[k], j = cj[k];
+          for (int d = 0; d < 3; ++d) {
+            xc[i][d] -= l0 * im[i] * gdir[k][d];
+            xc[j][d] += l0 * im[j] * gdir[k][d];
+          }
+          lam_tot[k] += l0;
         }
       }
+      int it = 0;
+      for (; it < max_iter; ++it) {
+        bool conv = true;
+        for (uint32_t k = 0; k < nc; ++k) {
+          const uint32_t i = ci[k], j = cj[k];
+          const double dx = xc[i][0] - xc[j][0], dy = xc[i][1] - xc[j][1], dz = xc[i][2] - xc[j][2];
+          const double sigma = dx * dx + dy * dy + dz * dz - tgt[k];
+          const double tk = rel ? tol * tgt[k] : tol;
+          if (fabs(sigma) > tk) {
+            conv = false;
+            const double den = 2.0 * (dx * gdir[k][0] + dy * gdir[k][1] + dz * gdir[k][2]) * (im[i] + im[j]);
+            if (den == 0.0) continue;
+            const double lam = sigma / den;
+            lam_tot[k] += lam;
+            for (int d = 0; d < 3; ++d) {
+              xc[i][d] -= lam * im[i] * gdir[k][d];
+              xc[j][d] += lam * im[j] * gdir[k][d];
+            }
+          }
+        }
+        if (conv) break;
+      }
+      it_used = (uint32_t)it;
+      if (iters) atomicMax(iters, (uint32_t)it);
+      if (lam_out)
+        for (uint32_t k = 0; k < nc; ++k) lam_out[c0 + k] = lam_tot[k];
+      double tm = 0.0, com[3] = {0, 0, 0};
+      for (uint32_t a = 0; a < na; ++a) {
+        tm += ms[a];
+        for (int d = 0; d < 3; ++d) com[d] += ms[a] * xc[a][d];
+      }
+      for (int d = 0; d < 3; ++d) com[d] = tm > 0.0 ? com[d] / tm : 0.0;
+      const double inv_dt = dt != 0.0f ? 1.0 / (double)dt : 0.0;
+      for (uint32_t a = 0; a < na; ++a) {
+        const uint32_t id = atoms[a0 + a];
+        float4 q = posq[id];
+        float4 v = vel[id];
+        double wv = 0.0;
+        double del[3];
+        for (int d = 0; d < 3; ++d) {
+          del[d] = xc[a][d] - xu[a][d];
+          wv += del[d] * (xc[a][d] - com[d]);
+        }
+        q.x += (float)del[0];
+        q.y += (float)del[1];
+        q.z += (float)del[2];
+        v.x += (float)(del[0] * inv_dt);
+        v.y += (float)(del[1] * inv_dt);
+        v.z += (float)(del[2] * inv_dt);
+        posq[id] = q;
+        vel[id] = v;
+        if (virial) virial[id] = (float)(ms[a] * inv_dt * inv_dt * wv);
+      }
     }
-    if (conv) break;
   }
-  if (iters) atomicMax(iters, (uint32_t)it);
-  double tm = 0.0, com[3] = {0, 0, 0};
-  for (uint32_t a = 0; a < na; ++a) {
-    tm += ms[a];
-    for (int d = 0; d < 3; ++d) com[d] += ms[a] * xc[a][d];
-  }
-  for (int d = 0; d < 3; ++d) com[d] = tm > 0.0 ? com[d] / tm : 0.0;
-  const double inv_dt = dt != 0.0f ? 1.0 / (double)dt : 0.0;
-  for (uint32_t a = 0; a < na; ++a) {
-    const uint32_t id = atoms[a0 + a];
-    float4 q = posq[id];
-    float4 v = vel[id];
-    double wv = 0.0;
-    double del[3];
-    for (int d = 0; d < 3; ++d) {
-      del[d] = xc[a][d] - xu[a][d];
-      wv += del[d] * (xc[a][d] - com[d]);
+  if (stats && !features_only) {
+    // group-sweeps and groups of this call, one atomic per warp
+    unsigned long long s0 = it_used, s1 = g < ng ? 1ull : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s0 += __shfl_xor_sync(0xFFFFFFFFu, s0, o);
+      s1 += __shfl_xor_sync(0xFFFFFFFFu, s1, o);
     }
-    q.x += (float)del[0];
-    q.y += (float)del[1];
-    q.z += (float)del[2];
-    v.x += (float)(del[0] * inv_dt);
-    v.y += (float)(del[1] * inv_dt);
-    v.z += (float)(del[2] * inv_dt);
-    posq[id] = q;
-    vel[id] = v;
-    if (virial) virial[id] = (float)(ms[a] * inv_dt * inv_dt * wv);
+    if ((threadIdx.x & 31u) == 0u && s1) {
+      atomicAdd(&stats[0], s0);
+      atomicAdd(&stats[1], s1);
+    }
   }
 }
 
@@ -351,11 +465,27 @@ int cons_positions(hb_constraints *c, double dt, cudaStream_t s) {
     k_settle_pos<<<hb_div_up(c->n_settle, 128), 128, 0, s>>>(
         c->d_settle_atoms, c->d_settle_geom, c->d_settle_mass, sys->d_posq, sys->d_vel,
         sys->d_pos_prev, sys->d_box, (float)dt, c->d_virial, c->n_settle);
-  if (c->n_shake)
-    k_shake_pos<<<hb_div_up(c->n_shake, 64), 64, 0, s>>>(
+  if (c->n_shake) {
+    const unsigned gs = hb_div_up(c->n_shake, 64);
+    const float *pred = nullptr;
+    if (c->mlp) {
+      // learned warm start: features, network, then the sweeps
+      k_shake_pos<<<gs, 64, 0, s>>>(
+          c->d_shake_aoff, c->d_shake_atoms, c->d_shake_coff, c->d_shake_pairs, c->d_shake_d2,
+          sys->d_posq, sys->d_vel, sys->d_pos_prev, sys->d_box, (float)dt, c->shake_tol,
+          c->shake_rel, (int)c->shake_max_iter, nullptr, nullptr, nullptr, nullptr, c->d_feat,
+          c->d_lam1, c->d_lsc, nullptr, 1, c->n_shake);
+      HB_TRY(mlp_infer(c->mlp, c->d_feat, c->n_shake_cons, c->d_pred, s));
+      pred = c->d_pred;
+    }
+    const bool rec = c->record;
+    k_shake_pos<<<gs, 64, 0, s>>>(
         c->d_shake_aoff, c->d_shake_atoms, c->d_shake_coff, c->d_shake_pairs, c->d_shake_d2,
         sys->d_posq, sys->d_vel, sys->d_pos_prev, sys->d_box, (float)dt, c->shake_tol,
-        (int)c->shake_max_iter, c->d_virial, c->d_iters, c->n_shake);
+        c->shake_rel, (int)c->shake_max_iter, c->d_virial, c->d_iters, c->d_stats, pred,
+        (rec && !pred) ? c->d_feat : nullptr, c->d_lam1, c->d_lsc, rec ? c->d_lam : nullptr, 0,
+        c->n_shake);
+  }
   HB_CUDA(cudaGetLastError());
   return HB_OK;
 }

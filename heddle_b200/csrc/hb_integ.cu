@@ -72,19 +72,23 @@ __global__ void k_scalars(unsigned long long *__restrict__ acc,
   const double lj = (double)(long long)acc[0] * HB_FP_INV_SCALE;
   const double pair = (double)(long long)acc[1] * HB_FP_INV_SCALE;
   const double wp = (double)(long long)acc[2] * HB_FP_INV_SCALE;
+  const double eb = (double)(long long)acc[3] * HB_FP_INV_SCALE;
   const double er = spme_sums ? spme_sums[0] : 0.0;
   const double wr = spme_sums ? spme_sums[1] : 0.0;
   out[0] = lj;
-  out[1] = pair - lj;
+  out[1] = pair - lj - eb;
   out[2] = er;
   out[3] = spme_sums ? e_self : 0.0;
   out[4] = pair + er - (spme_sums ? e_self : 0.0);
   out[5] = wp;
   out[6] = wr;
   out[7] = wp + wr;
+  out[8] = eb;
+  out[9] = 0.0;
   acc[0] = 0ull;
   acc[1] = 0ull;
   acc[2] = 0ull;
+  acc[3] = 0ull;
 }
 
 // Box-Muller cosine branch on the first two words, u = (x + 1/2) 2^-32

@@ -44,6 +44,7 @@ int hb_fail(int code, const std::string &msg);
 #define HB_FP_SCALE 1099511627776.0f        /* 2^40 */
 #define HB_FP_INV_SCALE (1.0 / 1099511627776.0)
 #define HB_RHO_SCALE 4294967296.0f          /* 2^32 */
+#define HB_N_SCALARS 10                     /* doubles of hb_forcefield_scalars */
 #define HB_XFIX_SCALE 1099511627776.0       /* 2^40 per bohr */
 #define HB_VFIX_SCALE 72057594037927936.0   /* 2^56 per bohr / aut */
 
@@ -233,6 +234,8 @@ struct SpmeState {
   float self_pref = 0.f;                      // alpha / sqrt(pi)
 };
 
+struct hb_shake_mlp;
+
 // process-wide creation counter: objects that captured graphs refer to are
 // compared by this id, never by address (a freed object's address can be
 // reused by a new one)
@@ -291,10 +294,19 @@ struct hb_forcefield {
   // ---- SPME
   SpmeState spme;
   // ---- scalars
-  double *d_scalars = nullptr;       // [8]
-  unsigned long long *d_acc = nullptr;  // int64 totals: [0] LJ energy, [1] pair
-                                        // energy, [2] pair virial
-  double h_scalars[8] = {0};
+  double *d_scalars = nullptr;       // [HB_N_SCALARS]
+  unsigned long long *d_acc = nullptr;  // int64 totals: [0] LJ energy, [1] pair +
+                                        // bonded energy, [2] pair + bonded virial,
+                                        // [3] bonded energy
+  // ---- bonded terms (per term: atoms and parameters)
+  uint32_t n_bonds = 0, n_angles = 0, n_dihedrals = 0;
+  uint2 *d_bond_atoms = nullptr;
+  float2 *d_bond_par = nullptr;      // k, r0
+  uint4 *d_angle_atoms = nullptr;    // i, j (vertex), k
+  float2 *d_angle_par = nullptr;     // k, theta0
+  uint4 *d_dih_atoms = nullptr;      // i, j, k, l
+  float4 *d_dih_par = nullptr;       // k, phi0, n
+  double h_scalars[HB_N_SCALARS] = {0};
   float *d_energy = nullptr;         // per atom (atom order)
   float *d_virial = nullptr;
 };
@@ -313,7 +325,18 @@ struct hb_constraints {
   uint2 *d_shake_pairs = nullptr;    // local i, j
   double *d_shake_d2 = nullptr;
   double shake_tol = 3.57e-6;
+  int shake_rel = 0;                 // tolerance relative to d^2
   uint32_t shake_max_iter = 32;
+  uint32_t n_shake_cons = 0;         // constraints of the SHAKE groups
+  // learned warm start and its training data (per SHAKE constraint)
+  hb_shake_mlp *mlp = nullptr;       // warm start when set
+  bool record = false;               // write features and converged multipliers
+  float *d_feat = nullptr;           // [n_shake_cons * 8]
+  double *d_lam1 = nullptr;          // first Gauss-Seidel multiplier
+  double *d_lsc = nullptr;           // multiplier -> sigma-unit scale
+  double *d_lam = nullptr;           // converged total multiplier
+  float *d_pred = nullptr;           // network output
+  unsigned long long *d_stats = nullptr;  // [0] group-sweeps, [1] group solves
   uint32_t n_slots = 0;
   float *d_virial = nullptr;         // per atom
   uint32_t *d_iters = nullptr;       // max sweeps of the last SHAKE call
@@ -344,7 +367,7 @@ struct hb_integrator {
 // step-size adaptation -- runs on the device with no host read.
 struct BaroState {
   double lattice_pre[6];   // lattice before the trial
-  double scalars_pre[8];   // force-field scalars before the trial
+  double scalars_pre[HB_N_SCALARS];  // force-field scalars before the trial
   double max_dv;           // current maximum volume displacement
   double u_old, u_new, dv, v_old, v_new, scale, u1, u2, w;
   double injection;        // sum of P dV over accepted moves
@@ -386,6 +409,10 @@ int nl_displacement_check(hb_forcefield *ff, cudaStream_t s);
 int nl_gather_positions(hb_forcefield *ff, cudaStream_t s);
 int nl_first_build(hb_forcefield *ff);
 int nl_pairs(hb_forcefield *ff, std::vector<uint32_t> &pairs, uint64_t &dups);
+// bonded terms (hb_bonded.cu): fixed-point adds into fp (sorted slots)
+int bonded_setup(hb_forcefield *ff, const hb_forcefield_desc *d);
+int bonded_free(hb_forcefield *ff);
+int bonded_launch(hb_forcefield *ff, bool ev, cudaStream_t s);
 // pair kernel (hb_pair.cu)
 int pair_launch(hb_forcefield *ff, bool ev, cudaStream_t s);
 // SPME (hb_spme.cu)
@@ -410,6 +437,8 @@ int sys_refresh_box(hb_system *sys);
 // evaluation with scalars) decide + revert
 int baro_propose(hb_barostat *b, hb_forcefield *ff, cudaStream_t s);
 int baro_decide(hb_barostat *b, hb_forcefield *ff, cudaStream_t s);
+// learned SHAKE warm start (hb_mlp.cu): network on device features
+int mlp_infer(hb_shake_mlp *m, const float *d_feat, uint32_t n, float *d_out, cudaStream_t s);
 // constraints (hb_cons.cu)
 int cons_positions(hb_constraints *c, double dt, cudaStream_t s);
 int cons_velocities(hb_constraints *c, double dt, bool virial, cudaStream_t s);

@@ -1,0 +1,815 @@
+// hb_mlp.cu -- the learned SHAKE warm start: a small MLP (8 -> 64 -> 64 -> 1,
+// tanh) whose two hidden layers run on the 5th-generation tensor cores.
+//
+// No reference counterpart (the reference's SHAKE starts every solve from
+// zero multipliers, kernels/shake.cu:108-348).  The network maps per-
+// constraint geometry features (hb_cons.cu) to a correction of the first
+// Gauss-Seidel multiplier; SHAKE then iterates from that warm start to the
+// same tolerance, so the network only ever changes how many sweeps are needed.
+//
+// Tensor-core path (sm_100a): operands are BF16 in shared memory in the
+// K-major no-swizzle canonical layout (8-row x 16-byte core matrices), one
+// elected thread issues tcgen05.mma (kind::f16, FP32 accumulate) into tensor
+// memory, tcgen05.commit arrives on an mbarrier, and every thread reads its
+// accumulator row back with tcgen05.ld (thread t of the 128 = TMEM lane t =
+// batch row t).  Each wait is bounded; a timeout sets an error word, the
+// kernel frees its tensor memory and returns.
+//
+//   forward   z1 = bf16(x) bf16(W1)^T + b1   (M=128, N=64, K=16)   h1 = tanh z1
+//             z2 = bf16(h1) bf16(W2)^T + b2  (M=128, N=64, K=64)   h2 = tanh z2
+//             y  = h2 . w3 + b3              (FP32 on the CUDA cores)
+//   backward  dy = 2 (y - t) / B, dz2 = dy w3 (1 - h2^2)
+//             dh1 = bf16(dz2) bf16(W2)        (M=128, N=64, K=64)
+//             dz1 = dh1 (1 - h1^2)
+//             [dW2 | . ; . | dW1] += [bf16(dz2)^T ; bf16(dz1)^T] [bf16(h1) | bf16(x)]
+//                                             (M=128, N=80, K=128 per tile,
+//                                              accumulated over the batch in TMEM)
+//             bias / w3 gradients: fixed-order column sums in FP32
+//   update    Adam on FP32 master weights held in shared memory.
+// One CTA of 128 threads trains (deterministic); inference uses one CTA per
+// 128 rows.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "hb_internal.cuh"
+
+namespace {
+
+constexpr int NF = 8;            // input features
+constexpr int KIN = 16;          // padded input width (one MMA K step)
+constexpr int HID = 64;          // hidden width
+constexpr int TILE = 128;        // rows per tile (MMA M, TMEM lanes)
+constexpr int GN = HID + KIN;    // N of the gradient GEMM (80)
+
+// packed parameter order: W1 [64][8], b1 [64], W2 [64][64], b2 [64], w3 [64], b3
+constexpr int OFF_W1 = 0, OFF_B1 = OFF_W1 + HID * NF, OFF_W2 = OFF_B1 + HID,
+              OFF_B2 = OFF_W2 + HID * HID, OFF_W3 = OFF_B2 + HID, OFF_B3 = OFF_W3 + HID,
+              NPARAM = OFF_B3 + 1;
+
+// TMEM columns
+constexpr uint32_t TM_Z1 = 0, TM_Z2 = 64, TM_G = 128, TM_COLS_TRAIN = 256, TM_COLS_INFER = 128;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// byte offset of element (r, k) of a K-major operand with R rows
+__device__ __forceinline__ uint32_t kmaj(uint32_t r, uint32_t k, uint32_t R) {
+  return ((k >> 3) * (R >> 3) + (r >> 3)) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
+}
+
+// shared-memory matrix descriptor, no swizzle: start, leading (K-chunk) and
+// stride (8-row group) byte offsets, descriptor version 1
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// instruction descriptor: BF16 x BF16 -> FP32, both K-major, M x N
+__host__ __device__ constexpr uint32_t idesc_bf16(uint32_t M, uint32_t N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                     uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   mbar)
+               : "memory");
+}
+
+// D[128, N] (+)= A[128, K] . B[N, K]^T; A and B K-major in shared memory
+__device__ __forceinline__ void gemm_issue(uint32_t d_tmem, uint32_t a_base, uint32_t b_base,
+                                           uint32_t N, uint32_t K, bool acc_first) {
+  const uint32_t a_lbo = (TILE / 8) * 128u, b_lbo = (N / 8) * 128u;
+  const uint32_t idesc = idesc_bf16(TILE, N);
+  for (uint32_t s = 0; s < K / 16; ++s) {
+    const uint64_t a = sdesc(a_base + s * 2u * a_lbo, a_lbo, 128u);
+    const uint64_t b = sdesc(b_base + s * 2u * b_lbo, b_lbo, 128u);
+    umma(d_tmem, a, b, idesc, (s > 0 || acc_first) ? 1u : 0u);
+  }
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
+  for (uint32_t i = 0; i < (1u << 22); ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void fence_before_sync() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after_sync() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ unsigned short bf16_bits(float x) {
+  return __bfloat16_as_ushort(__float2bfloat16_rn(x));
+}
+
+// 8 consecutive K values of one row as one 16-byte store
+__device__ __forceinline__ void st_row8(unsigned char *base, uint32_t r, uint32_t k0, uint32_t R,
+                                        const float *v) {
+  uint4 q;
+  q.x = (uint32_t)bf16_bits(v[0]) | ((uint32_t)bf16_bits(v[1]) << 16);
+  q.y = (uint32_t)bf16_bits(v[2]) | ((uint32_t)bf16_bits(v[3]) << 16);
+  q.z = (uint32_t)bf16_bits(v[4]) | ((uint32_t)bf16_bits(v[5]) << 16);
+  q.w = (uint32_t)bf16_bits(v[6]) | ((uint32_t)bf16_bits(v[7]) << 16);
+  *reinterpret_cast<uint4 *>(base + kmaj(r, k0, R)) = q;
+}
+
+__device__ __forceinline__ void st_elem(unsigned char *base, uint32_t r, uint32_t k, uint32_t R,
+                                        float v) {
+  *reinterpret_cast<unsigned short *>(base + kmaj(r, k, R)) = bf16_bits(v);
+}
+
+struct MlpNorm {
+  float mean[NF];
+  float inv_std[NF];
+  float t_scale;
+};
+
+// ---- shared-memory plan (bytes, 128-aligned) ----
+constexpr uint32_t SZ_W1 = HID * KIN * 2;        // [64 x 16]
+constexpr uint32_t SZ_W2 = HID * HID * 2;        // [64 x 64]
+constexpr uint32_t SZ_X = TILE * KIN * 2;        // [128 x 16]
+constexpr uint32_t SZ_H = TILE * HID * 2;        // [128 x 64]
+constexpr uint32_t SZ_G = TILE * TILE * 2;       // [128 x 128]
+constexpr uint32_t SZ_BT = GN * TILE * 2;        // [80 x 128]
+
+struct InferSmem {
+  unsigned char w1[SZ_W1];
+  unsigned char w2[SZ_W2];
+  unsigned char x[SZ_X];
+  unsigned char h1[SZ_H];
+  float b1[HID], b2[HID], w3[HID];
+  float b3;
+  unsigned long long mbar;
+  uint32_t tmem;
+};
+
+__device__ void load_weights_bf16(const float *P, unsigned char *w1, unsigned char *w2,
+                                  unsigned char *w2t, int tid) {
+  // W1 [64 out][16 in, 8 real]; W2 [64 out][64 in]; W2T [64 in][64 out]
+  if (tid < HID) {
+    float v[8], z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int q = 0; q < 8; ++q) v[q] = P[OFF_W1 + tid * NF + q];
+    st_row8(w1, tid, 0, HID, v);
+    st_row8(w1, tid, 8, HID, z);
+    for (int c = 0; c < HID; c += 8) {
+      for (int q = 0; q < 8; ++q) v[q] = P[OFF_W2 + tid * HID + c + q];
+      st_row8(w2, tid, c, HID, v);
+    }
+  } else if (w2t) {
+    const int i = tid - HID;  // input unit
+    float v[8];
+    for (int c = 0; c < HID; c += 8) {
+      for (int q = 0; q < 8; ++q) v[q] = P[OFF_W2 + (c + q) * HID + i];
+      st_row8(w2t, i, c, HID, v);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------
+// inference: one CTA per 128 rows
+// ---------------------------------------------------------------------
+__global__ void __launch_bounds__(TILE) k_mlp_infer(const float *__restrict__ params,
+                                                    MlpNorm norm, const float *__restrict__ feat,
+                                                    uint32_t n, float *__restrict__ out,
+                                                    uint32_t *__restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  InferSmem &S = *reinterpret_cast<InferSmem *>(smem_raw);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t row = blockIdx.x * TILE + tid;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&S.tmem)),
+                 "r"(TM_COLS_INFER));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&S.mbar)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  load_weights_bf16(params, S.w1, S.w2, nullptr, tid);
+  if (tid < HID) {
+    S.b1[tid] = params[OFF_B1 + tid];
+    S.b2[tid] = params[OFF_B2 + tid];
+    S.w3[tid] = params[OFF_W3 + tid];
+  }
+  if (tid == 0) S.b3 = params[OFF_B3];
+  {
+    float v[8], z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int q = 0; q < NF; ++q)
+      v[q] = row < n ? (feat[(size_t)row * NF + q] - norm.mean[q]) * norm.inv_std[q] : 0.0f;
+    st_row8(S.x, tid, 0, TILE, v);
+    st_row8(S.x, tid, 8, TILE, z);
+  }
+  fence_async_smem();
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = S.tmem, mbar = smem_u32(&S.mbar);
+  const uint32_t lane_base = tmem + ((uint32_t)(32 * warp) << 16);
+  bool ok = true;
+  uint32_t phase = 0;
+  // layer 1
+  if (tid == 0) {
+    gemm_issue(tmem + TM_Z1, smem_u32(S.x), smem_u32(S.w1), HID, KIN, false);
+    umma_commit(mbar);
+  }
+  ok = mbar_wait(mbar, phase);
+  phase ^= 1u;
+  fence_after_sync();
+  float h1[HID];
+  if (ok) {
+#pragma unroll
+    for (int c = 0; c < HID; c += 16) {
+      float v[16];
+      tmem_ld16(lane_base + TM_Z1 + c, v);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) h1[c + q] = tanhf(v[q] + S.b1[c + q]);
+    }
+#pragma unroll
+    for (int c = 0; c < HID; c += 8) st_row8(S.h1, tid, c, TILE, &h1[c]);
+  }
+  fence_async_smem();
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  ok = __syncthreads_and(ok);
+  float y = 0.0f;
+  if (ok) {
+    if (tid == 0) {
+      gemm_issue(tmem + TM_Z2, smem_u32(S.h1), smem_u32(S.w2), HID, HID, false);
+      umma_commit(mbar);
+    }
+    ok = mbar_wait(mbar, phase);
+    phase ^= 1u;
+    fence_after_sync();
+    if (ok) {
+      y = S.b3;
+#pragma unroll
+      for (int c = 0; c < HID; c += 16) {
+        float v[16];
+        tmem_ld16(lane_base + TM_Z2 + c, v);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) y += tanhf(v[q] + S.b2[c + q]) * S.w3[c + q];
+      }
+    }
+  }
+  if (!ok && tid == 0) atomicExch(err, 1u);
+  if (ok && row < n) out[row] = y * norm.t_scale;
+  fence_before_sync();
+  __syncthreads();
+  if (!ok) mbar_wait(mbar, phase);  // a late MMA: one more bounded wait
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(TM_COLS_INFER));
+}
+
+// ---------------------------------------------------------------------
+// training: one CTA, a whole epoch of minibatches per launch
+// ---------------------------------------------------------------------
+struct TrainSmem {
+  unsigned char w1[SZ_W1];
+  unsigned char w2[SZ_W2];
+  unsigned char w2t[SZ_W2];
+  unsigned char x[SZ_X];
+  unsigned char h1[SZ_H];
+  unsigned char dz2[SZ_H];
+  unsigned char g[SZ_G];
+  unsigned char bt[SZ_BT];
+  float scratch[TILE][HID + 1];
+  float P[NPARAM];                 // FP32 master parameters
+  float gb1[HID], gb2[HID], gw3[HID];
+  float gb3;
+  float loss;
+  unsigned long long mbar;
+  uint32_t tmem;
+};
+
+// fixed-order column sums of scratch[0..rows)[0..HID) into acc (threads < HID)
+__device__ __forceinline__ void colsum_into(TrainSmem &S, float *acc, int tid) {
+  __syncthreads();
+  if (tid < HID) {
+    float s = 0.0f;
+    for (int r = 0; r < TILE; ++r) s += S.scratch[r][tid];
+    acc[tid] += s;
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ float adam_step(float w, float g, float &m, float &v, float lr,
+                                           float c1, float c2) {
+  m = 0.9f * m + 0.1f * g;
+  v = 0.999f * v + 0.001f * g * g;
+  const float mh = m / c1, vh = v / c2;
+  return w - lr * mh / (sqrtf(vh) + 1e-8f);
+}
+
+// mode 0: train (n_batches minibatches of rows perm[b * B .. b * B + B)),
+// mode 1: gradients of one minibatch of B rows (written to grads, no update)
+__global__ void __launch_bounds__(TILE) k_mlp_train(
+    float *__restrict__ params, float *__restrict__ adam_m, float *__restrict__ adam_v,
+    uint32_t step0, MlpNorm norm, const float *__restrict__ feat, const float *__restrict__ tgt,
+    const uint32_t *__restrict__ perm, uint32_t n_batches, uint32_t B, float lr, int mode,
+    float *__restrict__ grads, float *__restrict__ loss_out, uint32_t *__restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  TrainSmem &S = *reinterpret_cast<TrainSmem *>(smem_raw);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&S.tmem)),
+                 "r"(TM_COLS_TRAIN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&S.mbar)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    S.loss = 0.0f;
+  }
+  for (int q = tid; q < NPARAM; q += TILE) S.P[q] = params[q];
+  __syncthreads();
+  load_weights_bf16(S.P, S.w1, S.w2, S.w2t, tid);
+  fence_async_smem();
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = S.tmem, mbar = smem_u32(&S.mbar);
+  const uint32_t lane_base = tmem + ((uint32_t)(32 * warp) << 16);
+  uint32_t phase = 0;
+  bool ok = true;
+  const uint32_t tiles = (B + TILE - 1) / TILE;
+  const float inv_b = 1.0f / (float)B;
+  float loss_acc = 0.0f;
+  for (uint32_t bt_i = 0; bt_i < n_batches && ok; ++bt_i) {
+    if (tid < HID) {
+      S.gb1[tid] = 0.0f;
+      S.gb2[tid] = 0.0f;
+      S.gw3[tid] = 0.0f;
+    }
+    if (tid == 0) S.gb3 = 0.0f;
+    for (uint32_t t = 0; t < tiles && ok; ++t) {
+      const uint32_t k = t * TILE + tid;
+      const bool valid = k < B;
+      const uint32_t srow = valid ? perm[(size_t)bt_i * B + k] : 0u;
+      float x[KIN];
+#pragma unroll
+      for (int q = 0; q < KIN; ++q) x[q] = 0.0f;
+      float target = 0.0f;
+      if (valid) {
+#pragma unroll
+        for (int q = 0; q < NF; ++q) x[q] = (feat[(size_t)srow * NF + q] - norm.mean[q]) * norm.inv_std[q];
+        target = tgt[srow] / norm.t_scale;
+      }
+      st_row8(S.x, tid, 0, TILE, x);
+      st_row8(S.x, tid, 8, TILE, x + 8);
+#pragma unroll
+      for (int q = 0; q < KIN; ++q) st_elem(S.bt, HID + q, tid, GN, x[q]);  // x^T rows 64..79
+      fence_async_smem();
+      fence_before_sync();
+      __syncthreads();
+      fence_after_sync();
+      // ---- layer 1
+      if (tid == 0) {
+        gemm_issue(tmem + TM_Z1, smem_u32(S.x), smem_u32(S.w1), HID, KIN, false);
+        umma_commit(mbar);
+      }
+      ok = mbar_wait(mbar, phase);
+      phase ^= 1u;
+      fence_after_sync();
+      float h1[HID];
+#pragma unroll
+      for (int c = 0; c < HID; c += 16) {
+        float v[16];
+        tmem_ld16(lane_base + TM_Z1 + c, v);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) h1[c + q] = tanhf(v[q] + S.P[OFF_B1 + c + q]);
+      }
+#pragma unroll
+      for (int c = 0; c < HID; c += 8) st_row8(S.h1, tid, c, TILE, &h1[c]);
+#pragma unroll 8
+      for (int f = 0; f < HID; ++f) st_elem(S.bt, f, tid, GN, h1[f]);  // h1^T rows 0..63
+      fence_async_smem();
+      fence_before_sync();
+      __syncthreads();
+      fence_after_sync();
+      ok = __syncthreads_and(ok);
+      if (!ok) break;
+      // ---- layer 2
+      if (tid == 0) {
+        gemm_issue(tmem + TM_Z2, smem_u32(S.h1), smem_u32(S.w2), HID, HID, false);
+        umma_commit(mbar);
+      }
+      ok = mbar_wait(mbar, phase);
+      phase ^= 1u;
+      fence_after_sync();
+      float y = S.P[OFF_B3];
+      float h2[HID];
+#pragma unroll
+      for (int c = 0; c < HID; c += 16) {
+        float v[16];
+        tmem_ld16(lane_base + TM_Z2 + c, v);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          h2[c + q] = tanhf(v[q] + S.P[OFF_B2 + c + q]);
+          y += h2[c + q] * S.P[OFF_W3 + c + q];
+        }
+      }
+      const float err_y = valid ? (y - target) : 0.0f;
+      loss_acc += err_y * err_y;
+      const float dy = 2.0f * err_y * inv_b;
+      float dz2[HID];
+#pragma unroll
+      for (int c = 0; c < HID; ++c) {
+        dz2[c] = dy * S.P[OFF_W3 + c] * (1.0f - h2[c] * h2[c]);
+        S.scratch[tid][c] = dy * h2[c];
+      }
+      colsum_into(S, S.gw3, tid);
+#pragma unroll
+      for (int c = 0; c < HID; ++c) S.scratch[tid][c] = dz2[c];
+      colsum_into(S, S.gb2, tid);
+      S.scratch[tid][0] = dy;
+      __syncthreads();
+      if (tid == 0) {
+        float s = 0.0f;
+        for (int r = 0; r < TILE; ++r) s += S.scratch[r][0];
+        S.gb3 += s;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int c = 0; c < HID; c += 8) st_row8(S.dz2, tid, c, TILE, &dz2[c]);
+#pragma unroll 8
+      for (int f = 0; f < HID; ++f) st_elem(S.g, f, tid, TILE, dz2[f]);  // dz2^T rows 0..63
+      fence_async_smem();
+      fence_before_sync();
+      __syncthreads();
+      fence_after_sync();
+      // ---- dh1 = dz2 . W2 (into the Z1 columns, consumed above)
+      if (tid == 0) {
+        gemm_issue(tmem + TM_Z1, smem_u32(S.dz2), smem_u32(S.w2t), HID, HID, false);
+        umma_commit(mbar);
+      }
+      ok = mbar_wait(mbar, phase);
+      phase ^= 1u;
+      fence_after_sync();
+      float dz1[HID];
+#pragma unroll
+      for (int c = 0; c < HID; c += 16) {
+        float v[16];
+        tmem_ld16(lane_base + TM_Z1 + c, v);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) dz1[c + q] = v[q] * (1.0f - h1[c + q] * h1[c + q]);
+      }
+#pragma unroll
+      for (int c = 0; c < HID; ++c) S.scratch[tid][c] = dz1[c];
+      colsum_into(S, S.gb1, tid);
+#pragma unroll 8
+      for (int f = 0; f < HID; ++f) st_elem(S.g, HID + f, tid, TILE, dz1[f]);  // dz1^T rows 64..127
+      fence_async_smem();
+      fence_before_sync();
+      __syncthreads();
+      fence_after_sync();
+      ok = __syncthreads_and(ok);
+      if (!ok) break;
+      // ---- weight gradients, accumulated over the batch's tiles
+      if (tid == 0) {
+        gemm_issue(tmem + TM_G, smem_u32(S.g), smem_u32(S.bt), GN, TILE, t > 0);
+        umma_commit(mbar);
+      }
+      ok = mbar_wait(mbar, phase);
+      phase ^= 1u;
+      fence_after_sync();
+      ok = __syncthreads_and(ok);
+    }
+    if (!ok) break;
+    // ---- gradients out of TMEM: row r < 64 -> dW2[r][0..63]; r >= 64 -> dW1[r-64][0..7]
+    float gw[HID];
+#pragma unroll
+    for (int c = 0; c < HID; c += 16) {
+      float v[16];
+      tmem_ld16(lane_base + TM_G + c, v);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) gw[c + q] = v[q];
+    }
+    float gw1[16];
+    tmem_ld16(lane_base + TM_G + HID, gw1);
+    if (mode == 1) {
+      if (tid < HID) {
+        for (int c = 0; c < HID; ++c) grads[OFF_W2 + tid * HID + c] = gw[c];
+        grads[OFF_B1 + tid] = S.gb1[tid];
+        grads[OFF_B2 + tid] = S.gb2[tid];
+        grads[OFF_W3 + tid] = S.gw3[tid];
+      } else {
+        for (int c = 0; c < NF; ++c) grads[OFF_W1 + (tid - HID) * NF + c] = gw1[c];
+      }
+      if (tid == 0) grads[OFF_B3] = S.gb3;
+    } else {
+      const uint32_t st = step0 + bt_i + 1;
+      const float c1 = 1.0f - powf(0.9f, (float)st), c2 = 1.0f - powf(0.999f, (float)st);
+      if (tid < HID) {
+        for (int c = 0; c < HID; ++c) {
+          const int q = OFF_W2 + tid * HID + c;
+          S.P[q] = adam_step(S.P[q], gw[c], adam_m[q], adam_v[q], lr, c1, c2);
+        }
+        int q = OFF_B1 + tid;
+        S.P[q] = adam_step(S.P[q], S.gb1[tid], adam_m[q], adam_v[q], lr, c1, c2);
+        q = OFF_B2 + tid;
+        S.P[q] = adam_step(S.P[q], S.gb2[tid], adam_m[q], adam_v[q], lr, c1, c2);
+        q = OFF_W3 + tid;
+        S.P[q] = adam_step(S.P[q], S.gw3[tid], adam_m[q], adam_v[q], lr, c1, c2);
+      } else {
+        for (int c = 0; c < NF; ++c) {
+          const int q = OFF_W1 + (tid - HID) * NF + c;
+          S.P[q] = adam_step(S.P[q], gw1[c], adam_m[q], adam_v[q], lr, c1, c2);
+        }
+      }
+      if (tid == 0) S.P[OFF_B3] = adam_step(S.P[OFF_B3], S.gb3, adam_m[OFF_B3], adam_v[OFF_B3], lr, c1, c2);
+      __syncthreads();
+      load_weights_bf16(S.P, S.w1, S.w2, S.w2t, tid);
+      fence_async_smem();
+    }
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+  }
+  // loss: per-thread sums, fixed-order reduction
+  S.scratch[tid][0] = loss_acc;
+  __syncthreads();
+  if (tid == 0) {
+    float s = 0.0f;
+    for (int r = 0; r < TILE; ++r) s += S.scratch[r][0];
+    *loss_out = s;
+    if (!ok) atomicExch(err, 1u);
+  }
+  if (mode == 0 && ok)
+    for (int q = tid; q < NPARAM; q += TILE) params[q] = S.P[q];
+  fence_before_sync();
+  __syncthreads();
+  if (!ok) mbar_wait(mbar, phase);
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(TM_COLS_TRAIN));
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------
+// host objects
+// ---------------------------------------------------------------------
+struct hb_shake_mlp {
+  hb_context *ctx = nullptr;
+  float *d_params = nullptr, *d_m = nullptr, *d_v = nullptr;
+  uint32_t *d_err = nullptr;
+  float *d_loss = nullptr;
+  uint32_t step = 0;
+  MlpNorm norm;
+};
+
+static int mlp_check_err(hb_shake_mlp *m) {
+  uint32_t e = 0;
+  HB_CUDA(cudaMemcpy(&e, m->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  if (e) {
+    HB_CUDA(cudaMemset(m->d_err, 0, sizeof(uint32_t)));
+    return hb_fail(HB_ERR_DEVICE_TIMEOUT, "tensor-core MLP: a bounded mbarrier wait gave up");
+  }
+  return HB_OK;
+}
+
+// dynamic shared memory of the inference kernel, padded well past InferSmem
+// so that every operand read of a descriptor stays inside the allocation
+constexpr size_t INFER_SMEM = 64 * 1024;
+static_assert(sizeof(InferSmem) <= INFER_SMEM, "inference shared memory plan");
+static_assert(sizeof(TrainSmem) <= 227 * 1024, "training shared memory plan");
+
+static int mlp_smem_attrs() {
+  static bool done = false;
+  if (done) return HB_OK;
+  HB_CUDA(cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(TrainSmem)));
+  HB_CUDA(cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)INFER_SMEM));
+  done = true;
+  return HB_OK;
+}
+
+int mlp_infer(hb_shake_mlp *m, const float *d_feat, uint32_t n, float *d_out, cudaStream_t s) {
+  if (n == 0) return HB_OK;
+  HB_TRY(mlp_smem_attrs());
+  k_mlp_infer<<<hb_div_up(n, TILE), TILE, INFER_SMEM, s>>>(m->d_params, m->norm, d_feat, n,
+                                                            d_out, m->d_err);
+  HB_CUDA(cudaGetLastError());
+  return HB_OK;
+}
+
+extern "C" int hb_shake_mlp_destroy(hb_shake_mlp *m) {
+  if (!m) return HB_OK;
+  cudaSetDevice(m->ctx->device);
+  cudaStreamSynchronize(m->ctx->stream);
+  cudaFree(m->d_params);
+  cudaFree(m->d_m);
+  cudaFree(m->d_v);
+  cudaFree(m->d_err);
+  cudaFree(m->d_loss);
+  delete m;
+  return HB_OK;
+}
+
+extern "C" int hb_shake_mlp_create(hb_context *ctx, uint64_t seed, hb_shake_mlp **out) {
+  HB_REQUIRE(ctx && out, HB_ERR_INVALID_ARGUMENT, "null argument");
+  hb_shake_mlp *m = new hb_shake_mlp();
+  m->ctx = ctx;
+  for (int q = 0; q < NF; ++q) {
+    m->norm.mean[q] = 0.0f;
+    m->norm.inv_std[q] = 1.0f;
+  }
+  m->norm.t_scale = 1.0f;
+  // Glorot-uniform weights from a seeded generator, zero biases
+  std::vector<float> p(NPARAM, 0.0f);
+  std::mt19937_64 rng(seed);
+  auto fill = [&](int off, int fan_out, int fan_in) {
+    const double lim = std::sqrt(6.0 / (fan_in + fan_out));
+    std::uniform_real_distribution<double> u(-lim, lim);
+    for (int q = 0; q < fan_out * fan_in; ++q) p[off + q] = (float)u(rng);
+  };
+  fill(OFF_W1, HID, NF);
+  fill(OFF_W2, HID, HID);
+  fill(OFF_W3, 1, HID);
+  bool ok = cudaSetDevice(ctx->device) == cudaSuccess &&
+            cudaMalloc(&m->d_params, sizeof(float) * NPARAM) == cudaSuccess &&
+            cudaMalloc(&m->d_m, sizeof(float) * NPARAM) == cudaSuccess &&
+            cudaMalloc(&m->d_v, sizeof(float) * NPARAM) == cudaSuccess &&
+            cudaMalloc(&m->d_err, sizeof(uint32_t)) == cudaSuccess &&
+            cudaMalloc(&m->d_loss, sizeof(float)) == cudaSuccess &&
+            cudaMemcpy(m->d_params, p.data(), sizeof(float) * NPARAM, cudaMemcpyHostToDevice) == cudaSuccess &&
+            cudaMemset(m->d_m, 0, sizeof(float) * NPARAM) == cudaSuccess &&
+            cudaMemset(m->d_v, 0, sizeof(float) * NPARAM) == cudaSuccess &&
+            cudaMemset(m->d_err, 0, sizeof(uint32_t)) == cudaSuccess;
+  if (!ok) {
+    hb_shake_mlp_destroy(m);
+    return hb_fail(HB_ERR_CUDA, "MLP allocation failed");
+  }
+  *out = m;
+  return HB_OK;
+}
+
+extern "C" uint32_t hb_shake_mlp_param_count(void) { return (uint32_t)NPARAM; }
+
+extern "C" int hb_shake_mlp_get_params(hb_shake_mlp *m, float *out, uint32_t n) {
+  HB_REQUIRE(m && out && n == (uint32_t)NPARAM, HB_ERR_INVALID_ARGUMENT, "need param_count floats");
+  HB_CUDA(cudaMemcpy(out, m->d_params, sizeof(float) * NPARAM, cudaMemcpyDeviceToHost));
+  return HB_OK;
+}
+
+extern "C" int hb_shake_mlp_set_params(hb_shake_mlp *m, const float *in, uint32_t n) {
+  HB_REQUIRE(m && in && n == (uint32_t)NPARAM, HB_ERR_INVALID_ARGUMENT, "need param_count floats");
+  HB_CUDA(cudaMemcpy(m->d_params, in, sizeof(float) * NPARAM, cudaMemcpyHostToDevice));
+  HB_CUDA(cudaMemset(m->d_m, 0, sizeof(float) * NPARAM));
+  HB_CUDA(cudaMemset(m->d_v, 0, sizeof(float) * NPARAM));
+  m->step = 0;
+  return HB_OK;
+}
+
+extern "C" int hb_shake_mlp_set_normalization(hb_shake_mlp *m, const float *mean,
+                                              const float *inv_std, float target_scale) {
+  HB_REQUIRE(m && mean && inv_std && target_scale > 0.0f, HB_ERR_INVALID_ARGUMENT, "bad argument");
+  for (int q = 0; q < NF; ++q) {
+    m->norm.mean[q] = mean[q];
+    m->norm.inv_std[q] = inv_std[q];
+  }
+  m->norm.t_scale = target_scale;
+  return HB_OK;
+}
+
+extern "C" int hb_shake_mlp_predict(hb_shake_mlp *m, const float *features, uint64_t n,
+                                    float *out) {
+  HB_REQUIRE(m && (n == 0 || (features && out)), HB_ERR_INVALID_ARGUMENT, "null argument");
+  if (n == 0) return HB_OK;
+  HB_REQUIRE(n < (1ull << 31), HB_ERR_INVALID_ARGUMENT, "too many rows");
+  cudaStream_t s = m->ctx->stream;
+  float *d_f = nullptr, *d_o = nullptr;
+  HB_CUDA(cudaMalloc(&d_f, sizeof(float) * NF * n));
+  HB_CUDA(cudaMalloc(&d_o, sizeof(float) * n));
+  int rc = HB_OK;
+  if (cudaMemcpyAsync(d_f, features, sizeof(float) * NF * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    rc = hb_fail(HB_ERR_CUDA, "copy");
+  if (rc == HB_OK) rc = mlp_infer(m, d_f, (uint32_t)n, d_o, s);
+  if (rc == HB_OK &&
+      (cudaMemcpyAsync(out, d_o, sizeof(float) * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+       cudaStreamSynchronize(s) != cudaSuccess))
+    rc = hb_fail(HB_ERR_CUDA, "predict");
+  cudaFree(d_f);
+  cudaFree(d_o);
+  if (rc == HB_OK) rc = mlp_check_err(m);
+  return rc;
+}
+
+// upload rows, run the training kernel (mode 0 or 1)
+static int mlp_run(hb_shake_mlp *m, const float *features, const float *targets, uint64_t n,
+                   const std::vector<uint32_t> &perm, uint32_t n_batches, uint32_t B, float lr,
+                   int mode, float *grads_host, double *loss) {
+  HB_TRY(mlp_smem_attrs());
+  cudaStream_t s = m->ctx->stream;
+  float *d_f = nullptr, *d_t = nullptr, *d_g = nullptr;
+  uint32_t *d_p = nullptr;
+  int rc = HB_OK;
+  auto ok = [](cudaError_t e) { return e == cudaSuccess; };
+  if (!(ok(cudaMalloc(&d_f, sizeof(float) * NF * n)) && ok(cudaMalloc(&d_t, sizeof(float) * n)) &&
+        ok(cudaMalloc(&d_p, sizeof(uint32_t) * perm.size())) &&
+        ok(cudaMalloc(&d_g, sizeof(float) * NPARAM)) &&
+        ok(cudaMemcpyAsync(d_f, features, sizeof(float) * NF * n, cudaMemcpyHostToDevice, s)) &&
+        ok(cudaMemcpyAsync(d_t, targets, sizeof(float) * n, cudaMemcpyHostToDevice, s)) &&
+        ok(cudaMemcpyAsync(d_p, perm.data(), sizeof(uint32_t) * perm.size(), cudaMemcpyHostToDevice, s))))
+    rc = hb_fail(HB_ERR_CUDA, "MLP upload failed");
+  if (rc == HB_OK) {
+    k_mlp_train<<<1, TILE, sizeof(TrainSmem), s>>>(m->d_params, m->d_m, m->d_v, m->step, m->norm,
+                                                   d_f, d_t, d_p, n_batches, B, lr, mode, d_g,
+                                                   m->d_loss, m->d_err);
+    if (cudaGetLastError() != cudaSuccess) rc = hb_fail(HB_ERR_CUDA, "MLP launch failed");
+  }
+  float lsum = 0.0f;
+  if (rc == HB_OK &&
+      !(ok(cudaMemcpyAsync(&lsum, m->d_loss, sizeof(float), cudaMemcpyDeviceToHost, s)) &&
+        (!grads_host ||
+         ok(cudaMemcpyAsync(grads_host, d_g, sizeof(float) * NPARAM, cudaMemcpyDeviceToHost, s))) &&
+        ok(cudaStreamSynchronize(s))))
+    rc = hb_fail(HB_ERR_CUDA, "MLP run failed");
+  cudaFree(d_f);
+  cudaFree(d_t);
+  cudaFree(d_p);
+  cudaFree(d_g);
+  if (rc == HB_OK) rc = mlp_check_err(m);
+  if (rc == HB_OK && loss) *loss = (double)lsum / (double)std::max<uint64_t>(1, (uint64_t)n_batches * B);
+  if (rc == HB_OK && mode == 0) m->step += n_batches;
+  return rc;
+}
+
+extern "C" int hb_shake_mlp_gradients(hb_shake_mlp *m, const float *features,
+                                      const float *targets, uint32_t n, float *grads,
+                                      double *loss) {
+  HB_REQUIRE(m && features && targets && grads && n > 0, HB_ERR_INVALID_ARGUMENT, "null argument");
+  HB_REQUIRE(n <= 4096, HB_ERR_INVALID_ARGUMENT, "at most 4096 rows per gradient call");
+  std::vector<uint32_t> perm(n);
+  for (uint32_t i = 0; i < n; ++i) perm[i] = i;
+  return mlp_run(m, features, targets, n, perm, 1, n, 0.0f, 1, grads, loss);
+}
+
+extern "C" int hb_shake_mlp_train(hb_shake_mlp *m, const float *features, const float *targets,
+                                  uint64_t n, uint32_t epochs, uint32_t batch, double lr,
+                                  uint64_t seed, double *loss_per_epoch) {
+  HB_REQUIRE(m && features && targets && n > 0 && epochs > 0, HB_ERR_INVALID_ARGUMENT,
+             "null argument");
+  HB_REQUIRE(batch >= 1 && batch <= 4096 && n >= batch, HB_ERR_INVALID_ARGUMENT,
+             "batch must be in [1, min(4096, n)]");
+  HB_REQUIRE(n < (1ull << 31), HB_ERR_INVALID_ARGUMENT, "too many rows");
+  const uint32_t n_batches = (uint32_t)(n / batch);
+  std::mt19937_64 rng(seed);
+  std::vector<uint32_t> perm(n);
+  for (uint32_t e = 0; e < epochs; ++e) {
+    for (uint64_t i = 0; i < n; ++i) perm[i] = (uint32_t)i;
+    std::shuffle(perm.begin(), perm.end(), rng);
+    perm.resize((size_t)n_batches * batch);
+    double l = 0.0;
+    HB_TRY(mlp_run(m, features, targets, n, perm, n_batches, batch, (float)lr, 0, nullptr, &l));
+    if (loss_per_epoch) loss_per_epoch[e] = l;
+    perm.resize(n);
+  }
+  return HB_OK;
+}

@@ -65,6 +65,7 @@ typedef struct hb_constraints hb_constraints;
 typedef struct hb_integrator hb_integrator;
 typedef struct hb_barostat hb_barostat;
 typedef struct hb_batch hb_batch;
+typedef struct hb_shake_mlp hb_shake_mlp;
 
 /* Message of the last failing call on this thread ("" when none). */
 const char *hb_last_error(void);
@@ -141,6 +142,26 @@ typedef struct {
    * neighbour list was rebuilt and of how it packed the pairs -- what
    * bit-exact time reversal of the lossless integrator needs. */
   int pair_mode;
+  /* bonded terms, one row per term (the reference's HarmonicBond,
+   * HarmonicAngle and PeriodicDihedral slots, src/forces/harmonic_bond.rs,
+   * src/forces/angle.rs, src/forces/dihedral.rs, expanded from their type
+   * tables): U = k/2 (r - r0)^2; U = k/2 (theta - theta0)^2 with the angle
+   * at the middle atom; U = k (1 + cos(n phi - phi0)).  Their exclusions
+   * (1-2, 1-3, scaled 1-4, src/forces/topology.rs:1185-1275) are the
+   * caller's, in the exclusion CSR above. */
+  uint32_t n_bonds;
+  const uint32_t *bond_atoms;        /* [2 n_bonds] */
+  const double *bond_k;
+  const double *bond_r0;
+  uint32_t n_angles;
+  const uint32_t *angle_atoms;       /* [3 n_angles]: i, j (vertex), k */
+  const double *angle_k;
+  const double *angle_theta0;
+  uint32_t n_dihedrals;
+  const uint32_t *dihedral_atoms;    /* [4 n_dihedrals]: i, j, k, l */
+  const double *dihedral_k;
+  const double *dihedral_phi0;
+  const uint32_t *dihedral_n;        /* multiplicity */
 } hb_forcefield_desc;
 
 int hb_forcefield_create(hb_system *sys, const hb_forcefield_desc *desc,
@@ -156,9 +177,10 @@ int hb_forcefield_step(hb_forcefield *ff, int level);
 int hb_forcefield_pre_step(hb_forcefield *ff, int force, int *rebuilt);
 /* FP64 scalars of the last HB_FORCES_AND_SCALARS step:
  * out[0] LJ energy, [1] real-space Coulomb, [2] reciprocal (k-space sum),
- * [3] self energy (subtracted), [4] total potential, [5] pair virial,
- * [6] reciprocal virial, [7] total virial. */
-int hb_forcefield_scalars(hb_forcefield *ff, double out[8]);
+ * [3] self energy (subtracted), [4] total potential, [5] pair + bonded
+ * virial, [6] reciprocal virial, [7] total virial, [8] bonded energy,
+ * [9] reserved (0). */
+int hb_forcefield_scalars(hb_forcefield *ff, double out[10]);
 /* per-atom energy and virial shares of the last scalar step ([n] each). */
 int hb_forcefield_get_per_atom(hb_forcefield *ff, double *energy,
                                double *virial);
@@ -192,8 +214,9 @@ typedef struct {
   const uint32_t *con_i;
   const uint32_t *con_j;
   const double *con_dist;
-  double shake_tol;                /* absolute tolerance on |r|^2 - d^2 */
+  double shake_tol;                /* tolerance on |r|^2 - d^2 (bohr^2) */
   uint32_t shake_max_iter;
+  int shake_tol_relative;          /* != 0: tolerance relative to d^2 */
 } hb_constraints_desc;
 
 int hb_constraints_create(hb_system *sys, const hb_constraints_desc *desc,
@@ -207,6 +230,47 @@ int hb_constraints_after_drift(hb_constraints *c, double dt);
 int hb_constraints_after_kick(hb_constraints *c, double dt);
 /* per-atom constraint virial of the last step ([n]) */
 int hb_constraints_get_virial(hb_constraints *c, double *virial);
+/* SHAKE sweep statistics since creation or the last reset: out[0]
+ * group-sweeps (sweeps that still moved something, summed over groups and
+ * calls), out[1] group solves, out[2] mean sweeps per solve. */
+int hb_constraints_shake_stats(hb_constraints *c, double out[3], int reset);
+/* Training data of the learned warm start: while recording, every SHAKE
+ * position call stores per SHAKE constraint (in group order) 8 geometry
+ * features, the first Gauss-Seidel multiplier lam1, the multiplier-to-sigma
+ * scale ls and the converged multiplier lam; get_record copies those of the
+ * last call (features [8 m], the others [m], m = SHAKE constraints). */
+int hb_constraints_record(hb_constraints *c, int enable);
+int hb_constraints_get_record(hb_constraints *c, float *features, double *lam1, double *lscale,
+                              double *lam, uint32_t *m);
+/* Warm-start SHAKE from the network (NULL switches it off): features ->
+ * network -> lam0 = lam1 + prediction / ls, then the usual sweeps to the
+ * same tolerance. */
+int hb_constraints_set_warm_start(hb_constraints *c, hb_shake_mlp *m);
+
+/* ---- learned SHAKE warm start (no reference counterpart: the reference's
+ * SHAKE starts from zero multipliers, kernels/shake.cu:108-348).  A
+ * 8 -> 64 -> 64 -> 1 tanh network; its hidden layers run as BF16 tcgen05
+ * tensor-core GEMMs with FP32 accumulation, forward and backward, trained by
+ * Adam in one deterministic CTA.  Parameters (FP32, packed): W1 [64][8], b1
+ * [64], W2 [64][64], b2 [64], w3 [64], b3.  Inputs are standardised by
+ * (x - mean) * inv_std and targets divided by target_scale inside. */
+int hb_shake_mlp_create(hb_context *ctx, uint64_t seed, hb_shake_mlp **out);
+int hb_shake_mlp_destroy(hb_shake_mlp *m);
+uint32_t hb_shake_mlp_param_count(void);
+int hb_shake_mlp_get_params(hb_shake_mlp *m, float *out, uint32_t n);
+int hb_shake_mlp_set_params(hb_shake_mlp *m, const float *in, uint32_t n);
+int hb_shake_mlp_set_normalization(hb_shake_mlp *m, const float *mean, const float *inv_std,
+                                   float target_scale);
+/* host rows in, host predictions out (target units) */
+int hb_shake_mlp_predict(hb_shake_mlp *m, const float *features, uint64_t n, float *out);
+/* gradients of the mean squared error (normalised units) over n <= 4096
+ * rows, no update; *loss = that error */
+int hb_shake_mlp_gradients(hb_shake_mlp *m, const float *features, const float *targets,
+                           uint32_t n, float *grads, double *loss);
+/* epochs of minibatch Adam (seeded shuffles); loss_per_epoch [epochs] */
+int hb_shake_mlp_train(hb_shake_mlp *m, const float *features, const float *targets,
+                       uint64_t n, uint32_t epochs, uint32_t batch, double lr, uint64_t seed,
+                       double *loss_per_epoch);
 
 /* ---- integrator: replaces integrator::run_step (src/integrator/mod.rs:344)
  * for velocity Verlet (src/integrator/velocity_verlet.rs) and Langevin

@@ -35,10 +35,14 @@ class OrFF(C.Structure):
         ("coul_poly_erfc", C.c_int),
         ("recip_on", C.c_int), ("grid", C.c_int * 3), ("order", C.c_int),
         ("excl_off", PI), ("excl_partner", PI), ("excl_lj_scale", PD), ("excl_coul_scale", PD),
+        ("n_bonds", C.c_int32), ("bond_atoms", PI), ("bond_k", PD), ("bond_r0", PD),
+        ("n_angles", C.c_int32), ("angle_atoms", PI), ("angle_k", PD), ("angle_theta0", PD),
+        ("n_dihedrals", C.c_int32), ("dihedral_atoms", PI), ("dihedral_k", PD),
+        ("dihedral_phi0", PD), ("dihedral_n", PI),
     ]
 
 
-TERMS = ["lj", "coulomb_real", "recip", "self", "virial_pair", "virial_recip", "near_cut"]
+TERMS = ["lj", "coulomb_real", "recip", "self", "virial_pair", "virial_recip", "near_cut", "bonded"]
 
 _lib = None
 
@@ -130,6 +134,24 @@ class FF:
                 a, p = conv(arr)
                 self.keep.append(a)
                 setattr(f, name, p)
+        bonded = (getattr(spec, "meta", None) or {}).get("bonded") or {}
+        for key, count, fields in (
+                ("harmonic_bond", "n_bonds", (("bond_atoms", "atoms", _i), ("bond_k", "k", _d),
+                                              ("bond_r0", "r0", _d))),
+                ("harmonic_angle", "n_angles", (("angle_atoms", "atoms", _i), ("angle_k", "k", _d),
+                                                ("angle_theta0", "theta0", _d))),
+                ("periodic_dihedral", "n_dihedrals", (("dihedral_atoms", "atoms", _i),
+                                                      ("dihedral_k", "k", _d),
+                                                      ("dihedral_phi0", "phi0", _d),
+                                                      ("dihedral_n", "n", _i)))):
+            p = bonded.get(key)
+            if p is None or len(p.k) == 0:
+                continue
+            setattr(f, count, len(p.k))
+            for cname, attr, conv in fields:
+                a, ptr = conv(np.asarray(getattr(p, attr)).reshape(-1))
+                self.keep.append(a)
+                setattr(f, cname, ptr)
         self.c = f
 
 

@@ -638,6 +638,117 @@ double or_ewald_recip_energy(int32_t n, const double *pos, const double *q,
 /* total force field                                                   */
 /* ------------------------------------------------------------------ */
 
+/* ---- bonded terms in FP64 (src/forces/harmonic_bond.rs:283-307,
+ * src/forces/angle.rs:260-313, src/forces/dihedral.rs:383-467); per-atom
+ * energy / virial shares split equally over each term's atoms ---- */
+static void mi_disp(const double *pos, int a, int b, const or_box *box, double d[3]) {
+  d[0] = pos[3 * a] - pos[3 * b];
+  d[1] = pos[3 * a + 1] - pos[3 * b + 1];
+  d[2] = pos[3 * a + 2] - pos[3 * b + 2];
+  or_min_image(box, &d[0], &d[1], &d[2]);
+}
+static double dot3(const double *a, const double *b) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+static void cross3(const double *a, const double *b, double *o) {
+  o[0] = a[1] * b[2] - a[2] * b[1];
+  o[1] = a[2] * b[0] - a[0] * b[2];
+  o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+static void bonded_terms(const double *pos, const or_box *box, const or_ff *ff, double *F,
+                         double *E, double *W, double *terms) {
+  double e_b = 0.0, w_b = 0.0;
+  for (int32_t q = 0; q < ff->n_bonds; ++q) {
+    const int i = ff->bond_atoms[2 * q], j = ff->bond_atoms[2 * q + 1];
+    double d[3];
+    mi_disp(pos, i, j, box, d);
+    const double r2 = dot3(d, d), r = sqrt(r2);
+    if (r < 1e-7) continue;
+    const double dr = r - ff->bond_r0[q];
+    const double fmag = -ff->bond_k[q] * dr / r;
+    const double u = 0.5 * ff->bond_k[q] * dr * dr, w = fmag * r2;
+    for (int x = 0; x < 3; ++x) {
+      F[3 * i + x] += fmag * d[x];
+      F[3 * j + x] -= fmag * d[x];
+    }
+    E[i] += 0.5 * u; E[j] += 0.5 * u;
+    W[i] += 0.5 * w; W[j] += 0.5 * w;
+    e_b += u;
+    w_b += w;
+  }
+  for (int32_t q = 0; q < ff->n_angles; ++q) {
+    const int i = ff->angle_atoms[3 * q], j = ff->angle_atoms[3 * q + 1],
+              k = ff->angle_atoms[3 * q + 2];
+    double a[3], c[3];
+    mi_disp(pos, i, j, box, a);
+    mi_disp(pos, k, j, box, c);
+    const double a2 = dot3(a, a), c2 = dot3(c, c);
+    if (a2 == 0.0 || c2 == 0.0) continue;
+    const double la = sqrt(a2), lc = sqrt(c2), dt = dot3(a, c);
+    double cs = dt / (la * lc);
+    if (cs > 1.0) cs = 1.0;
+    if (cs < -1.0) cs = -1.0;
+    const double sn = sqrt(fmax(1.0 - cs * cs, 0.0));
+    if (sn < 1e-7) continue;
+    const double th = atan2(la * lc * sn, dt), dth = th - ff->angle_theta0[q];
+    const double g = -ff->angle_k[q] * dth / sn;
+    double fi[3], fk[3];
+    for (int x = 0; x < 3; ++x) {
+      fi[x] = g * (cs / a2 * a[x] - c[x] / (la * lc));
+      fk[x] = g * (cs / c2 * c[x] - a[x] / (la * lc));
+      F[3 * i + x] += fi[x];
+      F[3 * k + x] += fk[x];
+      F[3 * j + x] -= fi[x] + fk[x];
+    }
+    const double u = 0.5 * ff->angle_k[q] * dth * dth, w = dot3(a, fi) + dot3(c, fk);
+    E[i] += u / 3; E[j] += u / 3; E[k] += u / 3;
+    W[i] += w / 3; W[j] += w / 3; W[k] += w / 3;
+    e_b += u;
+    w_b += w;
+  }
+  for (int32_t q = 0; q < ff->n_dihedrals; ++q) {
+    const int *at = ff->dihedral_atoms + 4 * q;
+    double b1[3], b2[3], b3[3], m[3], nn[3];
+    mi_disp(pos, at[0], at[1], box, b1);
+    mi_disp(pos, at[2], at[1], box, b2);
+    mi_disp(pos, at[2], at[3], box, b3);
+    cross3(b1, b2, m);
+    cross3(b2, b3, nn);
+    const double m2 = dot3(m, m), n2 = dot3(nn, nn), b22 = dot3(b2, b2);
+    if (m2 < 1e-14 || n2 < 1e-14 || b22 < 1e-14) continue;
+    const double lb2 = sqrt(b22);
+    const double phi = atan2(lb2 * dot3(b1, nn), dot3(m, nn));
+    const double mult = (double)ff->dihedral_n[q];
+    const double del = mult * phi - ff->dihedral_phi0[q];
+    const double fphi = ff->dihedral_k[q] * mult * sin(del);
+    const double ci = fphi * lb2 / m2, cl = -fphi * lb2 / n2;
+    const double s = dot3(b1, b2) / b22, t = dot3(b3, b2) / b22;
+    double fi[3], fj[3], fk[3], fl[3], bl[3];
+    for (int x = 0; x < 3; ++x) {
+      fi[x] = ci * m[x];
+      fl[x] = cl * nn[x];
+      fj[x] = (s - 1.0) * fi[x] - t * fl[x];
+      fk[x] = -s * fi[x] + (t - 1.0) * fl[x];
+      bl[x] = b2[x] - b3[x];
+      F[3 * at[0] + x] += fi[x];
+      F[3 * at[1] + x] += fj[x];
+      F[3 * at[2] + x] += fk[x];
+      F[3 * at[3] + x] += fl[x];
+    }
+    const double u = ff->dihedral_k[q] * (1.0 + cos(del));
+    const double w = dot3(b1, fi) + dot3(b2, fk) + dot3(bl, fl);
+    for (int a = 0; a < 4; ++a) {
+      E[at[a]] += 0.25 * u;
+      W[at[a]] += 0.25 * w;
+    }
+    e_b += u;
+    w_b += w;
+  }
+  terms[OR_E_BONDED] = e_b;
+  terms[OR_W_PAIR] += w_b;
+}
+
 int or_forces(int32_t n, const double *pos, const double *q,
               const int32_t *type, const or_box *box, const or_ff *ff,
               double *F, double *E, double *W, double *terms, int n_threads) {
@@ -726,6 +837,7 @@ int or_forces(int32_t n, const double *pos, const double *q,
   terms[OR_E_COUL_REAL] = e_c;
   terms[OR_W_PAIR] = w_p;
   terms[OR_N_PAIRS_NEAR_CUT] = near;
+  bonded_terms(pos, box, ff, F, E, W, terms);
   if (ff->recip_on && n > 0) spme_recip(n, pos, q, box, ff, F, E, W, terms);
   return 0;
 }

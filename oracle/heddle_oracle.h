@@ -52,6 +52,20 @@ typedef struct {
   const int32_t *excl_partner;
   const double *excl_lj_scale;
   const double *excl_coul_scale;
+  /* bonded terms, one row per term: harmonic bonds
+   * (src/forces/harmonic_bond.rs:283-307), harmonic angles with the vertex
+   * in the middle (src/forces/angle.rs:260-313), periodic dihedrals
+   * (src/forces/dihedral.rs:383-467). */
+  int32_t n_bonds;
+  const int32_t *bond_atoms;
+  const double *bond_k, *bond_r0;
+  int32_t n_angles;
+  const int32_t *angle_atoms;
+  const double *angle_k, *angle_theta0;
+  int32_t n_dihedrals;
+  const int32_t *dihedral_atoms;
+  const double *dihedral_k, *dihedral_phi0;
+  const int32_t *dihedral_n;
 } or_ff;
 
 /* terms[] layout written by or_forces */
@@ -63,6 +77,7 @@ enum {
   OR_W_PAIR = 4,       /* sum over pairs factor * r^2 */
   OR_W_RECIP = 5,      /* 0.5 * sum_k vf |rho_hat|^2 */
   OR_N_PAIRS_NEAR_CUT = 6, /* pairs within 1e-6 relative of a cutoff */
+  OR_E_BONDED = 7,     /* bonds + angles + dihedrals (their virial is in OR_W_PAIR) */
   OR_N_TERMS = 8
 };
 

@@ -191,3 +191,74 @@ def test_mc_scale_com_keeps_molecules_rigid():
     assert np.allclose(unwrapped, new_contig + K * box1[:3], atol=1e-12)
     # every stored atom is inside the new cell
     assert np.all(np.abs(p1) <= 0.5 * box1[:3] + 1e-12)
+
+
+def test_bonded_terms_are_energy_gradients():
+    # bonds, angles and dihedrals of the solvated chain, each term alone:
+    # F = -dE/dx by central differences (src/forces/*: analytic derivatives)
+    import dataclasses
+
+    spec = S.peptide_in_water()
+    b = spec.meta["bonded"]
+    p0 = spec.positions.copy()
+    p0[:166] += np.random.default_rng(3).normal(scale=0.05, size=(166, 3))  # off the minimum
+    for key in ("harmonic_bond", "harmonic_angle", "periodic_dihedral"):
+        sp = dataclasses.replace(spec, lj_sigma=None, alpha=None, excl_offsets=None,
+                                 meta={"bonded": {key: b[key]}})
+        F, _, _, T = O.forces(sp, p0)
+        assert T["bonded"] > 0.0
+        h = 1e-5
+        for a in (0, 3, 40, 100, 165):
+            for d in range(3):
+                pp = p0.copy()
+                pp[a, d] += h
+                pm = p0.copy()
+                pm[a, d] -= h
+                fd = -(O.forces(sp, pp)[3]["bonded"] - O.forces(sp, pm)[3]["bonded"]) / (2 * h)
+                assert abs(F[a, d] - fd) <= 1e-6 * max(1.0, abs(fd)) + 1e-9, (key, a, d)
+
+
+def test_topology_exclusion_rules():
+    # src/forces/topology.rs:1185-1275 on a 6-atom chain 0-1-2-3-4-5 with a
+    # constraint group {4, 5}, an explicit (0, 2) entry and two dihedrals
+    # sharing the 1-4 pair (0, 3)
+    from heddle_b200.topology import effective_exclusions, exclusion_csr
+
+    bonds = [(0, 1), (1, 2), (2, 3), (3, 4)]
+    angles = [(0, 1, 2), (1, 2, 3), (2, 3, 4)]
+    dihedrals = [(0, 1, 2, 3), (1, 2, 3, 4), (0, 1, 2, 3)]
+    scales = [(0.5, 0.8), (0.4, 0.7), (0.1, 0.1)]
+    eff = effective_exclusions(6, bonds, angles, dihedrals, scales, constraint_groups=[(4, 5)],
+                               explicit=[(2, 0, 0.9, 0.9)])
+    assert eff[(0, 2)] == (0.9, 0.9)          # explicit wins over the angle rule
+    assert eff[(0, 1)] == (0.0, 0.0) and eff[(1, 3)] == (0.0, 0.0)
+    assert eff[(4, 5)] == (0.0, 0.0)          # constraint group pair
+    assert eff[(0, 3)] == (0.5, 0.8)          # first dihedral in sorted order wins
+    assert eff[(1, 4)] == (0.4, 0.7)
+    assert (0, 4) not in eff and (2, 5) not in eff
+    off, part, slj, sc = exclusion_csr(6, eff)
+    assert off[-1] == 2 * len(eff)
+    row0 = part[off[0]:off[1]].tolist()
+    assert row0 == [1, 2, 3]
+
+
+def test_mlp_oracle_gradients_match_finite_differences():
+    # the CPU statement of the warm-start network: without the bf16 operand
+    # rounding its gradient is the exact derivative of the loss
+    from oracle import mlp as M
+
+    rng = np.random.default_rng(7)
+    p = rng.normal(scale=0.3, size=M.NPARAM)
+    x = rng.normal(size=(40, M.NF))
+    t = rng.normal(size=40)
+    g, loss = M.gradients(p, x, t, use_bf16=False)
+    h = 1e-6
+    for q in list(range(0, M.NPARAM, 97)) + [M.NPARAM - 1]:
+        pp = p.copy()
+        pp[q] += h
+        pm = p.copy()
+        pm[q] -= h
+        fd = (M.gradients(pp, x, t, use_bf16=False)[1] - M.gradients(pm, x, t, use_bf16=False)[1]) / (2 * h)
+        assert abs(g[q] - fd) <= 1e-6 * max(1.0, abs(fd)), q
+    # bf16 rounding is round-to-nearest-even on the top 16 bits
+    assert M.bf16(1.0 + 2.0 ** -8) == 1.0 and M.bf16(1.0 + 3 * 2.0 ** -8) == 1.0 + 2.0 ** -6
