@@ -461,12 +461,16 @@ extern "C" int hb_forcefield_create(hb_system *sys, const hb_forcefield_desc *d,
   hb_forcefield *ff = new hb_forcefield();
   *ff = tmp;
   ff->sys = sys;
-  // pair kernel: the rotation sweep by default; HB_PAIR_KERNEL=compact selects
-  // the compacted pair-list form (shared-memory int64 atomics); exact pairs
-  // use the compacted form with per-pair fixed point and minimum image
-  ff->pair_variant = 1;
-  if (const char *pk = std::getenv("HB_PAIR_KERNEL"))
-    ff->pair_variant = std::string(pk) == "compact" ? 0 : 1;
+  // pair kernel: the masked form for force-only steps (the rotation sweep
+  // for steps with energies); HB_PAIR_KERNEL=rotation / compact select the
+  // rotation sweep or the compacted pair-list form (shared-memory int64
+  // atomics) throughout; exact pairs use the compacted form with per-pair
+  // fixed point and minimum image
+  ff->pair_variant = 3;
+  if (const char *pk = std::getenv("HB_PAIR_KERNEL")) {
+    const std::string v(pk);
+    ff->pair_variant = v == "compact" ? 0 : (v == "rotation" ? 1 : 3);
+  }
   if (d->pair_mode == HB_PAIRS_EXACT) ff->pair_variant = 2;
   HB_CUDA(cudaSetDevice(sys->ctx->device));
   HB_CUDA(cudaMalloc(&ff->d_lj, sizeof(float4) * ff->h_lj.size()));

@@ -250,8 +250,9 @@ struct hb_forcefield {
   std::vector<float4> h_lj;        // per type pair: sigma^2, 24 eps, cut^2, r_switch^2
   float4 *d_lj = nullptr;
   float alpha = 0.f, coul_rc2 = 0.f;
-  int pair_variant = 1;            // 0: compacted pair list, 1: full rotation sweep,
-                                   // 2: compacted, per-pair fixed point + minimum image
+  int pair_variant = 3;            // 0: compacted pair list, 1: full rotation sweep,
+                                   // 2: compacted, per-pair fixed point + minimum image,
+                                   // 3: masked (rotation sweep for energy steps)
   float rc_max = 0.f, r_skin = 0.f, r_search = 0.f;
   int any_switch = 0;
   int excl_scaled = 0;             // some exclusion has a non-zero scale

@@ -8,11 +8,11 @@
 //     atoms form a compact tile and the order is deterministic;
 //   * all per-step force work runs in this sorted-slot space (positions are
 //     gathered once per step, forces are scattered back once);
-//   * one warp per i-tile sweeps j-tiles J > I through an AABB prune, keeps
-//     every j-atom within r_search of any i-atom, and packs 32 of them per
-//     entry together with a 32-bit exclusion mask per j-atom (bit m: the
-//     pair with i-atom m is in the exclusion list), so the pair kernel never
-//     scans exclusion lists for ordinary pairs;
+//   * one block per i-tile sweeps j-tiles J > I through an AABB prune, keeps
+//     every j-atom within r_search of any i-atom, and deals them round-robin
+//     into entries of 32 together with a 32-bit exclusion mask per j-atom
+//     (bit m: the pair with i-atom m is in the exclusion list), so the pair
+//     kernel never scans exclusion lists for ordinary pairs;
 //   * the self tile is entry 0 of each i-tile and is evaluated with a half
 //     rotation (each unordered pair once);
 //   * entries live in a fixed-size slab per i-tile (sized from a counting
@@ -415,14 +415,19 @@ __global__ void __launch_bounds__(NLT_WARPS * 32)
   const uint32_t has_self = (n - I * 32u >= 2u) ? 1u : 0u;
   const uint32_t nent = has_self + (H + 31u) / 32u;
 
-  // 4. entries
+  // 4. entries.  Hits are dealt round-robin over the tile's entries (hit h
+  // goes to entry h mod E, lane h / E), so every entry samples the whole
+  // shell of candidates around the i-tile and the pairs inside the cutoff
+  // spread evenly over the i-lanes instead of piling onto the lanes nearest
+  // one spatial cluster of j-atoms.
   if (WRITE) {
+    const uint32_t E = (H + 31u) / 32u;
     for (uint32_t e = w; e < nent && e < slab; e += NLT_WARPS) {
       uint32_t sj = HB_SENTINEL;
       if (has_self && e == 0) {
         if (ki < n) sj = ki;
       } else {
-        const uint32_t h = (e - has_self) * 32u + lane;
+        const uint32_t h = (e - has_self) + lane * E;
         if (h < H) {
           uint32_t lo = 0, hiidx = ncand;  // largest c with pre[c] <= h
           while (hiidx - lo > 1u) {

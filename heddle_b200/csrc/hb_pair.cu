@@ -287,6 +287,207 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, 8)
 }
 
 // ---------------------------------------------------------------------
+// Masked form (forces only).  Per entry: (1) a distance pass over the 32
+// rotations leaves, per lane, the bit mask of rotations whose pair is inside
+// the cutoff; (2) each lane walks its own set bits, so the LJ + erfc math
+// runs only for pairs inside the cutoff (about one slot in six at a 1.2 A
+// skin) and the warp loops max-over-lanes times instead of 32.  i-forces
+// stay in registers (each lane visits its pairs in a fixed order); j-forces
+// go to per-warp int32 fixed-point accumulators in shared memory (scale
+// 2^30, integer atomics: order-independent) that are added to the global
+// int64 accumulators once per entry.  A pair force component above
+// 0.06 hartree/bohr takes the exact global int64 path instead, so the int32
+// sums cannot wrap (32 pairs x 0.06 x 2^30 < 2^31).
+// ---------------------------------------------------------------------
+#define P3_WARPS 4
+#define P3_SHIFT 10               // 2^40 / 2^30
+#define P3_SCALE 1073741824.0f    // 2^30
+#define P3_FMAX 0.06f
+
+template <bool SCALED, bool SWITCH>
+__global__ void __launch_bounds__(P3_WARPS * 32)
+    k_pair3(const float4 *__restrict__ tile_posq, const int *__restrict__ tile_type,
+            const float4 *__restrict__ center, const uint32_t *__restrict__ tile_nent,
+            const uint32_t *__restrict__ entry_j, const uint32_t *__restrict__ entry_excl,
+            const DBox *__restrict__ box, const float4 *__restrict__ lj_table, PairParams P,
+            unsigned long long *__restrict__ fp, const uint32_t *__restrict__ sorted_ids,
+            const uint32_t *__restrict__ eoff, const uint32_t *__restrict__ epart,
+            const float2 *__restrict__ escale) {
+  extern __shared__ float4 sm_lj3[];
+  __shared__ float4 sm_jp[P3_WARPS][32];
+  __shared__ int sm_jt[P3_WARPS][32];
+  __shared__ uint32_t sm_oj[P3_WARPS][32];
+  __shared__ int sm_fj[P3_WARPS][3][32];
+  const int nt2 = P.n_types * P.n_types;
+  for (int k = threadIdx.x; k < nt2; k += blockDim.x) sm_lj3[k] = lj_table[k];
+  __syncthreads();
+
+  const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t I = blockIdx.x * P3_WARPS + w;
+  if (I >= P.n_tiles) return;
+  const DBox b = *box;
+  const float4 c = center[I];
+  const bool spc = ((int)c.w & 1) != 0;
+  const uint32_t si = I * 32u + lane;
+  const bool ivalid = si < P.n;
+  float4 pi = tile_posq[si];
+  if (ivalid) {
+    if (spc) shift_to(pi.x, pi.y, pi.z, c, b);
+  } else {
+    pi = make_float4(-1.0e18f, -1.0e18f, -1.0e18f, 0.0f);
+  }
+  const int ti_row = (ivalid ? tile_type[si] : 0) * P.n_types;
+  const uint32_t oi = SCALED ? (ivalid ? sorted_ids[si] : HB_SENTINEL) : 0u;
+  const size_t np = (size_t)P.n_tiles * 32u;
+  long long ax = 0, ay = 0, az = 0;
+
+  const uint32_t e0 = I * P.slab;
+  const uint32_t e1 = e0 + min(tile_nent[I], P.slab);
+  const bool has_self = P.n - I * 32u >= 2u;
+
+  for (uint32_t e = e0; e < e1; ++e) {
+    const bool self = has_self && (e == e0);
+    const uint32_t sj = entry_j[(uint64_t)e * 32u + lane];
+    const uint32_t xm = entry_excl[(uint64_t)e * 32u + lane];
+    const bool jvalid = sj != HB_SENTINEL;
+    float4 pj = make_float4(1.0e18f, 1.0e18f, 1.0e18f, 0.0f);
+    int tj = 0;
+    if (jvalid) {
+      pj = tile_posq[sj];
+      tj = tile_type[sj];
+      if (spc) shift_to(pj.x, pj.y, pj.z, c, b);
+    }
+    __syncwarp();
+    sm_jp[w][lane] = pj;
+    sm_jt[w][lane] = tj;
+    if (SCALED) sm_oj[w][lane] = jvalid ? sorted_ids[sj] : HB_SENTINEL;
+    sm_fj[w][0][lane] = 0;
+    sm_fj[w][1][lane] = 0;
+    sm_fj[w][2][lane] = 0;
+    __syncwarp();
+    // (1) distance pass
+    uint32_t m = 0u;
+    const uint32_t t0 = self ? 1u : 0u, t1 = self ? 17u : 32u;
+    for (uint32_t t = t0; t < t1; ++t) {
+      const float4 q = sm_jp[w][(lane + t) & 31u];
+      float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
+      if (!spc) hb_min_image(dx, dy, dz, b);
+      const float r2 = dx * dx + dy * dy + dz * dz;
+      bool act = r2 < P.rc2_max && (SCALED || !((xm >> t) & 1u));
+      if (self && t == 16u && lane >= 16u) act = false;
+      m |= (act ? 1u : 0u) << t;
+    }
+    // (2) math over this lane's pairs
+    float fix = 0.f, fiy = 0.f, fiz = 0.f;
+    while (__any_sync(0xFFFFFFFFu, m != 0u)) {
+      if (m != 0u) {
+        const uint32_t t = (uint32_t)__ffs(m) - 1u;
+        m &= m - 1u;
+        const uint32_t jl = (lane + t) & 31u;
+        const float4 q = sm_jp[w][jl];
+        float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
+        if (!spc) hb_min_image(dx, dy, dz, b);
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        float s_lj = 1.0f, s_c = 1.0f;
+        if (SCALED && ((xm >> t) & 1u)) {
+          s_lj = 0.0f;
+          s_c = 0.0f;
+          const uint32_t oj = sm_oj[w][jl];
+          for (uint32_t z = eoff[oj]; z < eoff[oj + 1]; ++z) {
+            if (epart[z] == oi) {
+              const float2 sc = escale[z];
+              s_lj = sc.x;
+              s_c = sc.y;
+              break;
+            }
+          }
+        }
+        const float inv_r = rsqrtf(r2);
+        const float inv_r2 = inv_r * inv_r;
+        float fac = 0.0f;
+        if (P.lj_on) {
+          const float4 L = sm_lj3[ti_row + sm_jt[w][jl]];
+          if (r2 <= L.z && L.y != 0.0f && s_lj != 0.0f) {
+            const float sr2 = L.x * inv_r2;
+            const float sr6 = sr2 * sr2 * sr2;
+            const float sr12 = sr6 * sr6;
+            float f = L.y * inv_r2 * (2.0f * sr12 - sr6);
+            if (SWITCH && r2 > L.w && L.z > L.w) {
+              const float u = (L.y * (1.0f / 6.0f)) * (sr12 - sr6);
+              const float inv_d = 1.0f / (L.z - L.w);
+              const float tau = (r2 - L.w) * inv_d;
+              const float omt = 1.0f - tau;
+              const float sw = omt * omt * (1.0f + 2.0f * tau);
+              const float chain = 12.0f * tau * omt * inv_d;
+              f = sw * f + chain * u;
+            }
+            fac += s_lj * f;
+          }
+        }
+        if (P.coul_on && r2 <= P.coul_rc2 && s_c != 0.0f) {
+          const float r = r2 * inv_r;
+          const float ar = P.alpha * r;
+          const float g = __expf(-ar * ar);
+          const float tt = __fdividef(1.0f, 1.0f + 0.3275911f * ar);
+          const float poly =
+              0.254829592f +
+              (-0.284496736f + (1.421413741f + (-1.453152027f + 1.061405429f * tt) * tt) * tt) * tt;
+          const float erfc_ar = poly * tt * g;
+          fac += s_c * pi.w * q.w * inv_r2 * (erfc_ar * inv_r + P.c2a * g);
+        }
+        const float fx = fac * dx, fy = fac * dy, fz = fac * dz;
+        fix += fx;
+        fiy += fy;
+        fiz += fz;
+        if (fabsf(fx) <= P3_FMAX && fabsf(fy) <= P3_FMAX && fabsf(fz) <= P3_FMAX) {
+          atomicAdd(&sm_fj[w][0][jl], -__float2int_rn(fx * P3_SCALE));
+          atomicAdd(&sm_fj[w][1][jl], -__float2int_rn(fy * P3_SCALE));
+          atomicAdd(&sm_fj[w][2][jl], -__float2int_rn(fz * P3_SCALE));
+        } else {
+          // rare: the exact int64 path straight to the j atom
+          const uint32_t tgt = self ? (I * 32u + jl) : entry_j[(uint64_t)e * 32u + jl];
+          red_add(&fp[0 * np + tgt], -to_fixed(fx));
+          red_add(&fp[1 * np + tgt], -to_fixed(fy));
+          red_add(&fp[2 * np + tgt], -to_fixed(fz));
+        }
+      }
+    }
+    __syncwarp();
+    const long long jx = (long long)sm_fj[w][0][lane] << P3_SHIFT;
+    const long long jy = (long long)sm_fj[w][1][lane] << P3_SHIFT;
+    const long long jz = (long long)sm_fj[w][2][lane] << P3_SHIFT;
+    if (self) {
+      ax += jx;
+      ay += jy;
+      az += jz;
+    } else if (jvalid) {
+      red_add(&fp[0 * np + sj], jx);
+      red_add(&fp[1 * np + sj], jy);
+      red_add(&fp[2 * np + sj], jz);
+    }
+    ax += to_fixed(fix);
+    ay += to_fixed(fiy);
+    az += to_fixed(fiz);
+  }
+  if (ivalid) {
+    red_add(&fp[0 * np + si], ax);
+    red_add(&fp[1 * np + si], ay);
+    red_add(&fp[2 * np + si], az);
+  }
+}
+
+template <bool SCALED, bool SWITCH>
+int launch3_t(hb_forcefield *ff, cudaStream_t s, const PairParams &P) {
+  size_t smem = sizeof(float4) * (size_t)P.n_types * P.n_types;
+  k_pair3<SCALED, SWITCH><<<hb_div_up(P.n_tiles, P3_WARPS), P3_WARPS * 32, smem, s>>>(
+      ff->d_tile_posq, ff->d_tile_type, ff->d_tile_center, ff->d_tile_nent, ff->d_entry_j,
+      ff->d_entry_excl, ff->sys->d_box, ff->d_lj, P, ff->d_fp, ff->d_sorted_ids, ff->d_excl_off,
+      ff->d_excl_partner, ff->d_excl_scale);
+  HB_CUDA(cudaGetLastError());
+  return HB_OK;
+}
+
+// ---------------------------------------------------------------------
 // Compacted form.  Per entry: (1) a distance pass, one lane per i-atom over
 // the 32 rotations, leaves a 32-bit mask of rotations whose pair is within
 // the cutoff; (2) the active pairs are listed in shared memory slot-major
@@ -563,6 +764,10 @@ int pair_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
   if (ev) {
     if (sc) return sw ? launch_t<true, true, true>(ff, s, P) : launch_t<true, true, false>(ff, s, P);
     return sw ? launch_t<true, false, true>(ff, s, P) : launch_t<true, false, false>(ff, s, P);
+  }
+  if (ff->pair_variant == 3) {
+    if (sc) return sw ? launch3_t<true, true>(ff, s, P) : launch3_t<true, false>(ff, s, P);
+    return sw ? launch3_t<false, true>(ff, s, P) : launch3_t<false, false>(ff, s, P);
   }
   if (sc) return sw ? launch_t<false, true, true>(ff, s, P) : launch_t<false, true, false>(ff, s, P);
   return sw ? launch_t<false, false, true>(ff, s, P) : launch_t<false, false, false>(ff, s, P);

@@ -200,3 +200,47 @@ def test_compiled_fft_sizes_match_oracle(ctx, grid):
     assert rms_rel(F, Fo) <= FORCE_RMS_TOL
     _, _, _, Tp = O.forces(spec, pos, poly_erfc=True)
     assert abs(sc["recip"] - Tp["recip"]) <= 1e-5 * abs(Tp["recip"])
+
+
+@pytest.mark.parametrize("maker", [
+    lambda: S.spc_water(512, skin_A=2.0),
+    lambda: S.lj_argon(),
+    lambda: S.peptide_in_water(),
+], ids=["water512", "argon10000", "chain"])
+def test_force_only_kernel_matches_oracle(ctx, maker):
+    # steps without energies run the masked pair kernel (compacted per-lane
+    # pair lists, int32 shared-memory j sums); steps with energies run the
+    # rotation sweep: both within the force tolerance, repeat runs identical
+    spec = maker()
+    sys_ = hb.System.from_spec(ctx, spec)
+    ff = hb.ForceField.from_spec(sys_, spec)
+    ff.step(scalars=False)
+    pos, F = sys_.positions(), sys_.forces()
+    ff.step(scalars=False)
+    assert np.array_equal(sys_.forces(), F)
+    ff.step(scalars=True)
+    F_rot = sys_.forces()
+    Fo, _, _, _ = O.forces(spec, pos)
+    assert rms_rel(F, Fo) <= FORCE_RMS_TOL
+    assert rms_rel(F, F_rot) <= 2e-6
+    ff.close(), sys_.close()
+
+
+def test_force_only_kernel_large_pair_forces(ctx):
+    # pair force components above 0.06 hartree/bohr bypass the int32 shared
+    # accumulators: an argon pair squeezed to 0.7 sigma
+    spec = S.lj_argon()
+    pos = spec.positions.copy()
+    sigma = spec.meta["sigma"]
+    d = pos[1] - pos[0]
+    pos[1] = pos[0] + 0.7 * sigma * d / np.linalg.norm(d)
+    spec.positions = pos
+    sys_ = hb.System.from_spec(ctx, spec)
+    ff = hb.ForceField.from_spec(sys_, spec)
+    ff.step(scalars=False)
+    p, F = sys_.positions(), sys_.forces()
+    Fo, _, _, _ = O.forces(spec, p)
+    assert np.abs(Fo[0]).max() > 0.06
+    assert rms_rel(F, Fo) <= FORCE_RMS_TOL
+    assert np.abs(F[:2] - Fo[:2]).max() <= 1e-5 * np.abs(Fo[:2]).max()
+    ff.close(), sys_.close()
