@@ -355,6 +355,7 @@ extern "C" int hb_forcefield_destroy(hb_forcefield *ff) {
   bonded_free(ff);
   if (ff->spme.on) spme_free(ff);
   cudaFree(ff->d_lj);
+  cudaFree(ff->d_lj_invd);
   cudaFree(ff->d_excl_off);
   cudaFree(ff->d_excl_partner);
   cudaFree(ff->d_excl_scale);
@@ -461,7 +462,7 @@ extern "C" int hb_forcefield_create(hb_system *sys, const hb_forcefield_desc *d,
   hb_forcefield *ff = new hb_forcefield();
   *ff = tmp;
   ff->sys = sys;
-  // pair kernel: the masked form for force-only steps (the rotation sweep
+  // pair kernel: the balanced form for force-only steps (the rotation sweep
   // for steps with energies); HB_PAIR_KERNEL=rotation / compact select the
   // rotation sweep or the compacted pair-list form (shared-memory int64
   // atomics) throughout; exact pairs use the compacted form with per-pair
@@ -476,6 +477,16 @@ extern "C" int hb_forcefield_create(hb_system *sys, const hb_forcefield_desc *d,
   HB_CUDA(cudaMalloc(&ff->d_lj, sizeof(float4) * ff->h_lj.size()));
   HB_CUDA(cudaMemcpy(ff->d_lj, ff->h_lj.data(), sizeof(float4) * ff->h_lj.size(),
                      cudaMemcpyHostToDevice));
+  {
+    std::vector<float> invd(ff->h_lj.size());
+    for (size_t q = 0; q < invd.size(); ++q) {
+      const float4 L = ff->h_lj[q];
+      invd[q] = L.z > L.w ? 1.0f / (L.z - L.w) : 0.0f;
+    }
+    HB_CUDA(cudaMalloc(&ff->d_lj_invd, sizeof(float) * invd.size()));
+    HB_CUDA(cudaMemcpy(ff->d_lj_invd, invd.data(), sizeof(float) * invd.size(),
+                       cudaMemcpyHostToDevice));
+  }
   if (!eoff.empty()) {
     HB_CUDA(cudaMalloc(&ff->d_excl_off, sizeof(uint32_t) * eoff.size()));
     HB_CUDA(cudaMemcpy(ff->d_excl_off, eoff.data(), sizeof(uint32_t) * eoff.size(), cudaMemcpyHostToDevice));

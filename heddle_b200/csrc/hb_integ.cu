@@ -29,8 +29,10 @@ __global__ void k_finalize(unsigned long long *__restrict__ fp, const float4 *__
                            const uint32_t *__restrict__ sorted_ids, float4 *__restrict__ force,
                            float *__restrict__ energy, float *__restrict__ virial,
                            const double *__restrict__ spme_sums,
-                           unsigned long long *__restrict__ acc, uint32_t n, uint32_t np) {
+                           unsigned long long *__restrict__ acc, uint32_t *__restrict__ work,
+                           uint32_t n, uint32_t np) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k == 0) *work = 0u;  // the pair kernel's work counter, for the next evaluation
   long long e_fix = 0, w_fix = 0;
   if (k < n) {
     const uint32_t id = sorted_ids[k];
@@ -376,12 +378,12 @@ int forces_finalize(hb_forcefield *ff, bool ev, cudaStream_t s) {
     if (ev)
       k_finalize<true><<<hb_div_up(n, 256), 256, 0, s>>>(ff->d_fp, recip, ff->d_sorted_ids,
                                                          sys->d_force, ff->d_energy, ff->d_virial,
-                                                         sums, ff->d_acc, n, ff->n_pad);
+                                                         sums, ff->d_acc, ff->d_work, n, ff->n_pad);
     else
       k_finalize<false><<<hb_div_up(n, 256), 256, 0, s>>>(ff->d_fp, recip, ff->d_sorted_ids,
                                                           sys->d_force, ff->d_energy,
-                                                          ff->d_virial, sums, ff->d_acc, n,
-                                                          ff->n_pad);
+                                                          ff->d_virial, sums, ff->d_acc,
+                                                          ff->d_work, n, ff->n_pad);
   }
   if (ev) {
     double e_self = 0.0;

@@ -249,10 +249,11 @@ struct hb_forcefield {
   uint32_t n_types = 0;
   std::vector<float4> h_lj;        // per type pair: sigma^2, 24 eps, cut^2, r_switch^2
   float4 *d_lj = nullptr;
+  float *d_lj_invd = nullptr;      // per type pair: 1 / (cut^2 - r_switch^2) (0: no switch)
   float alpha = 0.f, coul_rc2 = 0.f;
   int pair_variant = 3;            // 0: compacted pair list, 1: full rotation sweep,
                                    // 2: compacted, per-pair fixed point + minimum image,
-                                   // 3: masked (rotation sweep for energy steps)
+                                   // 3: balanced queue (rotation sweep for energy steps)
   float rc_max = 0.f, r_skin = 0.f, r_search = 0.f;
   int any_switch = 0;
   int excl_scaled = 0;             // some exclusion has a non-zero scale
@@ -288,6 +289,8 @@ struct hb_forcefield {
                                      // build, [2] running count of a build,
                                      // [3] largest candidate count seen
   uint32_t *h_status = nullptr;      // pinned mirror
+  uint32_t *d_work = nullptr;        // work counter of the balanced pair kernel
+                                     // (zeroed by the combine kernel)
   uint64_t rebuilds_host = 0;
   bool built = false;
   // ---- accumulators (sorted-slot space)

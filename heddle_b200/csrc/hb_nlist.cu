@@ -549,6 +549,8 @@ int nl_setup(hb_forcefield *ff) {
   HB_CUDA(cudaMalloc(&ff->d_status, sizeof(uint32_t)));
   HB_CUDA(cudaMemset(ff->d_status, 0, sizeof(uint32_t)));
   HB_CUDA(cudaMalloc(&ff->d_counters, sizeof(uint32_t) * 4));
+  HB_CUDA(cudaMalloc(&ff->d_work, sizeof(uint32_t)));
+  HB_CUDA(cudaMemset(ff->d_work, 0, sizeof(uint32_t)));
   HB_CUDA(cudaMemset(ff->d_counters, 0, sizeof(uint32_t) * 4));
   HB_CUDA(cudaMallocHost(&ff->h_status, sizeof(uint32_t) * 8));
   HB_CUDA(cudaMalloc(&ff->d_fp, sizeof(unsigned long long) * 5 * n_pad));
@@ -571,6 +573,7 @@ int nl_free(hb_forcefield *ff) {
   cudaFree(ff->d_entry_j);
   cudaFree(ff->d_entry_excl);
   cudaFree(ff->d_ref_pos);
+  cudaFree(ff->d_work);
   cudaFree(ff->d_ref_box);
   cudaFree(ff->d_status);
   cudaFree(ff->d_counters);

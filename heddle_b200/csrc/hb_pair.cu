@@ -20,6 +20,8 @@
 // ordinary pair costs no exclusion lookup.  Tiles that satisfy the
 // single-periodic-copy condition shift i and j positions against the tile
 // centre once per entry and skip the per-pair minimum image.
+#include <algorithm>
+
 #include "hb_internal.cuh"
 
 namespace {
@@ -58,7 +60,8 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, 8)
     k_pair(const float4 *__restrict__ tile_posq, const int *__restrict__ tile_type,
            const float4 *__restrict__ center, const uint32_t *__restrict__ tile_nent,
            const uint32_t *__restrict__ entry_j, const uint32_t *__restrict__ entry_excl,
-           const DBox *__restrict__ box, const float4 *__restrict__ lj_table, PairParams P,
+           const DBox *__restrict__ box, const float4 *__restrict__ lj_table,
+           const float *__restrict__ lj_invd, PairParams P,
            unsigned long long *__restrict__ fp, unsigned long long *__restrict__ e_lj_total,
            const uint32_t *__restrict__ sorted_ids, const uint32_t *__restrict__ eoff,
            const uint32_t *__restrict__ epart, const float2 *__restrict__ escale) {
@@ -68,7 +71,11 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, 8)
   __shared__ float4 sm_jp[PAIR_WARPS][32];
   __shared__ int sm_jt[PAIR_WARPS][32];
   const int nt2 = P.n_types * P.n_types;
-  for (int k = threadIdx.x; k < nt2; k += blockDim.x) sm_lj[k] = lj_table[k];
+  float *sm_ljd = reinterpret_cast<float *>(sm_lj + nt2);
+  for (int k = threadIdx.x; k < nt2; k += blockDim.x) {
+    sm_lj[k] = lj_table[k];
+    sm_ljd[k] = lj_invd[k];
+  }
   __syncthreads();
 
   const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
@@ -180,7 +187,7 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, 8)
             float f = L.y * inv_r2 * (2.0f * sr12 - sr6);
             float u = (L.y * (1.0f / 6.0f)) * (sr12 - sr6);
             if (SWITCH && r2 > L.w && L.z > L.w) {
-              const float inv_d = 1.0f / (L.z - L.w);
+              const float inv_d = sm_ljd[ti_row + tj];
               const float tau = (r2 - L.w) * inv_d;
               const float omt = 1.0f - tau;
               const float sw = omt * omt * (1.0f + 2.0f * tau);
@@ -287,112 +294,171 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, 8)
 }
 
 // ---------------------------------------------------------------------
-// Masked form (forces only).  Per entry: (1) a distance pass over the 32
-// rotations leaves, per lane, the bit mask of rotations whose pair is inside
-// the cutoff; (2) each lane walks its own set bits, so the LJ + erfc math
-// runs only for pairs inside the cutoff (about one slot in six at a 1.2 A
-// skin) and the warp loops max-over-lanes times instead of 32.  i-forces
-// stay in registers (each lane visits its pairs in a fixed order); j-forces
-// go to per-warp int32 fixed-point accumulators in shared memory (scale
-// 2^30, integer atomics: order-independent) that are added to the global
-// int64 accumulators once per entry.  A pair force component above
-// 0.06 hartree/bohr takes the exact global int64 path instead, so the int32
-// sums cannot wrap (32 pairs x 0.06 x 2^30 < 2^31).
+// Balanced form (forces only).  Per entry: (1) a distance pass over the 32
+// rotations (unrolled for ordinary entries) leaves each lane's mask of
+// rotations whose pair is inside the cutoff; exclusions are folded in with
+// one AND per entry; (2) the set bits are dealt slot-major into a per-warp
+// queue (each lane's first pair, then each lane's second, ...), so the
+// pairs spread evenly over the 32 lanes whatever their spatial imbalance;
+// (3) the math pass evaluates the queue 32 pairs at a time.  Both i- and
+// j-forces go to per-warp int32 fixed-point accumulators in shared memory
+// (scale 2^30, integer atomics: order-independent, so the result is the
+// same run to run) that are folded into int64 once per entry.  A pair force
+// component above 0.06 hartree/bohr takes the exact global int64 path
+// instead, so the int32 sums cannot wrap (32 pairs x 0.06 x 2^30 < 2^31).
 // ---------------------------------------------------------------------
-#define P3_WARPS 4
-#define P3_SHIFT 10               // 2^40 / 2^30
-#define P3_SCALE 1073741824.0f    // 2^30
-#define P3_FMAX 0.06f
+#define P4_WARPS 4
+#define P4_SHIFT 10               // 2^40 / 2^30
+#define P4_SCALE 1073741824.0f    // 2^30
+#define P4_FMAX 0.06f
+
+struct P4Warp {
+  float4 ipos[32];
+  float4 jpos[32];
+  int itype[32];
+  int jtype[32];
+  uint32_t oi[32];
+  uint32_t oj[32];
+  uint32_t xm[32];
+  uint32_t jslot[32];
+  int fi[3][32];
+  int fj[3][32];
+  uint16_t pairs[1024];
+};
 
 template <bool SCALED, bool SWITCH>
-__global__ void __launch_bounds__(P3_WARPS * 32)
-    k_pair3(const float4 *__restrict__ tile_posq, const int *__restrict__ tile_type,
+__global__ void __launch_bounds__(P4_WARPS * 32, 8)
+    k_pair4(const float4 *__restrict__ tile_posq, const int *__restrict__ tile_type,
             const float4 *__restrict__ center, const uint32_t *__restrict__ tile_nent,
             const uint32_t *__restrict__ entry_j, const uint32_t *__restrict__ entry_excl,
-            const DBox *__restrict__ box, const float4 *__restrict__ lj_table, PairParams P,
-            unsigned long long *__restrict__ fp, const uint32_t *__restrict__ sorted_ids,
-            const uint32_t *__restrict__ eoff, const uint32_t *__restrict__ epart,
-            const float2 *__restrict__ escale) {
-  extern __shared__ float4 sm_lj3[];
-  __shared__ float4 sm_jp[P3_WARPS][32];
-  __shared__ int sm_jt[P3_WARPS][32];
-  __shared__ uint32_t sm_oj[P3_WARPS][32];
-  __shared__ int sm_fj[P3_WARPS][3][32];
+            const DBox *__restrict__ box, const float4 *__restrict__ lj_table,
+            const float *__restrict__ lj_invd, PairParams P, unsigned long long *__restrict__ fp,
+            const uint32_t *__restrict__ sorted_ids, const uint32_t *__restrict__ eoff,
+            const uint32_t *__restrict__ epart, const float2 *__restrict__ escale,
+            uint32_t *__restrict__ work, uint32_t chunks, uint32_t chunk) {
+  extern __shared__ float4 sm_lj4[];
+  __shared__ P4Warp smw4[P4_WARPS];
   const int nt2 = P.n_types * P.n_types;
-  for (int k = threadIdx.x; k < nt2; k += blockDim.x) sm_lj3[k] = lj_table[k];
-  __syncthreads();
-
-  const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  const uint32_t I = blockIdx.x * P3_WARPS + w;
-  if (I >= P.n_tiles) return;
-  const DBox b = *box;
-  const float4 c = center[I];
-  const bool spc = ((int)c.w & 1) != 0;
-  const uint32_t si = I * 32u + lane;
-  const bool ivalid = si < P.n;
-  float4 pi = tile_posq[si];
-  if (ivalid) {
-    if (spc) shift_to(pi.x, pi.y, pi.z, c, b);
-  } else {
-    pi = make_float4(-1.0e18f, -1.0e18f, -1.0e18f, 0.0f);
+  float *sm_ljd4 = reinterpret_cast<float *>(sm_lj4 + nt2);
+  for (int k = threadIdx.x; k < nt2; k += blockDim.x) {
+    sm_lj4[k] = lj_table[k];
+    sm_ljd4[k] = lj_invd[k];
   }
-  const int ti_row = (ivalid ? tile_type[si] : 0) * P.n_types;
-  const uint32_t oi = SCALED ? (ivalid ? sorted_ids[si] : HB_SENTINEL) : 0u;
-  const size_t np = (size_t)P.n_tiles * 32u;
-  long long ax = 0, ay = 0, az = 0;
+  __syncthreads();
+  const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  P4Warp &S = smw4[w];
+  const DBox b = *box;
+  const size_t np_all = (size_t)P.n_tiles * 32u;
+  const uint32_t lt = (1u << lane) - 1u;
+  const uint32_t n_items = P.n_tiles * chunks;
 
-  const uint32_t e0 = I * P.slab;
-  const uint32_t e1 = e0 + min(tile_nent[I], P.slab);
-  const bool has_self = P.n - I * 32u >= 2u;
-
-  for (uint32_t e = e0; e < e1; ++e) {
-    const bool self = has_self && (e == e0);
-    const uint32_t sj = entry_j[(uint64_t)e * 32u + lane];
-    const uint32_t xm = entry_excl[(uint64_t)e * 32u + lane];
-    const bool jvalid = sj != HB_SENTINEL;
-    float4 pj = make_float4(1.0e18f, 1.0e18f, 1.0e18f, 0.0f);
-    int tj = 0;
-    if (jvalid) {
-      pj = tile_posq[sj];
-      tj = tile_type[sj];
-      if (spc) shift_to(pj.x, pj.y, pj.z, c, b);
+  // persistent warps take (tile, chunk of entries) items from a counter
+  for (;;) {
+    uint32_t g = 0u;
+    if (lane == 0) g = atomicAdd(work, 1u);
+    g = __shfl_sync(0xFFFFFFFFu, g, 0);
+    if (g >= n_items) break;
+    const uint32_t I = g / chunks, ch = g - I * chunks;
+    const uint32_t tile_e0 = I * P.slab;
+    const uint32_t tile_e1 = tile_e0 + min(tile_nent[I], P.slab);
+    const uint32_t e0 = tile_e0 + ch * chunk;
+    if (e0 >= tile_e1) continue;
+    const uint32_t e1 = min(e0 + chunk, tile_e1);
+    const float4 c = center[I];
+    const bool spc = ((int)c.w & 1) != 0;
+    const uint32_t si = I * 32u + lane;
+    const bool ivalid = si < P.n;
+    float4 pi = tile_posq[si];
+    if (ivalid) {
+      if (spc) shift_to(pi.x, pi.y, pi.z, c, b);
+    } else {
+      pi = make_float4(-1.0e18f, -1.0e18f, -1.0e18f, 0.0f);
     }
     __syncwarp();
-    sm_jp[w][lane] = pj;
-    sm_jt[w][lane] = tj;
-    if (SCALED) sm_oj[w][lane] = jvalid ? sorted_ids[sj] : HB_SENTINEL;
-    sm_fj[w][0][lane] = 0;
-    sm_fj[w][1][lane] = 0;
-    sm_fj[w][2][lane] = 0;
-    __syncwarp();
-    // (1) distance pass
-    uint32_t m = 0u;
-    const uint32_t t0 = self ? 1u : 0u, t1 = self ? 17u : 32u;
-    for (uint32_t t = t0; t < t1; ++t) {
-      const float4 q = sm_jp[w][(lane + t) & 31u];
-      float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
-      if (!spc) hb_min_image(dx, dy, dz, b);
-      const float r2 = dx * dx + dy * dy + dz * dz;
-      bool act = r2 < P.rc2_max && (SCALED || !((xm >> t) & 1u));
-      if (self && t == 16u && lane >= 16u) act = false;
-      m |= (act ? 1u : 0u) << t;
-    }
-    // (2) math over this lane's pairs
-    float fix = 0.f, fiy = 0.f, fiz = 0.f;
-    while (__any_sync(0xFFFFFFFFu, m != 0u)) {
-      if (m != 0u) {
-        const uint32_t t = (uint32_t)__ffs(m) - 1u;
-        m &= m - 1u;
-        const uint32_t jl = (lane + t) & 31u;
-        const float4 q = sm_jp[w][jl];
-        float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
+    S.ipos[lane] = pi;
+    S.itype[lane] = (ivalid ? tile_type[si] : 0) * P.n_types;
+    if (SCALED) S.oi[lane] = ivalid ? sorted_ids[si] : HB_SENTINEL;
+    long long ax = 0, ay = 0, az = 0;
+    const bool has_self = P.n - I * 32u >= 2u;
+
+    for (uint32_t e = e0; e < e1; ++e) {
+      const bool self = has_self && (e == tile_e0);
+      const uint32_t sj = entry_j[(uint64_t)e * 32u + lane];
+      const uint32_t xm = entry_excl[(uint64_t)e * 32u + lane];
+      const bool jvalid = sj != HB_SENTINEL;
+      float4 pj = make_float4(1.0e18f, 1.0e18f, 1.0e18f, 0.0f);
+      int tj = 0;
+      if (jvalid) {
+        pj = tile_posq[sj];
+        tj = tile_type[sj];
+        if (spc) shift_to(pj.x, pj.y, pj.z, c, b);
+      }
+      __syncwarp();
+      S.jpos[lane] = pj;
+      S.jtype[lane] = tj;
+      S.jslot[lane] = self ? si : sj;
+      if (SCALED) {
+        S.oj[lane] = jvalid ? sorted_ids[sj] : HB_SENTINEL;
+        S.xm[lane] = xm;
+      }
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        S.fi[q][lane] = 0;
+        S.fj[q][lane] = 0;
+      }
+      __syncwarp();
+
+      // (1) distance pass
+      uint32_t m = 0u;
+      if (!self) {
+#pragma unroll
+        for (uint32_t t = 0; t < 32u; ++t) {
+          const float4 q = S.jpos[(lane + t) & 31u];
+          float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
+          if (!spc) hb_min_image(dx, dy, dz, b);
+          const float r2 = dx * dx + dy * dy + dz * dz;
+          m |= (r2 < P.rc2_max ? 1u : 0u) << t;
+        }
+      } else {
+        for (uint32_t t = 1u; t < 17u; ++t) {
+          const float4 q = S.jpos[(lane + t) & 31u];
+          float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
+          if (!spc) hb_min_image(dx, dy, dz, b);
+          const float r2 = dx * dx + dy * dy + dz * dz;
+          m |= (r2 < P.rc2_max ? 1u : 0u) << t;
+        }
+        if (lane >= 16u) m &= ~(1u << 16);  // each self pair once
+      }
+      if (!SCALED) m &= ~xm;
+
+      // (2) slot-major queue of (i-lane, rotation)
+      uint32_t np = 0;
+      while (true) {
+        const bool has = m != 0u;
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
+        if (bal == 0u) break;
+        if (has) {
+          const uint32_t t = (uint32_t)__ffs(m) - 1u;
+          m &= m - 1u;
+          S.pairs[np + __popc(bal & lt)] = (uint16_t)((lane << 8) | t);
+        }
+        np += __popc(bal);
+      }
+      __syncwarp();
+
+      // (3) math over the queue
+      for (uint32_t k = lane; k < np; k += 32u) {
+        const uint32_t pr = S.pairs[k];
+        const uint32_t i = pr >> 8, t = pr & 255u, j = (i + t) & 31u;
+        const float4 a = S.ipos[i], q = S.jpos[j];
+        float dx = a.x - q.x, dy = a.y - q.y, dz = a.z - q.z;
         if (!spc) hb_min_image(dx, dy, dz, b);
         const float r2 = dx * dx + dy * dy + dz * dz;
         float s_lj = 1.0f, s_c = 1.0f;
-        if (SCALED && ((xm >> t) & 1u)) {
+        if (SCALED && ((S.xm[i] >> t) & 1u)) {
           s_lj = 0.0f;
           s_c = 0.0f;
-          const uint32_t oj = sm_oj[w][jl];
+          const uint32_t oi = S.oi[i], oj = S.oj[j];
           for (uint32_t z = eoff[oj]; z < eoff[oj + 1]; ++z) {
             if (epart[z] == oi) {
               const float2 sc = escale[z];
@@ -406,15 +472,16 @@ __global__ void __launch_bounds__(P3_WARPS * 32)
         const float inv_r2 = inv_r * inv_r;
         float fac = 0.0f;
         if (P.lj_on) {
-          const float4 L = sm_lj3[ti_row + sm_jt[w][jl]];
+          const int tp = S.itype[i] + S.jtype[j];
+          const float4 L = sm_lj4[tp];
           if (r2 <= L.z && L.y != 0.0f && s_lj != 0.0f) {
             const float sr2 = L.x * inv_r2;
             const float sr6 = sr2 * sr2 * sr2;
             const float sr12 = sr6 * sr6;
             float f = L.y * inv_r2 * (2.0f * sr12 - sr6);
-            if (SWITCH && r2 > L.w && L.z > L.w) {
+            if (SWITCH && r2 > L.w) {
               const float u = (L.y * (1.0f / 6.0f)) * (sr12 - sr6);
-              const float inv_d = 1.0f / (L.z - L.w);
+              const float inv_d = sm_ljd4[tp];
               const float tau = (r2 - L.w) * inv_d;
               const float omt = 1.0f - tau;
               const float sw = omt * omt * (1.0f + 2.0f * tau);
@@ -427,62 +494,75 @@ __global__ void __launch_bounds__(P3_WARPS * 32)
         if (P.coul_on && r2 <= P.coul_rc2 && s_c != 0.0f) {
           const float r = r2 * inv_r;
           const float ar = P.alpha * r;
-          const float g = __expf(-ar * ar);
+          const float gg = __expf(-ar * ar);
           const float tt = __fdividef(1.0f, 1.0f + 0.3275911f * ar);
           const float poly =
               0.254829592f +
               (-0.284496736f + (1.421413741f + (-1.453152027f + 1.061405429f * tt) * tt) * tt) * tt;
-          const float erfc_ar = poly * tt * g;
-          fac += s_c * pi.w * q.w * inv_r2 * (erfc_ar * inv_r + P.c2a * g);
+          const float erfc_ar = poly * tt * gg;
+          fac += s_c * a.w * q.w * inv_r2 * (erfc_ar * inv_r + P.c2a * gg);
         }
         const float fx = fac * dx, fy = fac * dy, fz = fac * dz;
-        fix += fx;
-        fiy += fy;
-        fiz += fz;
-        if (fabsf(fx) <= P3_FMAX && fabsf(fy) <= P3_FMAX && fabsf(fz) <= P3_FMAX) {
-          atomicAdd(&sm_fj[w][0][jl], -__float2int_rn(fx * P3_SCALE));
-          atomicAdd(&sm_fj[w][1][jl], -__float2int_rn(fy * P3_SCALE));
-          atomicAdd(&sm_fj[w][2][jl], -__float2int_rn(fz * P3_SCALE));
+        if (fabsf(fx) <= P4_FMAX && fabsf(fy) <= P4_FMAX && fabsf(fz) <= P4_FMAX) {
+          const int ix = __float2int_rn(fx * P4_SCALE), iy = __float2int_rn(fy * P4_SCALE),
+                    iz = __float2int_rn(fz * P4_SCALE);
+          atomicAdd(&S.fi[0][i], ix);
+          atomicAdd(&S.fi[1][i], iy);
+          atomicAdd(&S.fi[2][i], iz);
+          atomicAdd(&S.fj[0][j], -ix);
+          atomicAdd(&S.fj[1][j], -iy);
+          atomicAdd(&S.fj[2][j], -iz);
         } else {
-          // rare: the exact int64 path straight to the j atom
-          const uint32_t tgt = self ? (I * 32u + jl) : entry_j[(uint64_t)e * 32u + jl];
-          red_add(&fp[0 * np + tgt], -to_fixed(fx));
-          red_add(&fp[1 * np + tgt], -to_fixed(fy));
-          red_add(&fp[2 * np + tgt], -to_fixed(fz));
+          // rare: the exact int64 path for both atoms
+          const uint32_t ti_slot = I * 32u + i, tj_slot = S.jslot[j];
+          red_add(&fp[0 * np_all + ti_slot], to_fixed(fx));
+          red_add(&fp[1 * np_all + ti_slot], to_fixed(fy));
+          red_add(&fp[2 * np_all + ti_slot], to_fixed(fz));
+          red_add(&fp[0 * np_all + tj_slot], -to_fixed(fx));
+          red_add(&fp[1 * np_all + tj_slot], -to_fixed(fy));
+          red_add(&fp[2 * np_all + tj_slot], -to_fixed(fz));
         }
       }
+      __syncwarp();
+      ax += (long long)S.fi[0][lane] << P4_SHIFT;
+      ay += (long long)S.fi[1][lane] << P4_SHIFT;
+      az += (long long)S.fi[2][lane] << P4_SHIFT;
+      const long long jx = (long long)S.fj[0][lane] << P4_SHIFT;
+      const long long jy = (long long)S.fj[1][lane] << P4_SHIFT;
+      const long long jz = (long long)S.fj[2][lane] << P4_SHIFT;
+      if (self) {
+        ax += jx;
+        ay += jy;
+        az += jz;
+      } else if (jvalid) {
+        red_add(&fp[0 * np_all + sj], jx);
+        red_add(&fp[1 * np_all + sj], jy);
+        red_add(&fp[2 * np_all + sj], jz);
+      }
     }
-    __syncwarp();
-    const long long jx = (long long)sm_fj[w][0][lane] << P3_SHIFT;
-    const long long jy = (long long)sm_fj[w][1][lane] << P3_SHIFT;
-    const long long jz = (long long)sm_fj[w][2][lane] << P3_SHIFT;
-    if (self) {
-      ax += jx;
-      ay += jy;
-      az += jz;
-    } else if (jvalid) {
-      red_add(&fp[0 * np + sj], jx);
-      red_add(&fp[1 * np + sj], jy);
-      red_add(&fp[2 * np + sj], jz);
+    if (ivalid) {
+      red_add(&fp[0 * np_all + si], ax);
+      red_add(&fp[1 * np_all + si], ay);
+      red_add(&fp[2 * np_all + si], az);
     }
-    ax += to_fixed(fix);
-    ay += to_fixed(fiy);
-    az += to_fixed(fiz);
-  }
-  if (ivalid) {
-    red_add(&fp[0 * np + si], ax);
-    red_add(&fp[1 * np + si], ay);
-    red_add(&fp[2 * np + si], az);
   }
 }
 
+// entries per work item of the balanced kernel
+#define P4_CHUNK 4
+
 template <bool SCALED, bool SWITCH>
-int launch3_t(hb_forcefield *ff, cudaStream_t s, const PairParams &P) {
-  size_t smem = sizeof(float4) * (size_t)P.n_types * P.n_types;
-  k_pair3<SCALED, SWITCH><<<hb_div_up(P.n_tiles, P3_WARPS), P3_WARPS * 32, smem, s>>>(
+int launch4_t(hb_forcefield *ff, cudaStream_t s, const PairParams &P) {
+  size_t smem = (sizeof(float4) + sizeof(float)) * (size_t)P.n_types * P.n_types;
+  const uint32_t chunks = hb_div_up(P.slab, P4_CHUNK);
+  // persistent: 8 blocks of 4 warps per SM, or fewer for small systems
+  const uint32_t items = P.n_tiles * chunks;
+  const uint32_t grid = std::min<uint32_t>((uint32_t)ff->sys->ctx->n_sm * 8u,
+                                           hb_div_up(items, P4_WARPS));
+  k_pair4<SCALED, SWITCH><<<std::max(grid, 1u), P4_WARPS * 32, smem, s>>>(
       ff->d_tile_posq, ff->d_tile_type, ff->d_tile_center, ff->d_tile_nent, ff->d_entry_j,
-      ff->d_entry_excl, ff->sys->d_box, ff->d_lj, P, ff->d_fp, ff->d_sorted_ids, ff->d_excl_off,
-      ff->d_excl_partner, ff->d_excl_scale);
+      ff->d_entry_excl, ff->sys->d_box, ff->d_lj, ff->d_lj_invd, P, ff->d_fp, ff->d_sorted_ids,
+      ff->d_excl_off, ff->d_excl_partner, ff->d_excl_scale, ff->d_work, chunks, P4_CHUNK);
   HB_CUDA(cudaGetLastError());
   return HB_OK;
 }
@@ -718,10 +798,10 @@ int launch2_t(hb_forcefield *ff, cudaStream_t s, const PairParams &P) {
 
 template <bool EV, bool SCALED, bool SWITCH>
 int launch_t(hb_forcefield *ff, cudaStream_t s, const PairParams &P) {
-  size_t smem = sizeof(float4) * (size_t)P.n_types * P.n_types;
+  size_t smem = (sizeof(float4) + sizeof(float)) * (size_t)P.n_types * P.n_types;
   k_pair<EV, SCALED, SWITCH><<<hb_div_up(P.n_tiles, PAIR_WARPS), PAIR_WARPS * 32, smem, s>>>(
       ff->d_tile_posq, ff->d_tile_type, ff->d_tile_center, ff->d_tile_nent, ff->d_entry_j,
-      ff->d_entry_excl, ff->sys->d_box, ff->d_lj, P, ff->d_fp,
+      ff->d_entry_excl, ff->sys->d_box, ff->d_lj, ff->d_lj_invd, P, ff->d_fp,
       ff->d_acc,
       ff->d_sorted_ids, ff->d_excl_off, ff->d_excl_partner, ff->d_excl_scale);
   HB_CUDA(cudaGetLastError());
@@ -766,8 +846,8 @@ int pair_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
     return sw ? launch_t<true, false, true>(ff, s, P) : launch_t<true, false, false>(ff, s, P);
   }
   if (ff->pair_variant == 3) {
-    if (sc) return sw ? launch3_t<true, true>(ff, s, P) : launch3_t<true, false>(ff, s, P);
-    return sw ? launch3_t<false, true>(ff, s, P) : launch3_t<false, false>(ff, s, P);
+    if (sc) return sw ? launch4_t<true, true>(ff, s, P) : launch4_t<true, false>(ff, s, P);
+    return sw ? launch4_t<false, true>(ff, s, P) : launch4_t<false, false>(ff, s, P);
   }
   if (sc) return sw ? launch_t<false, true, true>(ff, s, P) : launch_t<false, true, false>(ff, s, P);
   return sw ? launch_t<false, false, true>(ff, s, P) : launch_t<false, false, false>(ff, s, P);

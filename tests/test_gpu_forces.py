@@ -208,9 +208,9 @@ def test_compiled_fft_sizes_match_oracle(ctx, grid):
     lambda: S.peptide_in_water(),
 ], ids=["water512", "argon10000", "chain"])
 def test_force_only_kernel_matches_oracle(ctx, maker):
-    # steps without energies run the masked pair kernel (compacted per-lane
-    # pair lists, int32 shared-memory j sums); steps with energies run the
-    # rotation sweep: both within the force tolerance, repeat runs identical
+    # steps without energies run the balanced pair kernel (slot-major pair
+    # queue, int32 shared-memory sums); steps with energies run the rotation
+    # sweep: both within the force tolerance, repeat runs identical
     spec = maker()
     sys_ = hb.System.from_spec(ctx, spec)
     ff = hb.ForceField.from_spec(sys_, spec)
