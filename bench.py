@@ -239,6 +239,8 @@ def run_ours(args):
         args.skin = float(tune["best_A"])
     spec.r_skin = U.angstrom_au(args.skin)
     ff = hb.ForceField.from_spec(sys_, spec)
+    if tune:
+        ff.set_launch(pair_blocks_per_sm=int(tune["pair_blocks_per_sm"]))
     it = hb.Integrator(sys_, **lang)
     baro = None
     if args.barostat:

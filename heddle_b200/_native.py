@@ -32,6 +32,7 @@ HB_FORCES_ONLY, HB_FORCES_AND_SCALARS = 0, 1
 HB_INTEGRATOR_VV, HB_INTEGRATOR_VV_LOSSLESS, HB_INTEGRATOR_LANGEVIN = 0, 1, 2
 HB_CONSTRAINT_SETTLE, HB_CONSTRAINT_SHAKE = 0, 1
 HB_PAIRS_FAST, HB_PAIRS_EXACT = 0, 1
+HB_LAUNCH_PAIR_BLOCKS_PER_SM = 0
 
 PD = C.POINTER(C.c_double)
 PU32 = C.POINTER(C.c_uint32)
@@ -154,6 +155,7 @@ SIGNATURES = {
     "hb_forcefield_step": (C.c_int, [VP, C.c_int]),
     "hb_forcefield_pre_step": (C.c_int, [VP, C.c_int, C.POINTER(C.c_int)]),
     "hb_forcefield_scalars": (C.c_int, [VP, PD]),
+    "hb_forcefield_set_launch": (C.c_int, [VP, C.c_int, C.c_int]),
     "hb_forcefield_get_per_atom": (C.c_int, [VP, PD, PD]),
     "hb_neighbor_pairs": (C.c_int, [VP, PU32, C.c_uint64, PU64, PU64]),
     "hb_neighbor_stats": (C.c_int, [VP, PU64]),

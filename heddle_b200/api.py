@@ -346,6 +346,13 @@ class ForceField:
         N.check(self.lib.hb_forcefield_pre_step(self.h, 1 if force else 0, C.byref(r)))
         return bool(r.value)
 
+    def set_launch(self, pair_blocks_per_sm: int | None = None) -> None:
+        """Launch shapes (autotuned): resident blocks per SM of the persistent
+        pair kernel."""
+        if pair_blocks_per_sm is not None:
+            N.check(self.lib.hb_forcefield_set_launch(self.h, N.HB_LAUNCH_PAIR_BLOCKS_PER_SM,
+                                                      int(pair_blocks_per_sm)))
+
     def scalars(self) -> dict:
         out = np.zeros(10)
         N.check(self.lib.hb_forcefield_scalars(self.h, N.dptr(out)))

@@ -48,7 +48,11 @@ extern "C" int hb_context_create(int device_ordinal, hb_context **out) {
   }
   c->n_sm = prop.multiProcessorCount;
   HB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-  HB_CUDA(cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking));
+  // the reciprocal-space chain is the step's critical path: its stream gets
+  // the highest priority, so its blocks go first whenever SM room frees up
+  int prio_lo = 0, prio_hi = 0;
+  HB_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+  HB_CUDA(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, prio_hi));
   HB_CUDA(cudaStreamCreateWithFlags(&c->stream3, cudaStreamNonBlocking));
   HB_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
   HB_CUDA(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
@@ -587,6 +591,18 @@ extern "C" int hb_forcefield_pre_step(hb_forcefield *ff, int force, int *rebuilt
   HB_CUDA(cudaStreamSynchronize(s));
   if (rebuilt) *rebuilt = after != before ? 1 : 0;
   return check_status(ff);
+}
+
+extern "C" int hb_forcefield_set_launch(hb_forcefield *ff, int param, int value) {
+  HB_REQUIRE(ff, HB_ERR_INVALID_ARGUMENT, "null force field");
+  if (param == HB_LAUNCH_PAIR_BLOCKS_PER_SM) {
+    HB_REQUIRE(value >= 1 && value <= 8, HB_ERR_INVALID_ARGUMENT, "pair blocks per SM in 1..8");
+    ff->pair_blocks_per_sm = value;
+  } else {
+    return hb_fail(HB_ERR_INVALID_ARGUMENT, "unknown launch parameter");
+  }
+  ff->layout_gen++;  // launch shapes are baked into captured graphs
+  return HB_OK;
 }
 
 extern "C" int hb_forcefield_scalars(hb_forcefield *ff, double out[HB_N_SCALARS]) {

@@ -289,6 +289,7 @@ struct hb_forcefield {
                                      // build, [2] running count of a build,
                                      // [3] largest candidate count seen
   uint32_t *h_status = nullptr;      // pinned mirror
+  int pair_blocks_per_sm = 8;        // persistent pair kernel residency (tunable)
   uint32_t *d_work = nullptr;        // work counter of the balanced pair kernel
                                      // (zeroed by the combine kernel)
   uint64_t rebuilds_host = 0;

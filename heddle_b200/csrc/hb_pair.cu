@@ -338,11 +338,19 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
             uint32_t *__restrict__ work, uint32_t chunks, uint32_t chunk) {
   extern __shared__ float4 sm_lj4[];
   __shared__ P4Warp smw4[P4_WARPS];
+  __shared__ uint32_t sm_ljtypes[32];  // per i-type: j-types with a Lennard-Jones term
   const int nt2 = P.n_types * P.n_types;
   float *sm_ljd4 = reinterpret_cast<float *>(sm_lj4 + nt2);
   for (int k = threadIdx.x; k < nt2; k += blockDim.x) {
     sm_lj4[k] = lj_table[k];
     sm_ljd4[k] = lj_invd[k];
+  }
+  const bool few_types = P.n_types <= 32;
+  if (few_types && (int)threadIdx.x < P.n_types) {
+    uint32_t bits = 0u;
+    for (int q = 0; q < P.n_types; ++q)
+      if (lj_table[threadIdx.x * P.n_types + q].y != 0.0f) bits |= 1u << q;
+    sm_ljtypes[threadIdx.x] = bits;
   }
   __syncthreads();
   const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
@@ -431,18 +439,38 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
       }
       if (!SCALED) m &= ~xm;
 
-      // (2) slot-major queue of (i-lane, rotation)
-      uint32_t np = 0;
-      while (true) {
-        const bool has = m != 0u;
-        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
-        if (bal == 0u) break;
-        if (has) {
-          const uint32_t t = (uint32_t)__ffs(m) - 1u;
-          m &= m - 1u;
-          S.pairs[np + __popc(bal & lt)] = (uint16_t)((lane << 8) | t);
+      // (2) slot-major queues of (i-lane, rotation): pairs with a
+      // Lennard-Jones term first, Coulomb-only pairs after them, so the LJ
+      // arithmetic runs only in the (few) iterations that need it
+      uint32_t lj_rot = 0xFFFFFFFFu;
+      if (!P.lj_on) {
+        lj_rot = 0u;
+      } else if (few_types) {
+        const uint32_t lj_types = sm_ljtypes[S.itype[lane] / P.n_types];
+        uint32_t lj_j = 0u;
+        for (int q = 0; q < P.n_types; ++q) {
+          const uint32_t bal_t = __ballot_sync(0xFFFFFFFFu, tj == q && jvalid);
+          if ((lj_types >> q) & 1u) lj_j |= bal_t;
         }
-        np += __popc(bal);
+        lj_rot = __funnelshift_r(lj_j, lj_j, lane);  // bit t <-> j-lane (lane + t) mod 32
+      }
+      uint32_t mq = m & lj_rot;
+      uint32_t mc = P.coul_on ? (m & ~lj_rot) : 0u;
+      uint32_t np = 0, n_lj = 0;
+      for (int pass = 0; pass < 2; ++pass) {
+        uint32_t mm = pass == 0 ? mq : mc;
+        while (true) {
+          const bool has = mm != 0u;
+          const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
+          if (bal == 0u) break;
+          if (has) {
+            const uint32_t t = (uint32_t)__ffs(mm) - 1u;
+            mm &= mm - 1u;
+            S.pairs[np + __popc(bal & lt)] = (uint16_t)((lane << 8) | t);
+          }
+          np += __popc(bal);
+        }
+        if (pass == 0) n_lj = np;
       }
       __syncwarp();
 
@@ -450,6 +478,7 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
       for (uint32_t k = lane; k < np; k += 32u) {
         const uint32_t pr = S.pairs[k];
         const uint32_t i = pr >> 8, t = pr & 255u, j = (i + t) & 31u;
+        const bool ljq = k < n_lj;
         const float4 a = S.ipos[i], q = S.jpos[j];
         float dx = a.x - q.x, dy = a.y - q.y, dz = a.z - q.z;
         if (!spc) hb_min_image(dx, dy, dz, b);
@@ -471,7 +500,7 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
         const float inv_r = rsqrtf(r2);
         const float inv_r2 = inv_r * inv_r;
         float fac = 0.0f;
-        if (P.lj_on) {
+        if (ljq) {
           const int tp = S.itype[i] + S.jtype[j];
           const float4 L = sm_lj4[tp];
           if (r2 <= L.z && L.y != 0.0f && s_lj != 0.0f) {
@@ -555,10 +584,11 @@ template <bool SCALED, bool SWITCH>
 int launch4_t(hb_forcefield *ff, cudaStream_t s, const PairParams &P) {
   size_t smem = (sizeof(float4) + sizeof(float)) * (size_t)P.n_types * P.n_types;
   const uint32_t chunks = hb_div_up(P.slab, P4_CHUNK);
-  // persistent: 8 blocks of 4 warps per SM, or fewer for small systems
+  // persistent: pair_blocks_per_sm blocks of 4 warps per SM (at most 8 fit),
+  // or fewer for small systems
   const uint32_t items = P.n_tiles * chunks;
-  const uint32_t grid = std::min<uint32_t>((uint32_t)ff->sys->ctx->n_sm * 8u,
-                                           hb_div_up(items, P4_WARPS));
+  const uint32_t grid = std::min<uint32_t>(
+      (uint32_t)ff->sys->ctx->n_sm * (uint32_t)ff->pair_blocks_per_sm, hb_div_up(items, P4_WARPS));
   k_pair4<SCALED, SWITCH><<<std::max(grid, 1u), P4_WARPS * 32, smem, s>>>(
       ff->d_tile_posq, ff->d_tile_type, ff->d_tile_center, ff->d_tile_nent, ff->d_entry_j,
       ff->d_entry_excl, ff->sys->d_box, ff->d_lj, ff->d_lj_invd, P, ff->d_fp, ff->d_sorted_ids,

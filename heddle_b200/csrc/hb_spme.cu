@@ -778,13 +778,15 @@ int spme_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
   const uint32_t n = sys->n;
   const int na = S.na, nb = S.nb, nc = S.nc;
   if (n > 0) {
+    // small blocks (128-thread spread, 64-thread gather): they fit in the SM
+    // room the persistent pair kernel leaves, so the chain overlaps it
     const uint64_t th = (uint64_t)n * S.order;
     switch (S.order) {
-      case 4: k_spread<4><<<hb_div_up(th, 256), 256, 0, s>>>(ff->d_tile_posq, sys->d_box, na, nb, nc, S.d_rho_fixed, n); break;
-      case 5: k_spread<5><<<hb_div_up(th, 256), 256, 0, s>>>(ff->d_tile_posq, sys->d_box, na, nb, nc, S.d_rho_fixed, n); break;
-      case 6: k_spread<6><<<hb_div_up(th, 256), 256, 0, s>>>(ff->d_tile_posq, sys->d_box, na, nb, nc, S.d_rho_fixed, n); break;
-      case 7: k_spread<7><<<hb_div_up(th, 256), 256, 0, s>>>(ff->d_tile_posq, sys->d_box, na, nb, nc, S.d_rho_fixed, n); break;
-      case 8: k_spread<8><<<hb_div_up(th, 256), 256, 0, s>>>(ff->d_tile_posq, sys->d_box, na, nb, nc, S.d_rho_fixed, n); break;
+      case 4: k_spread<4><<<hb_div_up(th, 128), 128, 0, s>>>(ff->d_tile_posq, sys->d_box, na, nb, nc, S.d_rho_fixed, n); break;
+      case 5: k_spread<5><<<hb_div_up(th, 128), 128, 0, s>>>(ff->d_tile_posq, sys->d_box, na, nb, nc, S.d_rho_fixed, n); break;
+      case 6: k_spread<6><<<hb_div_up(th, 128), 128, 0, s>>>(ff->d_tile_posq, sys->d_box, na, nb, nc, S.d_rho_fixed, n); break;
+      case 7: k_spread<7><<<hb_div_up(th, 128), 128, 0, s>>>(ff->d_tile_posq, sys->d_box, na, nb, nc, S.d_rho_fixed, n); break;
+      case 8: k_spread<8><<<hb_div_up(th, 128), 128, 0, s>>>(ff->d_tile_posq, sys->d_box, na, nb, nc, S.d_rho_fixed, n); break;
       default: return hb_fail(HB_ERR_INVALID_ARGUMENT, "spline order must be 4..8");
     }
   }
@@ -792,11 +794,11 @@ int spme_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
              S.alpha, S.d_part, s);
   if (n > 0) {
     switch (S.order) {
-      case 4: k_gather<4><<<hb_div_up(n, 128), 128, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
-      case 5: k_gather<5><<<hb_div_up(n, 128), 128, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
-      case 6: k_gather<6><<<hb_div_up(n, 128), 128, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
-      case 7: k_gather<7><<<hb_div_up(n, 128), 128, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
-      case 8: k_gather<8><<<hb_div_up(n, 128), 128, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
+      case 4: k_gather<4><<<hb_div_up(n, 64), 64, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
+      case 5: k_gather<5><<<hb_div_up(n, 64), 64, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
+      case 6: k_gather<6><<<hb_div_up(n, 64), 64, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
+      case 7: k_gather<7><<<hb_div_up(n, 64), 64, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
+      case 8: k_gather<8><<<hb_div_up(n, 64), 64, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
     }
   }
   if (ev) k_spme_sums<<<1, 256, 0, s>>>(S.d_part, S.n_part, S.d_sums);

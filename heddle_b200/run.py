@@ -1,0 +1,253 @@
+"""Run a simulation from a TOML configuration: the runner's setup path
+(src/runner.rs:785-1180) over this engine.
+
+    python -m heddle_b200.run path/to/name.in.toml
+
+reads the configuration, the initial extended-XYZ frame and the topology,
+builds the system, force field (LJ, SPME, bonded terms, exclusions by the
+topology rules), constraint groups and each phase's integrator / barostat,
+and writes `<root>.out.<phase>.xyz` and `<root>.out.<phase>.log` beside the
+configuration (`<root>` = file name without `.toml` and one `.in`), in SI
+units like the reference.  Initial velocities, when the XYZ frame has none,
+are Maxwell-Boltzmann at [simulation].temperature from the ChaCha8 seed.
+"""
+
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+from . import api as A
+from .io import ConfigError, LogWriter, TrajectoryWriter, load_config, read_topology, read_xyz
+from .systems import settle_geometry
+from .topology import effective_exclusions, exclusion_csr
+from .velocities import generate_velocities
+
+
+def config_root(path: Path) -> str:
+    name = path.name
+    if name.endswith(".toml"):
+        name = name[: -len(".toml")]
+    if name.endswith(".in"):
+        name = name[: -len(".in")]
+    return name
+
+
+def build(cfg, ctx):
+    """Device objects for a loaded configuration: (system, force field,
+    constraints or None, type names, extras dict)."""
+    frame = read_xyz(cfg.init)
+    topo = read_topology(cfg.topology) if cfg.topology else None
+    names = [t["name"] for t in cfg.particle_types]
+    try:
+        types = np.array([names.index(s) for s in frame.species], dtype=np.uint32)
+    except ValueError as e:
+        raise ConfigError(f"initial frame: unknown species ({e})")
+    n = len(types)
+    masses = np.array([cfg.particle_types[t]["mass"] for t in types])
+    charges = np.array([cfg.particle_types[t]["charge"] for t in types])
+    if topo:
+        for a, q in topo.charges.items():
+            charges[a] = q
+    # constraint groups
+    g_off, g_atoms, g_kind, ra, rb, rc = [0], [], [], [], [], []
+    c_off, c_i, c_j, c_d = [0], [], [], []
+    groups = []
+    n_cons = 0
+    if topo:
+        for atoms, tname in topo.constraints:
+            ct = cfg.constraint_types.get(tname)
+            if ct is None:
+                raise ConfigError(f"topology: unknown constraint type {tname!r}")
+            groups.append(atoms)
+            g_atoms += atoms
+            g_off.append(len(g_atoms))
+            if ct["kind"] == "settle":
+                d_oh, d_hh = ct["d_OH"], ct["d_HH"]
+                hoh = 2.0 * np.degrees(np.arcsin(0.5 * d_hh / d_oh))
+                a_, b_, c_ = settle_geometry(d_oh, hoh, masses[atoms[0]], masses[atoms[1]])
+                g_kind.append(0)
+                ra.append(a_), rb.append(b_), rc.append(c_)
+                n_cons += 3
+            else:
+                if len(atoms) != ct["atoms"]:
+                    raise ConfigError(f"constraint row of type {tname!r} needs {ct['atoms']} atoms")
+                g_kind.append(1)
+                ra.append(0.0), rb.append(0.0), rc.append(0.0)
+                for i, j, d in ct["constraints"]:
+                    c_i.append(i), c_j.append(j), c_d.append(d)
+                n_cons += len(ct["constraints"])
+            c_off.append(len(c_i))
+    vel = frame.velocities
+    if vel is None:
+        vel = generate_velocities(masses, cfg.temperature, cfg.seed, n_cons)
+    sys_ = A.System(ctx, frame.positions, masses, charges, types, frame.box, velocities=vel,
+                    images=frame.images)
+    # force field
+    nt = len(names)
+    sig, eps = np.ones((nt, nt)), np.zeros((nt, nt))
+    cut_max = max([p["cutoff"] for p in cfg.pair_interactions], default=0.0)
+    if cfg.spme:
+        cut_max = max(cut_max, cfg.spme["r_cut_real"])
+    cut, sw = np.full((nt, nt), cut_max), np.full((nt, nt), cut_max)
+    for p in cfg.pair_interactions:
+        for a, b in (p["between"], p["between"][::-1]):
+            sig[a, b], eps[a, b], cut[a, b], sw[a, b] = p["sigma"], p["epsilon"], p["cutoff"], p["r_switch"]
+    conf = {}
+    if cfg.pair_interactions:
+        conf["lennard_jones"] = A.LennardJonesParams(sig, eps, cut, sw)
+    if cfg.spme:
+        conf["spme"] = A.SpmeParams(cfg.spme["alpha"], cfg.spme["r_cut_real"], cfg.spme["grid"],
+                                    cfg.spme["spline_order"])
+    bonds, angles, dihedrals, dscales = [], [], [], []
+    if topo:
+        if topo.bonds:
+            bk = [cfg.bond_types[t] for *_, t in topo.bonds]
+            conf["harmonic_bond"] = A.HarmonicBondParams(
+                np.array([(i, j) for i, j, _ in topo.bonds], dtype=np.uint32),
+                np.array([b["k"] for b in bk]), np.array([b["r0"] for b in bk]))
+            bonds = [(i, j) for i, j, _ in topo.bonds]
+        if topo.angles:
+            at = [cfg.angle_types[t] for *_, t in topo.angles]
+            conf["harmonic_angle"] = A.HarmonicAngleParams(
+                np.array([(i, j, k) for i, j, k, _ in topo.angles], dtype=np.uint32),
+                np.array([a["k_theta"] for a in at]), np.array([a["theta_0"] for a in at]))
+            angles = [(i, j, k) for i, j, k, _ in topo.angles]
+        if topo.dihedrals:
+            dt = [cfg.dihedral_types[t] for *_, t in topo.dihedrals]
+            conf["periodic_dihedral"] = A.PeriodicDihedralParams(
+                np.array([(i, j, k, l) for i, j, k, l, _ in topo.dihedrals], dtype=np.uint32),
+                np.array([d["k_phi"] for d in dt]), np.array([d["phi_0"] for d in dt]),
+                np.array([d["n"] for d in dt], dtype=np.uint32))
+            dihedrals = [(i, j, k, l) for i, j, k, l, _ in topo.dihedrals]
+            dscales = [(d["scale_lj_14"], d["scale_coul_14"]) for d in dt]
+    eff = effective_exclusions(n, bonds, angles, dihedrals, dscales, groups,
+                               topo.exclusions if topo else ())
+    excl = exclusion_csr(n, eff) if eff else None
+    ff = A.ForceField(sys_, conf, excl, r_skin=cfg.r_skin)
+    cons = None
+    if groups:
+        cons = A.Constraints(sys_, g_off, g_atoms, g_kind, (ra, rb, rc) if any(k == 0 for k in g_kind) else None,
+                             (c_off, c_i, c_j, c_d) if c_i else None)
+        cons.after_kick(0.0)  # initial velocity projection
+    mols = None
+    if groups:
+        mols = molecule_csr(n, groups, bonds)
+    return sys_, ff, cons, names, {"n_constraints": n_cons, "molecules": mols}
+
+
+def molecule_csr(n, groups, bonds):
+    """Connected components of bonds and constraint groups (the molecule
+    partition the barostat scales)."""
+    parent = list(range(n))
+
+    def find(a):
+        while parent[a] != a:
+            parent[a] = parent[parent[a]]
+            a = parent[a]
+        return a
+
+    for g in groups:
+        for a in g[1:]:
+            parent[find(a)] = find(g[0])
+    for i, j in bonds:
+        parent[find(i)] = find(j)
+    comp = {}
+    for a in range(n):
+        comp.setdefault(find(a), []).append(a)
+    mols = sorted(comp.values(), key=lambda m: m[0])
+    off = np.cumsum([0] + [len(m) for m in mols]).astype(np.uint32)
+    return off, np.concatenate(mols).astype(np.uint32)
+
+
+def run(config_path, ctx=None) -> list:
+    """Run every phase; returns the written output paths."""
+    cfg = load_config(config_path)
+    own = ctx is None
+    ctx = ctx or A.Context(0)
+    sys_, ff, cons, names, extra = build(cfg, ctx)
+    root = config_root(Path(cfg.path))
+    base = Path(cfg.path).parent
+    written = []
+    n = sys_.n
+    dof = max(3 * n - extra["n_constraints"] - 3, 1)
+    step = 0
+    for ph in cfg.phases:
+        kw = dict(ph.integrator)
+        kind = kw.pop("kind")
+        it = A.Integrator(sys_, kind, ph.dt, step0=step, **kw)
+        baro = None
+        if ph.barostat:
+            b = ph.barostat
+            mols = extra["molecules"]
+            baro = A.Barostat(sys_, b["pressure"], b["temperature"], b["seed"], b["frequency"],
+                              b["volume_step"], molecules=mols)
+            it.set_barostat(baro)
+        out = ph.output
+        traj = log = None
+        if out["trajectory_every"] > 0:
+            tp = base / f"{root}.out.{ph.name}.xyz"
+            traj = TrajectoryWriter(tp, names, out["include_velocities"], out["include_images"])
+            written.append(tp)
+        if out["log_every"] > 0:
+            lp = base / f"{root}.out.{ph.name}.log"
+            cols = [("potential_energy", "energy")]
+            if baro:
+                cols += [("box_volume", "volume"), ("mc_acceptance", "dimensionless")]
+            log = LogWriter(lp, cols)
+            written.append(lp)
+        types = None
+        done = 0
+        cadence = [c for c in (out["trajectory_every"], out["log_every"]) if c > 0]
+        while done < ph.n_steps:
+            k = ph.n_steps - done
+            for c in cadence:
+                k = min(k, c - (done % c))
+            it.step(ff, cons, n_steps=k, scalar_every=k if (log and (done + k) % out["log_every"] == 0) else 0)
+            done += k
+            t_au = (step + done) * ph.dt
+            if traj and done % out["trajectory_every"] == 0:
+                pos, vel, img, _ = sys_.state()
+                if types is None:
+                    types = np.asarray(sys_._t)
+                traj.write(step + done, t_au, sys_.box(), types, pos, vel, img)
+            if log and done % out["log_every"] == 0:
+                ke = sys_.kinetic()[0]
+                ex = [ff.scalars()["potential"]]
+                if baro:
+                    st = baro.stats()
+                    ex += [st["volume"], st["acceptance"]]
+                log.write(step + done, t_au, ke, 2.0 * ke / dof, ex)
+        step += ph.n_steps
+        for w in (traj, log):
+            if w:
+                w.close()
+        it.close()
+        if baro:
+            baro.close()
+    for o in (cons, ff, sys_):
+        if o is not None:
+            o.close()
+    if own:
+        ctx.close()
+    return written
+
+
+def main(argv=None) -> int:
+    argv = sys.argv[1:] if argv is None else argv
+    if len(argv) != 1:
+        print("usage: python -m heddle_b200.run <config.toml>", file=sys.stderr)
+        return 2
+    try:
+        for p in run(argv[0]):
+            print(p)
+    except ConfigError as e:
+        print(f"configuration error: {e}", file=sys.stderr)
+        return 1
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -52,6 +52,13 @@ enum {
   HB_INTEGRATOR_LANGEVIN = 2     /* "langevin-baoab" (middle scheme) */
 };
 
+/* launch-shape parameters of hb_forcefield_set_launch (autotuned) */
+enum {
+  HB_LAUNCH_PAIR_BLOCKS_PER_SM = 0  /* resident blocks of the persistent pair kernel
+                                       per SM (1..8, default 8); fewer leave room
+                                       for the concurrent reciprocal-space chain */
+};
+
 /* pair accumulation modes (hb_forcefield_desc.pair_mode) */
 enum { HB_PAIRS_FAST = 0, HB_PAIRS_EXACT = 1 };
 
@@ -181,6 +188,9 @@ int hb_forcefield_pre_step(hb_forcefield *ff, int force, int *rebuilt);
  * virial, [6] reciprocal virial, [7] total virial, [8] bonded energy,
  * [9] reserved (0). */
 int hb_forcefield_scalars(hb_forcefield *ff, double out[10]);
+/* Set a launch-shape parameter (HB_LAUNCH_*); captured graphs of the force
+ * field's integrators are re-captured on their next call. */
+int hb_forcefield_set_launch(hb_forcefield *ff, int param, int value);
 /* per-atom energy and virial shares of the last scalar step ([n] each). */
 int hb_forcefield_get_per_atom(hb_forcefield *ff, double *energy,
                                double *virial);

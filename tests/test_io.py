@@ -1,0 +1,113 @@
+"""Configuration / extended-XYZ / topology I/O (src/io/config.rs,
+src/io/trajectory.rs, src/io/log_output.rs semantics) on CPU."""
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from heddle_b200 import units as U
+from heddle_b200.io import (ConfigError, LogWriter, TrajectoryWriter, fmt_e, load_config,
+                            read_topology, read_xyz)
+from heddle_b200.run import config_root, molecule_csr
+
+CFG = Path(__file__).resolve().parent / "golden" / "configs"
+
+
+def test_real_format_matches_rust_exponent_style():
+    # `{:.9e}`: no exponent padding, no '+'
+    assert fmt_e(2.0e-9) == "2.000000000e-9"
+    assert fmt_e(0.0) == "0.000000000e0"
+    assert fmt_e(-7.5e-10) == "-7.500000000e-10"
+    assert fmt_e(1234.5) == "1.234500000e3"
+    assert fmt_e(1.0) == "1.000000000e0"
+
+
+def test_config_units_are_converted_to_atomic():
+    c = load_config(CFG / "argon.in.toml")
+    assert c.schema_version == 1 and len(c.phases) == 1
+    ph = c.phases[0]
+    assert ph.n_steps == 100 and ph.dt == pytest.approx(U.time_au_fs(5.0))
+    assert ph.integrator == {"kind": "velocity-verlet"}
+    assert c.particle_types[0]["mass"] == pytest.approx(U.mass_au_kg(6.6335e-26))
+    p = c.pair_interactions[0]
+    assert p["sigma"] == pytest.approx(U.length_au(3.405e-10))
+    assert p["epsilon"] == pytest.approx(U.energy_au_j(1.654e-21))
+    assert c.r_skin == pytest.approx(U.length_au(1.0e-10))
+    w = load_config(CFG / "water.in.toml")
+    assert w.phases[0].barostat["kind"] == "monte-carlo"
+    assert w.phases[0].barostat["pressure"] == pytest.approx(1.0e5 / U.PRESSURE_PA)
+    assert w.spme["alpha"] == pytest.approx(4.4620e9 * U.BOHR_M)
+    assert w.constraint_types["SPC"]["kind"] == "settle"
+    ch = load_config(CFG / "chain.in.toml")
+    assert ch.bond_types["CC"]["k"] == pytest.approx(U.energy_au_j(4.3e2) * U.BOHR_M ** 2)
+    assert ch.dihedral_types["X"]["n"] == 3
+    assert ch.constraint_types["CH3"]["atoms"] == 4
+
+
+@pytest.mark.parametrize("patch,message", [
+    ("[phase.thermostat]\nkind = \"csvr\"\n", "thermostat kind 'csvr'"),
+    ("[phase.barostat]\nkind = \"c-rescale\"\n", "barostat kind 'c-rescale'"),
+])
+def test_unsupported_slots_are_rejected(tmp_path, patch, message):
+    text = (CFG / "argon.in.toml").read_text().replace("[phase.output]", patch + "\n[phase.output]")
+    (tmp_path / "argon.in.xyz").write_text((CFG / "argon.in.xyz").read_text())
+    p = tmp_path / "x.in.toml"
+    p.write_text(text)
+    with pytest.raises(ConfigError, match=message):
+        load_config(p)
+
+
+def test_bad_values_are_rejected(tmp_path):
+    (tmp_path / "argon.in.xyz").write_text((CFG / "argon.in.xyz").read_text())
+    for old, new, msg in (("schema_version = 1", "schema_version = 2", "schema_version"),
+                          ("dt = 5.0e-15", "dt = -1.0", "strictly positive"),
+                          ("r_switch = 8.5125e-10", "r_switch = 9.0e-10", "r_switch")):
+        p = tmp_path / "y.in.toml"
+        p.write_text((CFG / "argon.in.toml").read_text().replace(old, new))
+        with pytest.raises(ConfigError, match=msg):
+            load_config(p)
+
+
+def test_xyz_round_trip(tmp_path):
+    f = read_xyz(CFG / "water.in.xyz")
+    assert len(f.species) == 648 and f.species[:3] == ["O", "H", "H"]
+    rng = np.random.default_rng(1)
+    vel = rng.normal(scale=1e-4, size=f.positions.shape)
+    img = rng.integers(-2, 3, size=f.positions.shape)
+    w = TrajectoryWriter(tmp_path / "t.xyz", ["O", "H"], True, True)
+    types = np.array([0, 1, 1] * 216)
+    w.write(7, 123.0, f.box, types, f.positions, vel, img)
+    w.write(8, 124.0, f.box, types, f.positions + 0.5, vel, img)
+    w.close()
+    g = read_xyz(tmp_path / "t.xyz", index=-1)
+    assert g.step == 8 and g.time == pytest.approx(124.0, rel=1e-9)
+    assert np.allclose(g.positions, f.positions + 0.5, rtol=1e-9, atol=0)
+    assert np.allclose(g.velocities, vel, rtol=1e-9, atol=0)
+    assert np.array_equal(g.images, img)
+    assert np.allclose(g.box, f.box, rtol=1e-9)
+    with pytest.raises(FileExistsError):
+        TrajectoryWriter(tmp_path / "t.xyz", ["O"])
+
+
+def test_log_format(tmp_path):
+    w = LogWriter(tmp_path / "l.log", [("potential_energy", "energy")])
+    w.write(5, 10.0, 0.001, 0.00095, [-0.5])
+    w.close()
+    lines = (tmp_path / "l.log").read_text().splitlines()
+    assert lines[0] == "step,time,kinetic_energy,temperature,potential_energy"
+    cols = lines[1].split(",")
+    assert cols[0] == "5" and float(cols[3]) == pytest.approx(0.00095 * U.HARTREE_K)
+    assert float(cols[4]) == pytest.approx(-0.5 * U.HARTREE_J)
+
+
+def test_topology_sections_and_molecules():
+    t = read_topology(CFG / "chain.in.topology")
+    assert len(t.bonds) == 3 and len(t.angles) == 6 and len(t.dihedrals) == 1
+    assert t.constraints[0][1] == "CH3" and len(t.constraints[0][0]) == 4
+    assert len(t.charges) == 14
+    groups = [a for a, _ in t.constraints]
+    off, atoms = molecule_csr(638, groups, [(i, j) for i, j, _ in t.bonds])
+    # the 14-atom chain is one molecule, every water another
+    assert off[1] == 14 and len(off) - 1 == 1 + (638 - 14) // 3
+    assert config_root(Path("a/b/chain.in.toml")) == "chain"
