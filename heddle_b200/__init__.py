@@ -16,13 +16,16 @@ from .api import (  # noqa: F401
     LennardJonesParams,
     PeriodicDihedralParams,
     PotentialRegistry,
+    PressureCoupling,
     ShakeMLP,
     SpmeParams,
     System,
+    Thermostat,
 )
 
 __all__ = [
     "Context", "System", "ForceField", "Constraints", "Integrator", "Barostat", "Batch",
     "PotentialRegistry", "LennardJonesParams", "SpmeParams", "HarmonicBondParams",
-    "HarmonicAngleParams", "PeriodicDihedralParams", "ShakeMLP", "HeddleError", "load",
+    "HarmonicAngleParams", "PeriodicDihedralParams", "ShakeMLP", "Thermostat",
+    "PressureCoupling", "HeddleError", "load",
 ]

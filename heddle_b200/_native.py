@@ -67,6 +67,28 @@ class BarostatDesc(C.Structure):
     ]
 
 
+class ThermostatDesc(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int),
+        ("temperature", C.c_double),
+        ("tau", C.c_double),
+        ("collision_rate", C.c_double),
+        ("seed", C.c_uint64),
+        ("n_constraints", C.c_uint32),
+    ]
+
+
+class PcoupleDesc(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int),
+        ("pressure", C.c_double),
+        ("temperature", C.c_double),
+        ("tau", C.c_double),
+        ("compressibility", C.c_double),
+        ("seed", C.c_uint64),
+    ]
+
+
 class ForceFieldDesc(C.Structure):
     _fields_ = [
         ("lj_enabled", C.c_int),
@@ -189,6 +211,14 @@ SIGNATURES = {
     "hb_barostat_mc_move": (C.c_int, [VP, VP]),
     "hb_barostat_stats": (C.c_int, [VP, PD]),
     "hb_integrator_set_barostat": (C.c_int, [VP, VP]),
+    "hb_thermostat_create": (C.c_int, [VP, C.POINTER(ThermostatDesc), PVP]),
+    "hb_thermostat_destroy": (C.c_int, [VP]),
+    "hb_thermostat_stats": (C.c_int, [VP, PD]),
+    "hb_integrator_set_thermostat": (C.c_int, [VP, VP]),
+    "hb_pcouple_create": (C.c_int, [VP, C.POINTER(PcoupleDesc), PVP]),
+    "hb_pcouple_destroy": (C.c_int, [VP]),
+    "hb_pcouple_stats": (C.c_int, [VP, PD]),
+    "hb_integrator_set_pcouple": (C.c_int, [VP, VP]),
     "hb_batch_create": (C.c_int, [VP, C.c_uint32, PVP, PVP, PVP, PVP]),
     "hb_batch_destroy": (C.c_int, [VP]),
     "hb_batch_step": (C.c_int, [VP, C.c_uint32]),

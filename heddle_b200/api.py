@@ -522,9 +522,23 @@ class Integrator:
                                                       out.ctypes.data_as(N.PU64)))
         return int(out[0]), int(out[1]), int(out[2])
 
-    def set_barostat(self, baro: "Barostat | None") -> None:
-        N.check(self.lib.hb_integrator_set_barostat(self.h, baro.h if baro else None))
+    def set_barostat(self, baro: "Barostat | PressureCoupling | None") -> None:
+        """Attach a Monte-Carlo barostat or a per-step pressure coupling
+        (c-rescale, Berendsen); None detaches both."""
+        if baro is None:
+            N.check(self.lib.hb_integrator_set_barostat(self.h, None))
+            N.check(self.lib.hb_integrator_set_pcouple(self.h, None))
+        elif isinstance(baro, PressureCoupling):
+            N.check(self.lib.hb_integrator_set_pcouple(self.h, baro.h))
+        else:
+            N.check(self.lib.hb_integrator_set_barostat(self.h, baro.h))
         self._baro = baro
+
+    def set_thermostat(self, thermo: "Thermostat | None") -> None:
+        """Attach (or detach with None) a velocity thermostat (CSVR,
+        Andersen, Berendsen); velocity Verlet only."""
+        N.check(self.lib.hb_integrator_set_thermostat(self.h, thermo.h if thermo else None))
+        self._thermo = thermo
 
     def close(self) -> None:
         if getattr(self, "h", None):
@@ -583,6 +597,86 @@ class Barostat:
     def close(self) -> None:
         if getattr(self, "h", None):
             self.lib.hb_barostat_destroy(self.h)
+            self.h = None
+
+
+THERMOSTAT_KINDS = {"csvr": 0, "andersen": 1, "berendsen": 2}
+THERMOSTAT_STATS = ("injection", "kinetic", "factor", "sum_squares", "r", "draws", "dof")
+
+
+class Thermostat:
+    """Velocity thermostat for velocity Verlet, applied after each step's
+    constraint velocity projection (the reference's post-force slot):
+    "csvr" (Bussi stochastic velocity rescaling, tau), "andersen"
+    (per-atom Maxwell-Boltzmann collisions at collision_rate) or
+    "berendsen" (weak coupling, tau).  temperature as k_B T in hartree,
+    times in a.u.; n_constraints is removed from the degrees of freedom."""
+
+    def __init__(self, system: System, kind: str, temperature: float, seed: int = 0,
+                 tau: float = 0.0, collision_rate: float = 0.0, n_constraints: int = 0):
+        if kind not in THERMOSTAT_KINDS:
+            raise ValueError(f"unknown thermostat kind {kind!r}")
+        self.system = system
+        self.lib = system.lib
+        self.kind = kind
+        d = N.ThermostatDesc()
+        d.kind = THERMOSTAT_KINDS[kind]
+        d.temperature = float(temperature)
+        d.tau = float(tau)
+        d.collision_rate = float(collision_rate)
+        d.seed = int(seed)
+        d.n_constraints = int(n_constraints)
+        h = C.c_void_p()
+        N.check(self.lib.hb_thermostat_create(system.h, C.byref(d), C.byref(h)))
+        self.h = h
+
+    def stats(self) -> dict:
+        out = np.zeros(len(THERMOSTAT_STATS))
+        N.check(self.lib.hb_thermostat_stats(self.h, N.dptr(out)))
+        return dict(zip(THERMOSTAT_STATS, out.tolist()))
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.hb_thermostat_destroy(self.h)
+            self.h = None
+
+
+PCOUPLE_KINDS = {"c_rescale": 0, "berendsen": 1}
+PCOUPLE_STATS = ("pressure", "volume", "injection", "mu", "draws", "kinetic", "virial", "guarded")
+
+
+class PressureCoupling:
+    """Per-step isotropic pressure coupling for velocity Verlet: "c_rescale"
+    (stochastic cell rescaling) or "berendsen".  pressure in hartree/bohr^3,
+    temperature as k_B T in hartree, tau in a.u., compressibility in
+    bohr^3/hartree."""
+
+    def __init__(self, system: System, kind: str, pressure: float, tau: float,
+                 compressibility: float, temperature: float = 0.0, seed: int = 0):
+        if kind not in PCOUPLE_KINDS:
+            raise ValueError(f"unknown pressure coupling kind {kind!r}")
+        self.system = system
+        self.lib = system.lib
+        self.kind = kind
+        d = N.PcoupleDesc()
+        d.kind = PCOUPLE_KINDS[kind]
+        d.pressure = float(pressure)
+        d.temperature = float(temperature)
+        d.tau = float(tau)
+        d.compressibility = float(compressibility)
+        d.seed = int(seed)
+        h = C.c_void_p()
+        N.check(self.lib.hb_pcouple_create(system.h, C.byref(d), C.byref(h)))
+        self.h = h
+
+    def stats(self) -> dict:
+        out = np.zeros(len(PCOUPLE_STATS))
+        N.check(self.lib.hb_pcouple_stats(self.h, N.dptr(out)))
+        return dict(zip(PCOUPLE_STATS, out.tolist()))
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.hb_pcouple_destroy(self.h)
             self.h = None
 
 

@@ -936,10 +936,16 @@ static int one_step(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons, 
     HB_TRY(integ_vv_kick_drift(it, s));
     if (cons) HB_TRY(cons_positions(cons, it->dt, s));
     stage_end(4, t4, s);
-    HB_TRY(force_eval(ff, ev, capturing));
+    // per-step pressure coupling reads the virial of every step
+    HB_TRY(force_eval(ff, ev || it->pc != nullptr, capturing));
     cudaEvent_t t5 = stage_begin(s);
     if (cons) HB_TRY(cons_velocities(cons, it->dt, true, s));
-    HB_TRY(integ_vv_kick(it, s));
+    if (it->thermo || it->pc) {
+      HB_TRY(couple_prepare(it, ff, cons, s));
+      HB_TRY(couple_final_kick(it, s));
+    } else {
+      HB_TRY(integ_vv_kick(it, s));
+    }
     stage_end(4, t5, s);
   }
   it->step++;
@@ -970,6 +976,8 @@ extern "C" int hb_integrator_set_barostat(hb_integrator *it, hb_barostat *b) {
   HB_REQUIRE(it, HB_ERR_INVALID_ARGUMENT, "null integrator");
   HB_REQUIRE(!b || b->sys == it->sys, HB_ERR_INVALID_ARGUMENT,
              "integrator and barostat must share one system");
+  HB_REQUIRE(!b || !it->pc, HB_ERR_UNSUPPORTED,
+             "one barostat per integrator: detach the pressure coupling first");
   it->baro = b;
   return HB_OK;
 }
@@ -1073,8 +1081,10 @@ extern "C" int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
     it->forces_valid = true;
   }
   const uint64_t cons_uid = cons ? cons->uid : 0, baro_uid = it->baro ? it->baro->uid : 0;
+  const uint64_t thermo_uid = it->thermo ? it->thermo->uid : 0, pc_uid = it->pc ? it->pc->uid : 0;
   if (!it->graph_exec || it->graph_ff != ff->uid || it->graph_cons != cons_uid ||
-      it->graph_baro != baro_uid || it->graph_gen != ff->layout_gen) {
+      it->graph_baro != baro_uid || it->graph_gen != ff->layout_gen ||
+      it->graph_thermo != thermo_uid || it->graph_pc != pc_uid) {
     drop_graphs(it);
     HB_CUDA(cudaStreamSynchronize(s));
     HB_TRY(capture_step(it, ff, cons, false, &it->graph_exec));
@@ -1083,6 +1093,8 @@ extern "C" int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
     it->graph_cons = cons_uid;
     it->graph_baro = baro_uid;
     it->graph_gen = ff->layout_gen;
+    it->graph_thermo = thermo_uid;
+    it->graph_pc = pc_uid;
   }
   if (ctx->timing) HB_CUDA(cudaEventRecord(it->g_ev0, s));
   for (uint32_t k = 0; k < n_steps; ++k) {

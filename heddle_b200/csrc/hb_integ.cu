@@ -462,15 +462,23 @@ int integ_lang_drift_ou(hb_integrator *it, cudaStream_t s) {
   return HB_OK;
 }
 
+int reduce_kinetic_device(hb_system *sys, cudaStream_t s, const double **d_out) {
+  // with n = 0 the partial sums are zero and the result is zero
+  k_kinetic_part<<<RED_BLOCKS, 256, 0, s>>>(sys->d_vel, sys->d_red, sys->n);
+  k_kinetic_final<<<1, 256, 0, s>>>(sys->d_red, RED_BLOCKS, sys->d_red + 4 * RED_BLOCKS);
+  HB_CUDA(cudaGetLastError());
+  *d_out = sys->d_red + 4 * RED_BLOCKS;
+  return HB_OK;
+}
+
 int reduce_kinetic(hb_system *sys, double out[4]) {
   cudaStream_t s = sys->ctx->stream;
   if (sys->n == 0) {
     for (int q = 0; q < 4; ++q) out[q] = 0.0;
     return HB_OK;
   }
-  k_kinetic_part<<<RED_BLOCKS, 256, 0, s>>>(sys->d_vel, sys->d_red, sys->n);
-  k_kinetic_final<<<1, 256, 0, s>>>(sys->d_red, RED_BLOCKS, sys->d_red + 4 * RED_BLOCKS);
-  HB_CUDA(cudaGetLastError());
+  const double *d_ke = nullptr;
+  HB_TRY(reduce_kinetic_device(sys, s, &d_ke));
   HB_CUDA(cudaMemcpyAsync(sys->h_red, sys->d_red + 4 * RED_BLOCKS, sizeof(double) * 4,
                           cudaMemcpyDeviceToHost, s));
   HB_CUDA(cudaStreamSynchronize(s));

@@ -365,6 +365,10 @@ struct hb_integrator {
   hb_barostat *baro = nullptr;
   cudaGraphExec_t graph_exec_move = nullptr;
   uint64_t graph_baro = 0;
+  // velocity thermostat and per-step pressure coupling (velocity Verlet)
+  hb_thermostat *thermo = nullptr;
+  hb_pcouple *pc = nullptr;
+  uint64_t graph_thermo = 0, graph_pc = 0;
 };
 
 // Device-resident state of the Monte-Carlo barostat (FP64).  The whole move
@@ -396,6 +400,36 @@ struct hb_barostat {
   float4 *d_snap_pos = nullptr;      // pre-move positions, images, forces
   int4 *d_snap_img = nullptr;
   float4 *d_snap_force = nullptr;
+};
+
+// Device-resident state of a thermostat or a pressure coupling (FP64), so
+// a captured step reads and advances it with no host work.
+struct CoupleState {
+  double injection;        // thermostat: sum (K' - K); pressure: sum P0 dV
+  double k, factor, s, r;  // last kinetic energy, rescale factor, sum xi^2, r
+  double pressure, volume, w, mu;
+  unsigned long long draws, guarded;
+};
+
+struct hb_thermostat {
+  hb_system *sys = nullptr;
+  uint64_t uid = hb_next_uid();
+  int kind = 0;
+  double kt = 0.0, tau = 0.0, rate = 0.0;
+  uint64_t seed = 0;
+  uint32_t g_dof = 1;
+  CoupleState *d_st = nullptr;
+  double *d_part = nullptr;   // per-block partial sums of the CSVR draw
+};
+
+struct hb_pcouple {
+  hb_system *sys = nullptr;
+  uint64_t uid = hb_next_uid();
+  int kind = 0;
+  double pressure = 0.0, kt = 0.0, tau = 0.0, kappa = 0.0;
+  uint64_t seed = 0;
+  CoupleState *d_st = nullptr;
+  double *d_part = nullptr;   // partial sums of the constraint virial
 };
 
 // ---------------------------------------------------------------------
@@ -433,6 +467,13 @@ int integ_vv_kick(hb_integrator *it, cudaStream_t s);
 int integ_lang_kick(hb_integrator *it, cudaStream_t s);
 int integ_lang_drift_ou(hb_integrator *it, cudaStream_t s);
 int reduce_kinetic(hb_system *sys, double out[4]);
+// the same reduction left on the device: [0] kinetic energy, [1..3] momentum
+int reduce_kinetic_device(hb_system *sys, cudaStream_t s, const double **d_out);
+// thermostat / pressure coupling of a velocity-Verlet step (hb_couple.cu):
+// the factors after the velocity projection, then the final half kick with
+// the rescale, Andersen collisions and position scaling fused in
+int couple_prepare(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons, cudaStream_t s);
+int couple_final_kick(hb_integrator *it, cudaStream_t s);
 int integ_flip_velocities(hb_system *sys, cudaStream_t s);
 // lossless mode: fixed-point state from posq / vel (and posq / vel snapped to it)
 int integ_fix_derive(hb_system *sys, cudaStream_t s);

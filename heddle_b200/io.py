@@ -12,13 +12,13 @@ c = (xz, yz, lz) -- and `Properties=species:S:1:pos:R:3[:velo:R:3]
 `[charges]` sections.
 
 Supported slot kinds: integrators "velocity-verlet" (with `lossless`) and
-"langevin-baoab", barostat "monte-carlo", constraint types "settle" and
+"langevin-baoab", thermostats "csvr", "andersen" and "berendsen", barostats
+"monte-carlo", "c-rescale" and "berendsen", constraint types "settle" and
 "shake", bond/angle types "harmonic", dihedral types "periodic", pair
 potential "lennard-jones", neighbour list "cell-list".  Other kinds the
-reference registers (thermostats csvr / andersen / berendsen /
-nose-hoover-chain, barostats c-rescale / berendsen / mtk-npt, Morse bonds,
-minimisation phases, all-pairs lists) are rejected with a ConfigError that
-names them.
+reference registers (thermostat nose-hoover-chain, barostat mtk-npt, Morse
+bonds, minimisation phases, all-pairs lists) are rejected with a
+ConfigError that names them.
 """
 
 from __future__ import annotations
@@ -80,8 +80,8 @@ class Config:
 
 
 _UNSUPPORTED = {
-    "thermostat": ("csvr", "andersen", "berendsen", "nose-hoover-chain"),
-    "barostat": ("c-rescale", "berendsen", "mtk-npt"),
+    "thermostat": ("nose-hoover-chain",),
+    "barostat": ("mtk-npt",),
 }
 
 KB_J = 1.380649e-23  # J/K
@@ -105,6 +105,64 @@ def _positive(v, where):
     if v <= 0.0:
         raise ConfigError(f"{where}: value must be finite and strictly positive, got {v}")
     return v
+
+
+def _temperature(table, where):
+    return U.temperature_au_k(_positive(_req(table, "temperature", where), f"{where}.temperature"))
+
+
+def _thermostat(t: dict) -> dict:
+    """[phase.thermostat]: csvr (temperature, tau, seed), andersen
+    (temperature, collision_rate, seed), berendsen (temperature, tau);
+    src/integrator/csvr.rs:18-40, andersen.rs:18-50, berendsen.rs:20-60."""
+    kind = t.get("kind")
+    if kind == "csvr":
+        return {"kind": kind, "temperature": _temperature(t, "thermostat"),
+                "tau": _positive(_req(t, "tau", "thermostat"), "thermostat.tau") / U.AUT_S,
+                "seed": int(_req(t, "seed", "thermostat"))}
+    if kind == "andersen":
+        rate = _finite(_req(t, "collision_rate", "thermostat"), "thermostat.collision_rate")
+        if rate < 0.0:
+            raise ConfigError(f"thermostat.collision_rate: value must be finite and non-negative, "
+                              f"got {rate}")
+        return {"kind": kind, "temperature": _temperature(t, "thermostat"),
+                "collision_rate": rate * U.AUT_S, "seed": int(_req(t, "seed", "thermostat"))}
+    if kind == "berendsen":
+        return {"kind": kind, "temperature": _temperature(t, "thermostat"),
+                "tau": _positive(_req(t, "tau", "thermostat"), "thermostat.tau") / U.AUT_S}
+    raise ConfigError(f"thermostat kind {kind!r} is not supported by this engine "
+                      f"(known to the reference: {', '.join(_UNSUPPORTED['thermostat'])})")
+
+
+def _barostat(b: dict) -> dict:
+    """[phase.barostat]: monte-carlo (pressure, temperature, frequency,
+    volume_step, seed), c-rescale (pressure, temperature, tau,
+    compressibility, seed), berendsen (pressure, tau, compressibility);
+    src/integrator/mc_barostat.rs, c_rescale_barostat.rs:14-45,
+    berendsen_barostat.rs:20-60."""
+    kind = b.get("kind")
+    pressure = _finite(_req(b, "pressure", "barostat"), "barostat.pressure") / U.PRESSURE_PA
+    if kind == "monte-carlo":
+        vs = b.get("volume_step")
+        out = {"kind": kind, "pressure": pressure, "temperature": _temperature(b, "barostat"),
+               "frequency": int(b.get("frequency", 25)),
+               "volume_step": None if vs is None else
+               _positive(vs, "barostat.volume_step") / U.BOHR_M ** 3,
+               "seed": int(_req(b, "seed", "barostat"))}
+        if out["frequency"] < 1:
+            raise ConfigError("barostat.frequency: value must be >= 1, got 0")
+        return out
+    if kind in ("c-rescale", "berendsen"):
+        out = {"kind": kind, "pressure": pressure,
+               "tau": _positive(_req(b, "tau", "barostat"), "barostat.tau") / U.AUT_S,
+               "compressibility": _positive(_req(b, "compressibility", "barostat"),
+                                            "barostat.compressibility") * U.PRESSURE_PA}
+        if kind == "c-rescale":
+            out["temperature"] = _temperature(b, "barostat")
+            out["seed"] = int(_req(b, "seed", "barostat"))
+        return out
+    raise ConfigError(f"barostat kind {kind!r} is not supported by this engine "
+                      f"(known to the reference: {', '.join(_UNSUPPORTED['barostat'])})")
 
 
 def load_config(path) -> Config:
@@ -146,32 +204,19 @@ def load_config(path) -> Config:
                               "registered builder")
         thermo = p.get("thermostat")
         if thermo is not None:
-            tk = thermo.get("kind")
-            raise ConfigError(f"thermostat kind {tk!r} is not supported by this engine "
-                              f"(known to the reference: {', '.join(_UNSUPPORTED['thermostat'])})")
+            thermo = _thermostat(thermo)
         baro = p.get("barostat")
         if baro is not None:
-            bk = baro.get("kind")
-            if bk != "monte-carlo":
-                raise ConfigError(f"barostat kind {bk!r} is not supported by this engine")
-            vs = baro.get("volume_step")
-            baro = {"kind": bk,
-                    "pressure": _finite(_req(baro, "pressure", "barostat"), "barostat.pressure")
-                    / U.PRESSURE_PA,
-                    "temperature": U.temperature_au_k(_positive(_req(baro, "temperature", "barostat"),
-                                                                "barostat.temperature")),
-                    "frequency": int(baro.get("frequency", 25)),
-                    "volume_step": None if vs is None else
-                    _positive(vs, "barostat.volume_step") / U.BOHR_M ** 3,
-                    "seed": int(_req(baro, "seed", "barostat"))}
-            if baro["frequency"] < 1:
-                raise ConfigError("barostat.frequency: value must be >= 1, got 0")
+            baro = _barostat(baro)
+        if (thermo or (baro and baro["kind"] != "monte-carlo")) and integ["kind"] != "velocity-verlet":
+            raise ConfigError("a thermostat or a per-step barostat needs the (non-lossless) "
+                              "velocity-verlet integrator")
         out = dict(p.get("output", {}))
         output = {"trajectory_every": int(out.get("trajectory_every", 100)),
                   "include_velocities": bool(out.get("include_velocities", False)),
                   "include_images": bool(out.get("include_images", False)),
                   "log_every": int(out.get("log_every", 100))}
-        phases.append(PhaseConfig(name, n_steps, dt, integ, None, baro, output))
+        phases.append(PhaseConfig(name, n_steps, dt, integ, thermo, baro, output))
     if not phases:
         raise ConfigError("no [[phase]] entries")
     ptypes = []

@@ -162,6 +162,47 @@ def molecule_csr(n, groups, bonds):
     return off, np.concatenate(mols).astype(np.uint32)
 
 
+def log_columns(ph) -> list:
+    """Extra log columns after step,time,kinetic_energy,temperature: the
+    thermostat's, then the barostat's (src/runner.rs:1437-1443), with the
+    names and dimensions of their log_column_names (box volumes are written
+    in bohr^3, unconverted, like the reference's Dimensionless columns)."""
+    cols = []
+    t = ph.thermostat["kind"] if ph.thermostat else None
+    if t in ("csvr", "andersen", "berendsen"):
+        cols.append((f"{t}_conserved", "energy"))
+    b = ph.barostat["kind"] if ph.barostat else None
+    if b == "monte-carlo":
+        cols += [("box_volume", "dimensionless"), ("mc_acceptance", "dimensionless"),
+                 ("mc_volume_step", "dimensionless"), ("mc_conserved", "energy")]
+    elif b == "c-rescale":
+        cols += [("pressure", "pressure"), ("box_volume", "dimensionless"),
+                 ("c_rescale_conserved", "energy")]
+    elif b == "berendsen":
+        cols += [("pressure", "pressure"), ("box_volume", "dimensionless")]
+    return cols
+
+
+def log_values(ph, ke: float, pe: float, thermo, baro) -> list:
+    """Values of log_columns(ph) (csvr.rs:247-253, andersen.rs:180-187,
+    berendsen.rs:191-197, mc_barostat.rs:374-385,
+    c_rescale_barostat.rs:287-300, berendsen_barostat.rs:219-225)."""
+    vals = []
+    if thermo is not None:
+        st = thermo.stats()
+        vals.append(ke + pe if thermo.kind == "andersen" else ke + pe - st["injection"])
+    if baro is not None:
+        st = baro.stats()
+        if ph.barostat["kind"] == "monte-carlo":
+            vals += [st["volume"], st["acceptance"], st["max_volume_step"],
+                     ke + pe + st["conserved_term"]]
+        else:
+            vals += [st["pressure"], st["volume"]]
+            if ph.barostat["kind"] == "c-rescale":
+                vals.append(ke + pe + ph.barostat["pressure"] * st["volume"] - st["injection"])
+    return vals
+
+
 def run(config_path, ctx=None) -> list:
     """Run every phase; returns the written output paths."""
     cfg = load_config(config_path)
@@ -178,12 +219,22 @@ def run(config_path, ctx=None) -> list:
         kw = dict(ph.integrator)
         kind = kw.pop("kind")
         it = A.Integrator(sys_, kind, ph.dt, step0=step, **kw)
-        baro = None
+        thermo = baro = None
+        if ph.thermostat:
+            t = ph.thermostat
+            thermo = A.Thermostat(sys_, t["kind"], t["temperature"], seed=t.get("seed", 0),
+                                  tau=t.get("tau", 0.0), collision_rate=t.get("collision_rate", 0.0),
+                                  n_constraints=extra["n_constraints"])
+            it.set_thermostat(thermo)
         if ph.barostat:
             b = ph.barostat
-            mols = extra["molecules"]
-            baro = A.Barostat(sys_, b["pressure"], b["temperature"], b["seed"], b["frequency"],
-                              b["volume_step"], molecules=mols)
+            if b["kind"] == "monte-carlo":
+                baro = A.Barostat(sys_, b["pressure"], b["temperature"], b["seed"], b["frequency"],
+                                  b["volume_step"], molecules=extra["molecules"])
+            else:
+                baro = A.PressureCoupling(sys_, b["kind"].replace("-", "_"), b["pressure"], b["tau"],
+                                          b["compressibility"], temperature=b.get("temperature", 0.0),
+                                          seed=b.get("seed", 0))
             it.set_barostat(baro)
         out = ph.output
         traj = log = None
@@ -193,10 +244,7 @@ def run(config_path, ctx=None) -> list:
             written.append(tp)
         if out["log_every"] > 0:
             lp = base / f"{root}.out.{ph.name}.log"
-            cols = [("potential_energy", "energy")]
-            if baro:
-                cols += [("box_volume", "volume"), ("mc_acceptance", "dimensionless")]
-            log = LogWriter(lp, cols)
+            log = LogWriter(lp, log_columns(ph))
             written.append(lp)
         types = None
         done = 0
@@ -215,18 +263,16 @@ def run(config_path, ctx=None) -> list:
                 traj.write(step + done, t_au, sys_.box(), types, pos, vel, img)
             if log and done % out["log_every"] == 0:
                 ke = sys_.kinetic()[0]
-                ex = [ff.scalars()["potential"]]
-                if baro:
-                    st = baro.stats()
-                    ex += [st["volume"], st["acceptance"]]
-                log.write(step + done, t_au, ke, 2.0 * ke / dof, ex)
+                log.write(step + done, t_au, ke, 2.0 * ke / dof,
+                          log_values(ph, ke, ff.scalars()["potential"], thermo, baro))
         step += ph.n_steps
         for w in (traj, log):
             if w:
                 w.close()
         it.close()
-        if baro:
-            baro.close()
+        for c in (thermo, baro):
+            if c:
+                c.close()
     for o in (cons, ff, sys_):
         if o is not None:
             o.close()

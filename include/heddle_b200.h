@@ -71,6 +71,8 @@ typedef struct hb_forcefield hb_forcefield;
 typedef struct hb_constraints hb_constraints;
 typedef struct hb_integrator hb_integrator;
 typedef struct hb_barostat hb_barostat;
+typedef struct hb_thermostat hb_thermostat;
+typedef struct hb_pcouple hb_pcouple;
 typedef struct hb_batch hb_batch;
 typedef struct hb_shake_mlp hb_shake_mlp;
 
@@ -357,6 +359,83 @@ int hb_barostat_stats(hb_barostat *b, double out[15]);
  * number is a multiple of the barostat's frequency evaluates scalars and is
  * followed by a move (src/runner.rs:2693-2708). */
 int hb_integrator_set_barostat(hb_integrator *it, hb_barostat *b);
+
+/* ---- velocity thermostats for velocity Verlet: replace CsvrThermostat
+ * (src/integrator/csvr.rs:45-260, csvr_sample_and_factor /
+ * csvr_sample_partials / csvr_finish_from_partials in
+ * kernels/nose_hoover.cu:145-385), AndersenThermostat
+ * (src/integrator/andersen.rs:110-260, kernels/andersen.cu) and the
+ * Berendsen thermostat (src/integrator/berendsen.rs,
+ * berendsen_compute_factor in kernels/nose_hoover.cu:390-415).
+ * Each step, after the force evaluation and the constraint velocity
+ * projection and before the final half kick (the reference's composed
+ * post-force order, src/runner.rs:2661-2686):
+ *   CSVR:      K = sum m v^2 / 2 of the current velocities (FP64), then
+ *              K' = c K + (kT/2)(1 - c)(s + r^2) + 2 r sqrt(c (1 - c) K kT / 2)
+ *              with c = exp(-dt / tau), r and the g - 1 terms of s = sum xi^2
+ *              the Box-Muller normals of Philox (key seed, counter
+ *              (draw, 0, i, 0)), g = 3N - n_constraints - 3; factor
+ *              sqrt(K'/K) (1 when K' is not finite and positive or K = 0);
+ *   Berendsen: factor sqrt(max(0, 1 + dt/tau (g kT / 2K - 1)));
+ *   Andersen:  after the kick, every atom whose uniform (counter (draw, 0,
+ *              id, 3)) is below p = clamp(rate dt, 0, 1) gets the velocity
+ *              sqrt(kT / m) (xi_0, xi_1, xi_2) (counters (draw, 0, id, 0..2)).
+ * The draw counter lives on the device and advances once per step, so a
+ * captured step draws fresh numbers on every replay. */
+#define HB_THERMOSTAT_CSVR 0
+#define HB_THERMOSTAT_ANDERSEN 1
+#define HB_THERMOSTAT_BERENDSEN 2
+typedef struct {
+  int kind;                  /* HB_THERMOSTAT_* */
+  double temperature;        /* k_B T in hartree */
+  double tau;                /* coupling time (a.u.), CSVR and Berendsen */
+  double collision_rate;     /* collisions per a.u. time, Andersen */
+  uint64_t seed;
+  uint32_t n_constraints;    /* removed from the degrees of freedom */
+} hb_thermostat_desc;
+
+int hb_thermostat_create(hb_system *sys, const hb_thermostat_desc *desc, hb_thermostat **out);
+int hb_thermostat_destroy(hb_thermostat *t);
+/* out[0] cumulative injected energy sum (K' - K) (CSVR, Berendsen), [1] last
+ * K, [2] last factor, [3] last sum of squares s, [4] last r, [5] draws,
+ * [6] degrees of freedom g. */
+int hb_thermostat_stats(hb_thermostat *t, double out[7]);
+/* Attach (or detach with NULL) a thermostat; velocity Verlet only. */
+int hb_integrator_set_thermostat(hb_integrator *it, hb_thermostat *t);
+
+/* ---- per-step pressure coupling for velocity Verlet: replaces
+ * CRescaleBarostat (src/integrator/c_rescale_barostat.rs:60-300,
+ * c_rescale_compute_mu in kernels/barostat.cu:140-214) and the Berendsen
+ * barostat (src/integrator/berendsen_barostat.rs, berendsen_compute_mu in
+ * kernels/barostat.cu:216-255).  Every step evaluates energies and virial;
+ * after the constraint velocity projection, P = (2K + W) / 3V with W the
+ * force-field virial plus the constraint virial of the step, then
+ *   mu^3 = 1 - kappa dt/tau (P0 - P) [+ sqrt(2 kappa kT dt / (tau V)) r]
+ * (the noise term for c-rescale, r from Philox counter (draw, 0, 0, 0)),
+ * clamped below at 1e-18, the lattice scaled by mu (FP64) and, after the
+ * final half kick, every position scaled by mu about the origin.  A step
+ * that would take the narrowest perpendicular width below
+ * 2 (r_cut + r_skin) keeps mu = 1 and counts a guard. */
+#define HB_PCOUPLE_C_RESCALE 0
+#define HB_PCOUPLE_BERENDSEN 1
+typedef struct {
+  int kind;                  /* HB_PCOUPLE_* */
+  double pressure;           /* hartree / bohr^3 */
+  double temperature;        /* k_B T in hartree (c-rescale noise) */
+  double tau;                /* coupling time, a.u. */
+  double compressibility;    /* bohr^3 / hartree */
+  uint64_t seed;
+} hb_pcouple_desc;
+
+int hb_pcouple_create(hb_system *sys, const hb_pcouple_desc *desc, hb_pcouple **out);
+int hb_pcouple_destroy(hb_pcouple *p);
+/* out[0] last pressure, [1] volume after the last step, [2] cumulative
+ * P0 dV, [3] last mu, [4] draws, [5] last K, [6] last W, [7] guarded
+ * steps. */
+int hb_pcouple_stats(hb_pcouple *p, double out[8]);
+/* Attach (or detach with NULL); velocity Verlet only, and not together
+ * with a Monte-Carlo barostat. */
+int hb_integrator_set_pcouple(hb_integrator *it, hb_pcouple *p);
 
 /* ---- batched replicas: the runner's captured-graph replay
  * (src/runner.rs:2803-3000, src/gpu/graph.rs:222-242) extended to many

@@ -5,6 +5,9 @@ tests/test_gpu_run.py (SI units, extended XYZ, topology files):
   water.in.toml / water.in.xyz / water.in.topology
                                  216 SPC waters (SETTLE), SPME, Langevin,
                                  Monte-Carlo barostat
+  water_cr.in.toml              the same waters (water.in.xyz / .topology),
+                                 velocity Verlet + SETTLE with a CSVR
+                                 thermostat and c-rescale pressure coupling
   chain.in.toml / chain.in.xyz / chain.in.topology
                                  a 14-atom bonded chain (harmonic bonds and
                                  angles, periodic dihedrals, SHAKE X-H
@@ -154,6 +157,46 @@ pressure = 1.0e5
 temperature = 300.0
 frequency = 10
 seed = 7
+
+[phase.output]
+trajectory_every = 30
+include_images = true
+log_every = 10
+
+''' + WATER_TYPES)
+
+
+def water_cr():
+    (HERE / "water_cr.in.toml").write_text('''schema_version = 1
+init = "water.in.xyz"
+topology = "water.in.topology"
+
+[simulation]
+seed = 2
+temperature = 300.0
+
+[[phase]]
+name = "npt"
+n_steps = 60
+dt = 2.0e-15
+
+[phase.integrator]
+kind = "velocity-verlet"
+lossless = false
+
+[phase.thermostat]
+kind = "csvr"
+temperature = 300.0
+tau = 1.0e-13
+seed = 11
+
+[phase.barostat]
+kind = "c-rescale"
+pressure = 1.0e5
+temperature = 300.0
+tau = 1.0e-12
+compressibility = 4.5e-10
+seed = 13
 
 [phase.output]
 trajectory_every = 30
@@ -315,4 +358,5 @@ between = ["O", "O"]'''))
 if __name__ == "__main__":
     argon()
     water()
+    water_cr()
     chain()

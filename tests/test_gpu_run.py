@@ -33,12 +33,16 @@ def test_argon_run_is_byte_identical_and_conserves_energy(ctx, tmp_path):
         assert [p.name for p in paths] == ["argon.out.run.xyz", "argon.out.run.log"]
         outs.append([p.read_bytes() for p in paths])
     assert outs[0] == outs[1]
-    log = np.loadtxt(tmp_path / "r0" / "argon.out.run.log", delimiter=",", skiprows=1)
-    e_tot = log[:, 2] + log[:, 4]  # kinetic + potential (J)
-    # hard LJ cutoff (r_switch = cutoff) and dt = 5 fs: bounded fluctuation, no drift
-    assert np.ptp(e_tot) < 2e-2 * np.abs(log[:, 4]).mean()
+    logf = tmp_path / "r0" / "argon.out.run.log"
+    # an NVE phase logs only the base columns (src/io/log_output.rs:40-60)
+    assert logf.read_text().splitlines()[0] == "step,time,kinetic_energy,temperature"
+    log = np.loadtxt(logf, delimiter=",", skiprows=1)
     last = read_xyz(tmp_path / "r0" / "argon.out.run.xyz", index=-1)
     assert last.step == 100 and last.velocities is not None
+    # the logged kinetic energy (J) is that of the written velocities
+    m = 6.6335e-26
+    ke = 0.5 * m * float((last.velocities ** 2).sum()) * (5.29177210903e-11 / 2.4188843265857195e-17) ** 2
+    assert log[-1, 0] == 100 and log[-1, 2] == pytest.approx(ke, rel=1e-6)
 
 
 def test_water_npt_run(ctx, tmp_path):
@@ -54,6 +58,31 @@ def test_water_npt_run(ctx, tmp_path):
     d = p[:, 1] - p[:, 0]
     d -= last.box[:3] * np.round(d / last.box[:3])
     assert np.abs(np.linalg.norm(d, axis=1) - 1.8897261246).max() < 1e-4
+
+
+def test_water_csvr_c_rescale_run(ctx, tmp_path):
+    for f in CFG.glob("water.in.*"):
+        shutil.copy(f, tmp_path / f.name)
+    cfg = staged(tmp_path, "water_cr")
+    paths = R.run(cfg, ctx=ctx)
+    assert [p.name for p in paths] == ["water_cr.out.npt.xyz", "water_cr.out.npt.log"]
+    lines = (tmp_path / "water_cr.out.npt.log").read_text().splitlines()
+    assert lines[0] == ("step,time,kinetic_energy,temperature,csvr_conserved,pressure,box_volume,"
+                        "c_rescale_conserved")
+    log = np.loadtxt(tmp_path / "water_cr.out.npt.log", delimiter=",", skiprows=1)
+    assert list(log[:, 0]) == [10, 20, 30, 40, 50, 60]
+    first = read_xyz(load_config(cfg).init)
+    last = read_xyz(tmp_path / "water_cr.out.npt.xyz", index=-1)
+    # box_volume is written in bohr^3, like the reference's Dimensionless column
+    v_last = float(np.prod(last.box[:3]))
+    assert log[-1, 6] == pytest.approx(v_last, rel=1e-8)
+    assert not np.allclose(last.box, first.box)
+    p = last.positions.reshape(-1, 3, 3)
+    d = p[:, 1] - p[:, 0]
+    d -= last.box[:3] * np.round(d / last.box[:3])
+    # positions are scaled atom by atom after the constraint step (the
+    # reference's c-rescale fragment), so bonds carry the last mu
+    assert np.abs(np.linalg.norm(d, axis=1) / 1.8897261246 - 1.0).max() < 2e-3
 
 
 def test_bonded_chain_run(ctx, tmp_path):

@@ -39,6 +39,13 @@ def test_config_units_are_converted_to_atomic():
     assert w.phases[0].barostat["pressure"] == pytest.approx(1.0e5 / U.PRESSURE_PA)
     assert w.spme["alpha"] == pytest.approx(4.4620e9 * U.BOHR_M)
     assert w.constraint_types["SPC"]["kind"] == "settle"
+    cr = load_config(CFG / "water_cr.in.toml").phases[0]
+    assert cr.thermostat == {"kind": "csvr", "temperature": pytest.approx(U.temperature_au_k(300.0)),
+                             "tau": pytest.approx(1.0e-13 / U.AUT_S), "seed": 11}
+    assert cr.barostat["kind"] == "c-rescale" and cr.barostat["seed"] == 13
+    assert cr.barostat["tau"] == pytest.approx(1.0e-12 / U.AUT_S)
+    # inverse pressure: 4.5e-10 / Pa in bohr^3 / hartree
+    assert cr.barostat["compressibility"] == pytest.approx(4.5e-10 * U.PRESSURE_PA)
     ch = load_config(CFG / "chain.in.toml")
     assert ch.bond_types["CC"]["k"] == pytest.approx(U.energy_au_j(4.3e2) * U.BOHR_M ** 2)
     assert ch.dihedral_types["X"]["n"] == 3
@@ -46,8 +53,13 @@ def test_config_units_are_converted_to_atomic():
 
 
 @pytest.mark.parametrize("patch,message", [
-    ("[phase.thermostat]\nkind = \"csvr\"\n", "thermostat kind 'csvr'"),
-    ("[phase.barostat]\nkind = \"c-rescale\"\n", "barostat kind 'c-rescale'"),
+    ("[phase.thermostat]\nkind = \"nose-hoover-chain\"\n", "thermostat kind 'nose-hoover-chain'"),
+    ("[phase.barostat]\nkind = \"mtk-npt\"\npressure = 1.0e5\n", "barostat kind 'mtk-npt'"),
+    ("[phase.thermostat]\nkind = \"csvr\"\ntemperature = 300.0\nseed = 1\n", "missing `tau`"),
+    ("[phase.thermostat]\nkind = \"andersen\"\ntemperature = 300.0\ncollision_rate = -1.0\nseed = 1\n",
+     "collision_rate"),
+    ("[phase.barostat]\nkind = \"c-rescale\"\npressure = 1.0e5\ntau = 1e-12\ncompressibility = 0.0\n"
+     "temperature = 300.0\nseed = 1\n", "compressibility"),
 ])
 def test_unsupported_slots_are_rejected(tmp_path, patch, message):
     text = (CFG / "argon.in.toml").read_text().replace("[phase.output]", patch + "\n[phase.output]")
@@ -56,6 +68,29 @@ def test_unsupported_slots_are_rejected(tmp_path, patch, message):
     p.write_text(text)
     with pytest.raises(ConfigError, match=message):
         load_config(p)
+
+
+def test_thermostat_needs_velocity_verlet(tmp_path):
+    (tmp_path / "water.in.xyz").write_text((CFG / "water.in.xyz").read_text())
+    (tmp_path / "water.in.topology").write_text((CFG / "water.in.topology").read_text())
+    text = (CFG / "water.in.toml").read_text().replace(
+        "[phase.barostat]", "[phase.thermostat]\nkind = \"berendsen\"\ntemperature = 300.0\n"
+        "tau = 1.0e-13\n\n[phase.barostat]")
+    p = tmp_path / "w.in.toml"
+    p.write_text(text)
+    with pytest.raises(ConfigError, match="velocity-verlet"):
+        load_config(p)
+
+
+def test_log_columns_follow_the_reference_slots():
+    from heddle_b200.run import log_columns
+    w = load_config(CFG / "water.in.toml").phases[0]
+    assert [c for c, _ in log_columns(w)] == ["box_volume", "mc_acceptance", "mc_volume_step",
+                                              "mc_conserved"]
+    cr = load_config(CFG / "water_cr.in.toml").phases[0]
+    assert log_columns(cr) == [("csvr_conserved", "energy"), ("pressure", "pressure"),
+                               ("box_volume", "dimensionless"), ("c_rescale_conserved", "energy")]
+    assert log_columns(load_config(CFG / "argon.in.toml").phases[0]) == []
 
 
 def test_bad_values_are_rejected(tmp_path):

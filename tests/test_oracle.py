@@ -262,3 +262,62 @@ def test_mlp_oracle_gradients_match_finite_differences():
         assert abs(g[q] - fd) <= 1e-6 * max(1.0, abs(fd)), q
     # bf16 rounding is round-to-nearest-even on the top 16 bits
     assert M.bf16(1.0 + 2.0 ** -8) == 1.0 and M.bf16(1.0 + 3 * 2.0 ** -8) == 1.0 + 2.0 ** -6
+
+
+def test_coupling_philox_matches_the_pinned_c_oracle():
+    from oracle import coupling as OC
+    rng = np.random.default_rng(5)
+    for _ in range(20):
+        seed = int(rng.integers(0, 2 ** 63))
+        ctr = rng.integers(0, 2 ** 32, size=4, dtype=np.uint64)
+        o = OC.philox(seed, *ctr)
+        ref = O.philox(seed & 0xFFFFFFFF, seed >> 32, ctr.astype(np.uint32))
+        assert [int(x) for x in o] == [int(x) for x in ref]
+        draw = int(rng.integers(0, 2 ** 40))
+        i = int(rng.integers(0, 2 ** 32))
+        assert OC.normal(seed, draw, i, 2) == pytest.approx(O.philox_gaussian(seed, draw, i, 2),
+                                                            rel=1e-15, abs=1e-15)
+
+
+def test_csvr_chain_samples_the_canonical_kinetic_energy():
+    """Iterating the CSVR map leaves K Gamma(g/2, kT)-distributed: mean
+    g kT / 2 and variance g (kT)^2 / 2 (Bussi et al. 2007)."""
+    from oracle import coupling as OC
+    g, kt = 12, 1.0
+    k, ks = 0.1, []
+    for draw in range(6000):
+        k = OC.csvr(k, g, kt, 1.0, 5.0, 3, draw)["k_new"]
+        ks.append(k)
+    ks = np.array(ks[500:])
+    assert ks.mean() == pytest.approx(0.5 * g * kt, rel=0.06)
+    assert ks.var() == pytest.approx(0.5 * g * kt * kt, rel=0.25)
+    # no coupling (tau -> infinity): factor 1
+    assert OC.csvr(3.0, g, kt, 1.0, 1e30, 3, 0)["factor"] == pytest.approx(1.0, abs=1e-12)
+
+
+def test_berendsen_andersen_and_pressure_coupling_limits():
+    from oracle import coupling as OC
+    f, inj = OC.berendsen_thermostat(2.0, 4, 1.0, 0.1, 1.0)  # K_target = 2: no change
+    assert f == 1.0 and inj == 0.0
+    f, inj = OC.berendsen_thermostat(4.0, 4, 1.0, 0.1, 1.0)
+    assert f * f == pytest.approx(1.0 + 0.1 * (0.5 - 1.0)) and inj == pytest.approx(4.0 * (f * f - 1.0))
+    rng = np.random.default_rng(2)
+    v = rng.normal(size=(2000, 3))
+    inv_m = np.full(2000, 0.5)
+    same, hit = OC.andersen(v, inv_m, 2.0, 0.0, 7, 3)
+    assert not hit.any() and np.array_equal(same, v)
+    new, hit = OC.andersen(v, inv_m, 2.0, 1.0, 7, 3)
+    assert hit.all() and new.std() == pytest.approx(1.0, rel=0.05)  # sqrt(kT / m)
+    part, hit = OC.andersen(v, inv_m, 2.0, 0.25, 7, 3)
+    assert 0.2 < hit.mean() < 0.3 and np.array_equal(part[~hit], v[~hit])
+    box = np.array([30.0, 30.0, 30.0, 0.0, 0.0, 0.0])
+    # P = P0 without noise: mu = 1
+    k, w = 10.0, 50.0
+    p = (2 * k + w) / (3 * 27000.0)
+    b = OC.pressure_coupling("berendsen", k, w, box, p, 1.0, 1.0, 10.0, 2.0, 0, 0)
+    assert b["mu"] == pytest.approx(1.0, abs=1e-15)
+    # higher pressure than the target expands the box
+    assert OC.pressure_coupling("berendsen", k, w, box, 0.5 * p, 1.0, 1.0, 10.0, 2.0, 0, 0)["mu"] > 1.0
+    # the width guard keeps mu = 1 below 2 r_search
+    g = OC.pressure_coupling("berendsen", k, w, box, 100.0, 1.0, 1.0, 10.0, 2.0, 0, 0, r_search=14.99)
+    assert g["mu"] == 1.0
