@@ -14,6 +14,7 @@ from .api import (  # noqa: F401
     HarmonicAngleParams,
     HarmonicBondParams,
     LennardJonesParams,
+    Minimizer,
     PeriodicDihedralParams,
     PotentialRegistry,
     PressureCoupling,
@@ -27,5 +28,5 @@ __all__ = [
     "Context", "System", "ForceField", "Constraints", "Integrator", "Barostat", "Batch",
     "PotentialRegistry", "LennardJonesParams", "SpmeParams", "HarmonicBondParams",
     "HarmonicAngleParams", "PeriodicDihedralParams", "ShakeMLP", "Thermostat",
-    "PressureCoupling", "HeddleError", "load",
+    "PressureCoupling", "Minimizer", "HeddleError", "load",
 ]

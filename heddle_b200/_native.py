@@ -89,6 +89,29 @@ class PcoupleDesc(C.Structure):
     ]
 
 
+class MinimizerDesc(C.Structure):
+    _fields_ = [
+        ("initial_step", C.c_double),
+        ("max_step", C.c_double),
+        ("step_increase", C.c_double),
+        ("step_decrease", C.c_double),
+        ("force_tolerance", C.c_double),
+        ("energy_tolerance", C.c_double),
+        ("max_iterations", C.c_uint64),
+    ]
+
+
+class MinReport(C.Structure):
+    _fields_ = [
+        ("iteration", C.c_uint64),
+        ("energy", C.c_double),
+        ("max_force", C.c_double),
+        ("step", C.c_double),
+        ("accepted", C.c_int),
+        ("converged", C.c_int),
+    ]
+
+
 class ForceFieldDesc(C.Structure):
     _fields_ = [
         ("lj_enabled", C.c_int),
@@ -219,6 +242,10 @@ SIGNATURES = {
     "hb_pcouple_destroy": (C.c_int, [VP]),
     "hb_pcouple_stats": (C.c_int, [VP, PD]),
     "hb_integrator_set_pcouple": (C.c_int, [VP, VP]),
+    "hb_minimizer_create": (C.c_int, [VP, VP, C.POINTER(MinimizerDesc), PVP]),
+    "hb_minimizer_destroy": (C.c_int, [VP]),
+    "hb_minimizer_begin": (C.c_int, [VP, C.POINTER(MinReport)]),
+    "hb_minimizer_iterate": (C.c_int, [VP, C.c_uint32, C.POINTER(MinReport), C.POINTER(C.c_uint32)]),
     "hb_batch_create": (C.c_int, [VP, C.c_uint32, PVP, PVP, PVP, PVP]),
     "hb_batch_destroy": (C.c_int, [VP]),
     "hb_batch_step": (C.c_int, [VP, C.c_uint32]),

@@ -22,6 +22,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _native as N
+from . import units as U
 from .systems import SystemSpec
 
 
@@ -597,6 +598,71 @@ class Barostat:
     def close(self) -> None:
         if getattr(self, "h", None):
             self.lib.hb_barostat_destroy(self.h)
+            self.h = None
+
+
+MIN_REASONS = {1: "force_tolerance", 2: "energy_tolerance", 3: "force_zero"}
+
+
+class Minimizer:
+    """Steepest-descent minimisation ("steepest-descent") of ff's energy with
+    cons' groups projected after every trial step; lengths in bohr, forces
+    in hartree/bohr, energy_tolerance relative.  Defaults are the
+    reference's (initial_step 1e-12 m, max_step 1e-10 m, x1.2 / x0.2,
+    force_tolerance 1e-10 N, energy_tolerance 1e-7, 1000 iterations)."""
+
+    def __init__(self, ff: ForceField, cons: "Constraints | None" = None,
+                 initial_step: float = 1.0e-12 / U.BOHR_M,
+                 max_step: float = 1.0e-10 / U.BOHR_M, step_increase: float = 1.2,
+                 step_decrease: float = 0.2, force_tolerance: float = 1.0e-10 / U.FORCE_N,
+                 energy_tolerance: float = 1.0e-7, max_iterations: int = 1000):
+        self.ff = ff
+        self.lib = ff.lib
+        d = N.MinimizerDesc()
+        d.initial_step = float(initial_step)
+        d.max_step = float(max_step)
+        d.step_increase = float(step_increase)
+        d.step_decrease = float(step_decrease)
+        d.force_tolerance = float(force_tolerance)
+        d.energy_tolerance = float(energy_tolerance)
+        d.max_iterations = int(max_iterations)
+        self.max_iterations = int(max_iterations)
+        h = C.c_void_p()
+        N.check(self.lib.hb_minimizer_create(ff.h, cons.h if cons else None, C.byref(d), C.byref(h)))
+        self.h = h
+
+    @staticmethod
+    def _row(r) -> dict:
+        return {"iteration": int(r.iteration), "energy": r.energy, "max_force": r.max_force,
+                "step": r.step, "accepted": bool(r.accepted),
+                "converged": MIN_REASONS.get(int(r.converged))}
+
+    def begin(self) -> dict:
+        """Forces and energy at the current positions: the iteration-0 report."""
+        r = N.MinReport()
+        N.check(self.lib.hb_minimizer_begin(self.h, C.byref(r)))
+        return self._row(r)
+
+    def iterate(self, n: int) -> list:
+        """Up to n iterations (fewer at convergence or max_iterations)."""
+        buf = (N.MinReport * max(int(n), 1))()
+        done = C.c_uint32(0)
+        N.check(self.lib.hb_minimizer_iterate(self.h, int(n), buf, C.byref(done)))
+        return [self._row(buf[k]) for k in range(done.value)]
+
+    def run(self, chunk: int = 64) -> list:
+        """begin() then iterations until convergence or max_iterations; all reports."""
+        out = [self.begin()]
+        while out[-1]["converged"] is None and out[-1]["iteration"] < self.max_iterations:
+            rows = self.iterate(chunk)
+            if not rows:
+                break
+            out += rows
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.hb_minimizer_destroy(self.h)
             self.h = None
 
 

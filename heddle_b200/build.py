@@ -22,7 +22,7 @@ LIB = PKG / "libheddle_b200.so"
 INCLUDE = PKG.parent / "include"
 
 SOURCES = ["hb_api.cu", "hb_nlist.cu", "hb_pair.cu", "hb_spme.cu", "hb_integ.cu", "hb_cons.cu",
-           "hb_baro.cu", "hb_bonded.cu", "hb_mlp.cu", "hb_couple.cu"]
+           "hb_baro.cu", "hb_bonded.cu", "hb_mlp.cu", "hb_couple.cu", "hb_min.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [

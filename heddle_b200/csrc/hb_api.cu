@@ -972,6 +972,112 @@ extern "C" int hb_barostat_mc_move(hb_barostat *b, hb_forcefield *ff) {
   return check_status(ff);
 }
 
+// ---------------------------------------------------------------------
+// steepest-descent minimiser
+// ---------------------------------------------------------------------
+extern "C" int hb_minimizer_create(hb_forcefield *ff, hb_constraints *cons,
+                                   const hb_minimizer_desc *d, hb_minimizer **out) {
+  HB_REQUIRE(ff && d && out, HB_ERR_INVALID_ARGUMENT, "null argument");
+  HB_REQUIRE(!cons || cons->sys == ff->sys, HB_ERR_INVALID_ARGUMENT,
+             "force field and constraints must share one system");
+  // the reference's schema checks (steepest_descent.rs:300-380)
+  HB_REQUIRE(std::isfinite(d->initial_step) && d->initial_step > 0.0, HB_ERR_INVALID_ARGUMENT,
+             "minimization.algorithm.initial_step: expected finite and strictly positive");
+  HB_REQUIRE(std::isfinite(d->max_step) && d->max_step > 0.0, HB_ERR_INVALID_ARGUMENT,
+             "minimization.algorithm.max_step: expected finite and strictly positive");
+  HB_REQUIRE(d->max_step >= d->initial_step, HB_ERR_INVALID_ARGUMENT,
+             "minimization.algorithm.max_step must be >= initial_step");
+  HB_REQUIRE(std::isfinite(d->step_increase) && d->step_increase >= 1.0, HB_ERR_INVALID_ARGUMENT,
+             "minimization.algorithm.step_increase must be finite and >= 1.0");
+  HB_REQUIRE(std::isfinite(d->step_decrease) && d->step_decrease > 0.0 && d->step_decrease < 1.0,
+             HB_ERR_INVALID_ARGUMENT,
+             "minimization.algorithm.step_decrease must be finite and in (0.0, 1.0)");
+  HB_REQUIRE(std::isfinite(d->force_tolerance) && d->force_tolerance >= 0.0,
+             HB_ERR_INVALID_ARGUMENT,
+             "minimization.algorithm.force_tolerance must be finite and >= 0.0");
+  HB_REQUIRE(std::isfinite(d->energy_tolerance) && d->energy_tolerance >= 0.0,
+             HB_ERR_INVALID_ARGUMENT,
+             "minimization.algorithm.energy_tolerance must be finite and >= 0.0");
+  HB_REQUIRE(d->max_iterations > 0, HB_ERR_INVALID_ARGUMENT,
+             "minimization.algorithm.max_iterations must be strictly positive");
+  hb_minimizer *m = new hb_minimizer();
+  m->ff = ff;
+  m->cons = cons;
+  m->initial_step = (float)d->initial_step;
+  m->max_step = (float)d->max_step;
+  m->inc = (float)d->step_increase;
+  m->dec = (float)d->step_decrease;
+  m->ftol = d->force_tolerance;
+  m->etol = d->energy_tolerance;
+  m->max_iter = d->max_iterations;
+  const int rc = min_alloc(m);
+  if (rc != HB_OK) {
+    std::string msg = hb_last_error();
+    hb_minimizer_destroy(m);
+    return hb_fail(rc, msg);
+  }
+  *out = m;
+  return HB_OK;
+}
+
+extern "C" int hb_minimizer_destroy(hb_minimizer *m) {
+  if (!m) return HB_OK;
+  cudaStreamSynchronize(m->ff->sys->ctx->stream);
+  min_free(m);
+  delete m;
+  return HB_OK;
+}
+
+extern "C" int hb_minimizer_begin(hb_minimizer *m, hb_min_report *out) {
+  HB_REQUIRE(m && out, HB_ERR_INVALID_ARGUMENT, "null argument");
+  hb_forcefield *ff = m->ff;
+  cudaStream_t s = ff->sys->ctx->stream;
+  ff->sys->fix_valid = false;
+  HB_TRY(force_eval(ff, true));
+  HB_TRY(min_init(m, s));
+  HB_CUDA(cudaMemcpyAsync(out, m->d_rep, sizeof(hb_min_report), cudaMemcpyDeviceToHost, s));
+  HB_CUDA(cudaStreamSynchronize(s));
+  HB_TRY(check_status(ff));
+  m->begun = true;
+  m->done = 0;
+  m->converged = out->converged;
+  return HB_OK;
+}
+
+extern "C" int hb_minimizer_iterate(hb_minimizer *m, uint32_t n, hb_min_report *out,
+                                    uint32_t *n_done) {
+  HB_REQUIRE(m && n_done && (out || n == 0), HB_ERR_INVALID_ARGUMENT, "null argument");
+  HB_REQUIRE(m->begun, HB_ERR_INVALID_ARGUMENT, "hb_minimizer_begin must come first");
+  *n_done = 0;
+  hb_forcefield *ff = m->ff;
+  cudaStream_t s = ff->sys->ctx->stream;
+  ff->sys->fix_valid = false;
+  while (n > 0 && !m->converged && m->done < m->max_iter) {
+    uint32_t chunk = std::min<uint64_t>({(uint64_t)n, (uint64_t)m->rep_cap, m->max_iter - m->done});
+    MinState before, after;
+    HB_CUDA(cudaMemcpyAsync(&before, m->d_st, sizeof(MinState), cudaMemcpyDeviceToHost, s));
+    for (uint32_t k = 0; k < chunk; ++k) {
+      HB_TRY(min_trial(m, s));
+      if (m->cons) HB_TRY(cons_project(m->cons, &m->d_st->skip, s));
+      HB_TRY(force_eval(ff, true));
+      HB_TRY(min_finish(m, k, s));
+    }
+    HB_CUDA(cudaMemcpyAsync(&after, m->d_st, sizeof(MinState), cudaMemcpyDeviceToHost, s));
+    HB_CUDA(cudaStreamSynchronize(s));
+    const uint32_t got = (uint32_t)(after.iteration - before.iteration);
+    if (got)
+      HB_CUDA(cudaMemcpy(out + *n_done, m->d_rep, sizeof(hb_min_report) * got,
+                         cudaMemcpyDeviceToHost));
+    HB_TRY(check_status(ff));
+    *n_done += got;
+    m->done += got;
+    n -= chunk;
+    m->converged = after.converged;
+    if (got < chunk && !after.converged) break;  // F_max = 0 at a rejected state
+  }
+  return HB_OK;
+}
+
 extern "C" int hb_integrator_set_barostat(hb_integrator *it, hb_barostat *b) {
   HB_REQUIRE(it, HB_ERR_INVALID_ARGUMENT, "null integrator");
   HB_REQUIRE(!b || b->sys == it->sys, HB_ERR_INVALID_ARGUMENT,

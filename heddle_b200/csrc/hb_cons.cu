@@ -389,6 +389,117 @@ __global__ void k_shake_pos(const uint32_t *__restrict__ aoff, const uint32_t *_
   }
 }
 
+// Position-only projection (the minimizer's apply_position_projection_only,
+// settle_positions_no_velocity kernels/settle.cu:519-584 and
+// shake_positions_no_velocity kernels/shake.cu:558-697): Gauss-Seidel
+// sweeps with gradient directions taken at the current off-manifold
+// positions, FP64, |r^2 - d^2| below tol (absolute, or relative to d^2),
+// at most max_iter sweeps; no velocity change, no virial.  skip (optional):
+// a device flag that turns the launch into a no-op.
+__device__ void project_group(uint32_t nc, const uint32_t *ci, const uint32_t *cj,
+                              const double *tgt, const double *im, double (*xc)[3], double tol,
+                              int rel, int max_iter) {
+  double g[SHAKE_MAX_CONS][3];
+  for (uint32_t k = 0; k < nc; ++k)
+    for (int d = 0; d < 3; ++d) g[k][d] = xc[ci[k]][d] - xc[cj[k]][d];
+  for (int it = 0; it < max_iter; ++it) {
+    bool conv = true;
+    for (uint32_t k = 0; k < nc; ++k) {
+      const uint32_t i = ci[k], j = cj[k];
+      const double dx = xc[i][0] - xc[j][0], dy = xc[i][1] - xc[j][1], dz = xc[i][2] - xc[j][2];
+      const double sigma = dx * dx + dy * dy + dz * dz - tgt[k];
+      if (fabs(sigma) > (rel ? tol * tgt[k] : tol)) {
+        conv = false;
+        const double den = 2.0 * (dx * g[k][0] + dy * g[k][1] + dz * g[k][2]) * (im[i] + im[j]);
+        if (den == 0.0) continue;
+        const double lam = sigma / den;
+        for (int d = 0; d < 3; ++d) {
+          xc[i][d] -= lam * im[i] * g[k][d];
+          xc[j][d] += lam * im[j] * g[k][d];
+        }
+      }
+    }
+    if (conv) break;
+  }
+}
+
+__global__ void k_settle_project(const uint4 *__restrict__ at, const float4 *__restrict__ geom,
+                                 const float2 *__restrict__ mass, float4 *__restrict__ posq,
+                                 const DBox *__restrict__ box, double tol, int max_iter,
+                                 const int *__restrict__ skip, uint32_t ng) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ng || (skip && *skip)) return;
+  const DBox bx = *box;
+  const uint4 a = at[g];
+  const uint32_t id[3] = {a.x, a.y, a.z};
+  const float4 gm = geom[g];
+  const float2 m = mass[g];
+  const double ra = gm.x, rb = gm.y, rc = gm.z;
+  const double tgt[3] = {(ra + rb) * (ra + rb) + rc * rc, (ra + rb) * (ra + rb) + rc * rc,
+                         4.0 * rc * rc};
+  const double im[3] = {m.x > 0.f ? 1.0 / m.x : 0.0, m.y > 0.f ? 1.0 / m.y : 0.0,
+                        m.y > 0.f ? 1.0 / m.y : 0.0};
+  const uint32_t ci[3] = {0, 0, 1}, cj[3] = {1, 2, 2};
+  const float4 p0 = posq[id[0]];
+  double xc[SHAKE_MAX_ATOMS][3], xu[3][3];
+  for (int q = 0; q < 3; ++q) {
+    const float4 p = posq[id[q]];
+    const V3 d = mi(v3(p.x - p0.x, p.y - p0.y, p.z - p0.z), bx);
+    xu[q][0] = xc[q][0] = d.x;
+    xu[q][1] = xc[q][1] = d.y;
+    xu[q][2] = xc[q][2] = d.z;
+  }
+  project_group(3, ci, cj, tgt, im, xc, tol, 0, max_iter);
+  for (int q = 0; q < 3; ++q) {
+    float4 p = posq[id[q]];
+    p.x += (float)(xc[q][0] - xu[q][0]);
+    p.y += (float)(xc[q][1] - xu[q][1]);
+    p.z += (float)(xc[q][2] - xu[q][2]);
+    posq[id[q]] = p;
+  }
+}
+
+__global__ void k_shake_project(const uint32_t *__restrict__ aoff, const uint32_t *__restrict__ atoms,
+                                const uint32_t *__restrict__ coff, const uint2 *__restrict__ pairs,
+                                const double *__restrict__ d2, float4 *__restrict__ posq,
+                                const float4 *__restrict__ vel, const DBox *__restrict__ box,
+                                double tol, int rel, int max_iter, const int *__restrict__ skip,
+                                uint32_t ng) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ng || (skip && *skip)) return;
+  const DBox bx = *box;
+  const uint32_t a0 = aoff[g], na = aoff[g + 1] - a0;
+  const uint32_t c0 = coff[g], nc = coff[g + 1] - c0;
+  double xc[SHAKE_MAX_ATOMS][3], xu[SHAKE_MAX_ATOMS][3], im[SHAKE_MAX_ATOMS];
+  const float4 p0 = posq[atoms[a0]];
+  for (uint32_t a = 0; a < na; ++a) {
+    const uint32_t id = atoms[a0 + a];
+    const float4 p = posq[id];
+    im[a] = (double)vel[id].w;
+    const V3 d = mi(v3(p.x - p0.x, p.y - p0.y, p.z - p0.z), bx);
+    xu[a][0] = xc[a][0] = d.x;
+    xu[a][1] = xc[a][1] = d.y;
+    xu[a][2] = xc[a][2] = d.z;
+  }
+  uint32_t ci[SHAKE_MAX_CONS], cj[SHAKE_MAX_CONS];
+  double tgt[SHAKE_MAX_CONS];
+  for (uint32_t k = 0; k < nc; ++k) {
+    const uint2 pr = pairs[c0 + k];
+    ci[k] = pr.x;
+    cj[k] = pr.y;
+    tgt[k] = d2[c0 + k];
+  }
+  project_group(nc, ci, cj, tgt, im, xc, tol, rel, max_iter);
+  for (uint32_t a = 0; a < na; ++a) {
+    const uint32_t id = atoms[a0 + a];
+    float4 p = posq[id];
+    p.x += (float)(xc[a][0] - xu[a][0]);
+    p.y += (float)(xc[a][1] - xu[a][1]);
+    p.z += (float)(xc[a][2] - xu[a][2]);
+    posq[id] = p;
+  }
+}
+
 __global__ void k_rattle_vel(const uint32_t *__restrict__ aoff, const uint32_t *__restrict__ atoms,
                              const uint32_t *__restrict__ coff, const uint2 *__restrict__ pairs,
                              const float4 *__restrict__ posq, float4 *__restrict__ vel,
@@ -486,6 +597,23 @@ int cons_positions(hb_constraints *c, double dt, cudaStream_t s) {
         (rec && !pred) ? c->d_feat : nullptr, c->d_lam1, c->d_lsc, rec ? c->d_lam : nullptr, 0,
         c->n_shake);
   }
+  HB_CUDA(cudaGetLastError());
+  return HB_OK;
+}
+
+int cons_project(hb_constraints *c, const int *skip, cudaStream_t s) {
+  hb_system *sys = c->sys;
+  // the reference's projection tolerance for SETTLE groups (SETTLE_TOL2,
+  // kernels/settle.cu:105); SHAKE groups keep their configured tolerance
+  if (c->n_settle)
+    k_settle_project<<<hb_div_up(c->n_settle, 128), 128, 0, s>>>(
+        c->d_settle_atoms, c->d_settle_geom, c->d_settle_mass, sys->d_posq, sys->d_box, 3.57e-6,
+        32, skip, c->n_settle);
+  if (c->n_shake)
+    k_shake_project<<<hb_div_up(c->n_shake, 64), 64, 0, s>>>(
+        c->d_shake_aoff, c->d_shake_atoms, c->d_shake_coff, c->d_shake_pairs, c->d_shake_d2,
+        sys->d_posq, sys->d_vel, sys->d_box, c->shake_tol, c->shake_rel, (int)c->shake_max_iter,
+        skip, c->n_shake);
   HB_CUDA(cudaGetLastError());
   return HB_OK;
 }

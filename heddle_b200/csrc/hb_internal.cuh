@@ -432,6 +432,33 @@ struct hb_pcouple {
   double *d_part = nullptr;   // partial sums of the constraint virial
 };
 
+// Device state of the steepest-descent minimiser (hb_min.cu)
+struct MinState {
+  double last_energy;      // energy of the accepted configuration
+  double prev_energy;      // accepted energy before the current iteration
+  double e_trial;
+  float step, step_used, fmax, scale;
+  int skip, reject, converged, pad;
+  unsigned long long iteration;
+};
+
+struct hb_minimizer {
+  hb_forcefield *ff = nullptr;
+  hb_constraints *cons = nullptr;
+  float initial_step = 0.f, max_step = 0.f, inc = 1.f, dec = 0.5f;
+  double ftol = 0.0, etol = 0.0;
+  uint64_t max_iter = 0, done = 0;
+  bool begun = false;
+  int converged = 0;
+  MinState *d_st = nullptr;
+  hb_min_report *d_rep = nullptr;   // [rep_cap] reports of the current call
+  uint32_t rep_cap = 256;
+  float *d_part = nullptr;          // per-block |F|^2 maxima
+  float4 *d_snap_pos = nullptr, *d_snap_force = nullptr;
+  int4 *d_snap_img = nullptr;
+  double *d_snap_scal = nullptr;
+};
+
 // ---------------------------------------------------------------------
 // internal entry points implemented across the translation units
 // ---------------------------------------------------------------------
@@ -488,6 +515,14 @@ int mlp_infer(hb_shake_mlp *m, const float *d_feat, uint32_t n, float *d_out, cu
 // constraints (hb_cons.cu)
 int cons_positions(hb_constraints *c, double dt, cudaStream_t s);
 int cons_velocities(hb_constraints *c, double dt, bool virial, cudaStream_t s);
+// position-only projection (minimiser); skip: optional device no-op flag
+int cons_project(hb_constraints *c, const int *skip, cudaStream_t s);
+// steepest descent (hb_min.cu): warm-up report, trial step, decision + report
+int min_alloc(hb_minimizer *m);
+void min_free(hb_minimizer *m);
+int min_init(hb_minimizer *m, cudaStream_t s);
+int min_trial(hb_minimizer *m, cudaStream_t s);
+int min_finish(hb_minimizer *m, uint32_t slot, cudaStream_t s);
 
 static inline unsigned int hb_div_up(uint64_t a, uint64_t b) {
   return (unsigned int)((a + b - 1) / b);

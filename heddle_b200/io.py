@@ -17,13 +17,15 @@ Supported slot kinds: integrators "velocity-verlet" (with `lossless`) and
 "shake", bond/angle types "harmonic", dihedral types "periodic", pair
 potential "lennard-jones", neighbour list "cell-list".  Other kinds the
 reference registers (thermostat nose-hoover-chain, barostat mtk-npt, Morse
-bonds, minimisation phases, all-pairs lists) are rejected with a
-ConfigError that names them.
+bonds, all-pairs lists) are rejected with a ConfigError that names them.
+[[minimization]] phases (steepest descent) run in document order with the
+[[phase]] entries.
 """
 
 from __future__ import annotations
 
 import math
+import re
 import tomllib
 from dataclasses import dataclass, field
 from pathlib import Path
@@ -165,6 +167,54 @@ def _barostat(b: dict) -> dict:
                       f"(known to the reference: {', '.join(_UNSUPPORTED['barostat'])})")
 
 
+def _out_path(base: Path, p):
+    return None if p is None else (Path(p) if Path(p).is_absolute() else base / p)
+
+
+@dataclass
+class MinimizationConfig:
+    name: str
+    algorithm: dict                # steepest-descent parameters (a.u.)
+    output: dict = field(default_factory=dict)
+
+
+def _minimization(m: dict, base: Path) -> MinimizationConfig:
+    """[[minimization]]: name, [minimization.algorithm] kind
+    "steepest-descent" (SteepestDescentParams with the reference's defaults
+    and checks, src/minimizer/steepest_descent.rs:20-62, 300-380) and
+    [minimization.output] (src/io/config.rs:680-710)."""
+    name = str(_req(m, "name", "minimization"))
+    alg = dict(_req(m, "algorithm", f"minimization {name}"))
+    if alg.get("kind") != "steepest-descent":
+        raise ConfigError(f"minimizer kind {alg.get('kind')!r} does not match any registered builder")
+    w = "minimization.algorithm"
+    a = {"initial_step": _positive(alg.get("initial_step", 1.0e-12), f"{w}.initial_step") / U.BOHR_M,
+         "max_step": _positive(alg.get("max_step", 1.0e-10), f"{w}.max_step") / U.BOHR_M,
+         "step_increase": _finite(alg.get("step_increase", 1.2), f"{w}.step_increase"),
+         "step_decrease": _finite(alg.get("step_decrease", 0.2), f"{w}.step_decrease"),
+         "force_tolerance": _finite(alg.get("force_tolerance", 1.0e-10), f"{w}.force_tolerance")
+         / U.FORCE_N,
+         "energy_tolerance": _finite(alg.get("energy_tolerance", 1.0e-7), f"{w}.energy_tolerance"),
+         "max_iterations": int(alg.get("max_iterations", 1000))}
+    if a["max_step"] < a["initial_step"]:
+        raise ConfigError(f"{w}.max_step must be >= initial_step")
+    if a["step_increase"] < 1.0:
+        raise ConfigError(f"{w}.step_increase must be finite and >= 1.0, got {a['step_increase']}")
+    if not 0.0 < a["step_decrease"] < 1.0:
+        raise ConfigError(f"{w}.step_decrease must be finite and in (0.0, 1.0), got {a['step_decrease']}")
+    if a["force_tolerance"] < 0.0 or a["energy_tolerance"] < 0.0:
+        raise ConfigError(f"{w}: tolerances must be finite and >= 0.0")
+    if a["max_iterations"] <= 0:
+        raise ConfigError(f"{w}.max_iterations must be strictly positive")
+    out = dict(m.get("output", {}))
+    output = {"minlog_every": int(out.get("minlog_every", 1)),
+              "trajectory_every": int(out.get("trajectory_every", 0)),
+              "include_images": bool(out.get("include_images", True)),
+              "minlog_path": _out_path(base, out.get("minlog_path")),
+              "trajectory_path": _out_path(base, out.get("trajectory_path"))}
+    return MinimizationConfig(name, a, output)
+
+
 def load_config(path) -> Config:
     """Parse and validate a schema-1 TOML configuration (SI units)."""
     path = Path(path)
@@ -181,9 +231,7 @@ def load_config(path) -> Config:
     sim = _req(doc, "simulation", "top level")
     seed = int(_req(sim, "seed", "simulation"))
     temp_k = _finite(_req(sim, "temperature", "simulation"), "simulation.temperature")
-    if doc.get("minimization"):
-        raise ConfigError("[[minimization]] phases are not supported by this engine")
-    phases = []
+    md_phases = []
     for p in doc.get("phase", []):
         name = str(_req(p, "name", "phase"))
         n_steps = int(_req(p, "n_steps", f"phase {name}"))
@@ -212,13 +260,24 @@ def load_config(path) -> Config:
             raise ConfigError("a thermostat or a per-step barostat needs the (non-lossless) "
                               "velocity-verlet integrator")
         out = dict(p.get("output", {}))
+        # defaults of RawOutputConfig (src/io/config.rs:595-604, 860-875)
         output = {"trajectory_every": int(out.get("trajectory_every", 100)),
-                  "include_velocities": bool(out.get("include_velocities", False)),
-                  "include_images": bool(out.get("include_images", False)),
-                  "log_every": int(out.get("log_every", 100))}
-        phases.append(PhaseConfig(name, n_steps, dt, integ, thermo, baro, output))
+                  "include_velocities": bool(out.get("include_velocities", True)),
+                  "include_images": bool(out.get("include_images", True)),
+                  "log_every": int(out.get("log_every", 100)),
+                  "trajectory_path": _out_path(base, out.get("trajectory_path")),
+                  "log_path": _out_path(base, out.get("log_path"))}
+        md_phases.append(PhaseConfig(name, n_steps, dt, integ, thermo, baro, output))
+    min_phases = [_minimization(m, base) for m in doc.get("minimization", [])]
+    # [[phase]] and [[minimization]] run in document order
+    # (src/io/config.rs:1255-1290)
+    order = re.findall(r"^\s*\[\[\s*(phase|minimization)\s*\]\]", path.read_text(), flags=re.M)
+    if sorted(order) != sorted(["phase"] * len(md_phases) + ["minimization"] * len(min_phases)):
+        raise ConfigError("could not order the [[phase]] / [[minimization]] entries")
+    it_md, it_min = iter(md_phases), iter(min_phases)
+    phases = [next(it_md) if k == "phase" else next(it_min) for k in order]
     if not phases:
-        raise ConfigError("no [[phase]] entries")
+        raise ConfigError("no [[phase]] or [[minimization]] entries")
     ptypes = []
     for t in _req(doc, "particle_types", "top level"):
         ptypes.append({"name": str(_req(t, "name", "particle_types")),
@@ -448,6 +507,23 @@ class LogWriter:
                 fmt_e(temp_au * U.HARTREE_K)] + [
                     fmt_e(v * DIMENSION_SI[d]) for v, (_, d) in zip(extras, self.extra)]
         self.f.write(",".join(vals) + "\n")
+
+    def close(self) -> None:
+        self.f.close()
+
+
+class MinlogWriter:
+    """Minimisation log `iter,energy,max_force,step,accepted` in SI
+    (src/io/minlog_output.rs:30-70); rows are Minimizer reports."""
+
+    def __init__(self, path):
+        self.f = open(path, "x")
+        self.f.write("iter,energy,max_force,step,accepted\n")
+
+    def write(self, r: dict) -> None:
+        self.f.write(f"{r['iteration']},{fmt_e(r['energy'] * U.HARTREE_J)},"
+                     f"{fmt_e(r['max_force'] * U.FORCE_N)},{fmt_e(r['step'] * U.BOHR_M)},"
+                     f"{1 if r['accepted'] else 0}\n")
 
     def close(self) -> None:
         self.f.close()

@@ -20,7 +20,9 @@ from pathlib import Path
 import numpy as np
 
 from . import api as A
-from .io import ConfigError, LogWriter, TrajectoryWriter, load_config, read_topology, read_xyz
+from . import units as U
+from .io import (ConfigError, LogWriter, MinimizationConfig, MinlogWriter, TrajectoryWriter,
+                 load_config, read_topology, read_xyz)
 from .systems import settle_geometry
 from .topology import effective_exclusions, exclusion_csr
 from .velocities import generate_velocities
@@ -203,6 +205,74 @@ def log_values(ph, ke: float, pe: float, thermo, baro) -> list:
     return vals
 
 
+class MinimizationError(RuntimeError):
+    """A minimisation phase ended without converging (the reference's
+    RunnerError::MinimizerNonConvergence)."""
+
+
+def minimize(ph, sys_, ff, cons, names, base: Path, root: str) -> list:
+    """One [[minimization]] phase (src/runner.rs:1804-2140): the iteration-0
+    row and frame, a minlog row every minlog_every iterations (and the final
+    one), a frame every trajectory_every accepted iterations (positions
+    only, time 0); non-convergence is an error."""
+    out = ph.output
+    written = []
+    log = traj = None
+    if out["minlog_every"] > 0:
+        lp = out.get("minlog_path") or base / f"{root}.out.{ph.name}.minlog"
+        log = MinlogWriter(lp)
+        written.append(lp)
+    if out["trajectory_every"] > 0:
+        tp = out.get("trajectory_path") or base / f"{root}.out.{ph.name}.xyz"
+        traj = TrajectoryWriter(tp, names, False, out["include_images"])
+        written.append(tp)
+    a = ph.algorithm
+    m = A.Minimizer(ff, cons, a["initial_step"], a["max_step"], a["step_increase"],
+                    a["step_decrease"], a["force_tolerance"], a["energy_tolerance"],
+                    a["max_iterations"])
+    types = np.asarray(sys_._t)
+
+    def frame(it):
+        pos, _, img, _ = sys_.state()
+        traj.write(it, 0.0, sys_.box(), types, pos, None, img)
+
+    try:
+        r = m.begin()
+        last_logged = None
+        if log:
+            log.write(r)
+            last_logged = 0
+        if traj:
+            frame(0)
+        while r["converged"] is None and r["iteration"] < a["max_iterations"]:
+            # chunks end on the trajectory cadence so frames see their state
+            k = a["max_iterations"] - r["iteration"]
+            if traj:
+                k = min(k, out["trajectory_every"] - r["iteration"] % out["trajectory_every"])
+            rows = m.iterate(min(k, 256))
+            if not rows:
+                break
+            for r in rows:
+                if log and r["iteration"] % out["minlog_every"] == 0:
+                    log.write(r)
+                    last_logged = r["iteration"]
+            if traj and r["accepted"] and r["iteration"] % out["trajectory_every"] == 0:
+                frame(r["iteration"])
+        if r["converged"] is None:
+            raise MinimizationError(
+                f"minimization phase `{ph.name}` failed to converge after {r['iteration']} "
+                f"iterations (max_force = {r['max_force'] * U.FORCE_N:.3e} N, "
+                f"step = {r['step'] * U.BOHR_M:.3e} m)")
+        if log and last_logged != r["iteration"]:
+            log.write(r)
+    finally:
+        m.close()
+        for w in (log, traj):
+            if w:
+                w.close()
+    return written
+
+
 def run(config_path, ctx=None) -> list:
     """Run every phase; returns the written output paths."""
     cfg = load_config(config_path)
@@ -216,6 +286,9 @@ def run(config_path, ctx=None) -> list:
     dof = max(3 * n - extra["n_constraints"] - 3, 1)
     step = 0
     for ph in cfg.phases:
+        if isinstance(ph, MinimizationConfig):
+            written += minimize(ph, sys_, ff, cons, names, base, root)
+            continue
         kw = dict(ph.integrator)
         kind = kw.pop("kind")
         it = A.Integrator(sys_, kind, ph.dt, step0=step, **kw)
@@ -239,11 +312,11 @@ def run(config_path, ctx=None) -> list:
         out = ph.output
         traj = log = None
         if out["trajectory_every"] > 0:
-            tp = base / f"{root}.out.{ph.name}.xyz"
+            tp = out.get("trajectory_path") or base / f"{root}.out.{ph.name}.xyz"
             traj = TrajectoryWriter(tp, names, out["include_velocities"], out["include_images"])
             written.append(tp)
         if out["log_every"] > 0:
-            lp = base / f"{root}.out.{ph.name}.log"
+            lp = out.get("log_path") or base / f"{root}.out.{ph.name}.log"
             log = LogWriter(lp, log_columns(ph))
             written.append(lp)
         types = None

@@ -73,6 +73,7 @@ typedef struct hb_integrator hb_integrator;
 typedef struct hb_barostat hb_barostat;
 typedef struct hb_thermostat hb_thermostat;
 typedef struct hb_pcouple hb_pcouple;
+typedef struct hb_minimizer hb_minimizer;
 typedef struct hb_batch hb_batch;
 typedef struct hb_shake_mlp hb_shake_mlp;
 
@@ -436,6 +437,50 @@ int hb_pcouple_stats(hb_pcouple *p, double out[8]);
 /* Attach (or detach with NULL); velocity Verlet only, and not together
  * with a Monte-Carlo barostat. */
 int hb_integrator_set_pcouple(hb_integrator *it, hb_pcouple *p);
+
+/* ---- steepest-descent minimisation: replaces SteepestDescentMinimizer
+ * (src/minimizer/steepest_descent.rs:123-300, kernels/minimize.cu) and the
+ * runner's minimisation loop (src/runner.rs:1804-2140).  An iteration:
+ * F_max = max |F_i| (single precision), x += s F / F_max, the constraint
+ * groups projected back onto their manifold (position-only Gauss-Seidel with
+ * gradients at the current positions; settle_positions_no_velocity /
+ * shake_positions_no_velocity), forces + energy; accepted when the energy
+ * drops (s = min(s * step_increase, max_step)), else the previous state is
+ * restored (s = s * step_decrease).  Convergence: F_max = 0, F_max <=
+ * force_tolerance (when > 0), or on an accepted iteration |E - E_prev| <=
+ * energy_tolerance max(|E|, |E_prev|, 1e-30) (when > 0).  Every decision is
+ * made on the device; a call runs up to n iterations with one host read. */
+#define HB_MIN_FORCE_TOLERANCE 1
+#define HB_MIN_ENERGY_TOLERANCE 2
+#define HB_MIN_FORCE_ZERO 3
+typedef struct {
+  double initial_step;       /* bohr (> 0) */
+  double max_step;           /* bohr (>= initial_step) */
+  double step_increase;      /* >= 1 */
+  double step_decrease;      /* in (0, 1) */
+  double force_tolerance;    /* hartree / bohr; 0 disables */
+  double energy_tolerance;   /* relative; 0 disables */
+  uint64_t max_iterations;   /* > 0 */
+} hb_minimizer_desc;
+
+typedef struct {
+  uint64_t iteration;        /* 0: the state before the first iteration */
+  double energy;             /* hartree: accepted energy after the iteration */
+  double max_force;          /* hartree / bohr at the accepted configuration */
+  double step;               /* bohr: the step the iteration tried (0 for 0) */
+  int accepted;
+  int converged;             /* HB_MIN_* once converged, else 0 */
+} hb_min_report;
+
+/* cons may be NULL.  The minimiser evaluates ff (with energies) itself. */
+int hb_minimizer_create(hb_forcefield *ff, hb_constraints *cons, const hb_minimizer_desc *desc,
+                        hb_minimizer **out);
+int hb_minimizer_destroy(hb_minimizer *m);
+/* Forces and energy at the current positions; the iteration-0 report. */
+int hb_minimizer_begin(hb_minimizer *m, hb_min_report *out);
+/* Up to n iterations (stopping at convergence or max_iterations); their
+ * reports in out[0 .. *n_done). */
+int hb_minimizer_iterate(hb_minimizer *m, uint32_t n, hb_min_report *out, uint32_t *n_done);
 
 /* ---- batched replicas: the runner's captured-graph replay
  * (src/runner.rs:2803-3000, src/gpu/graph.rs:222-242) extended to many

@@ -5,6 +5,9 @@ tests/test_gpu_run.py (SI units, extended XYZ, topology files):
   water.in.toml / water.in.xyz / water.in.topology
                                  216 SPC waters (SETTLE), SPME, Langevin,
                                  Monte-Carlo barostat
+  argon_min.in.toml             the argon atoms (argon.in.xyz): a
+                                 steepest-descent [[minimization]] phase, then
+                                 a short velocity-Verlet [[phase]]
   water_cr.in.toml              the same waters (water.in.xyz / .topology),
                                  velocity Verlet + SETTLE with a CSVR
                                  thermostat and c-rescale pressure coupling
@@ -164,6 +167,57 @@ include_images = true
 log_every = 10
 
 ''' + WATER_TYPES)
+
+
+def argon_min():
+    (HERE / "argon_min.in.toml").write_text('''schema_version = 1
+init = "argon.in.xyz"
+
+[simulation]
+seed = 1
+temperature = 94.4
+
+[[minimization]]
+name = "relax"
+
+[minimization.algorithm]
+kind = "steepest-descent"
+force_tolerance = 1.0e-13
+energy_tolerance = 1.0e-7
+max_iterations = 2000
+
+[minimization.output]
+minlog_every = 5
+trajectory_every = 10
+
+[[phase]]
+name = "run"
+n_steps = 20
+dt = 5.0e-15
+
+[phase.integrator]
+kind = "velocity-verlet"
+
+[phase.output]
+trajectory_every = 10
+log_every = 10
+
+[[particle_types]]
+name = "Ar"
+mass = 6.6335e-26
+
+[[pair_interactions]]
+between = ["Ar", "Ar"]
+potential = "lennard-jones"
+sigma = 3.405e-10
+epsilon = 1.654e-21
+cutoff = 8.5125e-10
+r_switch = 7.5e-10
+
+[neighbor_list]
+mode = "cell-list"
+r_skin = 1.0e-10
+''')
 
 
 def water_cr():
@@ -357,6 +411,7 @@ between = ["O", "O"]'''))
 
 if __name__ == "__main__":
     argon()
+    argon_min()
     water()
     water_cr()
     chain()

@@ -4,6 +4,7 @@ runs byte-identical at file level (tests/determinism.rs:93-121), energy
 conservation of the NVE argon run, the NPT water run's barostat and the
 bonded chain's constraints."""
 
+import re
 import shutil
 from pathlib import Path
 
@@ -83,6 +84,30 @@ def test_water_csvr_c_rescale_run(ctx, tmp_path):
     # positions are scaled atom by atom after the constraint step (the
     # reference's c-rescale fragment), so bonds carry the last mu
     assert np.abs(np.linalg.norm(d, axis=1) / 1.8897261246 - 1.0).max() < 2e-3
+
+
+def test_argon_minimization_then_md(ctx, tmp_path):
+    shutil.copy(CFG / "argon.in.xyz", tmp_path / "argon.in.xyz")
+    cfg = staged(tmp_path, "argon_min")
+    paths = R.run(cfg, ctx=ctx)
+    assert [p.name for p in paths] == ["argon_min.out.relax.minlog", "argon_min.out.relax.xyz",
+                                       "argon_min.out.run.xyz", "argon_min.out.run.log"]
+    lines = (tmp_path / "argon_min.out.relax.minlog").read_text().splitlines()
+    assert lines[0] == "iter,energy,max_force,step,accepted"
+    rows = np.loadtxt(tmp_path / "argon_min.out.relax.minlog", delimiter=",", skiprows=1)
+    assert rows[0, 0] == 0 and rows[0, 3] == 0.0 and rows[0, 4] == 1
+    assert all(int(i) % 5 == 0 for i in rows[:-1, 0])
+    acc = rows[rows[:, 4] == 1, 1]
+    assert np.all(np.diff(acc) < 0)  # accepted energies fall
+    first = read_xyz(tmp_path / "argon_min.out.relax.xyz", index=0)
+    assert first.step == 0 and first.velocities is None and first.images is not None
+    # frames: iteration 0, then accepted iterations that are multiples of 10
+    text = (tmp_path / "argon_min.out.relax.xyz").read_text()
+    steps = [int(x) for x in re.findall(r"Step=(\d+)", text)]
+    want = [0] + [int(i) for i, a in zip(rows[1:, 0], rows[1:, 4]) if a == 1 and int(i) % 10 == 0]
+    assert steps == want and len(steps) > 1
+    md = read_xyz(tmp_path / "argon_min.out.run.xyz", index=-1)
+    assert md.step == 20
 
 
 def test_bonded_chain_run(ctx, tmp_path):

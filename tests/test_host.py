@@ -39,7 +39,8 @@ def test_struct_layouts_match_header_field_order():
     for struct, cname in ((N.SystemDesc, "hb_system_desc"), (N.ForceFieldDesc, "hb_forcefield_desc"),
                           (N.ConstraintsDesc, "hb_constraints_desc"), (N.IntegratorDesc, "hb_integrator_desc"),
                           (N.BarostatDesc, "hb_barostat_desc"), (N.ThermostatDesc, "hb_thermostat_desc"),
-                          (N.PcoupleDesc, "hb_pcouple_desc")):
+                          (N.PcoupleDesc, "hb_pcouple_desc"), (N.MinimizerDesc, "hb_minimizer_desc"),
+                          (N.MinReport, "hb_min_report")):
         body = re.search(r"typedef struct \{([^}]*)\}\s*" + cname + ";", HEADER).group(1)
         body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
         names = []

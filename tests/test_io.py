@@ -93,6 +93,56 @@ def test_log_columns_follow_the_reference_slots():
     assert log_columns(load_config(CFG / "argon.in.toml").phases[0]) == []
 
 
+def test_minimization_phase_order_and_defaults(tmp_path):
+    from heddle_b200.io import MinimizationConfig, PhaseConfig
+    c = load_config(CFG / "argon_min.in.toml")
+    assert [type(p) for p in c.phases] == [MinimizationConfig, PhaseConfig]
+    m = c.phases[0]
+    assert m.name == "relax"
+    a = m.algorithm
+    # reference defaults (src/minimizer/steepest_descent.rs:43-62) in a.u.
+    assert a["initial_step"] == pytest.approx(1.0e-12 / U.BOHR_M)
+    assert a["max_step"] == pytest.approx(1.0e-10 / U.BOHR_M)
+    assert (a["step_increase"], a["step_decrease"]) == (1.2, 0.2)
+    assert a["force_tolerance"] == pytest.approx(1.0e-13 / U.FORCE_N)
+    assert a["energy_tolerance"] == 1.0e-7 and a["max_iterations"] == 2000
+    assert m.output["minlog_every"] == 5 and m.output["trajectory_every"] == 10
+    assert m.output["include_images"] is True
+    # a [[phase]] before a [[minimization]] keeps its place
+    text = (CFG / "argon_min.in.toml").read_text()
+    i, j = text.index("[[minimization]]"), text.index("[[phase]]")
+    k = text.index("[[particle_types]]")
+    swapped = text[:i] + text[j:k] + text[i:j] + text[k:]
+    (tmp_path / "argon.in.xyz").write_text((CFG / "argon.in.xyz").read_text())
+    p = tmp_path / "s.in.toml"
+    p.write_text(swapped)
+    assert [type(q) for q in load_config(p).phases] == [PhaseConfig, MinimizationConfig]
+    for old, new, msg in (('kind = "steepest-descent"', 'kind = "lbfgs"', "lbfgs"),
+                          ("max_iterations = 2000", "max_iterations = 0", "max_iterations"),
+                          ("max_iterations = 2000", "step_decrease = 1.5", "step_decrease")):
+        p.write_text(text.replace(old, new))
+        with pytest.raises(ConfigError, match=msg):
+            load_config(p)
+
+
+def test_output_defaults_follow_the_reference():
+    ph = load_config(CFG / "water.in.toml").phases[0]
+    # include_velocities defaults to true (src/io/config.rs:865-868)
+    assert ph.output["include_velocities"] is True and ph.output["include_images"] is True
+
+
+def test_minlog_rows_are_si(tmp_path):
+    from heddle_b200.io import MinlogWriter
+    w = MinlogWriter(tmp_path / "m.minlog")
+    w.write({"iteration": 0, "energy": 1.0, "max_force": 2.0, "step": 0.0, "accepted": True})
+    w.write({"iteration": 10, "energy": -1.0, "max_force": 0.5, "step": 1.0, "accepted": False})
+    w.close()
+    lines = (tmp_path / "m.minlog").read_text().splitlines()
+    assert lines[0] == "iter,energy,max_force,step,accepted"
+    assert lines[1] == f"0,{fmt_e(U.HARTREE_J)},{fmt_e(2.0 * U.FORCE_N)},0.000000000e0,1"
+    assert lines[2] == f"10,{fmt_e(-U.HARTREE_J)},{fmt_e(0.5 * U.FORCE_N)},{fmt_e(U.BOHR_M)},0"
+
+
 def test_bad_values_are_rejected(tmp_path):
     (tmp_path / "argon.in.xyz").write_text((CFG / "argon.in.xyz").read_text())
     for old, new, msg in (("schema_version = 1", "schema_version = 2", "schema_version"),
