@@ -319,15 +319,37 @@ __global__ void __launch_bounds__(256) k_fft_c_fwd(unsigned long long *__restric
   for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = tw_g[i];
   const int row0 = blockIdx.x * L;
   const int nr = min(L, nrows - row0);
-  for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
-    const int r = idx / n, c = idx - (idx / n) * n;
-    float v = 0.0f;
-    if (r < nr) {
-      const size_t gi = (size_t)(row0 + r) * n + c;
-      v = (float)(long long)rho[gi] * (1.0f / HB_RHO_SCALE);
-      rho[gi] = 0ull;
+  if constexpr (N > 0) {
+    // every load of the thread first, then the clearing stores: interleaved
+    // with stores to the same array the loads would run one at a time
+    constexpr int LN = lines_of(N) * N, IT = (LN + 255) / 256;
+    unsigned long long *base = rho + (size_t)row0 * N;
+    long long v[IT];
+#pragma unroll
+    for (int q = 0; q < IT; ++q) {
+      const int idx = (int)threadIdx.x + q * 256;
+      v[q] = (idx < LN && idx / N < nr) ? (long long)base[idx] : 0ll;
     }
-    A[r * S + c] = make_float2(v, 0.0f);
+#pragma unroll
+    for (int q = 0; q < IT; ++q) {
+      const int idx = (int)threadIdx.x + q * 256;
+      if (idx < LN) {
+        const int r = idx / N, c = idx - r * N;
+        if (r < nr) base[idx] = 0ull;
+        A[r * S + c] = make_float2((float)v[q] * (1.0f / HB_RHO_SCALE), 0.0f);
+      }
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
+      const int r = idx / n, c = idx - (idx / n) * n;
+      float v = 0.0f;
+      if (r < nr) {
+        const size_t gi = (size_t)(row0 + r) * n + c;
+        v = (float)(long long)rho[gi] * (1.0f / HB_RHO_SCALE);
+        rho[gi] = 0ull;
+      }
+      A[r * S + c] = make_float2(v, 0.0f);
+    }
   }
   __syncthreads();
   float2 *R = fft_run<N, false>(A, B, tw, n, L, pl);
