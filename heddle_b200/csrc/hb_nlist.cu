@@ -302,7 +302,9 @@ __device__ __forceinline__ uint32_t select_bit(uint32_t m, uint32_t k) {
 //     set when j-atom l of the candidate lies within r_search of any i-atom.
 //     Far from the r_search boundary a j-atom shifted once to the image
 //     nearest I's centre decides with plain differences; inside a 1e-4
-//     relative band the exact single-precision rule decides;
+//     relative band the exact single-precision rule decides.  With the
+//     single shift, only the i-atoms of the 8-atom sub-tiles whose box lies
+//     within r_search of the j-atom are tested;
 //  3. a prefix sum of the masks' popcounts fixes where every hit goes;
 //  4. the warps write the entries (self tile first) into I's slab, each
 //     with the exclusion masks of its 32 j-atoms.
@@ -376,6 +378,34 @@ __global__ void __launch_bounds__(NLT_WARPS * 32)
   const uint32_t ivalid = __ballot_sync(0xFFFFFFFFu, ki < n);
   const bool shift_ok = ortho && (hi.x + rb <= 0.5f * b.lx) && (hi.y + rb <= 0.5f * b.ly) &&
                         (hi.z + rb <= 0.5f * b.lz);
+  // With the single shift, the tile's four 8-atom sub-tiles (lanes 8q..8q+7)
+  // get their own boxes: a j-atom is refined only against the atoms of the
+  // sub-tiles whose box lies within r_search (plus the rounding margin), so
+  // a j-atom near one corner of the tile costs 8 or 16 tests instead of 32.
+  // Every pair within r_search lies in the box of its i-atom's sub-tile, so
+  // the hits are those of the full refinement.
+  float sc[4][3], sh[4][3];
+  if (shift_ok) {
+    const bool iv = ki < n;
+    float lo3[3] = {iv ? pim.x : 3.0e38f, iv ? pim.y : 3.0e38f, iv ? pim.z : 3.0e38f};
+    float hi3[3] = {iv ? pim.x : -3.0e38f, iv ? pim.y : -3.0e38f, iv ? pim.z : -3.0e38f};
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        lo3[d] = fminf(lo3[d], __shfl_xor_sync(0xFFFFFFFFu, lo3[d], o));
+        hi3[d] = fmaxf(hi3[d], __shfl_xor_sync(0xFFFFFFFFu, hi3[d], o));
+      }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const float l = __shfl_sync(0xFFFFFFFFu, lo3[d], 8 * q);
+        const float h = __shfl_sync(0xFFFFFFFFu, hi3[d], 8 * q);
+        sc[q][d] = 0.5f * (l + h);
+        sh[q][d] = h >= l ? 0.5f * (h - l) : -1.0f;  // empty sub-tile: never near
+      }
+  }
   for (uint32_t c = w; c < ncand; c += NLT_WARPS) {
     const uint32_t kj = cand[c] * 32u + lane;
     const bool jvalid = kj < n;
@@ -386,10 +416,46 @@ __global__ void __launch_bounds__(NLT_WARPS * 32)
       sy -= b.ly * rintf((sy - ci.y) * b.ily);
       sz -= b.lz * rintf((sz - ci.z) * b.ilz);
     }
+    if (shift_ok) {
+      uint32_t qm = 0u;
+      if (jvalid) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float ex = fmaxf(fabsf(sx - sc[q][0]) - sh[q][0], 0.0f);
+          const float ey = fmaxf(fabsf(sy - sc[q][1]) - sh[q][1], 0.0f);
+          const float ez = fmaxf(fabsf(sz - sc[q][2]) - sh[q][2], 0.0f);
+          if (sh[q][0] >= 0.0f && ex * ex + ey * ey + ez * ez <= rb2) qm |= 1u << q;
+        }
+      }
+      bool hit = false;
+#pragma unroll
+      for (uint32_t q = 0; q < 4u; ++q) {
+        const bool want = (qm >> q) & 1u;
+        uint32_t open = __ballot_sync(0xFFFFFFFFu, want && !hit);
+        for (uint32_t m = 8u * q; m < 8u * q + 8u && open != 0u; ++m) {
+          const float xi = __shfl_sync(0xFFFFFFFFu, pim.x, m);
+          const float yi = __shfl_sync(0xFFFFFFFFu, pim.y, m);
+          const float zi = __shfl_sync(0xFFFFFFFFu, pim.z, m);
+          if (want && !hit && ((ivalid >> m) & 1u)) {
+            const float dx = xi - sx, dy = yi - sy, dz = zi - sz;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 < band_lo) {
+              hit = true;
+            } else if (r2 <= band_hi && hb_exact_r2(xi - pj.x, yi - pj.y, zi - pj.z, b) <= rs2) {
+              hit = true;
+            }
+          }
+          open = __ballot_sync(0xFFFFFFFFu, want && !hit);
+        }
+      }
+      const uint32_t hm = __ballot_sync(0xFFFFFFFFu, hit);
+      if (lane == 0) hmask[c] = hm;
+      continue;
+    }
     bool near = jvalid;
     if (near && ortho) {
       float dx = sx - ci.x, dy = sy - ci.y, dz = sz - ci.z;
-      if (!shift_ok) hb_min_image(dx, dy, dz, b);
+      hb_min_image(dx, dy, dz, b);
       const float ex = fmaxf(fabsf(dx) - hi.x, 0.0f);
       const float ey = fmaxf(fabsf(dy) - hi.y, 0.0f);
       const float ez = fmaxf(fabsf(dz) - hi.z, 0.0f);
@@ -403,7 +469,7 @@ __global__ void __launch_bounds__(NLT_WARPS * 32)
       const float zi = __shfl_sync(0xFFFFFFFFu, pim.z, m);
       if (near && !hit && ((ivalid >> m) & 1u)) {
         float dx = xi - sx, dy = yi - sy, dz = zi - sz;
-        if (!shift_ok) hb_min_image(dx, dy, dz, b);
+        hb_min_image(dx, dy, dz, b);
         const float r2 = dx * dx + dy * dy + dz * dz;
         if (r2 < band_lo) {
           hit = true;
