@@ -310,7 +310,7 @@ __device__ __forceinline__ uint32_t select_bit(uint32_t m, uint32_t k) {
 //     with the exclusion masks of its 32 j-atoms.
 // WRITE = false only counts entries and candidates (first-build sizing).
 template <bool WRITE>
-__global__ void __launch_bounds__(NLT_WARPS * 32)
+__global__ void __launch_bounds__(NLT_WARPS * 32, 4)
     k_nl_tile(const uint32_t *gate, const float4 *__restrict__ tile_posq,
               const float4 *__restrict__ center, const float4 *__restrict__ half,
               const DBox *__restrict__ box, float rs2, float rb, float band_lo, float band_hi,
@@ -326,8 +326,10 @@ __global__ void __launch_bounds__(NLT_WARPS * 32)
   uint32_t *pre = hmask + maxc;       // [maxc + 1] exclusive prefix of hits
   __shared__ uint32_t s_cnt[NLT_WARPS];
   __shared__ uint32_t s_ncand;
+  __shared__ float4 s_ipos[32];       // the i-tile's positions (padding at 1e18)
   const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t I = blockIdx.x;
+  if (w == 0) s_ipos[lane] = tile_posq[I * 32u + lane];
   const DBox b = *box;
   const float4 ci = center[I], hi = half[I];
   const bool ortho = ((int)ci.w & 2) != 0;
@@ -427,25 +429,28 @@ __global__ void __launch_bounds__(NLT_WARPS * 32)
           if (sh[q][0] >= 0.0f && ex * ex + ey * ey + ez * ez <= rb2) qm |= 1u << q;
         }
       }
+      // i-atoms come from shared memory as broadcasts, two per round
+      // between votes; padding slots sit at 1e18 and never hit
       bool hit = false;
-#pragma unroll
+#pragma unroll 1
       for (uint32_t q = 0; q < 4u; ++q) {
-        const bool want = (qm >> q) & 1u;
-        uint32_t open = __ballot_sync(0xFFFFFFFFu, want && !hit);
-        for (uint32_t m = 8u * q; m < 8u * q + 8u && open != 0u; ++m) {
-          const float xi = __shfl_sync(0xFFFFFFFFu, pim.x, m);
-          const float yi = __shfl_sync(0xFFFFFFFFu, pim.y, m);
-          const float zi = __shfl_sync(0xFFFFFFFFu, pim.z, m);
-          if (want && !hit && ((ivalid >> m) & 1u)) {
-            const float dx = xi - sx, dy = yi - sy, dz = zi - sz;
+        bool want = (qm >> q) & 1u;
+#pragma unroll 1
+        for (uint32_t m = 8u * q; m < 8u * q + 8u && __any_sync(0xFFFFFFFFu, want); m += 2u) {
+#pragma unroll
+          for (uint32_t u = 0; u < 2u; ++u) {
+            const float4 a = s_ipos[m + u];
+            const float dx = a.x - sx, dy = a.y - sy, dz = a.z - sz;
             const float r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 < band_lo) {
-              hit = true;
-            } else if (r2 <= band_hi && hb_exact_r2(xi - pj.x, yi - pj.y, zi - pj.z, b) <= rs2) {
-              hit = true;
+            if (want) {
+              if (r2 < band_lo) {
+                hit = true;
+              } else if (r2 <= band_hi && hb_exact_r2(a.x - pj.x, a.y - pj.y, a.z - pj.z, b) <= rs2) {
+                hit = true;
+              }
             }
+            want = want && !hit;
           }
-          open = __ballot_sync(0xFFFFFFFFu, want && !hit);
         }
       }
       const uint32_t hm = __ballot_sync(0xFFFFFFFFu, hit);
