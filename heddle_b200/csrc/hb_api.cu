@@ -466,8 +466,8 @@ extern "C" int hb_forcefield_create(hb_system *sys, const hb_forcefield_desc *d,
   hb_forcefield *ff = new hb_forcefield();
   *ff = tmp;
   ff->sys = sys;
-  // pair kernel: the balanced form for force-only steps (the rotation sweep
-  // for steps with energies); HB_PAIR_KERNEL=rotation / compact select the
+  // pair kernel: the balanced form (with or without energies);
+  // HB_PAIR_KERNEL=rotation / compact select the
   // rotation sweep or the compacted pair-list form (shared-memory int64
   // atomics) throughout; exact pairs use the compacted form with per-pair
   // fixed point and minimum image

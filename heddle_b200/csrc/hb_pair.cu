@@ -294,7 +294,8 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, 8)
 }
 
 // ---------------------------------------------------------------------
-// Balanced form (forces only).  Per entry: (1) a distance pass over the 32
+// Balanced form (every step; with EV also per-atom energy and virial).
+// Per entry: (1) a distance pass over the 32
 // rotations (unrolled for ordinary entries) leaves each lane's mask of
 // rotations whose pair is inside the cutoff; exclusions are folded in with
 // one AND per entry; (2) the set bits are dealt slot-major into a per-warp
@@ -306,11 +307,17 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, 8)
 // same run to run) that are folded into int64 once per entry.  A pair force
 // component above 0.06 hartree/bohr takes the exact global int64 path
 // instead, so the int32 sums cannot wrap (32 pairs x 0.06 x 2^30 < 2^31).
+// With EV the energy and virial halves of each pair go the same way at
+// scale 2^28 (guard 0.25 hartree), and the LJ energy total is summed per
+// lane in int64.
 // ---------------------------------------------------------------------
 #define P4_WARPS 4
 #define P4_SHIFT 10               // 2^40 / 2^30
 #define P4_SCALE 1073741824.0f    // 2^30
 #define P4_FMAX 0.06f
+#define P4_ESHIFT 12              // 2^40 / 2^28
+#define P4_ESCALE 268435456.0f    // 2^28
+#define P4_EMAX 0.25f
 
 struct P4Warp {
   float4 ipos[32];
@@ -326,7 +333,7 @@ struct P4Warp {
   uint16_t pairs[1024];
 };
 
-template <bool SCALED, bool SWITCH>
+template <bool EV, bool SCALED, bool SWITCH>
 __global__ void __launch_bounds__(P4_WARPS * 32, 8)
     k_pair4(const float4 *__restrict__ tile_posq, const int *__restrict__ tile_type,
             const float4 *__restrict__ center, const uint32_t *__restrict__ tile_nent,
@@ -335,10 +342,16 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
             const float *__restrict__ lj_invd, PairParams P, unsigned long long *__restrict__ fp,
             const uint32_t *__restrict__ sorted_ids, const uint32_t *__restrict__ eoff,
             const uint32_t *__restrict__ epart, const float2 *__restrict__ escale,
-            uint32_t *__restrict__ work, uint32_t chunks, uint32_t chunk) {
+            uint32_t *__restrict__ work, uint32_t chunks, uint32_t chunk,
+            unsigned long long *__restrict__ e_lj_total) {
   extern __shared__ float4 sm_lj4[];
   __shared__ P4Warp smw4[P4_WARPS];
   __shared__ uint32_t sm_ljtypes[32];  // per i-type: j-types with a Lennard-Jones term
+  // with energies: per warp int32 fixed-point (2^28) energy / virial halves
+  // of the i-atoms [0, 32) and [32, 64) and of the j-atoms [64, 96) and
+  // [96, 128); a half above 0.25 hartree takes the int64 path, so the int32
+  // sums cannot wrap (32 pairs x 0.25 x 2^28 < 2^31)
+  __shared__ int sm_ev[EV ? P4_WARPS * 128 : 1];
   const int nt2 = P.n_types * P.n_types;
   float *sm_ljd4 = reinterpret_cast<float *>(sm_lj4 + nt2);
   for (int k = threadIdx.x; k < nt2; k += blockDim.x) {
@@ -355,6 +368,8 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
   __syncthreads();
   const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   P4Warp &S = smw4[w];
+  int *Ev = sm_ev + (EV ? w * 128u : 0u);
+  long long elj_fix = 0;  // LJ energy of this lane's pairs (fixed point)
   const DBox b = *box;
   const size_t np_all = (size_t)P.n_tiles * 32u;
   const uint32_t lt = (1u << lane) - 1u;
@@ -386,7 +401,7 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
     S.ipos[lane] = pi;
     S.itype[lane] = (ivalid ? tile_type[si] : 0) * P.n_types;
     if (SCALED) S.oi[lane] = ivalid ? sorted_ids[si] : HB_SENTINEL;
-    long long ax = 0, ay = 0, az = 0;
+    long long ax = 0, ay = 0, az = 0, ae = 0, aw = 0;
     const bool has_self = P.n - I * 32u >= 2u;
 
     for (uint32_t e = e0; e < e1; ++e) {
@@ -413,6 +428,10 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
       for (int q = 0; q < 3; ++q) {
         S.fi[q][lane] = 0;
         S.fj[q][lane] = 0;
+      }
+      if (EV) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) Ev[32 * q + lane] = 0;
       }
       __syncwarp();
 
@@ -499,7 +518,7 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
         }
         const float inv_r = rsqrtf(r2);
         const float inv_r2 = inv_r * inv_r;
-        float fac = 0.0f;
+        float fac = 0.0f, en = 0.0f;
         if (ljq) {
           const int tp = S.itype[i] + S.jtype[j];
           const float4 L = sm_lj4[tp];
@@ -508,16 +527,21 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
             const float sr6 = sr2 * sr2 * sr2;
             const float sr12 = sr6 * sr6;
             float f = L.y * inv_r2 * (2.0f * sr12 - sr6);
+            float u = (L.y * (1.0f / 6.0f)) * (sr12 - sr6);
             if (SWITCH && r2 > L.w) {
-              const float u = (L.y * (1.0f / 6.0f)) * (sr12 - sr6);
               const float inv_d = sm_ljd4[tp];
               const float tau = (r2 - L.w) * inv_d;
               const float omt = 1.0f - tau;
               const float sw = omt * omt * (1.0f + 2.0f * tau);
               const float chain = 12.0f * tau * omt * inv_d;
               f = sw * f + chain * u;
+              u = sw * u;
             }
             fac += s_lj * f;
+            if (EV) {
+              en += s_lj * u;
+              elj_fix += to_fixed(s_lj * u);
+            }
           }
         }
         if (P.coul_on && r2 <= P.coul_rc2 && s_c != 0.0f) {
@@ -530,8 +554,27 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
               (-0.284496736f + (1.421413741f + (-1.453152027f + 1.061405429f * tt) * tt) * tt) * tt;
           const float erfc_ar = poly * tt * gg;
           fac += s_c * a.w * q.w * inv_r2 * (erfc_ar * inv_r + P.c2a * gg);
+          if (EV) en += s_c * a.w * q.w * erfc_ar * inv_r;
         }
         const float fx = fac * dx, fy = fac * dy, fz = fac * dz;
+        if (EV) {
+          // half of the pair's energy and virial to each atom (integer sums:
+          // order-independent)
+          const float he = 0.5f * en, hw = 0.5f * fac * r2;
+          if (fabsf(he) <= P4_EMAX && fabsf(hw) <= P4_EMAX) {
+            const int ie = __float2int_rn(he * P4_ESCALE), iw = __float2int_rn(hw * P4_ESCALE);
+            atomicAdd(&Ev[i], ie);
+            atomicAdd(&Ev[32 + i], iw);
+            atomicAdd(&Ev[64 + j], ie);
+            atomicAdd(&Ev[96 + j], iw);
+          } else {
+            const uint32_t ti_slot = I * 32u + i, tj_slot = S.jslot[j];
+            red_add(&fp[3 * np_all + ti_slot], to_fixed(he));
+            red_add(&fp[4 * np_all + ti_slot], to_fixed(hw));
+            red_add(&fp[3 * np_all + tj_slot], to_fixed(he));
+            red_add(&fp[4 * np_all + tj_slot], to_fixed(hw));
+          }
+        }
         if (fabsf(fx) <= P4_FMAX && fabsf(fy) <= P4_FMAX && fabsf(fz) <= P4_FMAX) {
           const int ix = __float2int_rn(fx * P4_SCALE), iy = __float2int_rn(fy * P4_SCALE),
                     iz = __float2int_rn(fz * P4_SCALE);
@@ -568,19 +611,42 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
         red_add(&fp[1 * np_all + sj], jy);
         red_add(&fp[2 * np_all + sj], jz);
       }
+      if (EV) {
+        ae += (long long)Ev[lane] << P4_ESHIFT;
+        aw += (long long)Ev[32 + lane] << P4_ESHIFT;
+        const long long je = (long long)Ev[64 + lane] << P4_ESHIFT;
+        const long long jw = (long long)Ev[96 + lane] << P4_ESHIFT;
+        if (self) {
+          ae += je;
+          aw += jw;
+        } else if (jvalid) {
+          red_add(&fp[3 * np_all + sj], je);
+          red_add(&fp[4 * np_all + sj], jw);
+        }
+      }
     }
     if (ivalid) {
       red_add(&fp[0 * np_all + si], ax);
       red_add(&fp[1 * np_all + si], ay);
       red_add(&fp[2 * np_all + si], az);
+      if (EV) {
+        red_add(&fp[3 * np_all + si], ae);
+        red_add(&fp[4 * np_all + si], aw);
+      }
     }
+  }
+  if (EV) {
+    // LJ energy total for the scalar split: one integer reduction per warp
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) elj_fix += __shfl_xor_sync(0xFFFFFFFFu, elj_fix, o);
+    if (lane == 0) red_add(e_lj_total, elj_fix);
   }
 }
 
 // entries per work item of the balanced kernel
 #define P4_CHUNK 4
 
-template <bool SCALED, bool SWITCH>
+template <bool EV, bool SCALED, bool SWITCH>
 int launch4_t(hb_forcefield *ff, cudaStream_t s, const PairParams &P) {
   size_t smem = (sizeof(float4) + sizeof(float)) * (size_t)P.n_types * P.n_types;
   const uint32_t chunks = hb_div_up(P.slab, P4_CHUNK);
@@ -589,10 +655,11 @@ int launch4_t(hb_forcefield *ff, cudaStream_t s, const PairParams &P) {
   const uint32_t items = P.n_tiles * chunks;
   const uint32_t grid = std::min<uint32_t>(
       (uint32_t)ff->sys->ctx->n_sm * (uint32_t)ff->pair_blocks_per_sm, hb_div_up(items, P4_WARPS));
-  k_pair4<SCALED, SWITCH><<<std::max(grid, 1u), P4_WARPS * 32, smem, s>>>(
+  k_pair4<EV, SCALED, SWITCH><<<std::max(grid, 1u), P4_WARPS * 32, smem, s>>>(
       ff->d_tile_posq, ff->d_tile_type, ff->d_tile_center, ff->d_tile_nent, ff->d_entry_j,
       ff->d_entry_excl, ff->sys->d_box, ff->d_lj, ff->d_lj_invd, P, ff->d_fp, ff->d_sorted_ids,
-      ff->d_excl_off, ff->d_excl_partner, ff->d_excl_scale, ff->d_work, chunks, P4_CHUNK);
+      ff->d_excl_off, ff->d_excl_partner, ff->d_excl_scale, ff->d_work, chunks, P4_CHUNK,
+      ff->d_acc);
   HB_CUDA(cudaGetLastError());
   return HB_OK;
 }
@@ -871,13 +938,17 @@ int pair_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
     if (sc) return sw ? launch2_t<false, true, true, true>(ff, s, P) : launch2_t<false, true, false, true>(ff, s, P);
     return sw ? launch2_t<false, false, true, true>(ff, s, P) : launch2_t<false, false, false, true>(ff, s, P);
   }
+  if (ff->pair_variant == 3) {
+    if (ev) {
+      if (sc) return sw ? launch4_t<true, true, true>(ff, s, P) : launch4_t<true, true, false>(ff, s, P);
+      return sw ? launch4_t<true, false, true>(ff, s, P) : launch4_t<true, false, false>(ff, s, P);
+    }
+    if (sc) return sw ? launch4_t<false, true, true>(ff, s, P) : launch4_t<false, true, false>(ff, s, P);
+    return sw ? launch4_t<false, false, true>(ff, s, P) : launch4_t<false, false, false>(ff, s, P);
+  }
   if (ev) {
     if (sc) return sw ? launch_t<true, true, true>(ff, s, P) : launch_t<true, true, false>(ff, s, P);
     return sw ? launch_t<true, false, true>(ff, s, P) : launch_t<true, false, false>(ff, s, P);
-  }
-  if (ff->pair_variant == 3) {
-    if (sc) return sw ? launch4_t<true, true>(ff, s, P) : launch4_t<true, false>(ff, s, P);
-    return sw ? launch4_t<false, true>(ff, s, P) : launch4_t<false, false>(ff, s, P);
   }
   if (sc) return sw ? launch_t<false, true, true>(ff, s, P) : launch_t<false, true, false>(ff, s, P);
   return sw ? launch_t<false, false, true>(ff, s, P) : launch_t<false, false, false>(ff, s, P);
