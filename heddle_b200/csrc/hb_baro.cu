@@ -7,12 +7,12 @@
 // Here the move is four kernels around one force evaluation and never
 // synchronises:
 //   k_baro_propose   1 thread: U_old from the scalars, Philox draw, dV, the
-//                    width guard, FP64 lattice scale, raises the neighbour
-//                    rebuild bit;
+//                    width guard, FP64 lattice scale;
 //   k_baro_scale     1 thread per molecule: snapshot of the molecule's
 //                    positions/images/forces, FP64 centre of mass, rigid
 //                    translation by (s - 1) COM, wrap into the new cell;
-//   (force evaluation with scalars -- rebuilds against the new box)
+//   (force evaluation with scalars; the neighbour list is kept when the
+//    scaling is within its tolerance, else rebuilt against the new box)
 //   k_baro_decide    1 thread: Metropolis test in FP64, box/scalars revert on
 //                    rejection, step-size adaptation, diagnostics;
 //   k_baro_restore   1 thread per atom: positions/images/forces revert.
@@ -40,8 +40,7 @@ __device__ __forceinline__ double baro_volume(const double *lat) {
 
 __global__ void k_baro_propose(BaroState *__restrict__ st, double *__restrict__ lat,
                                DBox *__restrict__ dbox, const double *__restrict__ scalars,
-                               double r_search, uint32_t seed_lo, uint32_t seed_hi,
-                               uint32_t *__restrict__ nl_status) {
+                               double r_search, uint32_t seed_lo, uint32_t seed_hi) {
   st->u_old = scalars[4];
   for (int q = 0; q < HB_N_SCALARS; ++q) st->scalars_pre[q] = scalars[q];
   st->draw += 1ull;
@@ -68,7 +67,6 @@ __global__ void k_baro_propose(BaroState *__restrict__ st, double *__restrict__ 
       lat[d] *= scale;
     }
     *dbox = hb_make_dbox(lat);
-    atomicOr(nl_status, HB_ST_DISPLACED);
   }
   st->u1 = u1;
   st->u2 = u2;
@@ -154,8 +152,7 @@ __global__ void k_baro_scale(const BaroState *__restrict__ st,
 
 __global__ void k_baro_decide(BaroState *__restrict__ st, double *__restrict__ lat,
                               DBox *__restrict__ dbox, double *__restrict__ scalars,
-                              double pressure, double kt, double n_mol,
-                              uint32_t *__restrict__ nl_status) {
+                              double pressure, double kt, double n_mol) {
   bool accepted = false;
   double v_post = st->v_old;
   st->u_new = st->u_old;
@@ -173,7 +170,6 @@ __global__ void k_baro_decide(BaroState *__restrict__ st, double *__restrict__ l
       for (int d = 0; d < 6; ++d) lat[d] = st->lattice_pre[d];
       *dbox = hb_make_dbox(lat);
       for (int q = 0; q < HB_N_SCALARS; ++q) scalars[q] = st->scalars_pre[q];
-      atomicOr(nl_status, HB_ST_DISPLACED);
     }
   }
   // adaptive step (src/integrator/mc_barostat.rs:157-179)
@@ -214,7 +210,7 @@ int baro_propose(hb_barostat *b, hb_forcefield *ff, cudaStream_t s) {
   hb_system *sys = b->sys;
   const double r_search = ff ? (double)ff->r_search : 0.0;
   k_baro_propose<<<1, 1, 0, s>>>(b->d_state, sys->d_box64, sys->d_box, ff->d_scalars, r_search,
-                                 (uint32_t)b->seed, (uint32_t)(b->seed >> 32), ff->d_status);
+                                 (uint32_t)b->seed, (uint32_t)(b->seed >> 32));
   if (b->n_mol)
     k_baro_scale<<<hb_div_up(b->n_mol, 128), 128, 0, s>>>(
         b->d_state, b->d_mol_off, b->d_mol_atoms, b->d_mass, sys->d_posq, sys->d_image,
@@ -226,7 +222,7 @@ int baro_propose(hb_barostat *b, hb_forcefield *ff, cudaStream_t s) {
 int baro_decide(hb_barostat *b, hb_forcefield *ff, cudaStream_t s) {
   hb_system *sys = b->sys;
   k_baro_decide<<<1, 1, 0, s>>>(b->d_state, sys->d_box64, sys->d_box, ff->d_scalars, b->pressure,
-                                b->kt, (double)b->n_mol, ff->d_status);
+                                b->kt, (double)b->n_mol);
   if (sys->n)
     k_baro_restore<<<hb_div_up(sys->n, 256), 256, 0, s>>>(b->d_state, sys->d_posq, sys->d_image,
                                                           sys->d_force, b->d_snap_pos,

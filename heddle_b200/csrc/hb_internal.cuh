@@ -45,6 +45,9 @@ int hb_fail(int code, const std::string &msg);
 #define HB_FP_INV_SCALE (1.0 / 1099511627776.0)
 #define HB_RHO_SCALE 4294967296.0f          /* 2^32 */
 #define HB_N_SCALARS 10                     /* doubles of hb_forcefield_scalars */
+/* largest isotropic lattice scaling |mu - 1| since the last neighbour
+ * rebuild under which the list is kept (the tile boxes carry this margin) */
+#define HB_BOX_SLACK 0.01f
 #define HB_XFIX_SCALE 1099511627776.0       /* 2^40 per bohr */
 #define HB_VFIX_SCALE 72057594037927936.0   /* 2^56 per bohr / aut */
 

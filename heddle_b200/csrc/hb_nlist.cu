@@ -259,9 +259,12 @@ __global__ void k_tile_bbox(const uint32_t *gate, const float4 *__restrict__ til
       c[d] = 0.5f * (lo[d] + hi[d]);
       h[d] = 0.5f * (hi[d] - lo[d]);
     }
+    // the margin also covers a cell scaled by up to HB_BOX_SLACK before the
+    // next rebuild (atoms move by up to that fraction of the half width)
     float m = 0.5f * r_skin + rc_max;
-    bool spc = b.ortho && (h[0] + m <= 0.5f * b.lx) && (h[1] + m <= 0.5f * b.ly) &&
-               (h[2] + m <= 0.5f * b.lz);
+    const float hw = 0.5f - HB_BOX_SLACK;
+    bool spc = b.ortho && (h[0] + m <= hw * b.lx) && (h[1] + m <= hw * b.ly) &&
+               (h[2] + m <= hw * b.lz);
     // bit 0: single periodic copy; bit 1: per-axis minimum-image box tests
     // are exact (orthorhombic cell)
     const int flags = (spc ? 1 : 0) | (b.ortho ? 2 : 0);
@@ -572,24 +575,34 @@ __global__ void k_nl_finish(const uint32_t *gate, uint32_t *status, uint32_t *co
   counters[2] = 0u;
 }
 
+// The list built at reference positions x0 in cell L0 holds every pair
+// within r_c while each atom stays within r_skin / 2 of x0.  A barostat
+// scales the cell (and the positions about the origin): for an isotropic
+// scaling L = mu L0 with |mu - 1| <= HB_BOX_SLACK the test is against the
+// scaled reference mu x0, and a pair within r_c now was within
+// (r_c + 2 d) / mu of its reference separation, so the bound on each
+// atom's displacement d becomes min(r_skin, mu (r_c + r_skin) - r_c) / 2.
+// Any other change of the cell (a shear, a larger scaling, set_box to a new
+// shape) invalidates the list.
 __global__ void k_disp_check(const float4 *__restrict__ posq, const float4 *__restrict__ ref,
                              const DBox *__restrict__ box, const DBox *__restrict__ ref_box,
-                             float thr2, uint32_t *status, uint32_t n) {
+                             float r_skin, float rc_max, uint32_t *status, uint32_t n) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  bool moved = false;
-  // a box that changed since the last rebuild (set_box, a barostat move)
-  // invalidates the list as well
-  if (i == 0u) {
-    const DBox a = *box, r = *ref_box;
-    moved = a.lx != r.lx || a.ly != r.ly || a.lz != r.lz || a.xy != r.xy || a.xz != r.xz ||
-            a.yz != r.yz;
-  }
-  if (i < n) {
-    DBox b = *box;
-    float4 p = posq[i], r = ref[i];
-    float dx = p.x - r.x, dy = p.y - r.y, dz = p.z - r.z;
-    hb_min_image(dx, dy, dz, b);
-    moved = moved || dx * dx + dy * dy + dz * dz > thr2;
+  const DBox a = *box, r = *ref_box;
+  const float mu = a.lx / r.lx;  // r.lx = 0 before the first build: not finite
+  const float tol = 1.0e-6f * a.lx;
+  const bool iso = isfinite(mu) && fabsf(mu - 1.0f) <= HB_BOX_SLACK &&
+                   fabsf(a.ly - mu * r.ly) <= tol && fabsf(a.lz - mu * r.lz) <= tol &&
+                   fabsf(a.xy - mu * r.xy) <= tol && fabsf(a.xz - mu * r.xz) <= tol &&
+                   fabsf(a.yz - mu * r.yz) <= tol;
+  float thr = 0.5f * r_skin;
+  if (mu < 1.0f) thr = fminf(thr, 0.5f * (mu * (rc_max + r_skin) - rc_max));
+  bool moved = i == 0u && (!iso || !(thr > 0.0f));
+  if (i < n && iso) {
+    const float4 p = posq[i], q = ref[i];
+    float dx = p.x - mu * q.x, dy = p.y - mu * q.y, dz = p.z - mu * q.z;
+    hb_min_image(dx, dy, dz, a);
+    moved = moved || dx * dx + dy * dy + dz * dz > thr * thr;
   }
   // one atomic per warp at most
   if (__any_sync(0xFFFFFFFFu, moved) && (threadIdx.x & 31u) == 0u) atomicOr(status, HB_ST_DISPLACED);
@@ -844,10 +857,9 @@ int nl_rebuild_conditional(hb_forcefield *ff, cudaStream_t s) {
 int nl_displacement_check(hb_forcefield *ff, cudaStream_t s) {
   hb_system *sys = ff->sys;
   if (sys->n == 0) return HB_OK;
-  float thr = 0.5f * ff->r_skin;
   k_disp_check<<<hb_div_up(sys->n, 256), 256, 0, s>>>(sys->d_posq, ff->d_ref_pos, sys->d_box,
-                                                       ff->d_ref_box, thr * thr, ff->d_status,
-                                                       sys->n);
+                                                       ff->d_ref_box, ff->r_skin, ff->rc_max,
+                                                       ff->d_status, sys->n);
   HB_CUDA(cudaGetLastError());
   return HB_OK;
 }
