@@ -94,11 +94,17 @@ class System:
         return cls(ctx, spec.positions, spec.masses, spec.charges, spec.types, spec.box,
                    velocities=spec.velocities)
 
-    def state(self):
-        pos = np.zeros(3 * self.n)
-        vel = np.zeros(3 * self.n)
-        img = np.zeros(3 * self.n, dtype=np.int32)
-        frc = np.zeros(3 * self.n)
+    def state(self, out=None):
+        """(positions, velocities, images, forces) as (n, 3) arrays; out: four
+        C-contiguous arrays to fill instead (float64, float64, int32, float64;
+        page-locked ones make the copies fastest)."""
+        if out is None:
+            out = (np.zeros((self.n, 3)), np.zeros((self.n, 3)), np.zeros((self.n, 3), dtype=np.int32),
+                   np.zeros((self.n, 3)))
+        pos, vel, img, frc = out
+        for a, dt in ((pos, np.float64), (vel, np.float64), (img, np.int32), (frc, np.float64)):
+            if a.dtype != dt or not a.flags["C_CONTIGUOUS"] or a.size != 3 * self.n:
+                raise ValueError("state(out=...): four C-contiguous (n, 3) arrays of the right types")
         N.check(self.lib.hb_system_get_state(self.h, N.dptr(pos), N.dptr(vel), N.i32ptr(img), N.dptr(frc)))
         return pos.reshape(-1, 3), vel.reshape(-1, 3), img.reshape(-1, 3), frc.reshape(-1, 3)
 

@@ -259,69 +259,165 @@ extern "C" int hb_system_destroy(hb_system *s) {
   cudaFree(s->d_xfix);
   cudaFree(s->d_red);
   cudaFreeHost(s->h_red);
+  cudaFree(s->d_stage);
+  cudaFree(s->d_stage_img);
+  cudaFree(s->d_bad);
   delete s;
   return HB_OK;
 }
 
+// ---- state transfer: FP64 host arrays <-> the device SoA, converted on the
+// device (the host only copies), so a per-step exchange costs the PCIe
+// transfers and two small kernels.
+namespace {
+
+__global__ void k_state_check(const double *__restrict__ pos, uint32_t *__restrict__ bad,
+                              uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (!isfinite(pos[3 * i]) || !isfinite(pos[3 * i + 1]) || !isfinite(pos[3 * i + 2]))
+    atomicMin(bad, i);
+}
+
+// wrap into the primary cell in FP64, operation by operation as the host
+// upload does it (no contraction), keeping image counts continuous
+__global__ void k_state_in(const double *__restrict__ pos, const double *__restrict__ vel,
+                           const double *__restrict__ b, float4 *__restrict__ posq,
+                           float4 *__restrict__ v, int4 *__restrict__ image, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (pos) {
+    double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+    const double sc = __ddiv_rn(z, b[2]);
+    const double sb = __ddiv_rn(__dsub_rn(y, __dmul_rn(sc, b[5])), b[1]);
+    const double sa =
+        __ddiv_rn(__dsub_rn(__dsub_rn(x, __dmul_rn(sb, b[3])), __dmul_rn(sc, b[4])), b[0]);
+    const double fa = floor(__dadd_rn(sa, 0.5)), fb = floor(__dadd_rn(sb, 0.5)),
+                 fc = floor(__dadd_rn(sc, 0.5));
+    x = __dsub_rn(x, __dadd_rn(__dadd_rn(__dmul_rn(fa, b[0]), __dmul_rn(fb, b[3])),
+                               __dmul_rn(fc, b[4])));
+    y = __dsub_rn(y, __dadd_rn(__dmul_rn(fb, b[1]), __dmul_rn(fc, b[5])));
+    z = __dsub_rn(z, __dmul_rn(fc, b[2]));
+    float4 p = posq[i];
+    p.x = (float)x;
+    p.y = (float)y;
+    p.z = (float)z;
+    posq[i] = p;
+    int4 im = image[i];
+    im.x += (int)fa;
+    im.y += (int)fb;
+    im.z += (int)fc;
+    image[i] = im;
+  }
+  if (vel) {
+    float4 q = v[i];
+    q.x = (float)vel[3 * i];
+    q.y = (float)vel[3 * i + 1];
+    q.z = (float)vel[3 * i + 2];
+    v[i] = q;
+  }
+}
+
+__global__ void k_state_out(const float4 *__restrict__ posq, const float4 *__restrict__ vel,
+                            const float4 *__restrict__ force, const int4 *__restrict__ image,
+                            double *__restrict__ pos, double *__restrict__ velo,
+                            double *__restrict__ frc, int32_t *__restrict__ img, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (pos) {
+    const float4 p = posq[i];
+    pos[3 * i] = p.x;
+    pos[3 * i + 1] = p.y;
+    pos[3 * i + 2] = p.z;
+  }
+  if (velo) {
+    const float4 q = vel[i];
+    velo[3 * i] = q.x;
+    velo[3 * i + 1] = q.y;
+    velo[3 * i + 2] = q.z;
+  }
+  if (frc) {
+    const float4 f = force[i];
+    frc[3 * i] = f.x;
+    frc[3 * i + 1] = f.y;
+    frc[3 * i + 2] = f.z;
+  }
+  if (img) {
+    const int4 m = image[i];
+    img[3 * i] = m.x;
+    img[3 * i + 1] = m.y;
+    img[3 * i + 2] = m.z;
+  }
+}
+
+int stage_alloc(hb_system *sys) {
+  if (sys->d_stage) return HB_OK;
+  const size_t nn = std::max<size_t>(sys->n, 1);
+  HB_CUDA(cudaMalloc(&sys->d_stage, sizeof(double) * 9 * nn));
+  HB_CUDA(cudaMalloc(&sys->d_stage_img, sizeof(int32_t) * 3 * nn));
+  HB_CUDA(cudaMalloc(&sys->d_bad, sizeof(uint32_t)));
+  return HB_OK;
+}
+
+}  // namespace
+
 extern "C" int hb_system_set_state(hb_system *sys, const double *positions,
                                    const double *velocities) {
   HB_REQUIRE(sys, HB_ERR_INVALID_ARGUMENT, "null system");
-  HB_CUDA(cudaStreamSynchronize(sys->ctx->stream));
   const uint32_t n = sys->n;
+  if (!n || (!positions && !velocities)) return HB_OK;
+  HB_TRY(stage_alloc(sys));
+  cudaStream_t s = sys->ctx->stream;
+  double *dp = sys->d_stage, *dv = sys->d_stage + 3 * (size_t)n;
+  const unsigned g = hb_div_up(n, 256);
   if (positions) {
-    HB_TRY(upload_state(sys, positions, velocities, nullptr, true));
-  } else if (velocities && n) {
-    sys->fix_valid = false;
-    std::vector<float4> v(n);
-    for (uint32_t i = 0; i < n; ++i)
-      v[i] = make_float4((float)velocities[3 * i], (float)velocities[3 * i + 1],
-                         (float)velocities[3 * i + 2], (float)(1.0 / sys->h_mass[i]));
-    HB_CUDA(cudaMemcpy(sys->d_vel, v.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+    HB_CUDA(cudaMemcpyAsync(dp, positions, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+    const uint32_t none = 0xFFFFFFFFu;
+    HB_CUDA(cudaMemcpyAsync(sys->d_bad, &none, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    k_state_check<<<g, 256, 0, s>>>(dp, sys->d_bad, n);
+    uint32_t bad = none;
+    HB_CUDA(cudaMemcpyAsync(&bad, sys->d_bad, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    HB_CUDA(cudaStreamSynchronize(s));
+    if (bad != none)
+      return hb_fail(HB_ERR_NOT_FINITE, "non-finite position for atom " + std::to_string(bad));
   }
+  if (velocities)
+    HB_CUDA(cudaMemcpyAsync(dv, velocities, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+  sys->fix_valid = false;
+  k_state_in<<<g, 256, 0, s>>>(positions ? dp : nullptr, velocities ? dv : nullptr,
+                               sys->d_box64, sys->d_posq, sys->d_vel, sys->d_image, n);
+  HB_CUDA(cudaGetLastError());
+  // the host arrays may be reused as soon as the call returns
+  HB_CUDA(cudaStreamSynchronize(s));
   return HB_OK;
 }
 
 extern "C" int hb_system_get_state(hb_system *sys, double *positions, double *velocities,
                                    int32_t *images, double *forces) {
   HB_REQUIRE(sys, HB_ERR_INVALID_ARGUMENT, "null system");
-  HB_CUDA(cudaStreamSynchronize(sys->ctx->stream));
-  HB_CUDA(cudaStreamSynchronize(sys->ctx->stream2));
   const uint32_t n = sys->n;
-  if (!n) return HB_OK;
-  std::vector<float4> buf(n);
-  if (positions) {
-    HB_CUDA(cudaMemcpy(buf.data(), sys->d_posq, sizeof(float4) * n, cudaMemcpyDeviceToHost));
-    for (uint32_t i = 0; i < n; ++i) {
-      positions[3 * i] = buf[i].x;
-      positions[3 * i + 1] = buf[i].y;
-      positions[3 * i + 2] = buf[i].z;
-    }
-  }
-  if (velocities) {
-    HB_CUDA(cudaMemcpy(buf.data(), sys->d_vel, sizeof(float4) * n, cudaMemcpyDeviceToHost));
-    for (uint32_t i = 0; i < n; ++i) {
-      velocities[3 * i] = buf[i].x;
-      velocities[3 * i + 1] = buf[i].y;
-      velocities[3 * i + 2] = buf[i].z;
-    }
-  }
-  if (forces) {
-    HB_CUDA(cudaMemcpy(buf.data(), sys->d_force, sizeof(float4) * n, cudaMemcpyDeviceToHost));
-    for (uint32_t i = 0; i < n; ++i) {
-      forces[3 * i] = buf[i].x;
-      forces[3 * i + 1] = buf[i].y;
-      forces[3 * i + 2] = buf[i].z;
-    }
-  }
-  if (images) {
-    std::vector<int4> im(n);
-    HB_CUDA(cudaMemcpy(im.data(), sys->d_image, sizeof(int4) * n, cudaMemcpyDeviceToHost));
-    for (uint32_t i = 0; i < n; ++i) {
-      images[3 * i] = im[i].x;
-      images[3 * i + 1] = im[i].y;
-      images[3 * i + 2] = im[i].z;
-    }
-  }
+  if (!n || (!positions && !velocities && !images && !forces)) return HB_OK;
+  HB_TRY(stage_alloc(sys));
+  cudaStream_t s = sys->ctx->stream;
+  // work on the second stream is joined into the first one by every force
+  // evaluation; wait for it anyway in case a caller queued some there
+  HB_CUDA(cudaStreamSynchronize(sys->ctx->stream2));
+  const size_t n3 = 3 * (size_t)n;
+  double *dp = sys->d_stage, *dv = dp + n3, *df = dv + n3;
+  k_state_out<<<hb_div_up(n, 256), 256, 0, s>>>(
+      sys->d_posq, sys->d_vel, sys->d_force, sys->d_image, positions ? dp : nullptr,
+      velocities ? dv : nullptr, forces ? df : nullptr, images ? sys->d_stage_img : nullptr, n);
+  HB_CUDA(cudaGetLastError());
+  if (positions)
+    HB_CUDA(cudaMemcpyAsync(positions, dp, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
+  if (velocities)
+    HB_CUDA(cudaMemcpyAsync(velocities, dv, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
+  if (forces)
+    HB_CUDA(cudaMemcpyAsync(forces, df, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
+  if (images)
+    HB_CUDA(cudaMemcpyAsync(images, sys->d_stage_img, sizeof(int32_t) * n3,
+                            cudaMemcpyDeviceToHost, s));
+  HB_CUDA(cudaStreamSynchronize(s));
   return HB_OK;
 }
 

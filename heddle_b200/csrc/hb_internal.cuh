@@ -218,6 +218,12 @@ struct hb_system {
   // FP64 reduction scratch
   double *d_red = nullptr;       // partials
   double *h_red = nullptr;       // pinned
+  // state transfer staging (allocated at the first set_state / get_state):
+  // [3n] positions, [3n] velocities, [3n] forces as FP64, [3n] images, and
+  // the first non-finite atom index of an upload
+  double *d_stage = nullptr;
+  int32_t *d_stage_img = nullptr;
+  uint32_t *d_bad = nullptr;
 };
 
 // SPME reciprocal state
