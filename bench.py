@@ -342,7 +342,7 @@ def run_ours(args):
                           "skin_autotune": tune},
             "launch_mode": ("CUDA graph per step; neighbour rebuild = device-side conditional node"
                             if args.graphs else "eager launches"),
-            "roofline": {"bound": "hbm", "kernel": "k_pair (LJ + erfc pair kernel)",
+            "roofline": {"bound": "hbm", "kernel": "k_pair4 (LJ + erfc pair kernel)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind,
