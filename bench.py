@@ -198,6 +198,36 @@ def run_reference(args):
     return 0
 
 
+def dist_setup(backend: str, local: int = 0):
+    """(world size, rank, torch.distributed or None) from the launcher's
+    environment: one process per GPU, replicas only (no exchange step); the
+    group carries only barriers and the max-over-ranks timing.  A short
+    timeout ends a rank that waits for a dead peer with an error."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world <= 1:
+        return world, rank, None
+    from datetime import timedelta
+
+    import torch
+    import torch.distributed as dist
+
+    kw = {"device_id": torch.device("cuda", local)} if backend == "nccl" else {}
+    dist.init_process_group(backend, timeout=timedelta(seconds=300), **kw)
+    return world, rank, dist
+
+
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest value over all ranks (every rank gets it)."""
+    if dist is None:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args):
     import torch
 
@@ -205,16 +235,9 @@ def run_ours(args):
     from heddle_b200 import systems as S
     from heddle_b200 import units as U
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    world, rank, dist = dist_setup("nccl", local)
 
     spec = S.spc_water(args.molecules, skin_A=args.skin, seed=11 + rank, velocity_seed=5 + rank)
     ctx = hb.Context(local)
@@ -282,10 +305,7 @@ def run_ours(args):
     rebuilds = ff.stats()["rebuilds"] - rebuilds0
     baro_stats = baro.stats() if baro else None
     moves = int(baro_stats["attempted"] - moves0) if baro else 0
-    if dist is not None:
-        tt = torch.tensor([t_ms], device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
+    t_ms = max_over_ranks(t_ms, dist, f"cuda:{local}")
     steps_s = args.steps / (t_ms / 1e3)
     value = world * spec.n * steps_s
     clocks = clk.summary()
@@ -304,10 +324,7 @@ def run_ours(args):
         run(ff, cons, n_steps=1)
         sys_.state(out=host)
     t_e2e = time.perf_counter() - t0
-    if dist is not None:
-        te = torch.tensor([t_e2e], device=f"cuda:{local}")
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        t_e2e = float(te.item())
+    t_e2e = max_over_ranks(t_e2e, dist, f"cuda:{local}")
     e2e_value = world * spec.n * k2 / t_e2e
 
     peak, peak_kind = measured_peaks()
