@@ -105,10 +105,15 @@ typedef struct {
 int hb_system_create(hb_context *ctx, const hb_system_desc *desc,
                      hb_system **out);
 int hb_system_destroy(hb_system *sys);
-/* Overwrite positions / velocities from host ([3n] each, NULL = keep). */
+/* Overwrite positions / velocities from host ([3n] each, NULL = keep).
+ * Positions are wrapped into the cell on the device (FP64, image counts
+ * carried on); a non-finite position is rejected before anything changes.
+ * The arrays are copied as they are (page-locked host memory copies
+ * fastest) and may be reused when the call returns. */
 int hb_system_set_state(hb_system *sys, const double *positions,
                         const double *velocities);
-/* Download positions, velocities, images, forces (any may be NULL). */
+/* Download positions, velocities, images, forces (any may be NULL); the
+ * conversion to FP64 runs on the device. */
 int hb_system_get_state(hb_system *sys, double *positions, double *velocities,
                         int32_t *images, double *forces);
 int hb_system_set_box(hb_system *sys, const double box[6]);
