@@ -47,11 +47,33 @@ __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // a * conj(b)
   return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
 
-// p-point DFT of v (forward: exp(-2 pi i qr / p)), p in {2, 3, 4, 5, 7};
+// p-point DFT of v (forward: exp(-2 pi i qr / p)), p in {2, 3, 4, 5, 7, 8};
 // the twiddle constants are cos / sin of 2 pi k / p.
 template <int P, bool INV>
 __device__ __forceinline__ void butterfly(float2 *v) {
-  if constexpr (P == 2) {
+  if constexpr (P == 8) {
+    // two 4-point DFTs of the even and odd elements, the odd ones turned by
+    // w^k (w = exp(-+2 pi i / 8)), then X_k = E_k + w^k O_k, X_{k+4} = E_k - w^k O_k
+    float2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+    butterfly<4, INV>(e);
+    butterfly<4, INV>(o);
+    const float h = 0.70710678118654752f;
+    const float2 o1 = o[1], o2 = o[2], o3 = o[3];
+    if (INV) {
+      o[1] = make_float2((o1.x - o1.y) * h, (o1.x + o1.y) * h);
+      o[2] = make_float2(-o2.y, o2.x);
+      o[3] = make_float2((-o3.x - o3.y) * h, (o3.x - o3.y) * h);
+    } else {
+      o[1] = make_float2((o1.x + o1.y) * h, (o1.y - o1.x) * h);
+      o[2] = make_float2(o2.y, -o2.x);
+      o[3] = make_float2((o3.y - o3.x) * h, (-o3.x - o3.y) * h);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      v[k] = make_float2(e[k].x + o[k].x, e[k].y + o[k].y);
+      v[k + 4] = make_float2(e[k].x - o[k].x, e[k].y - o[k].y);
+    }
+  } else if constexpr (P == 2) {
     const float2 a = v[0], b = v[1];
     v[0] = make_float2(a.x + b.x, a.y + b.y);
     v[1] = make_float2(a.x - b.x, a.y - b.y);
@@ -152,9 +174,11 @@ __device__ float2 *fft_lines(float2 *A, float2 *B, const float2 *__restrict__ tw
   return A;
 }
 
-// ---- compile-time transforms: radix order 4, 2, 3, 5, 7 (as make_plan) ----
+// ---- compile-time transforms: radix order 8, 4, 2, 3, 5, 7 (fewer shared-
+// memory stages than the runtime plans of make_plan, which start at 4) ----
 __host__ __device__ constexpr int radix_first(int n) {
-  return n % 4 == 0 ? 4 : (n % 2 == 0 ? 2 : (n % 3 == 0 ? 3 : (n % 5 == 0 ? 5 : 7)));
+  return n % 8 == 0 ? 8
+                    : (n % 4 == 0 ? 4 : (n % 2 == 0 ? 2 : (n % 3 == 0 ? 3 : (n % 5 == 0 ? 5 : 7))));
 }
 __host__ __device__ constexpr int stage_radix(int n, int s) {
   int p = radix_first(n);
