@@ -39,7 +39,7 @@ def _time_steps(ctx, sys_, ff, cons, integrator_kwargs, steps, warm) -> float:
 
 def tune_skin(ctx, sys_: System, spec, cons: Constraints | None, integrator_kwargs: dict,
               candidates_A=(1.2, 1.6, 2.0, 2.5, 3.0), residencies=(4, 5, 6, 7, 8),
-              steps: int = 40, warm: int = 10, cache: Path | None = None) -> dict:
+              steps: int = 150, warm: int = 20, cache: Path | None = None) -> dict:
     """Time `steps` graph-mode MD steps per candidate skin (angstrom), then
     per pair-kernel residency at the best skin; return {"best_A": skin,
     "pair_blocks_per_sm": r, "ms_per_step": {skin: ms}, "residency_ms":
