@@ -21,6 +21,7 @@
 // single-periodic-copy condition shift i and j positions against the tile
 // centre once per entry and skip the per-pair minimum image.
 #include <algorithm>
+#include <type_traits>
 
 #include "hb_internal.cuh"
 
@@ -321,7 +322,7 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, 8)
 
 struct P4Warp {
   float4 ipos[32];
-  float4 jpos[32];
+  float4 jpos[64];  // j-slot k at k and k + 32: rotation t of lane L reads L + t
   int itype[32];
   int jtype[32];
   uint32_t oi[32];
@@ -372,7 +373,6 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
   long long elj_fix = 0;  // LJ energy of this lane's pairs (fixed point)
   const DBox b = *box;
   const size_t np_all = (size_t)P.n_tiles * 32u;
-  const uint32_t lt = (1u << lane) - 1u;
   const uint32_t n_items = P.n_tiles * chunks;
 
   // persistent warps take (tile, chunk of entries) items from a counter
@@ -418,6 +418,7 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
       }
       __syncwarp();
       S.jpos[lane] = pj;
+      S.jpos[lane + 32u] = pj;
       S.jtype[lane] = tj;
       S.jslot[lane] = self ? si : sj;
       if (SCALED) {
@@ -435,32 +436,40 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
       }
       __syncwarp();
 
-      // (1) distance pass
+      // (1) distance pass; the tile's single-periodic-copy flag is uniform
+      // over the warp, so each form is its own code path (no per-pair
+      // minimum-image instructions where the shift already placed the atoms)
       uint32_t m = 0u;
-      if (!self) {
+      auto dist_pass = [&](auto sp) {
+        constexpr bool SP = decltype(sp)::value;
+        if (!self) {
 #pragma unroll
-        for (uint32_t t = 0; t < 32u; ++t) {
-          const float4 q = S.jpos[(lane + t) & 31u];
-          float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
-          if (!spc) hb_min_image(dx, dy, dz, b);
-          const float r2 = dx * dx + dy * dy + dz * dz;
-          m |= (r2 < P.rc2_max ? 1u : 0u) << t;
+          for (uint32_t t = 0; t < 32u; ++t) {
+            const float4 q = S.jpos[lane + t];
+            float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
+            if constexpr (!SP) hb_min_image(dx, dy, dz, b);
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            m |= (r2 < P.rc2_max ? 1u : 0u) << t;
+          }
+        } else {
+          for (uint32_t t = 1u; t < 17u; ++t) {
+            const float4 q = S.jpos[lane + t];
+            float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
+            if constexpr (!SP) hb_min_image(dx, dy, dz, b);
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            m |= (r2 < P.rc2_max ? 1u : 0u) << t;
+          }
+          if (lane >= 16u) m &= ~(1u << 16);  // each self pair once
         }
-      } else {
-        for (uint32_t t = 1u; t < 17u; ++t) {
-          const float4 q = S.jpos[(lane + t) & 31u];
-          float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
-          if (!spc) hb_min_image(dx, dy, dz, b);
-          const float r2 = dx * dx + dy * dy + dz * dz;
-          m |= (r2 < P.rc2_max ? 1u : 0u) << t;
-        }
-        if (lane >= 16u) m &= ~(1u << 16);  // each self pair once
-      }
+      };
+      if (spc) dist_pass(std::true_type{});
+      else dist_pass(std::false_type{});
       if (!SCALED) m &= ~xm;
 
-      // (2) slot-major queues of (i-lane, rotation): pairs with a
-      // Lennard-Jones term first, Coulomb-only pairs after them, so the LJ
-      // arithmetic runs only in the (few) iterations that need it
+      // (2) lane-major queues of (i-lane, rotation): each lane writes its
+      // pairs with a Lennard-Jones term to [0, n_lj) and its Coulomb-only
+      // pairs to [n_lj, n_lj + n_c) at offsets from one warp scan of the
+      // packed counts; the LJ arithmetic runs only over the first range
       uint32_t lj_rot = 0xFFFFFFFFu;
       if (!P.lj_on) {
         lj_rot = 0u;
@@ -475,125 +484,149 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
       }
       uint32_t mq = m & lj_rot;
       uint32_t mc = P.coul_on ? (m & ~lj_rot) : 0u;
-      uint32_t np = 0, n_lj = 0;
-      for (int pass = 0; pass < 2; ++pass) {
-        uint32_t mm = pass == 0 ? mq : mc;
-        while (true) {
-          const bool has = mm != 0u;
-          const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
-          if (bal == 0u) break;
-          if (has) {
-            const uint32_t t = (uint32_t)__ffs(mm) - 1u;
-            mm &= mm - 1u;
-            S.pairs[np + __popc(bal & lt)] = (uint16_t)((lane << 8) | t);
-          }
-          np += __popc(bal);
+      const uint32_t cnt = ((uint32_t)__popc(mq) << 16) | (uint32_t)__popc(mc);
+      uint32_t incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= (uint32_t)o) incl += v;
+      }
+      const uint32_t tot = __shfl_sync(0xFFFFFFFFu, incl, 31);
+      const uint32_t n_lj = tot >> 16, n_c = tot & 0xFFFFu;
+      {
+        const uint32_t ex = incl - cnt;
+        uint32_t pos = ex >> 16;
+        while (mq != 0u) {
+          const uint32_t t = (uint32_t)__ffs(mq) - 1u;
+          mq &= mq - 1u;
+          S.pairs[pos++] = (uint16_t)((lane << 8) | t);
         }
-        if (pass == 0) n_lj = np;
+        pos = n_lj + (ex & 0xFFFFu);
+        while (mc != 0u) {
+          const uint32_t t = (uint32_t)__ffs(mc) - 1u;
+          mc &= mc - 1u;
+          S.pairs[pos++] = (uint16_t)((lane << 8) | t);
+        }
       }
       __syncwarp();
 
-      // (3) math over the queue
-      for (uint32_t k = lane; k < np; k += 32u) {
-        const uint32_t pr = S.pairs[k];
-        const uint32_t i = pr >> 8, t = pr & 255u, j = (i + t) & 31u;
-        const bool ljq = k < n_lj;
-        const float4 a = S.ipos[i], q = S.jpos[j];
-        float dx = a.x - q.x, dy = a.y - q.y, dz = a.z - q.z;
-        if (!spc) hb_min_image(dx, dy, dz, b);
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        float s_lj = 1.0f, s_c = 1.0f;
-        if (SCALED && ((S.xm[i] >> t) & 1u)) {
-          s_lj = 0.0f;
-          s_c = 0.0f;
-          const uint32_t oi = S.oi[i], oj = S.oj[j];
-          for (uint32_t z = eoff[oj]; z < eoff[oj + 1]; ++z) {
-            if (epart[z] == oi) {
-              const float2 sc = escale[z];
-              s_lj = sc.x;
-              s_c = sc.y;
-              break;
+      // (3) math over each range: in round `it` lane L takes pair
+      // L * rounds + it, so one round's pairs come from different i-lanes
+      // (few same-address accumulator atomics); one code path per periodic
+      // form and per range
+      auto math_pass = [&](auto sp, auto ljc, uint32_t q0, uint32_t cnt_r) {
+        constexpr bool SP = decltype(sp)::value, LJQ = decltype(ljc)::value;
+        const uint32_t rounds = (cnt_r + 31u) >> 5;
+        for (uint32_t it = 0; it < rounds; ++it) {
+          const uint32_t kk = lane * rounds + it;
+          if (kk < cnt_r) {
+            const uint32_t pr = S.pairs[q0 + kk];
+            const uint32_t i = pr >> 8, t = pr & 255u, j = (i + t) & 31u;
+            const float4 a = S.ipos[i], q = S.jpos[j];
+            float dx = a.x - q.x, dy = a.y - q.y, dz = a.z - q.z;
+            if constexpr (!SP) hb_min_image(dx, dy, dz, b);
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            float s_lj = 1.0f, s_c = 1.0f;
+            if (SCALED && ((S.xm[i] >> t) & 1u)) {
+              s_lj = 0.0f;
+              s_c = 0.0f;
+              const uint32_t oi = S.oi[i], oj = S.oj[j];
+              for (uint32_t z = eoff[oj]; z < eoff[oj + 1]; ++z) {
+                if (epart[z] == oi) {
+                  const float2 sc = escale[z];
+                  s_lj = sc.x;
+                  s_c = sc.y;
+                  break;
+                }
+              }
             }
-          }
-        }
-        const float inv_r = rsqrtf(r2);
-        const float inv_r2 = inv_r * inv_r;
-        float fac = 0.0f, en = 0.0f;
-        if (ljq) {
-          const int tp = S.itype[i] + S.jtype[j];
-          const float4 L = sm_lj4[tp];
-          if (r2 <= L.z && L.y != 0.0f && s_lj != 0.0f) {
-            const float sr2 = L.x * inv_r2;
-            const float sr6 = sr2 * sr2 * sr2;
-            const float sr12 = sr6 * sr6;
-            float f = L.y * inv_r2 * (2.0f * sr12 - sr6);
-            float u = (L.y * (1.0f / 6.0f)) * (sr12 - sr6);
-            if (SWITCH && r2 > L.w) {
-              const float inv_d = sm_ljd4[tp];
-              const float tau = (r2 - L.w) * inv_d;
-              const float omt = 1.0f - tau;
-              const float sw = omt * omt * (1.0f + 2.0f * tau);
-              const float chain = 12.0f * tau * omt * inv_d;
-              f = sw * f + chain * u;
-              u = sw * u;
+            const float inv_r = rsqrtf(r2);
+            const float inv_r2 = inv_r * inv_r;
+            float fac = 0.0f, en = 0.0f;
+            if constexpr (LJQ) {
+              const int tp = S.itype[i] + S.jtype[j];
+              const float4 L = sm_lj4[tp];
+              if (r2 <= L.z && L.y != 0.0f && s_lj != 0.0f) {
+                const float sr2 = L.x * inv_r2;
+                const float sr6 = sr2 * sr2 * sr2;
+                const float sr12 = sr6 * sr6;
+                float f = L.y * inv_r2 * (2.0f * sr12 - sr6);
+                float u = (L.y * (1.0f / 6.0f)) * (sr12 - sr6);
+                if (SWITCH && r2 > L.w) {
+                  const float inv_d = sm_ljd4[tp];
+                  const float tau = (r2 - L.w) * inv_d;
+                  const float omt = 1.0f - tau;
+                  const float sw = omt * omt * (1.0f + 2.0f * tau);
+                  const float chain = 12.0f * tau * omt * inv_d;
+                  f = sw * f + chain * u;
+                  u = sw * u;
+                }
+                fac += s_lj * f;
+                if (EV) {
+                  en += s_lj * u;
+                  elj_fix += to_fixed(s_lj * u);
+                }
+              }
             }
-            fac += s_lj * f;
+            if (P.coul_on && r2 <= P.coul_rc2 && s_c != 0.0f) {
+              const float r = r2 * inv_r;
+              const float ar = P.alpha * r;
+              const float gg = __expf(-ar * ar);
+              const float tt = __fdividef(1.0f, 1.0f + 0.3275911f * ar);
+              const float poly =
+                  0.254829592f +
+                  (-0.284496736f + (1.421413741f + (-1.453152027f + 1.061405429f * tt) * tt) * tt) * tt;
+              const float erfc_ar = poly * tt * gg;
+              fac += s_c * a.w * q.w * inv_r2 * (erfc_ar * inv_r + P.c2a * gg);
+              if (EV) en += s_c * a.w * q.w * erfc_ar * inv_r;
+            }
+            const float fx = fac * dx, fy = fac * dy, fz = fac * dz;
             if (EV) {
-              en += s_lj * u;
-              elj_fix += to_fixed(s_lj * u);
+              // half of the pair's energy and virial to each atom (integer sums:
+              // order-independent)
+              const float he = 0.5f * en, hw = 0.5f * fac * r2;
+              if (fabsf(he) <= P4_EMAX && fabsf(hw) <= P4_EMAX) {
+                const int ie = __float2int_rn(he * P4_ESCALE), iw = __float2int_rn(hw * P4_ESCALE);
+                atomicAdd(&Ev[i], ie);
+                atomicAdd(&Ev[32 + i], iw);
+                atomicAdd(&Ev[64 + j], ie);
+                atomicAdd(&Ev[96 + j], iw);
+              } else {
+                const uint32_t ti_slot = I * 32u + i, tj_slot = S.jslot[j];
+                red_add(&fp[3 * np_all + ti_slot], to_fixed(he));
+                red_add(&fp[4 * np_all + ti_slot], to_fixed(hw));
+                red_add(&fp[3 * np_all + tj_slot], to_fixed(he));
+                red_add(&fp[4 * np_all + tj_slot], to_fixed(hw));
+              }
+            }
+            if (fabsf(fx) <= P4_FMAX && fabsf(fy) <= P4_FMAX && fabsf(fz) <= P4_FMAX) {
+              const int ix = __float2int_rn(fx * P4_SCALE), iy = __float2int_rn(fy * P4_SCALE),
+                        iz = __float2int_rn(fz * P4_SCALE);
+              atomicAdd(&S.fi[0][i], ix);
+              atomicAdd(&S.fi[1][i], iy);
+              atomicAdd(&S.fi[2][i], iz);
+              atomicAdd(&S.fj[0][j], -ix);
+              atomicAdd(&S.fj[1][j], -iy);
+              atomicAdd(&S.fj[2][j], -iz);
+            } else {
+              // rare: the exact int64 path for both atoms
+              const uint32_t ti_slot = I * 32u + i, tj_slot = S.jslot[j];
+              red_add(&fp[0 * np_all + ti_slot], to_fixed(fx));
+              red_add(&fp[1 * np_all + ti_slot], to_fixed(fy));
+              red_add(&fp[2 * np_all + ti_slot], to_fixed(fz));
+              red_add(&fp[0 * np_all + tj_slot], -to_fixed(fx));
+              red_add(&fp[1 * np_all + tj_slot], -to_fixed(fy));
+              red_add(&fp[2 * np_all + tj_slot], -to_fixed(fz));
             }
           }
         }
-        if (P.coul_on && r2 <= P.coul_rc2 && s_c != 0.0f) {
-          const float r = r2 * inv_r;
-          const float ar = P.alpha * r;
-          const float gg = __expf(-ar * ar);
-          const float tt = __fdividef(1.0f, 1.0f + 0.3275911f * ar);
-          const float poly =
-              0.254829592f +
-              (-0.284496736f + (1.421413741f + (-1.453152027f + 1.061405429f * tt) * tt) * tt) * tt;
-          const float erfc_ar = poly * tt * gg;
-          fac += s_c * a.w * q.w * inv_r2 * (erfc_ar * inv_r + P.c2a * gg);
-          if (EV) en += s_c * a.w * q.w * erfc_ar * inv_r;
-        }
-        const float fx = fac * dx, fy = fac * dy, fz = fac * dz;
-        if (EV) {
-          // half of the pair's energy and virial to each atom (integer sums:
-          // order-independent)
-          const float he = 0.5f * en, hw = 0.5f * fac * r2;
-          if (fabsf(he) <= P4_EMAX && fabsf(hw) <= P4_EMAX) {
-            const int ie = __float2int_rn(he * P4_ESCALE), iw = __float2int_rn(hw * P4_ESCALE);
-            atomicAdd(&Ev[i], ie);
-            atomicAdd(&Ev[32 + i], iw);
-            atomicAdd(&Ev[64 + j], ie);
-            atomicAdd(&Ev[96 + j], iw);
-          } else {
-            const uint32_t ti_slot = I * 32u + i, tj_slot = S.jslot[j];
-            red_add(&fp[3 * np_all + ti_slot], to_fixed(he));
-            red_add(&fp[4 * np_all + ti_slot], to_fixed(hw));
-            red_add(&fp[3 * np_all + tj_slot], to_fixed(he));
-            red_add(&fp[4 * np_all + tj_slot], to_fixed(hw));
-          }
-        }
-        if (fabsf(fx) <= P4_FMAX && fabsf(fy) <= P4_FMAX && fabsf(fz) <= P4_FMAX) {
-          const int ix = __float2int_rn(fx * P4_SCALE), iy = __float2int_rn(fy * P4_SCALE),
-                    iz = __float2int_rn(fz * P4_SCALE);
-          atomicAdd(&S.fi[0][i], ix);
-          atomicAdd(&S.fi[1][i], iy);
-          atomicAdd(&S.fi[2][i], iz);
-          atomicAdd(&S.fj[0][j], -ix);
-          atomicAdd(&S.fj[1][j], -iy);
-          atomicAdd(&S.fj[2][j], -iz);
-        } else {
-          // rare: the exact int64 path for both atoms
-          const uint32_t ti_slot = I * 32u + i, tj_slot = S.jslot[j];
-          red_add(&fp[0 * np_all + ti_slot], to_fixed(fx));
-          red_add(&fp[1 * np_all + ti_slot], to_fixed(fy));
-          red_add(&fp[2 * np_all + ti_slot], to_fixed(fz));
-          red_add(&fp[0 * np_all + tj_slot], -to_fixed(fx));
-          red_add(&fp[1 * np_all + tj_slot], -to_fixed(fy));
-          red_add(&fp[2 * np_all + tj_slot], -to_fixed(fz));
-        }
+      };
+      if (spc) {
+        math_pass(std::true_type{}, std::true_type{}, 0u, n_lj);
+        math_pass(std::true_type{}, std::false_type{}, n_lj, n_c);
+      } else {
+        math_pass(std::false_type{}, std::true_type{}, 0u, n_lj);
+        math_pass(std::false_type{}, std::false_type{}, n_lj, n_c);
       }
       __syncwarp();
       ax += (long long)S.fi[0][lane] << P4_SHIFT;
