@@ -296,21 +296,23 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, 8)
 
 // ---------------------------------------------------------------------
 // Balanced form (every step; with EV also per-atom energy and virial).
-// Per entry: (1) a distance pass over the 32
-// rotations (unrolled for ordinary entries) leaves each lane's mask of
-// rotations whose pair is inside the cutoff; exclusions are folded in with
-// one AND per entry; (2) the set bits are dealt slot-major into a per-warp
-// queue (each lane's first pair, then each lane's second, ...), so the
-// pairs spread evenly over the 32 lanes whatever their spatial imbalance;
-// (3) the math pass evaluates the queue 32 pairs at a time.  Both i- and
-// j-forces go to per-warp int32 fixed-point accumulators in shared memory
-// (scale 2^30, integer atomics: order-independent, so the result is the
-// same run to run) that are folded into int64 once per entry.  A pair force
-// component above 0.06 hartree/bohr takes the exact global int64 path
-// instead, so the int32 sums cannot wrap (32 pairs x 0.06 x 2^30 < 2^31).
-// With EV the energy and virial halves of each pair go the same way at
-// scale 2^28 (guard 0.25 hartree), and the LJ energy total is summed per
-// lane in int64.
+// One lane per i-atom of the tile.  Per entry: (1) a distance pass over the
+// 32 rotations (unrolled for ordinary entries) leaves each lane's mask of
+// the rotations whose pair is inside the cutoff (bit t: j-slot
+// (lane + t) mod 32), with exclusions and padding slots masked out; (2) one
+// warp scan of the mask counts places every lane's pairs contiguously in a
+// per-warp queue (pairs with a Lennard-Jones term first); (3) the math pass
+// gives each lane a run of the queue, so all lanes stay busy whatever the
+// spatial imbalance.  Forces are int32 fixed point (scale 2^30, integer
+// sums: order-independent, so the result is the same run to run): the
+// i-side sums of a lane's run, which touches few i-atoms, stay in registers
+// and are added to shared memory once per atom; the j-side sums go to
+// shared memory by atomics, into one of two copies per slot.  Both are
+// folded into int64 once per entry.  A pair force component above 0.06
+// hartree/bohr takes the exact global int64 path instead, so the int32
+// sums cannot wrap (32 pairs x 0.06 x 2^30 < 2^31).  With EV the energy and
+// virial halves of each pair go to shared int32 sums at scale 2^28 (guard
+// 0.25 hartree), and the LJ energy total is summed per lane in int64.
 // ---------------------------------------------------------------------
 #define P4_WARPS 4
 #define P4_SHIFT 10               // 2^40 / 2^30
@@ -322,7 +324,9 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, 8)
 
 struct P4Warp {
   float4 ipos[32];
-  float4 jpos[64];  // j-slot k at k and k + 32: rotation t of lane L reads L + t
+  float4 jpos[32];
+  float2 jxy[64];  // j-slot k's x, y at k and k + 32: rotation t of lane L reads L + t
+  float jz[64];
   int itype[32];
   int jtype[32];
   uint32_t oi[32];
@@ -330,7 +334,7 @@ struct P4Warp {
   uint32_t xm[32];
   uint32_t jslot[32];
   int fi[3][32];
-  int fj[3][32];
+  int fj[3][80];  // two copies per j-slot, [j] and [48 + j], 16 banks apart
   uint16_t pairs[1024];
 };
 
@@ -418,7 +422,10 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
       }
       __syncwarp();
       S.jpos[lane] = pj;
-      S.jpos[lane + 32u] = pj;
+      S.jxy[lane] = make_float2(pj.x, pj.y);
+      S.jxy[lane + 32u] = make_float2(pj.x, pj.y);
+      S.jz[lane] = pj.z;
+      S.jz[lane + 32u] = pj.z;
       S.jtype[lane] = tj;
       S.jslot[lane] = self ? si : sj;
       if (SCALED) {
@@ -429,6 +436,7 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
       for (int q = 0; q < 3; ++q) {
         S.fi[q][lane] = 0;
         S.fj[q][lane] = 0;
+        S.fj[q][48 + lane] = 0;
       }
       if (EV) {
 #pragma unroll
@@ -445,16 +453,18 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
         if (!self) {
 #pragma unroll
           for (uint32_t t = 0; t < 32u; ++t) {
-            const float4 q = S.jpos[lane + t];
-            float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
+            const float2 q = S.jxy[lane + t];
+            const float qz = S.jz[lane + t];
+            float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - qz;
             if constexpr (!SP) hb_min_image(dx, dy, dz, b);
             const float r2 = dx * dx + dy * dy + dz * dz;
             m |= (r2 < P.rc2_max ? 1u : 0u) << t;
           }
         } else {
           for (uint32_t t = 1u; t < 17u; ++t) {
-            const float4 q = S.jpos[lane + t];
-            float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
+            const float2 q = S.jxy[lane + t];
+            const float qz = S.jz[lane + t];
+            float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - qz;
             if constexpr (!SP) hb_min_image(dx, dy, dz, b);
             const float r2 = dx * dx + dy * dy + dz * dz;
             m |= (r2 < P.rc2_max ? 1u : 0u) << t;
@@ -464,6 +474,10 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
       };
       if (spc) dist_pass(std::true_type{});
       else dist_pass(std::false_type{});
+      // padding slots take part in no pair, whatever their placeholder
+      // coordinates give under the minimum image
+      const uint32_t jv_mask = __ballot_sync(0xFFFFFFFFu, jvalid);
+      m &= ivalid ? __funnelshift_r(jv_mask, jv_mask, lane) : 0u;
       if (!SCALED) m &= ~xm;
 
       // (2) lane-major queues of (i-lane, rotation): each lane writes its
@@ -511,12 +525,17 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
       __syncwarp();
 
       // (3) math over each range: in round `it` lane L takes pair
-      // L * rounds + it, so one round's pairs come from different i-lanes
-      // (few same-address accumulator atomics); one code path per periodic
-      // form and per range
+      // L * rounds + it, so a lane's pairs are a run of the queue that spans
+      // few i-lanes: their i-side sums stay in registers and reach shared
+      // memory once per i-atom.  The j-side sums go to one of two copies
+      // (by lane parity), which halves the same-slot atomics of a round.
+      // One code path per periodic form and per range.
+      const uint32_t jo = (lane & 1u) * 48u;
       auto math_pass = [&](auto sp, auto ljc, uint32_t q0, uint32_t cnt_r) {
         constexpr bool SP = decltype(sp)::value, LJQ = decltype(ljc)::value;
         const uint32_t rounds = (cnt_r + 31u) >> 5;
+        uint32_t ci = 32u;  // i-lane of the running sums (32: none)
+        int sx = 0, sy = 0, sz = 0;
         for (uint32_t it = 0; it < rounds; ++it) {
           const uint32_t kk = lane * rounds + it;
           if (kk < cnt_r) {
@@ -576,11 +595,15 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
               const float poly =
                   0.254829592f +
                   (-0.284496736f + (1.421413741f + (-1.453152027f + 1.061405429f * tt) * tt) * tt) * tt;
-              const float erfc_ar = poly * tt * gg;
-              fac += s_c * a.w * q.w * inv_r2 * (erfc_ar * inv_r + P.c2a * gg);
-              if (EV) en += s_c * a.w * q.w * erfc_ar * inv_r;
+              // erfc(ar) / r + c2a exp(-a^2 r^2) = gg (poly tt / r + c2a)
+              const float pt = poly * tt;
+              fac += s_c * a.w * q.w * inv_r2 * (gg * fmaf(pt, inv_r, P.c2a));
+              if (EV) en += s_c * a.w * q.w * (pt * gg) * inv_r;
             }
-            const float fx = fac * dx, fy = fac * dy, fz = fac * dz;
+            // the pair force in units of 2^-30 (an exact power-of-two scale,
+            // so the rounding is that of fac * d)
+            const float fs = fac * P4_SCALE;
+            const float fx = fs * dx, fy = fs * dy, fz = fs * dz;
             if (EV) {
               // half of the pair's energy and virial to each atom (integer sums:
               // order-independent)
@@ -599,26 +622,45 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
                 red_add(&fp[4 * np_all + tj_slot], to_fixed(hw));
               }
             }
-            if (fabsf(fx) <= P4_FMAX && fabsf(fy) <= P4_FMAX && fabsf(fz) <= P4_FMAX) {
-              const int ix = __float2int_rn(fx * P4_SCALE), iy = __float2int_rn(fy * P4_SCALE),
-                        iz = __float2int_rn(fz * P4_SCALE);
-              atomicAdd(&S.fi[0][i], ix);
-              atomicAdd(&S.fi[1][i], iy);
-              atomicAdd(&S.fi[2][i], iz);
-              atomicAdd(&S.fj[0][j], -ix);
-              atomicAdd(&S.fj[1][j], -iy);
-              atomicAdd(&S.fj[2][j], -iz);
+            constexpr float FLIM = P4_FMAX * P4_SCALE;
+            if (fabsf(fx) <= FLIM && fabsf(fy) <= FLIM && fabsf(fz) <= FLIM) {
+              const int ix = __float2int_rn(fx), iy = __float2int_rn(fy), iz = __float2int_rn(fz);
+              atomicAdd(&S.fj[0][jo + j], -ix);
+              atomicAdd(&S.fj[1][jo + j], -iy);
+              atomicAdd(&S.fj[2][jo + j], -iz);
+              // an i-atom has at most 32 pairs in an entry, so the running
+              // sums stay below 32 x 0.06 x 2^30 < 2^31 like the shared ones
+              if (i != ci) {
+                if (ci < 32u) {
+                  atomicAdd(&S.fi[0][ci], sx);
+                  atomicAdd(&S.fi[1][ci], sy);
+                  atomicAdd(&S.fi[2][ci], sz);
+                }
+                ci = i;
+                sx = sy = sz = 0;
+              }
+              sx += ix;
+              sy += iy;
+              sz += iz;
             } else {
               // rare: the exact int64 path for both atoms
               const uint32_t ti_slot = I * 32u + i, tj_slot = S.jslot[j];
-              red_add(&fp[0 * np_all + ti_slot], to_fixed(fx));
-              red_add(&fp[1 * np_all + ti_slot], to_fixed(fy));
-              red_add(&fp[2 * np_all + ti_slot], to_fixed(fz));
-              red_add(&fp[0 * np_all + tj_slot], -to_fixed(fx));
-              red_add(&fp[1 * np_all + tj_slot], -to_fixed(fy));
-              red_add(&fp[2 * np_all + tj_slot], -to_fixed(fz));
+              const long long lx = __float2ll_rn(fx * (HB_FP_SCALE / P4_SCALE)),
+                              ly = __float2ll_rn(fy * (HB_FP_SCALE / P4_SCALE)),
+                              lz = __float2ll_rn(fz * (HB_FP_SCALE / P4_SCALE));
+              red_add(&fp[0 * np_all + ti_slot], lx);
+              red_add(&fp[1 * np_all + ti_slot], ly);
+              red_add(&fp[2 * np_all + ti_slot], lz);
+              red_add(&fp[0 * np_all + tj_slot], -lx);
+              red_add(&fp[1 * np_all + tj_slot], -ly);
+              red_add(&fp[2 * np_all + tj_slot], -lz);
             }
           }
+        }
+        if (ci < 32u) {
+          atomicAdd(&S.fi[0][ci], sx);
+          atomicAdd(&S.fi[1][ci], sy);
+          atomicAdd(&S.fi[2][ci], sz);
         }
       };
       if (spc) {
@@ -632,9 +674,9 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
       ax += (long long)S.fi[0][lane] << P4_SHIFT;
       ay += (long long)S.fi[1][lane] << P4_SHIFT;
       az += (long long)S.fi[2][lane] << P4_SHIFT;
-      const long long jx = (long long)S.fj[0][lane] << P4_SHIFT;
-      const long long jy = (long long)S.fj[1][lane] << P4_SHIFT;
-      const long long jz = (long long)S.fj[2][lane] << P4_SHIFT;
+      const long long jx = ((long long)S.fj[0][lane] + S.fj[0][48 + lane]) << P4_SHIFT;
+      const long long jy = ((long long)S.fj[1][lane] + S.fj[1][48 + lane]) << P4_SHIFT;
+      const long long jz = ((long long)S.fj[2][lane] + S.fj[2][48 + lane]) << P4_SHIFT;
       if (self) {
         ax += jx;
         ay += jy;
