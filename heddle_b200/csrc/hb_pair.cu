@@ -142,6 +142,11 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, 8)
     }                                                                 \
   }
 
+    // valid j-slots in this lane's rotation order; padding slots take part
+    // in no pair, whatever their placeholder coordinates give under the
+    // minimum image
+    const uint32_t jv_mask = __ballot_sync(0xFFFFFFFFu, jvalid);
+    const uint32_t jv_rot = ivalid ? __funnelshift_r(jv_mask, jv_mask, lane) : 0u;
     uint32_t t0 = 0u, t1 = 32u;
     if (self) {
       HB_ROTATE();
@@ -159,7 +164,7 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, 8)
       if (!spc) hb_min_image(dx, dy, dz, b);
       const float r2 = dx * dx + dy * dy + dz * dz;
       const bool excl = (xm >> t) & 1u;
-      bool active = r2 < P.rc2_max && (SCALED || !excl);
+      bool active = r2 < P.rc2_max && (SCALED || !excl) && ((jv_rot >> t) & 1u);
       if (self && t == 16u && lane >= 16u) active = false;
       if (active) {
         float s_lj = 1.0f, s_c = 1.0f;
@@ -841,6 +846,12 @@ __global__ void __launch_bounds__(P2_WARPS * 32)
       bool act = r2 < P.rc2_max && (SCALED || !((xm >> t) & 1u));
       if (self && t == 16 && lane >= 16u) act = false;
       mask |= (act ? 1u : 0u) << t;
+    }
+    // padding slots take part in no pair, whatever their placeholder
+    // coordinates give under the minimum image
+    {
+      const uint32_t jv_mask = __ballot_sync(0xFFFFFFFFu, jvalid);
+      mask &= ivalid ? __funnelshift_r(jv_mask, jv_mask, lane) : 0u;
     }
     // (2) slot-major pair list
     const uint32_t maxcnt = __reduce_max_sync(0xFFFFFFFFu, (uint32_t)__popc(mask));

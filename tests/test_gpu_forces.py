@@ -208,9 +208,9 @@ def test_compiled_fft_sizes_match_oracle(ctx, grid):
     lambda: S.peptide_in_water(),
 ], ids=["water512", "argon10000", "chain"])
 def test_force_only_kernel_matches_oracle(ctx, maker):
-    # steps without energies run the balanced pair kernel (slot-major pair
-    # queue, int32 shared-memory sums); steps with energies run the rotation
-    # sweep: both within the force tolerance, repeat runs identical
+    # steps without and with energies both run the balanced pair kernel
+    # (int32 fixed-point sums, energies only in the second): both within the
+    # force tolerance, repeat runs identical
     spec = maker()
     sys_ = hb.System.from_spec(ctx, spec)
     ff = hb.ForceField.from_spec(sys_, spec)
@@ -244,3 +244,26 @@ def test_force_only_kernel_large_pair_forces(ctx):
     assert rms_rel(F, Fo) <= FORCE_RMS_TOL
     assert np.abs(F[:2] - Fo[:2]).max() <= 1e-5 * np.abs(Fo[:2]).max()
     ff.close(), sys_.close()
+
+
+@pytest.mark.parametrize("kernel", ["balanced", "compact", "rotation", "exact"])
+def test_small_cells_with_padding_slots(ctx, monkeypatch, kernel):
+    # 127 waters (381 atoms: the last tile and many list entries end in
+    # padding slots) in cells so small that no tile fits a single periodic
+    # copy, so every pair takes the minimum image; over a range of cell
+    # sizes the padding slots' placeholder coordinates wrap to arbitrary
+    # places under the minimum image and must still take part in no pair
+    if kernel in ("compact", "rotation"):
+        monkeypatch.setenv("HB_PAIR_KERNEL", kernel)
+    else:
+        monkeypatch.delenv("HB_PAIR_KERNEL", raising=False)
+    for density in (997.0, 985.0, 971.0, 958.0, 944.0, 930.0):
+        spec = S.spc_water(127, density=density, r_cut_A=6.0, skin_A=1.0, seed=9)
+        sys_ = hb.System.from_spec(ctx, spec)
+        ff = hb.ForceField.from_spec(sys_, spec, exact_pairs=(kernel == "exact"))
+        ff.step(scalars=False)
+        pos, F = sys_.positions(), sys_.forces()
+        ff.close(), sys_.close()
+        assert np.isfinite(F).all()
+        Fo, _, _, _ = O.forces(spec, pos)
+        assert rms_rel(F, Fo) <= FORCE_RMS_TOL, (density, rms_rel(F, Fo))
