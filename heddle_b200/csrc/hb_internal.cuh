@@ -238,6 +238,7 @@ struct SpmeState {
   float2 *d_tw = nullptr;                     // twiddles a | b | c
   double *d_part = nullptr;                   // energy / virial partials
   int n_part = 0;
+  int use_plane = 0;                          // kc-major planes + whole-plane pass
   double *d_sums = nullptr;                   // [2] E_recip, W_recip
   float4 *d_recip = nullptr;                  // per sorted atom fx, fy, fz, e
   float self_pref = 0.f;                      // alpha / sqrt(pi)

@@ -24,9 +24,14 @@
 //              transform -- the convolution costs no extra grid pass;
 //   ifft_b, ifft_c (Hermitian extension, real part) -> V;
 //   gather   : one thread per atom, p^3 reads of V, force, energy share.
-// The FFT is a Stockham autosort transform with radix 4, 2, 3, 5, 7
-// butterflies, twiddles from an FP64-built table, lines held in shared
-// memory with a padded stride.  It is deterministic by construction.
+// The line passes are Stockham autosort transforms with radix 8, 4, 2, 3,
+// 5, 7 butterflies, twiddles from an FP64-built table, lines held in shared
+// memory with a padded stride.  For 64 x 64 and 128 x 128 (a, b) planes
+// the c pass writes kc-major planes instead, and one whole-plane pass per
+// kc replaces fft_b, fft_a and ifft_b: both forward transforms, the
+// influence function and both inverse transforms run in place on the plane
+// in shared memory (radix-16 and radix-8 stages).  Deterministic by
+// construction.
 #include <cmath>
 #include <vector>
 
@@ -72,6 +77,41 @@ __device__ __forceinline__ void butterfly(float2 *v) {
     for (int k = 0; k < 4; ++k) {
       v[k] = make_float2(e[k].x + o[k].x, e[k].y + o[k].y);
       v[k + 4] = make_float2(e[k].x - o[k].x, e[k].y - o[k].y);
+    }
+  } else if constexpr (P == 16) {
+    // 4 x 4: 4-point DFTs of the elements n2, n2 + 4, n2 + 8, n2 + 12, turned
+    // by w^(n2 k1) (w = exp(-+2 pi i / 16)), then 4-point DFTs across n2:
+    // X[k1 + 4 k2]; the twiddles are cos / sin of multiples of pi / 8
+    float2 a[4][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+      float2 t[4] = {v[n2], v[n2 + 4], v[n2 + 8], v[n2 + 12]};
+      butterfly<4, INV>(t);
+#pragma unroll
+      for (int k1 = 0; k1 < 4; ++k1) a[n2][k1] = t[k1];
+    }
+    constexpr float c16[10] = {1.0f, 0.92387953251128674f, 0.70710678118654752f,
+                               0.38268343236508977f, 0.0f, -0.38268343236508977f,
+                               -0.70710678118654752f, -0.92387953251128674f, -1.0f,
+                               -0.92387953251128674f};
+    constexpr float s16[10] = {0.0f, 0.38268343236508977f, 0.70710678118654752f,
+                               0.92387953251128674f, 1.0f, 0.92387953251128674f,
+                               0.70710678118654752f, 0.38268343236508977f, 0.0f,
+                               -0.38268343236508977f};
+#pragma unroll
+    for (int n2 = 1; n2 < 4; ++n2)
+#pragma unroll
+      for (int k1 = 1; k1 < 4; ++k1) {
+        const int e = n2 * k1;
+        const float2 w = make_float2(c16[e], INV ? s16[e] : -s16[e]);
+        a[n2][k1] = cmul(a[n2][k1], w);
+      }
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+      float2 t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+      butterfly<4, INV>(t);
+#pragma unroll
+      for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = t[k2];
     }
   } else if constexpr (P == 2) {
     const float2 a = v[0], b = v[1];
@@ -328,8 +368,10 @@ __global__ void k_spread(const float4 *__restrict__ tile_posq, const DBox *__res
   }
 }
 
-// forward transform along c, one CTA per L rows; clears the int64 grid
-template <int N>
+// forward transform along c, one CTA per L rows; clears the int64 grid.
+// The half spectrum goes out row-major ([row][kc], KCM = false) or as
+// kc-major planes ([kc][row], KCM = true) for the whole-plane pass.
+template <int N, bool KCM = false>
 __global__ void __launch_bounds__(256) k_fft_c_fwd(unsigned long long *__restrict__ rho,
                                                    float2 *__restrict__ grid,
                                                    const float2 *__restrict__ tw_g, FftPlan pl,
@@ -377,9 +419,16 @@ __global__ void __launch_bounds__(256) k_fft_c_fwd(unsigned long long *__restric
   }
   __syncthreads();
   float2 *R = fft_run<N, false>(A, B, tw, n, L, pl);
-  for (int idx = threadIdx.x; idx < L * nch; idx += blockDim.x) {
-    const int r = idx / nch, c = idx - (idx / nch) * nch;
-    if (r < nr) grid[(size_t)(row0 + r) * nch + c] = R[r * S + c];
+  if constexpr (KCM) {
+    for (int idx = threadIdx.x; idx < L * nch; idx += blockDim.x) {
+      const int r = idx % L, c = idx / L;
+      if (r < nr) grid[(size_t)c * nrows + row0 + r] = R[r * S + c];
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < L * nch; idx += blockDim.x) {
+      const int r = idx / nch, c = idx - (idx / nch) * nch;
+      if (r < nr) grid[(size_t)(row0 + r) * nch + c] = R[r * S + c];
+    }
   }
 }
 
@@ -501,8 +550,9 @@ __global__ void __launch_bounds__(256) k_fft_a_conv(float2 *__restrict__ grid,
   }
 }
 
-// inverse transform along c with Hermitian extension; writes V (real)
-template <int N>
+// inverse transform along c with Hermitian extension; writes V (real).
+// KCM: the half spectrum is stored as kc-major planes.
+template <int N, bool KCM = false>
 __global__ void __launch_bounds__(256) k_fft_c_inv(const float2 *__restrict__ grid,
                                                    float *__restrict__ v,
                                                    const float2 *__restrict__ tw_g, FftPlan pl,
@@ -516,24 +566,236 @@ __global__ void __launch_bounds__(256) k_fft_c_inv(const float2 *__restrict__ gr
   for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = tw_g[i];
   const int row0 = blockIdx.x * L;
   const int nr = min(L, nrows - row0);
-  for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
-    const int r = idx / n, c = idx - (idx / n) * n;
-    float2 x = make_float2(0.f, 0.f);
-    if (r < nr) {
-      if (c < nch) {
-        x = grid[(size_t)(row0 + r) * nch + c];
-      } else {
-        float2 y = grid[(size_t)(row0 + r) * nch + (n - c)];
-        x = make_float2(y.x, -y.y);
+  if constexpr (KCM) {
+    for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
+      const int r = idx % L, c = idx / L;
+      float2 x = make_float2(0.f, 0.f);
+      if (r < nr) {
+        if (c < nch) {
+          x = grid[(size_t)c * nrows + row0 + r];
+        } else {
+          float2 y = grid[(size_t)(n - c) * nrows + row0 + r];
+          x = make_float2(y.x, -y.y);
+        }
       }
+      A[r * S + c] = x;
     }
-    A[r * S + c] = x;
+  } else {
+    for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
+      const int r = idx / n, c = idx - (idx / n) * n;
+      float2 x = make_float2(0.f, 0.f);
+      if (r < nr) {
+        if (c < nch) {
+          x = grid[(size_t)(row0 + r) * nch + c];
+        } else {
+          float2 y = grid[(size_t)(row0 + r) * nch + (n - c)];
+          x = make_float2(y.x, -y.y);
+        }
+      }
+      A[r * S + c] = x;
+    }
   }
   __syncthreads();
   float2 *R = fft_run<N, true>(A, B, tw, n, L, pl);
   for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
     const int r = idx / n, c = idx - (idx / n) * n;
     if (r < nr) v[(size_t)(row0 + r) * n + c] = R[r * S + c].x;
+  }
+}
+
+// ---------------------------------------------------------------------
+// Whole-plane pass: one CTA per kc plane of the kc-major half spectrum,
+// the plane (na x nb complex, padded stride nb + 1) held in shared memory.
+// Forward transforms along b and along a run in place as decimation in
+// frequency (output in digit-reversed order), the influence function
+// multiplies each mode at its digit-reversed position, and the inverse
+// transforms run in place as decimation in time (digit-reversed input,
+// natural output): no reordering pass and no ping-pong buffer, so a 128 x
+// 128 plane fits one CTA.  Replaces the b, a + convolution and inverse b
+// passes (two grid round trips fewer).
+// ---------------------------------------------------------------------
+constexpr int PLANE_THREADS = 512;
+
+// the whole-plane pass's stages: a radix-16 first stage where the rest
+// still splits into radix-8 or smaller stages (128 = 16 x 8), else the
+// line passes' order (8, 4, 2, 3, 5, 7)
+__host__ __device__ constexpr int plane_radix_first(int n) {
+  return (n % 16 == 0 && n >= 128) ? 16 : radix_first(n);
+}
+__host__ __device__ constexpr int plane_radix(int n, int s) {
+  int p = plane_radix_first(n);
+  while (s > 0) {
+    n /= p;
+    p = plane_radix_first(n);
+    --s;
+  }
+  return p;
+}
+__host__ __device__ constexpr int plane_stages(int n) {
+  int c = 0;
+  while (n > 1) {
+    n /= plane_radix_first(n);
+    ++c;
+  }
+  return c;
+}
+
+// product of the radices of stages [0, s)
+__host__ __device__ constexpr int radix_prod(int n, int s) {
+  int p = 1;
+  for (int k = 0; k < s; ++k) p *= plane_radix(n, k);
+  return p;
+}
+
+// One in-place stage STG over LINES lines of length N (line and element
+// strides LS and ES in float2).  Forward (decimation in frequency): butterfly on
+// elements j + q h of each block of length m, then twiddles W_m^(r j);
+// inverse (decimation in time): conjugate twiddles, then the inverse
+// butterfly.  The inverse stage undoes the forward one up to the factor p.
+template <int N, int STG, bool INV, int LINES, int LS, int ES>
+__device__ __forceinline__ void plane_stage(float2 *P, const float2 *tw) {
+  constexpr int p = plane_radix(N, STG);
+  constexpr int m = N / radix_prod(N, STG);
+  constexpr int h = m / p;
+  constexpr int NBF = N / p;  // butterflies per line
+  for (int w = threadIdx.x; w < LINES * NBF; w += PLANE_THREADS) {
+    const int line = w % LINES, beta = w / LINES;
+    const int blk = beta / h, j = beta - blk * h;
+    float2 *x = P + line * LS + (blk * m + j) * ES;
+    float2 v[p];
+#pragma unroll
+    for (int q = 0; q < p; ++q) v[q] = x[q * h * ES];
+    if constexpr (!INV) {
+      butterfly<p, false>(v);
+#pragma unroll
+      for (int r = 1; r < p; ++r) v[r] = cmul(v[r], tw[(N / m) * r * j]);
+    } else {
+#pragma unroll
+      for (int r = 1; r < p; ++r) v[r] = cmulc(v[r], tw[(N / m) * r * j]);
+      butterfly<p, true>(v);
+    }
+#pragma unroll
+    for (int q = 0; q < p; ++q) x[q * h * ES] = v[q];
+  }
+}
+
+template <int N, int STG, int LINES, int LS, int ES>
+__device__ __forceinline__ void plane_dif(float2 *P, const float2 *tw) {
+  if constexpr (STG < plane_stages(N)) {
+    plane_stage<N, STG, false, LINES, LS, ES>(P, tw);
+    __syncthreads();
+    plane_dif<N, STG + 1, LINES, LS, ES>(P, tw);
+  }
+}
+
+template <int N, int STG, int LINES, int LS, int ES>
+__device__ __forceinline__ void plane_dit(float2 *P, const float2 *tw) {
+  if constexpr (STG >= 0) {
+    plane_stage<N, STG, true, LINES, LS, ES>(P, tw);
+    __syncthreads();
+    plane_dit<N, STG - 1, LINES, LS, ES>(P, tw);
+  }
+}
+
+// frequency index held at position pos after the forward stages: pos has
+// digit r_s at weight N / (p_0 ... p_s), the frequency has it at weight
+// p_0 ... p_(s-1)
+template <int N>
+__device__ __forceinline__ int plane_freq(int pos) {
+  int k = 0;
+#pragma unroll
+  for (int s = 0; s < plane_stages(N); ++s) {
+    const int p = plane_radix(N, s);
+    const int h = N / (radix_prod(N, s) * p);
+    k += ((pos / h) % p) * radix_prod(N, s);
+  }
+  return k;
+}
+
+__host__ __device__ constexpr size_t plane_smem(int na, int nb) {
+  return sizeof(float2) * ((size_t)na * (nb + 1) + na + nb);
+}
+
+template <int NA, int NB>
+__global__ void __launch_bounds__(PLANE_THREADS) k_fft_plane(
+    float2 *__restrict__ grid, const float2 *__restrict__ tw_g, int nc,
+    const DBox *__restrict__ box, const float *__restrict__ bfac, float alpha,
+    double *__restrict__ part) {
+  extern __shared__ float2 smp[];
+  __shared__ double red_e[PLANE_THREADS / 32], red_w[PLANE_THREADS / 32];
+  constexpr int S = NB + 1;
+  float2 *P = smp;
+  float2 *twa = P + NA * S;
+  float2 *twb = twa + NA;
+  const int kc = blockIdx.x;
+  for (int i = threadIdx.x; i < NA; i += PLANE_THREADS) twa[i] = tw_g[i];
+  for (int i = threadIdx.x; i < NB; i += PLANE_THREADS) twb[i] = tw_g[NA + i];
+  float2 *g = grid + (size_t)kc * NA * NB;
+  for (int idx = threadIdx.x; idx < NA * NB; idx += PLANE_THREADS) {
+    const int a = idx / NB, b = idx - a * NB;
+    P[a * S + b] = g[idx];
+  }
+  __syncthreads();
+  plane_dif<NB, 0, NA, S, 1>(P, twb);  // along b: the NA rows
+  plane_dif<NA, 0, NB, 1, S>(P, twa);  // along a: the NB columns
+
+  // influence function at each mode, FP64 energy / virial partials
+  const DBox bx = *box;
+  const float ilx = bx.ilx, ily = bx.ily, ilz = bx.ilz;
+  const float bax = ilx, bay = -bx.xy * ilx * ily, baz = (bx.xy * bx.yz - bx.xz * bx.ly) * ilx * ily * ilz;
+  const float bby = ily, bbz = -bx.yz * ily * ilz, bcz = ilz;
+  const float two_pi = 6.283185307179586f;
+  const float inv_vol = ilx * ily * ilz;
+  const float inv4a2 = 1.0f / (4.0f * alpha * alpha);
+  const float inv2a2 = 1.0f / (2.0f * alpha * alpha);
+  const float mc = (float)kc;
+  const float bfc = bfac[NA + NB + kc];
+  const double hw = (kc == 0 || ((nc & 1) == 0 && 2 * kc == nc)) ? 1.0 : 2.0;
+  double e_acc = 0.0, w_acc = 0.0;
+  for (int idx = threadIdx.x; idx < NA * NB; idx += PLANE_THREADS) {
+    const int pa = idx / NB, pb = idx - pa * NB;
+    const int ka = plane_freq<NA>(pa), kb = plane_freq<NB>(pb);
+    const float ma = (ka <= NA / 2) ? (float)ka : (float)(ka - NA);
+    const float mb = (kb <= NB / 2) ? (float)kb : (float)(kb - NB);
+    const float kx = two_pi * (ma * bax);
+    const float ky = two_pi * (ma * bay + mb * bby);
+    const float kz = two_pi * (ma * baz + mb * bbz + mc * bcz);
+    const float k2 = kx * kx + ky * ky + kz * kz;
+    float G = 0.0f, vf = 0.0f;
+    if (k2 > 0.0f) {
+      G = inv_vol * (12.566370614359172f / k2) * expf(-k2 * inv4a2) * bfac[ka] * bfac[NA + kb] * bfc;
+      vf = G * (1.0f - k2 * inv2a2);
+    }
+    float2 &X = P[pa * S + pb];
+    const double x2 = (double)X.x * X.x + (double)X.y * X.y;
+    e_acc += hw * (double)G * x2;
+    w_acc += hw * (double)vf * x2;
+    X = make_float2(G * X.x, G * X.y);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    e_acc += __shfl_xor_sync(0xFFFFFFFFu, e_acc, o);
+    w_acc += __shfl_xor_sync(0xFFFFFFFFu, w_acc, o);
+  }
+  if ((threadIdx.x & 31u) == 0u) {
+    red_e[threadIdx.x >> 5] = e_acc;
+    red_w[threadIdx.x >> 5] = w_acc;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double e = 0.0, w = 0.0;
+    for (int k = 0; k < PLANE_THREADS / 32; ++k) {
+      e += red_e[k];
+      w += red_w[k];
+    }
+    part[2 * kc] = e;
+    part[2 * kc + 1] = w;
+  }
+  plane_dit<NA, plane_stages(NA) - 1, NB, 1, S>(P, twa);
+  plane_dit<NB, plane_stages(NB) - 1, NA, S, 1>(P, twb);
+  for (int idx = threadIdx.x; idx < NA * NB; idx += PLANE_THREADS) {
+    const int a = idx / NB, b = idx - a * NB;
+    g[idx] = P[a * S + b];
   }
 }
 
@@ -710,18 +972,55 @@ SpmeLaunch spme_plan(int na, int nb, int nc) {
   return q;
 }
 
-// the five transform passes of one step: c forward (+ int64 -> f32 and
-// clearing), b forward, a forward + influence + a inverse, b inverse,
-// c inverse -> V
+// planes handled by the whole-plane pass: square, and small enough for one
+// CTA's shared memory (128 x 129 complex = 132 KB)
+bool plane_supported(int na, int nb) { return na == nb && (na == 64 || na == 128); }
+
+// once per size, outside any stream capture: the 128 x 128 plane needs more
+// than the default 48 KB of dynamic shared memory
+int plane_prepare(int na) {
+  if (na == 128)
+    HB_CUDA(cudaFuncSetAttribute(k_fft_plane<128, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)plane_smem(128, 128)));
+  else
+    HB_CUDA(cudaFuncSetAttribute(k_fft_plane<64, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)plane_smem(64, 64)));
+  return HB_OK;
+}
+
+// the transform passes of one step.  Row layout: c forward (+ int64 -> f32
+// and clearing), b forward, a forward + influence + a inverse, b inverse,
+// c inverse -> V.  Plane layout (plane = true, sizes with plane_supported):
+// c forward into kc-major planes, the whole-plane pass, c inverse.
 void fft_passes(const SpmeLaunch &q, unsigned long long *rho, float2 *grid, float *v,
                 const float2 *tw, const DBox *box, const float *bfac, float alpha, double *part,
-                cudaStream_t s) {
+                cudaStream_t s, bool plane) {
   const int nrows = q.na * q.nb;
   const float2 *twa = tw, *twb = tw + q.na, *twc = tw + q.na + q.nb;
   const int gc = hb_div_up(nrows, q.Lc);
   const int gb = q.na * ((q.nch + q.Lb - 1) / q.Lb);
   const int ga = q.nb * ((q.nch + q.La - 1) / q.La);
   const size_t sc = fft_smem(q.nc, q.Lc), sb = fft_smem(q.nb, q.Lb), sa = fft_smem(q.na, q.La);
+  if (plane) {
+    switch (q.nc) {
+#define HB_C(NN) case NN: k_fft_c_fwd<NN, true><<<gc, 256, sc, s>>>(rho, grid, twc, q.pc, nrows, q.nch, q.Lc); break;
+      HB_FFT_SIZES(HB_C)
+#undef HB_C
+      default: k_fft_c_fwd<0, true><<<gc, 256, sc, s>>>(rho, grid, twc, q.pc, nrows, q.nch, q.Lc);
+    }
+    const size_t sp = plane_smem(q.na, q.nb);
+    if (q.na == 128)
+      k_fft_plane<128, 128><<<q.nch, PLANE_THREADS, sp, s>>>(grid, tw, q.nc, box, bfac, alpha, part);
+    else
+      k_fft_plane<64, 64><<<q.nch, PLANE_THREADS, sp, s>>>(grid, tw, q.nc, box, bfac, alpha, part);
+    switch (q.nc) {
+#define HB_C(NN) case NN: k_fft_c_inv<NN, true><<<gc, 256, sc, s>>>(grid, v, twc, q.pc, nrows, q.nch, q.Lc); break;
+      HB_FFT_SIZES(HB_C)
+#undef HB_C
+      default: k_fft_c_inv<0, true><<<gc, 256, sc, s>>>(grid, v, twc, q.pc, nrows, q.nch, q.Lc);
+    }
+    return;
+  }
   switch (q.nc) {
 #define HB_C(NN) case NN: k_fft_c_fwd<NN><<<gc, 256, sc, s>>>(rho, grid, twc, q.pc, nrows, q.nch, q.Lc); break;
     HB_FFT_SIZES(HB_C)
@@ -795,7 +1094,9 @@ int spme_setup(hb_forcefield *ff, const hb_forcefield_desc *d) {
   HB_CUDA(cudaMalloc(&S.d_tw, sizeof(float2) * tw.size()));
   HB_CUDA(cudaMemcpy(S.d_tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice));
   const int La = lines_per_cta(S.na);
-  S.n_part = S.nb * ((S.nch + La - 1) / La);
+  S.use_plane = plane_supported(S.na, S.nb) ? 1 : 0;
+  if (S.use_plane) HB_TRY(plane_prepare(S.na));
+  S.n_part = S.use_plane ? S.nch : S.nb * ((S.nch + La - 1) / La);
   HB_CUDA(cudaMalloc(&S.d_part, sizeof(double) * 2 * S.n_part));
   HB_CUDA(cudaMalloc(&S.d_sums, sizeof(double) * 2));
   HB_CUDA(cudaMemset(S.d_sums, 0, sizeof(double) * 2));
@@ -837,7 +1138,7 @@ int spme_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
     }
   }
   fft_passes(spme_plan(na, nb, nc), S.d_rho_fixed, S.d_grid, S.d_v, S.d_tw, sys->d_box, S.d_bfac,
-             S.alpha, S.d_part, s);
+             S.alpha, S.d_part, s, S.use_plane != 0);
   if (n > 0) {
     switch (S.order) {
       case 4: k_gather<4><<<hb_div_up(n, 64), 64, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
@@ -1014,7 +1315,7 @@ extern "C" int hb_spme_recip_noalloc(const float *posq, uint32_t n, const double
       default: k_spread<8><<<hb_div_up(th, 256), 256, 0, s>>>(pq, dbox, na, nb, nc, rho, n); break;
     }
   }
-  fft_passes(spme_plan(na, nb, nc), rho, cgrid, v, tw, dbox, bfac, (float)alpha, part, s);
+  fft_passes(spme_plan(na, nb, nc), rho, cgrid, v, tw, dbox, bfac, (float)alpha, part, s, false);
   if (n > 0) {
     switch (order) {
       case 4: k_gather<4><<<hb_div_up(n, 128), 128, 0, s>>>(pq, v, dbox, na, nb, nc, self_pref, o, n); break;

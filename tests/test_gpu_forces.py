@@ -188,11 +188,15 @@ def test_tiny_systems(ctx):
     empty.close()
 
 
-@pytest.mark.parametrize("grid", [(27, 27, 27), (30, 36, 45), (50, 54, 60), (20, 24, 25)],
+@pytest.mark.parametrize("grid", [(27, 27, 27), (30, 36, 45), (50, 54, 60), (20, 24, 25),
+                                  (64, 64, 64), (128, 128, 40), (128, 128, 27)],
                          ids=lambda g: "x".join(map(str, g)))
 def test_compiled_fft_sizes_match_oracle(ctx, grid):
     # every compile-time specialised FFT length (radix 2/3/4/5 stage plans),
-    # also anisotropic grids: reciprocal energy and total forces vs FP64
+    # also anisotropic grids: reciprocal energy and total forces vs FP64.
+    # 64 x 64 and 128 x 128 (a, b) planes take the whole-plane pass (kc-major
+    # half spectrum, in-place transforms of each plane in shared memory),
+    # with even and odd c lengths
     spec = S.spc_water(216, r_cut_A=7.0, skin_A=1.0, seed=4)
     spec.grid = grid
     pos, F, sc, _, _ = gpu_forces(ctx, spec)
