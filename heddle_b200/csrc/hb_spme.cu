@@ -12,9 +12,10 @@
 // uniform per-atom virial share W_recip / N.
 //
 // Device pipeline (own design):
-//   spread   : 4 threads per atom (sorted, spatially coherent order), each
-//              adds its p^2 contributions to an int64 grid with scale 2^32
-//              (order-independent, byte-identical repeat runs);
+//   spread   : p threads per atom (sorted, spatially coherent order), one
+//              per c stencil offset, each adding its p^2 contributions to
+//              an int64 grid with scale 2^32 (order-independent,
+//              byte-identical repeat runs);
 //   fft_c    : per row, int64 -> f32, clears the int64 grid for the next
 //              step, length-n_c transform, keeps n_c / 2 + 1 modes;
 //   fft_b    : batches of 16 lines along b, transform in shared memory;
@@ -327,13 +328,17 @@ __device__ __forceinline__ void grid_setup(float x, float y, float z, const DBox
   }
 }
 
+// P threads per atom, one per c stencil offset, each adding the P^2 points
+// of its (a, b) stencil: the P threads of one atom differ only in c, so one
+// atomic instruction of a warp writes runs of P consecutive grid words (few
+// L2 sectors) instead of 32 scattered ones
 template <int P>
 __global__ void k_spread(const float4 *__restrict__ tile_posq, const DBox *__restrict__ box,
                          int na, int nb, int nc, unsigned long long *__restrict__ rho,
                          uint32_t n) {
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t k = g / P;
-  const int da = (int)(g - k * P);
+  const int dc = (int)(g - k * P);
   if (k >= n) return;
   const float4 p = tile_posq[k];
   if (p.w == 0.0f) return;
@@ -345,25 +350,24 @@ __global__ void k_spread(const float4 *__restrict__ tile_posq, const DBox *__res
   bspline<P, false>(t[0], wa, nullptr);
   bspline<P, false>(t[1], wb, nullptr);
   bspline<P, false>(t[2], wc, nullptr);
-  int ga = g0[0] - da;
-  if (ga < 0) ga += na;
-  float wda = 0.0f;
+  int gc = g0[2] - dc;
+  if (gc < 0) gc += nc;
+  float wdc = 0.0f;
 #pragma unroll
   for (int d = 0; d < P; ++d)
-    if (d == da) wda = wa[d];
-  const float qa = p.w * wda;
+    if (d == dc) wdc = wc[d];
 #pragma unroll
-  for (int db = 0; db < P; ++db) {
-    int gb = g0[1] - db;
-    if (gb < 0) gb += nb;
-    const float qab = qa * wb[db];
-    const size_t rowbase = ((size_t)ga * nb + gb) * nc;
+  for (int da = 0; da < P; ++da) {
+    int ga = g0[0] - da;
+    if (ga < 0) ga += na;
+    const float qa = p.w * wa[da];
 #pragma unroll
-    for (int dc = 0; dc < P; ++dc) {
-      int gc = g0[2] - dc;
-      if (gc < 0) gc += nc;
-      const long long v = __float2ll_rn(qab * wc[dc] * HB_RHO_SCALE);
-      if (v != 0) atomicAdd(&rho[rowbase + gc], (unsigned long long)v);
+    for (int db = 0; db < P; ++db) {
+      int gb = g0[1] - db;
+      if (gb < 0) gb += nb;
+      const float qab = qa * wb[db];
+      const long long v = __float2ll_rn(qab * wdc * HB_RHO_SCALE);
+      if (v != 0) atomicAdd(&rho[((size_t)ga * nb + gb) * nc + gc], (unsigned long long)v);
     }
   }
 }
@@ -716,7 +720,9 @@ __host__ __device__ constexpr size_t plane_smem(int na, int nb) {
   return sizeof(float2) * ((size_t)na * (nb + 1) + na + nb);
 }
 
-template <int NA, int NB>
+// EV: also the FP64 energy / virial partials of the plane (steps that
+// report energies or pressure); without, the influence function alone
+template <int NA, int NB, bool EV>
 __global__ void __launch_bounds__(PLANE_THREADS) k_fft_plane(
     float2 *__restrict__ grid, const float2 *__restrict__ tw_g, int nc,
     const DBox *__restrict__ box, const float *__restrict__ bfac, float alpha,
@@ -764,25 +770,29 @@ __global__ void __launch_bounds__(PLANE_THREADS) k_fft_plane(
     float G = 0.0f, vf = 0.0f;
     if (k2 > 0.0f) {
       G = inv_vol * (12.566370614359172f / k2) * expf(-k2 * inv4a2) * bfac[ka] * bfac[NA + kb] * bfc;
-      vf = G * (1.0f - k2 * inv2a2);
+      if constexpr (EV) vf = G * (1.0f - k2 * inv2a2);
     }
     float2 &X = P[pa * S + pb];
-    const double x2 = (double)X.x * X.x + (double)X.y * X.y;
-    e_acc += hw * (double)G * x2;
-    w_acc += hw * (double)vf * x2;
+    if constexpr (EV) {
+      const double x2 = (double)X.x * X.x + (double)X.y * X.y;
+      e_acc += hw * (double)G * x2;
+      w_acc += hw * (double)vf * x2;
+    }
     X = make_float2(G * X.x, G * X.y);
   }
+  if constexpr (EV) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    e_acc += __shfl_xor_sync(0xFFFFFFFFu, e_acc, o);
-    w_acc += __shfl_xor_sync(0xFFFFFFFFu, w_acc, o);
-  }
-  if ((threadIdx.x & 31u) == 0u) {
-    red_e[threadIdx.x >> 5] = e_acc;
-    red_w[threadIdx.x >> 5] = w_acc;
+    for (int o = 16; o > 0; o >>= 1) {
+      e_acc += __shfl_xor_sync(0xFFFFFFFFu, e_acc, o);
+      w_acc += __shfl_xor_sync(0xFFFFFFFFu, w_acc, o);
+    }
+    if ((threadIdx.x & 31u) == 0u) {
+      red_e[threadIdx.x >> 5] = e_acc;
+      red_w[threadIdx.x >> 5] = w_acc;
+    }
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (EV && threadIdx.x == 0) {
     double e = 0.0, w = 0.0;
     for (int k = 0; k < PLANE_THREADS / 32; ++k) {
       e += red_e[k];
@@ -979,12 +989,17 @@ bool plane_supported(int na, int nb) { return na == nb && (na == 64 || na == 128
 // once per size, outside any stream capture: the 128 x 128 plane needs more
 // than the default 48 KB of dynamic shared memory
 int plane_prepare(int na) {
-  if (na == 128)
-    HB_CUDA(cudaFuncSetAttribute(k_fft_plane<128, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)plane_smem(128, 128)));
-  else
-    HB_CUDA(cudaFuncSetAttribute(k_fft_plane<64, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)plane_smem(64, 64)));
+  if (na == 128) {
+    HB_CUDA(cudaFuncSetAttribute(k_fft_plane<128, 128, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane_smem(128, 128)));
+    HB_CUDA(cudaFuncSetAttribute(k_fft_plane<128, 128, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane_smem(128, 128)));
+  } else {
+    HB_CUDA(cudaFuncSetAttribute(k_fft_plane<64, 64, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane_smem(64, 64)));
+    HB_CUDA(cudaFuncSetAttribute(k_fft_plane<64, 64, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane_smem(64, 64)));
+  }
   return HB_OK;
 }
 
@@ -994,7 +1009,7 @@ int plane_prepare(int na) {
 // c forward into kc-major planes, the whole-plane pass, c inverse.
 void fft_passes(const SpmeLaunch &q, unsigned long long *rho, float2 *grid, float *v,
                 const float2 *tw, const DBox *box, const float *bfac, float alpha, double *part,
-                cudaStream_t s, bool plane) {
+                cudaStream_t s, bool plane, bool ev = true) {
   const int nrows = q.na * q.nb;
   const float2 *twa = tw, *twb = tw + q.na, *twc = tw + q.na + q.nb;
   const int gc = hb_div_up(nrows, q.Lc);
@@ -1009,10 +1024,13 @@ void fft_passes(const SpmeLaunch &q, unsigned long long *rho, float2 *grid, floa
       default: k_fft_c_fwd<0, true><<<gc, 256, sc, s>>>(rho, grid, twc, q.pc, nrows, q.nch, q.Lc);
     }
     const size_t sp = plane_smem(q.na, q.nb);
-    if (q.na == 128)
-      k_fft_plane<128, 128><<<q.nch, PLANE_THREADS, sp, s>>>(grid, tw, q.nc, box, bfac, alpha, part);
-    else
-      k_fft_plane<64, 64><<<q.nch, PLANE_THREADS, sp, s>>>(grid, tw, q.nc, box, bfac, alpha, part);
+    if (q.na == 128) {
+      if (ev) k_fft_plane<128, 128, true><<<q.nch, PLANE_THREADS, sp, s>>>(grid, tw, q.nc, box, bfac, alpha, part);
+      else k_fft_plane<128, 128, false><<<q.nch, PLANE_THREADS, sp, s>>>(grid, tw, q.nc, box, bfac, alpha, part);
+    } else {
+      if (ev) k_fft_plane<64, 64, true><<<q.nch, PLANE_THREADS, sp, s>>>(grid, tw, q.nc, box, bfac, alpha, part);
+      else k_fft_plane<64, 64, false><<<q.nch, PLANE_THREADS, sp, s>>>(grid, tw, q.nc, box, bfac, alpha, part);
+    }
     switch (q.nc) {
 #define HB_C(NN) case NN: k_fft_c_inv<NN, true><<<gc, 256, sc, s>>>(grid, v, twc, q.pc, nrows, q.nch, q.Lc); break;
       HB_FFT_SIZES(HB_C)
@@ -1138,7 +1156,7 @@ int spme_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
     }
   }
   fft_passes(spme_plan(na, nb, nc), S.d_rho_fixed, S.d_grid, S.d_v, S.d_tw, sys->d_box, S.d_bfac,
-             S.alpha, S.d_part, s, S.use_plane != 0);
+             S.alpha, S.d_part, s, S.use_plane != 0, ev);
   if (n > 0) {
     switch (S.order) {
       case 4: k_gather<4><<<hb_div_up(n, 64), 64, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
