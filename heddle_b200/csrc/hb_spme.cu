@@ -24,7 +24,9 @@
 //              refresh pass), FP64 energy / virial partials, inverse
 //              transform -- the convolution costs no extra grid pass;
 //   ifft_b, ifft_c (Hermitian extension, real part) -> V;
-//   gather   : one thread per atom, p^3 reads of V, force, energy share.
+//   gather   : p^3 reads of V per atom, force, energy share; for p = 4 and
+//              8 one thread per c offset (runs of consecutive reads, sums
+//              met by shuffles), else one thread per atom.
 // The line passes are Stockham autosort transforms with radix 8, 4, 2, 3,
 // 5, 7 butterflies, twiddles from an FP64-built table, lines held in shared
 // memory with a padded stride.  For 64 x 64 and 128 x 128 (a, b) planes
@@ -869,6 +871,80 @@ __global__ void k_gather(const float4 *__restrict__ tile_posq, const float *__re
   out[k] = o;
 }
 
+// Gather with P threads per atom (P a power of two), one per c stencil
+// offset: the P threads of an atom read runs of P consecutive potential
+// words (few L1 sectors per load instruction instead of 32 scattered ones),
+// and their partial sums meet by shuffles within the aligned group of P
+// lanes
+template <int P>
+__global__ void k_gather_c(const float4 *__restrict__ tile_posq, const float *__restrict__ V,
+                           const DBox *__restrict__ box, int na, int nb, int nc, float self_pref,
+                           float4 *__restrict__ out, uint32_t n) {
+  static_assert(P == 4 || P == 8, "lane groups must tile the warp");
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t k = g / P;
+  const int dc = (int)(g % P);
+  const bool valid = k < n;
+  // lanes past the end follow the last atom so that every lane of the warp
+  // takes part in the shuffles; they write nothing
+  const float4 p = tile_posq[valid ? k : n - 1];
+  const DBox b = *box;
+  float t[3];
+  int g0[3];
+  grid_setup(p.x, p.y, p.z, b, na, nb, nc, t, g0);
+  float wa[P], wb[P], wc[P], dwa[P], dwb[P], dwc[P];
+  bspline<P, true>(t[0], wa, dwa);
+  bspline<P, true>(t[1], wb, dwb);
+  bspline<P, true>(t[2], wc, dwc);
+  int ic = g0[2] - dc;
+  if (ic < 0) ic += nc;
+  float A = 0.f, B = 0.f, C = 0.f;
+#pragma unroll
+  for (int da = 0; da < P; ++da) {
+    int ia = g0[0] - da;
+    if (ia < 0) ia += na;
+#pragma unroll
+    for (int db = 0; db < P; ++db) {
+      int ib = g0[1] - db;
+      if (ib < 0) ib += nb;
+      const float v = __ldg(V + ((size_t)ia * nb + ib) * nc + ic);
+      A += wa[da] * wb[db] * v;
+      B += dwa[da] * wb[db] * v;
+      C += wa[da] * dwb[db] * v;
+    }
+  }
+  float wdc = 0.f, dwdc = 0.f;
+#pragma unroll
+  for (int d = 0; d < P; ++d)
+    if (d == dc) {
+      wdc = wc[d];
+      dwdc = dwc[d];
+    }
+  float phi = wdc * A, ga = wdc * B, gb = wdc * C, gcc = dwdc * A;
+#pragma unroll
+  for (int o = P / 2; o > 0; o >>= 1) {
+    phi += __shfl_xor_sync(0xFFFFFFFFu, phi, o);
+    ga += __shfl_xor_sync(0xFFFFFFFFu, ga, o);
+    gb += __shfl_xor_sync(0xFFFFFFFFu, gb, o);
+    gcc += __shfl_xor_sync(0xFFFFFFFFu, gcc, o);
+  }
+  if (!valid || dc != 0) return;
+  ga *= (float)na;
+  gb *= (float)nb;
+  gcc *= (float)nc;
+  // rows of H^{-T} (spme_spread_gather.cuh:128-148)
+  const float bax = b.ilx, bay = -b.xy * b.ilx * b.ily,
+              baz = (b.xy * b.yz - b.xz * b.ly) * b.ilx * b.ily * b.ilz;
+  const float bby = b.ily, bbz = -b.yz * b.ily * b.ilz, bcz = b.ilz;
+  const float q = p.w;
+  float4 o;
+  o.x = -q * (ga * bax);
+  o.y = -q * (ga * bay + gb * bby);
+  o.z = -q * (ga * baz + gb * bbz + gcc * bcz);
+  o.w = 0.5f * q * phi - self_pref * q * q;
+  out[k] = o;
+}
+
 __global__ void k_spme_sums(const double *__restrict__ part, int n_part,
                             double *__restrict__ sums) {
   __shared__ double se[256], sw[256];
@@ -1159,11 +1235,11 @@ int spme_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
              S.alpha, S.d_part, s, S.use_plane != 0, ev);
   if (n > 0) {
     switch (S.order) {
-      case 4: k_gather<4><<<hb_div_up(n, 64), 64, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
+      case 4: k_gather_c<4><<<hb_div_up((uint64_t)n * 4u, 128), 128, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
       case 5: k_gather<5><<<hb_div_up(n, 64), 64, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
       case 6: k_gather<6><<<hb_div_up(n, 64), 64, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
       case 7: k_gather<7><<<hb_div_up(n, 64), 64, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
-      case 8: k_gather<8><<<hb_div_up(n, 64), 64, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
+      case 8: k_gather_c<8><<<hb_div_up((uint64_t)n * 8u, 128), 128, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
     }
   }
   if (ev) k_spme_sums<<<1, 256, 0, s>>>(S.d_part, S.n_part, S.d_sums);
