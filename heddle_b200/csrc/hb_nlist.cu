@@ -293,9 +293,19 @@ __device__ __forceinline__ uint32_t excl_mask(uint32_t sj, uint32_t I,
 #define NLT_WARPS 8
 
 // k-th set bit (0-based) of a 32-bit mask
+// (k < popc(m)), by a binary search on the popcounts of low halves
 __device__ __forceinline__ uint32_t select_bit(uint32_t m, uint32_t k) {
-  for (uint32_t i = 0; i < k; ++i) m &= m - 1u;
-  return (uint32_t)__ffs(m) - 1u;
+  uint32_t pos = 0u;
+#pragma unroll
+  for (uint32_t w = 16u; w > 0u; w >>= 1) {
+    const uint32_t c = (uint32_t)__popc(m & ((1u << w) - 1u));
+    if (k >= c) {
+      k -= c;
+      m >>= w;
+      pos += w;
+    }
+  }
+  return pos;
 }
 
 // Packed-entry construction, one 256-thread block per i-tile I:
@@ -306,8 +316,9 @@ __device__ __forceinline__ uint32_t select_bit(uint32_t m, uint32_t k) {
 //     Far from the r_search boundary a j-atom shifted once to the image
 //     nearest I's centre decides with plain differences; inside a 1e-4
 //     relative band the exact single-precision rule decides.  With the
-//     single shift, only the i-atoms of the 8-atom sub-tiles whose box lies
-//     within r_search of the j-atom are tested;
+//     single shift, only the j-atoms within r_search of one of the i-tile's
+//     8-atom sub-tile boxes are refined, one at a time, with the lanes as
+//     i-atoms and one vote per j-atom;
 //  3. a prefix sum of the masks' popcounts fixes where every hit goes;
 //  4. the warps write the entries (self tile first) into I's slab, each
 //     with the exclusion masks of its 32 j-atoms.
@@ -329,10 +340,9 @@ __global__ void __launch_bounds__(NLT_WARPS * 32, 4)
   uint32_t *pre = hmask + maxc;       // [maxc + 1] exclusive prefix of hits
   __shared__ uint32_t s_cnt[NLT_WARPS];
   __shared__ uint32_t s_ncand;
-  __shared__ float4 s_ipos[32];       // the i-tile's positions (padding at 1e18)
+  __shared__ float4 s_jsh[NLT_WARPS][32], s_jor[NLT_WARPS][32];  // a candidate's j-atoms: shifted, as stored
   const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t I = blockIdx.x;
-  if (w == 0) s_ipos[lane] = tile_posq[I * 32u + lane];
   const DBox b = *box;
   const float4 ci = center[I], hi = half[I];
   const bool ortho = ((int)ci.w & 2) != 0;
@@ -432,31 +442,32 @@ __global__ void __launch_bounds__(NLT_WARPS * 32, 4)
           if (sh[q][0] >= 0.0f && ex * ex + ey * ey + ez * ez <= rb2) qm |= 1u << q;
         }
       }
-      // i-atoms come from shared memory as broadcasts, two per round
-      // between votes; padding slots sit at 1e18 and never hit
-      bool hit = false;
-#pragma unroll 1
-      for (uint32_t q = 0; q < 4u; ++q) {
-        bool want = (qm >> q) & 1u;
-#pragma unroll 1
-        for (uint32_t m = 8u * q; m < 8u * q + 8u && __any_sync(0xFFFFFFFFu, want); m += 2u) {
-#pragma unroll
-          for (uint32_t u = 0; u < 2u; ++u) {
-            const float4 a = s_ipos[m + u];
-            const float dx = a.x - sx, dy = a.y - sy, dz = a.z - sz;
-            const float r2 = dx * dx + dy * dy + dz * dz;
-            if (want) {
-              if (r2 < band_lo) {
-                hit = true;
-              } else if (r2 <= band_hi && hb_exact_r2(a.x - pj.x, a.y - pj.y, a.z - pj.z, b) <= rs2) {
-                hit = true;
-              }
-            }
-            want = want && !hit;
-          }
+      // the j-atoms near a sub-tile box are refined one at a time with the
+      // lanes as i-atoms: each lane tests its own i-atom against the
+      // broadcast j-atom and one vote decides (padding i-slots sit at 1e18
+      // and never hit); the exact rule runs only when some pair falls in
+      // the band
+      uint32_t rem = __ballot_sync(0xFFFFFFFFu, qm != 0u);
+      s_jsh[w][lane] = make_float4(sx, sy, sz, 0.0f);
+      s_jor[w][lane] = pj;
+      __syncwarp();
+      uint32_t hm = 0u;
+      while (rem != 0u) {
+        const uint32_t jl = (uint32_t)__ffs(rem) - 1u;
+        rem &= rem - 1u;
+        const float4 q = s_jsh[w][jl];
+        const float dx = pim.x - q.x, dy = pim.y - q.y, dz = pim.z - q.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        bool hit = __any_sync(0xFFFFFFFFu, r2 < band_lo);
+        const bool inb = r2 >= band_lo && r2 <= band_hi;
+        if (!hit && __any_sync(0xFFFFFFFFu, inb)) {
+          const float4 qo = s_jor[w][jl];
+          const bool ex = inb && hb_exact_r2(pim.x - qo.x, pim.y - qo.y, pim.z - qo.z, b) <= rs2;
+          hit = __any_sync(0xFFFFFFFFu, ex);
         }
+        if (hit) hm |= 1u << jl;
       }
-      const uint32_t hm = __ballot_sync(0xFFFFFFFFu, hit);
+      __syncwarp();
       if (lane == 0) hmask[c] = hm;
       continue;
     }
