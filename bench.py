@@ -364,7 +364,9 @@ def run_ours(args):
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind,
                          "note": "algorithmic bytes 28 B/atom per launch; the kernel is bound by "
-                                 "instruction issue, not HBM"},
+                                 "instruction issue (77 % issue active) and the shared-memory "
+                                 "pipe (80 % of LSU wavefronts), not HBM: "
+                                 "profiles/k_pair4_spc_water_65536.md"},
             "step_roofline": {"bytes_per_step": step_bytes,
                               "achieved_gbs": step_bytes / (t_ms / args.steps * 1e-3) / 1e9,
                               "frac": step_bytes / (t_ms / args.steps * 1e-3) / 1e9 / peak},
