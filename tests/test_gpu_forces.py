@@ -271,3 +271,22 @@ def test_small_cells_with_padding_slots(ctx, monkeypatch, kernel):
         assert np.isfinite(F).all()
         Fo, _, _, _ = O.forces(spec, pos)
         assert rms_rel(F, Fo) <= FORCE_RMS_TOL, (density, rms_rel(F, Fo))
+
+
+@pytest.mark.parametrize("grid,order", [((64, 64, 60), 4), ((128, 128, 50), 8), ((48, 50, 45), 8)],
+                         ids=["plane64-p4", "plane128-p8", "lines-p8"])
+def test_triclinic_reciprocal_paths_match_oracle(ctx, grid, order):
+    # a tilted cell through the whole-plane pass (64 x 64 and 128 x 128
+    # (a, b) planes) and the line passes, with spline orders 4 and 8 (the
+    # spread and gather with one thread per c offset): reciprocal energy
+    # and total forces against the FP64 oracle
+    spec = S.spc_water(216, r_cut_A=7.0, skin_A=1.0, seed=6)
+    lx, ly, lz = spec.box[:3]
+    spec.box = np.array([lx, ly, lz, 0.12 * lx, -0.08 * lx, 0.1 * ly])
+    spec.grid = grid
+    spec.order = order
+    pos, F, sc, _, _ = gpu_forces(ctx, spec)
+    Fo, _, _, _ = O.forces(spec, pos)
+    assert rms_rel(F, Fo) <= FORCE_RMS_TOL, rms_rel(F, Fo)
+    _, _, _, Tp = O.forces(spec, pos, poly_erfc=True)
+    assert abs(sc["recip"] - Tp["recip"]) <= 1e-5 * abs(Tp["recip"])
