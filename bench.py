@@ -73,7 +73,6 @@ def workload_config(args, spec, world):
                     f"SPME p={spec.order} grid {spec.grid[0]}^3, Langevin 300 K, dt {spec.dt_fs} fs",
         "atoms": spec.n,
         "grid": list(spec.grid),
-        "r_skin_A": args.skin,
         "barostat": ("Monte-Carlo, 1 bar, a volume move every 25 steps (device-side, inside the "
                      "step graphs)" if args.barostat else "none (NVT)"),
         "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
