@@ -289,6 +289,23 @@ __device__ __forceinline__ float2 *fft_run(float2 *A, float2 *B, const float2 *_
 // derivatives, by the Cox-de Boor recursion raised one order at a time.
 template <int P, bool DERIV>
 __device__ __forceinline__ void bspline(float t, float *w, float *dw) {
+  if constexpr (P == 4) {
+    // the cubic case in closed form (the recursion below, multiplied out):
+    // w = (t^3, 1 + 3t + 3t^2 - 3t^3, 4 - 6t^2 + 3t^3, (1 - t)^3) / 6,
+    // dw = (t^2, 1 + 2t - 3t^2, 3t^2 - 4t, -(1 - t)^2) / 2
+    const float t2 = t * t, t3 = t2 * t, s = 1.0f - t, s2 = s * s;
+    w[0] = t3 * (1.0f / 6.0f);
+    w[1] = fmaf(0.5f, (t + t2) - t3, 1.0f / 6.0f);
+    w[2] = fmaf(0.5f, t3, (2.0f / 3.0f) - t2);
+    w[3] = s2 * s * (1.0f / 6.0f);
+    if constexpr (DERIV) {
+      dw[0] = 0.5f * t2;
+      dw[1] = fmaf(-1.5f, t2, 0.5f + t);
+      dw[2] = fmaf(1.5f, t2, -2.0f * t);
+      dw[3] = -0.5f * s2;
+    }
+    return;
+  }
   float c[P];
   c[0] = 1.0f;
 #pragma unroll
