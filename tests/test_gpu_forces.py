@@ -285,7 +285,16 @@ def test_triclinic_reciprocal_paths_match_oracle(ctx, grid, order):
     spec.box = np.array([lx, ly, lz, 0.12 * lx, -0.08 * lx, 0.1 * ly])
     spec.grid = grid
     spec.order = order
-    pos, F, sc, _, _ = gpu_forces(ctx, spec)
+    # a force-only step (no energy partials in the plane pass) and a step
+    # with energies on the same positions
+    sys_ = hb.System.from_spec(ctx, spec)
+    ff = hb.ForceField.from_spec(sys_, spec)
+    ff.step(scalars=False)
+    F0 = sys_.forces()
+    ff.step(scalars=True)
+    F, sc, pos = sys_.forces(), ff.scalars(), sys_.positions()
+    ff.close(), sys_.close()
+    assert rms_rel(F0, F) <= 2e-6
     Fo, _, _, _ = O.forces(spec, pos)
     assert rms_rel(F, Fo) <= FORCE_RMS_TOL, rms_rel(F, Fo)
     _, _, _, Tp = O.forces(spec, pos, poly_erfc=True)
