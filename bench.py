@@ -188,7 +188,9 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / (k + 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": workload_config(args, spec, 1),
+        "data": "synthetic",
+        # the same workload description as the GPU arm at this world size
+        "config": workload_config(args, spec, int(os.environ.get("WORLD_SIZE", "1"))),
         "ns_per_day": spec.dt_fs * ((k + 1) / dt) * 0.0864,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
