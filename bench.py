@@ -73,8 +73,9 @@ def workload_config(args, spec, world):
                     f"SPME p={spec.order} grid {spec.grid[0]}^3, Langevin 300 K, dt {spec.dt_fs} fs",
         "atoms": spec.n,
         "grid": list(spec.grid),
-        "barostat": ("Monte-Carlo, 1 bar, a volume move every 25 steps (device-side, inside the "
-                     "step graphs)" if args.barostat else "none (NVT)"),
+        "barostat": ("Monte-Carlo, 1 bar, a volume move after every 25th step (device-side, "
+                     "inside the step graphs); the step counter is phased so that the timed "
+                     "window holds at least one move" if args.barostat else "none (NVT)"),
         "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
         "l2": "flushed between timed steps (256 MiB write, outside the timed region)",
         "start": f"lattice, relaxed by {args.equilibrate} untimed Langevin steps (50/ps)",
@@ -143,14 +144,36 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(spec, budget_s=25.0):
+def force_error(F, Fo):
+    """RMS and max force error relative to the reference forces Fo."""
+    rms = float(np.sqrt(((F - Fo) ** 2).sum() / (Fo ** 2).sum()))
+    mx = float(np.abs(F - Fo).max() / np.sqrt((Fo ** 2).sum(axis=1).mean()))
+    return rms, mx
+
+
+def cpu_baseline(spec, state=None, forces_gpu=None, budget_s=25.0):
     """The FP64 CPU restatement (oracle/) timed on the host cores on a bounded
-    sample of the same workload: whole MD steps until ~budget_s."""
+    sample of the same workload: whole MD steps until ~budget_s, from the
+    GPU arm's relaxed state when given.  As the checker it also evaluates
+    the FP64 forces at that state, which gives the GPU forces' error."""
     import oracle as O
 
     cores = os.cpu_count() or 1
+    err = None
+    pos0 = vel0 = None
+    if state is not None:
+        import copy
+
+        pos0, vel0, box = state
+        spec = copy.copy(spec)
+        spec.box = np.asarray(box, dtype=np.float64)  # the barostat has moved the cell
+        if forces_gpu is not None:
+            Fo, _, _, _ = O.forces(spec, pos0, n_threads=cores)
+            rms, mx = force_error(forces_gpu, Fo)
+            err = {"rms_rel": rms, "max_rel": mx,
+                   "vs": "FP64 CPU oracle (exact erfc) at the state the timed steps ended in"}
     t0 = time.perf_counter()
-    pos, vel, _ = O.md_run(spec, 1, "langevin", n_threads=cores)
+    pos, vel, _ = O.md_run(spec, 1, "langevin", positions=pos0, velocities=vel0, n_threads=cores)
     first = time.perf_counter() - t0  # one step + initial force evaluation
     per_step_guess = first / 2.0
     k = max(1, min(20, int(budget_s / max(per_step_guess, 1e-3))))
@@ -159,9 +182,11 @@ def cpu_baseline(spec, budget_s=25.0):
     dt = time.perf_counter() - t0
     # md_run evaluates the starting forces once before its k steps
     steps_equiv = k + 1
-    return {"value": spec.n * steps_equiv / dt, "unit": UNIT, "cores": cores, "kind": "port",
+    start = "the GPU arm's relaxed state" if state is not None else "the lattice start"
+    base = {"value": spec.n * steps_equiv / dt, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"{k} Langevin+SETTLE MD steps (+1 initial force evaluation) of the full "
-                      f"{spec.n}-atom system, FP64 oracle, {dt:.1f} s"}
+                      f"{spec.n}-atom system from {start}, FP64 oracle (no barostat), {dt:.1f} s"}
+    return base, err
 
 
 def run_reference(args):
@@ -171,7 +196,7 @@ def run_reference(args):
     from heddle_b200 import systems as S
     import oracle as O
 
-    spec = S.spc_water(args.molecules, skin_A=args.skin)
+    spec = S.spc_water(args.molecules, skin_A=2.0)
     cores = os.cpu_count() or 1
     # warm-up: one step (capped so the whole run stays within minutes)
     t0 = time.perf_counter()
@@ -189,8 +214,13 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / (k + 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        # the same workload description as the GPU arm at this world size
-        "config": workload_config(args, spec, int(os.environ.get("WORLD_SIZE", "1"))),
+        # the GPU arm's system, integrator and cut-offs; this arm's own
+        # start, barostat and arithmetic
+        "config": dict(workload_config(args, spec, int(os.environ.get("WORLD_SIZE", "1"))),
+                       barostat="none (the CPU restatement makes no volume moves; on the GPU a "
+                                "move costs one energy evaluation every 25 steps, about +4 %)",
+                       start="lattice start, no relaxation",
+                       arithmetic="FP64 throughout (the GPU arm: FP32 with fixed-point sums)"),
         "ns_per_day": spec.dt_fs * ((k + 1) / dt) * 0.0864,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -265,7 +295,12 @@ def run_ours(args):
     ff = hb.ForceField.from_spec(sys_, spec)
     if tune:
         ff.set_launch(pair_blocks_per_sm=int(tune["pair_blocks_per_sm"]))
-    it = hb.Integrator(sys_, **lang)
+    # phase the step counter so that a barostat move falls in the middle of
+    # the timed window: before it run max(3, W) warm-up steps and the stage
+    # breakdown's min(K, 20) steps; a move follows every 25th step
+    done_before = max(3, args.warmup) + min(args.steps, 20)
+    step0 = (-(done_before + (args.steps + 1) // 2)) % 25 if args.barostat else 0
+    it = hb.Integrator(sys_, **lang, step0=step0)
     baro = None
     if args.barostat:
         baro = hb.Barostat(sys_, U.pressure_au_bar(1.0), spec.temperature, seed=4321 + rank,
@@ -303,6 +338,13 @@ def run_ours(args):
     if dist is not None:
         dist.barrier()
     ctx.timing(False)
+    # the state the timed steps ended in and its forces (outside the timed
+    # region), for the force error against the FP64 oracle
+    final_state = final_forces = None
+    if rank == 0 and not args.no_cpu_baseline:
+        ff.step(scalars=False)
+        st = sys_.state()
+        final_state, final_forces = (st[0], st[1], sys_.box()), sys_.forces()
     rebuilds = ff.stats()["rebuilds"] - rebuilds0
     baro_stats = baro.stats() if baro else None
     moves = int(baro_stats["attempted"] - moves0) if baro else 0
@@ -365,9 +407,7 @@ def run_ours(args):
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind,
                          "note": "algorithmic bytes 28 B/atom per launch; the kernel is bound by "
-                                 "instruction issue (77 % issue active) and the shared-memory "
-                                 "pipe (80 % of LSU wavefronts), not HBM: "
-                                 "profiles/k_pair4_spc_water_65536.md"},
+                                 "instruction issue and the shared-memory pipe, not HBM"},
             "step_roofline": {"bytes_per_step": step_bytes,
                               "achieved_gbs": step_bytes / (t_ms / args.steps * 1e-3) / 1e9,
                               "frac": step_bytes / (t_ms / args.steps * 1e-3) / 1e9 / peak},
@@ -384,7 +424,7 @@ def run_ours(args):
                          if baro else None),
         }
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(spec)
+            line["cpu_baseline"], line["force_error"] = cpu_baseline(spec, final_state, final_forces)
         print(json.dumps(line), flush=True)
     it.close()
     if baro:
@@ -401,8 +441,8 @@ def run_ours(args):
 
 def run_batch(args):
     """The 64-box uneven replica batch: every box's step in one CUDA graph
-    (one launch per step) against the same boxes advanced one after another
-    with plain eager steps (64 sequential plain runs)."""
+    (one launch per step) against the same boxes advanced one after another,
+    each with its own CUDA-graph steps (64 sequential plain runs)."""
     import torch
 
     import heddle_b200 as hb
@@ -442,14 +482,15 @@ def run_batch(args):
             t_ms += float(master.timings()[0])
     master.timing(False)
     rebuilds = sum(o[2].stats()["rebuilds"] for o in objs) - rebuilds0
-    # 64 sequential plain runs (eager launches, one box after another), wall clock
+    # 64 sequential plain runs (each box's own CUDA-graph steps, one box
+    # after another), wall clock
     k_seq = max(1, args.steps // 4)
     for o in objs:
-        o[4].step(o[2], o[3], n_steps=1)
+        o[4].step_graph(o[2], o[3], n_steps=1)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for o in objs:
-        o[4].step(o[2], o[3], n_steps=k_seq)
+        o[4].step_graph(o[2], o[3], n_steps=k_seq)
     torch.cuda.synchronize()
     t_seq = time.perf_counter() - t0
     # batched, wall clock over the same number of steps (no flush); one

@@ -33,6 +33,7 @@ HB_INTEGRATOR_VV, HB_INTEGRATOR_VV_LOSSLESS, HB_INTEGRATOR_LANGEVIN = 0, 1, 2
 HB_CONSTRAINT_SETTLE, HB_CONSTRAINT_SHAKE = 0, 1
 HB_PAIRS_FAST, HB_PAIRS_EXACT = 0, 1
 HB_LAUNCH_PAIR_BLOCKS_PER_SM = 0
+HB_LAUNCH_NL_SLAB = 1
 
 PD = C.POINTER(C.c_double)
 PU32 = C.POINTER(C.c_uint32)
@@ -204,6 +205,7 @@ SIGNATURES = {
     "hb_forcefield_get_per_atom": (C.c_int, [VP, PD, PD]),
     "hb_neighbor_pairs": (C.c_int, [VP, PU32, C.c_uint64, PU64, PU64]),
     "hb_neighbor_stats": (C.c_int, [VP, PU64]),
+    "hb_neighbor_capacity": (C.c_int, [VP, PU64]),
     "hb_constraints_create": (C.c_int, [VP, C.POINTER(ConstraintsDesc), PVP]),
     "hb_constraints_destroy": (C.c_int, [VP]),
     "hb_constraints_before_drift": (C.c_int, [VP]),
@@ -221,6 +223,7 @@ SIGNATURES = {
     "hb_shake_mlp_set_params": (C.c_int, [VP, PF32, C.c_uint32]),
     "hb_shake_mlp_set_normalization": (C.c_int, [VP, PF32, PF32, C.c_float]),
     "hb_shake_mlp_predict": (C.c_int, [VP, PF32, C.c_uint64, PF32]),
+    "hb_shake_mlp_set_wait_limit": (C.c_int, [VP, C.c_uint32, C.c_int]),
     "hb_shake_mlp_gradients": (C.c_int, [VP, PF32, PF32, C.c_uint32, PF32, PD]),
     "hb_shake_mlp_train": (C.c_int, [VP, PF32, PF32, C.c_uint64, C.c_uint32, C.c_uint32,
                                      C.c_double, C.c_uint64, PD]),

@@ -353,12 +353,24 @@ class ForceField:
         N.check(self.lib.hb_forcefield_pre_step(self.h, 1 if force else 0, C.byref(r)))
         return bool(r.value)
 
-    def set_launch(self, pair_blocks_per_sm: int | None = None) -> None:
+    def set_launch(self, pair_blocks_per_sm: int | None = None, nl_slab: int | None = None) -> None:
         """Launch shapes (autotuned): resident blocks per SM of the persistent
-        pair kernel."""
+        pair kernel.  nl_slab rebuilds the packed list at once into slabs of
+        that many entries per i-tile (grown again above 3/4 full; too small
+        raises HB_ERR_NL_OVERFLOW and halts the force field until a larger
+        slab is set)."""
         if pair_blocks_per_sm is not None:
             N.check(self.lib.hb_forcefield_set_launch(self.h, N.HB_LAUNCH_PAIR_BLOCKS_PER_SM,
                                                       int(pair_blocks_per_sm)))
+        if nl_slab is not None:
+            N.check(self.lib.hb_forcefield_set_launch(self.h, N.HB_LAUNCH_NL_SLAB, int(nl_slab)))
+
+    def capacity(self) -> dict:
+        """Packed-list capacity: entries per slab, the most entries of one
+        i-tile in the last build, slab reallocations, status word."""
+        out = np.zeros(4, dtype=np.uint64)
+        N.check(self.lib.hb_neighbor_capacity(self.h, out.ctypes.data_as(N.PU64)))
+        return dict(zip(["slab", "max_tile_entries", "reallocations", "status"], [int(x) for x in out]))
 
     def scalars(self) -> dict:
         out = np.zeros(10)
@@ -819,6 +831,12 @@ class ShakeMLP:
         s = np.ascontiguousarray(inv_std, dtype=np.float32)
         N.check(self.lib.hb_shake_mlp_set_normalization(self.h, N.f32ptr(m), N.f32ptr(s),
                                                         float(target_scale)))
+
+    def set_wait_limit(self, polls: int = 1 << 22, issue: bool = True) -> None:
+        """Poll limit of the network kernels' bounded waits; issue=False makes
+        the next inference issue no tensor-core work, so its wait runs out
+        (HB_ERR_DEVICE_TIMEOUT, the failure-path test)."""
+        N.check(self.lib.hb_shake_mlp_set_wait_limit(self.h, int(polls), 1 if issue else 0))
 
     def predict(self, features) -> np.ndarray:
         f = np.ascontiguousarray(features, dtype=np.float32).reshape(-1)

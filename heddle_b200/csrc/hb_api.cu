@@ -562,17 +562,9 @@ extern "C" int hb_forcefield_create(hb_system *sys, const hb_forcefield_desc *d,
   hb_forcefield *ff = new hb_forcefield();
   *ff = tmp;
   ff->sys = sys;
-  // pair kernel: the balanced form (with or without energies);
-  // HB_PAIR_KERNEL=rotation / compact select the
-  // rotation sweep or the compacted pair-list form (shared-memory int64
-  // atomics) throughout; exact pairs use the compacted form with per-pair
-  // fixed point and minimum image
-  ff->pair_variant = 3;
-  if (const char *pk = std::getenv("HB_PAIR_KERNEL")) {
-    const std::string v(pk);
-    ff->pair_variant = v == "compact" ? 0 : (v == "rotation" ? 1 : 3);
-  }
-  if (d->pair_mode == HB_PAIRS_EXACT) ff->pair_variant = 2;
+  // pair kernel: the balanced queue form (with or without energies); exact
+  // pairs take the compacted form with per-pair fixed point and minimum image
+  ff->exact_pairs = d->pair_mode == HB_PAIRS_EXACT;
   HB_CUDA(cudaSetDevice(sys->ctx->device));
   HB_CUDA(cudaMalloc(&ff->d_lj, sizeof(float4) * ff->h_lj.size()));
   HB_CUDA(cudaMemcpy(ff->d_lj, ff->h_lj.data(), sizeof(float4) * ff->h_lj.size(),
@@ -694,6 +686,10 @@ extern "C" int hb_forcefield_set_launch(hb_forcefield *ff, int param, int value)
   if (param == HB_LAUNCH_PAIR_BLOCKS_PER_SM) {
     HB_REQUIRE(value >= 1 && value <= 8, HB_ERR_INVALID_ARGUMENT, "pair blocks per SM in 1..8");
     ff->pair_blocks_per_sm = value;
+  } else if (param == HB_LAUNCH_NL_SLAB) {
+    HB_REQUIRE(value >= 2, HB_ERR_INVALID_ARGUMENT, "neighbour slab must hold at least 2 entries");
+    HB_TRY(nl_set_slab(ff, (uint32_t)value));
+    return check_status(ff);
   } else {
     return hb_fail(HB_ERR_INVALID_ARGUMENT, "unknown launch parameter");
   }
@@ -751,6 +747,25 @@ extern "C" int hb_neighbor_stats(hb_forcefield *ff, uint64_t out[6]) {
   out[3] = cnt[0];
   out[4] = st;
   out[5] = (uint64_t)total * 32u * 32u;
+  return HB_OK;
+}
+
+extern "C" int hb_neighbor_capacity(hb_forcefield *ff, uint64_t out[4]) {
+  HB_REQUIRE(ff && out, HB_ERR_INVALID_ARGUMENT, "null argument");
+  cudaStream_t s = ff->sys->ctx->stream;
+  std::vector<uint32_t> nent(ff->n_tiles);
+  uint32_t st = 0;
+  if (ff->n_tiles)
+    HB_CUDA(cudaMemcpyAsync(nent.data(), ff->d_tile_nent, sizeof(uint32_t) * ff->n_tiles,
+                            cudaMemcpyDeviceToHost, s));
+  HB_CUDA(cudaMemcpyAsync(&st, ff->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  HB_CUDA(cudaStreamSynchronize(s));
+  uint32_t mx = 0;
+  for (uint32_t v : nent) mx = std::max(mx, v);
+  out[0] = ff->slab;
+  out[1] = mx;
+  out[2] = ff->reallocations;
+  out[3] = st;
   return HB_OK;
 }
 
@@ -1231,6 +1246,7 @@ extern "C" int hb_integrator_step(hb_integrator *it, hb_forcefield *ff, hb_const
   g_timer = nullptr;
   if (rc != HB_OK) return rc;
   HB_TRY(check_status(ff));
+  if (cons && cons->mlp) HB_TRY(mlp_status(cons->mlp));
   if (ctx->timing) {
     HB_CUDA(cudaStreamSynchronize(ctx->stream));
     HB_CUDA(cudaStreamSynchronize(ctx->stream2));
@@ -1313,6 +1329,7 @@ extern "C" int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
     ctx->t_ms[0] = ms;
   }
   HB_TRY(check_status(ff));
+  if (cons && cons->mlp) HB_TRY(mlp_status(cons->mlp));
   // buffers or sizes changed: the captured graphs are stale
   if (ff->layout_gen != it->graph_gen) drop_graphs(it);
   return HB_OK;

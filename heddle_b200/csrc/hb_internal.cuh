@@ -261,9 +261,7 @@ struct hb_forcefield {
   float4 *d_lj = nullptr;
   float *d_lj_invd = nullptr;      // per type pair: 1 / (cut^2 - r_switch^2) (0: no switch)
   float alpha = 0.f, coul_rc2 = 0.f;
-  int pair_variant = 3;            // 0: compacted pair list, 1: full rotation sweep,
-                                   // 2: compacted, per-pair fixed point + minimum image,
-                                   // 3: balanced queue (rotation sweep for energy steps)
+  bool exact_pairs = false;        // per-pair fixed point and minimum image (lossless mode)
   float rc_max = 0.f, r_skin = 0.f, r_search = 0.f;
   int any_switch = 0;
   int excl_scaled = 0;             // some exclusion has a non-zero scale
@@ -290,6 +288,7 @@ struct hb_forcefield {
   uint32_t *d_entry_j = nullptr;     // [n_tiles * slab * 32] sorted j slots
   uint32_t *d_entry_excl = nullptr;  // [n_tiles * slab * 32] exclusion masks
   uint64_t entry_cap = 0;            // n_tiles * slab
+  uint32_t reallocations = 0;        // slab (re)allocations after the first
   uint64_t layout_gen = 0;           // bumped when list buffers or sizes change:
                                      // captured graphs older than it are stale
   float4 *d_ref_pos = nullptr;       // positions at the last rebuild
@@ -484,6 +483,7 @@ int nl_rebuild_conditional(hb_forcefield *ff, cudaStream_t s);
 int nl_displacement_check(hb_forcefield *ff, cudaStream_t s);
 int nl_gather_positions(hb_forcefield *ff, cudaStream_t s);
 int nl_first_build(hb_forcefield *ff);
+int nl_set_slab(hb_forcefield *ff, uint32_t slab);
 int nl_pairs(hb_forcefield *ff, std::vector<uint32_t> &pairs, uint64_t &dups);
 // bonded terms (hb_bonded.cu): fixed-point adds into fp (sorted slots)
 int bonded_setup(hb_forcefield *ff, const hb_forcefield_desc *d);
@@ -522,6 +522,7 @@ int baro_propose(hb_barostat *b, hb_forcefield *ff, cudaStream_t s);
 int baro_decide(hb_barostat *b, hb_forcefield *ff, cudaStream_t s);
 // learned SHAKE warm start (hb_mlp.cu): network on device features
 int mlp_infer(hb_shake_mlp *m, const float *d_feat, uint32_t n, float *d_out, cudaStream_t s);
+int mlp_status(hb_shake_mlp *m);
 // constraints (hb_cons.cu)
 int cons_positions(hb_constraints *c, double dt, cudaStream_t s);
 int cons_velocities(hb_constraints *c, double dt, bool virial, cudaStream_t s);

@@ -101,8 +101,12 @@ __device__ __forceinline__ void gemm_issue(uint32_t d_tmem, uint32_t a_base, uin
   }
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
-  for (uint32_t i = 0; i < (1u << 22); ++i) {
+// default poll limit of every mbarrier wait (each poll may suspend the
+// thread for a short, hardware-defined time before it returns)
+constexpr uint32_t MLP_POLLS = 1u << 22;
+
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase, uint32_t polls) {
+  for (uint32_t i = 0; i < polls; ++i) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -212,7 +216,8 @@ __device__ void load_weights_bf16(const float *P, unsigned char *w1, unsigned ch
 __global__ void __launch_bounds__(TILE) k_mlp_infer(const float *__restrict__ params,
                                                     MlpNorm norm, const float *__restrict__ feat,
                                                     uint32_t n, float *__restrict__ out,
-                                                    uint32_t *__restrict__ err) {
+                                                    uint32_t *__restrict__ err, uint32_t polls,
+                                                    uint32_t issue) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   InferSmem &S = *reinterpret_cast<InferSmem *>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -249,12 +254,13 @@ __global__ void __launch_bounds__(TILE) k_mlp_infer(const float *__restrict__ pa
   const uint32_t lane_base = tmem + ((uint32_t)(32 * warp) << 16);
   bool ok = true;
   uint32_t phase = 0;
-  // layer 1
-  if (tid == 0) {
+  // layer 1 (issue = 0 only in the failure-path test: no tensor-core work
+  // is issued, so the bounded wait below runs out with nothing in flight)
+  if (tid == 0 && issue) {
     gemm_issue(tmem + TM_Z1, smem_u32(S.x), smem_u32(S.w1), HID, KIN, false);
     umma_commit(mbar);
   }
-  ok = mbar_wait(mbar, phase);
+  ok = mbar_wait(mbar, phase, polls);
   phase ^= 1u;
   fence_after_sync();
   float h1[HID];
@@ -280,7 +286,7 @@ __global__ void __launch_bounds__(TILE) k_mlp_infer(const float *__restrict__ pa
       gemm_issue(tmem + TM_Z2, smem_u32(S.h1), smem_u32(S.w2), HID, HID, false);
       umma_commit(mbar);
     }
-    ok = mbar_wait(mbar, phase);
+    ok = mbar_wait(mbar, phase, polls);
     phase ^= 1u;
     fence_after_sync();
     if (ok) {
@@ -295,10 +301,11 @@ __global__ void __launch_bounds__(TILE) k_mlp_infer(const float *__restrict__ pa
     }
   }
   if (!ok && tid == 0) atomicExch(err, 1u);
-  if (ok && row < n) out[row] = y * norm.t_scale;
+  // after a timeout the rows get no correction (a plain SHAKE start)
+  if (row < n) out[row] = ok ? y * norm.t_scale : 0.0f;
   fence_before_sync();
   __syncthreads();
-  if (!ok) mbar_wait(mbar, phase);  // a late MMA: one more bounded wait
+  if (!ok) mbar_wait(mbar, phase, polls);  // a late MMA: one more bounded wait
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(TM_COLS_INFER));
@@ -350,7 +357,8 @@ __global__ void __launch_bounds__(TILE) k_mlp_train(
     float *__restrict__ params, float *__restrict__ adam_m, float *__restrict__ adam_v,
     uint32_t step0, MlpNorm norm, const float *__restrict__ feat, const float *__restrict__ tgt,
     const uint32_t *__restrict__ perm, uint32_t n_batches, uint32_t B, float lr, int mode,
-    float *__restrict__ grads, float *__restrict__ loss_out, uint32_t *__restrict__ err) {
+    float *__restrict__ grads, float *__restrict__ loss_out, uint32_t *__restrict__ err,
+    uint32_t polls) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   TrainSmem &S = *reinterpret_cast<TrainSmem *>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -412,7 +420,7 @@ __global__ void __launch_bounds__(TILE) k_mlp_train(
         gemm_issue(tmem + TM_Z1, smem_u32(S.x), smem_u32(S.w1), HID, KIN, false);
         umma_commit(mbar);
       }
-      ok = mbar_wait(mbar, phase);
+      ok = mbar_wait(mbar, phase, polls);
       phase ^= 1u;
       fence_after_sync();
       float h1[HID];
@@ -438,7 +446,7 @@ __global__ void __launch_bounds__(TILE) k_mlp_train(
         gemm_issue(tmem + TM_Z2, smem_u32(S.h1), smem_u32(S.w2), HID, HID, false);
         umma_commit(mbar);
       }
-      ok = mbar_wait(mbar, phase);
+      ok = mbar_wait(mbar, phase, polls);
       phase ^= 1u;
       fence_after_sync();
       float y = S.P[OFF_B3];
@@ -487,7 +495,7 @@ __global__ void __launch_bounds__(TILE) k_mlp_train(
         gemm_issue(tmem + TM_Z1, smem_u32(S.dz2), smem_u32(S.w2t), HID, HID, false);
         umma_commit(mbar);
       }
-      ok = mbar_wait(mbar, phase);
+      ok = mbar_wait(mbar, phase, polls);
       phase ^= 1u;
       fence_after_sync();
       float dz1[HID];
@@ -514,7 +522,7 @@ __global__ void __launch_bounds__(TILE) k_mlp_train(
         gemm_issue(tmem + TM_G, smem_u32(S.g), smem_u32(S.bt), GN, TILE, t > 0);
         umma_commit(mbar);
       }
-      ok = mbar_wait(mbar, phase);
+      ok = mbar_wait(mbar, phase, polls);
       phase ^= 1u;
       fence_after_sync();
       ok = __syncthreads_and(ok);
@@ -583,7 +591,7 @@ __global__ void __launch_bounds__(TILE) k_mlp_train(
     for (int q = tid; q < NPARAM; q += TILE) params[q] = S.P[q];
   fence_before_sync();
   __syncthreads();
-  if (!ok) mbar_wait(mbar, phase);
+  if (!ok) mbar_wait(mbar, phase, polls);
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(TM_COLS_TRAIN));
@@ -600,6 +608,8 @@ struct hb_shake_mlp {
   uint32_t *d_err = nullptr;
   float *d_loss = nullptr;
   uint32_t step = 0;
+  uint32_t polls = MLP_POLLS;  // poll limit of every bounded wait
+  uint32_t issue = 1;          // 0: the next inference issues no MMA (failure-path test)
   MlpNorm norm;
 };
 
@@ -634,7 +644,7 @@ int mlp_infer(hb_shake_mlp *m, const float *d_feat, uint32_t n, float *d_out, cu
   if (n == 0) return HB_OK;
   HB_TRY(mlp_smem_attrs());
   k_mlp_infer<<<hb_div_up(n, TILE), TILE, INFER_SMEM, s>>>(m->d_params, m->norm, d_feat, n,
-                                                            d_out, m->d_err);
+                                                            d_out, m->d_err, m->polls, m->issue);
   HB_CUDA(cudaGetLastError());
   return HB_OK;
 }
@@ -687,6 +697,16 @@ extern "C" int hb_shake_mlp_create(hb_context *ctx, uint64_t seed, hb_shake_mlp 
     return hb_fail(HB_ERR_CUDA, "MLP allocation failed");
   }
   *out = m;
+  return HB_OK;
+}
+
+// the error word of the last kernels (inference inside integrator steps)
+int mlp_status(hb_shake_mlp *m) { return mlp_check_err(m); }
+
+extern "C" int hb_shake_mlp_set_wait_limit(hb_shake_mlp *m, uint32_t polls, int issue) {
+  HB_REQUIRE(m && polls >= 1, HB_ERR_INVALID_ARGUMENT, "need a network and polls >= 1");
+  m->polls = polls;
+  m->issue = issue ? 1u : 0u;
   return HB_OK;
 }
 
@@ -761,7 +781,7 @@ static int mlp_run(hb_shake_mlp *m, const float *features, const float *targets,
   if (rc == HB_OK) {
     k_mlp_train<<<1, TILE, sizeof(TrainSmem), s>>>(m->d_params, m->d_m, m->d_v, m->step, m->norm,
                                                    d_f, d_t, d_p, n_batches, B, lr, mode, d_g,
-                                                   m->d_loss, m->d_err);
+                                                   m->d_loss, m->d_err, m->polls);
     if (cudaGetLastError() != cudaSuccess) rc = hb_fail(HB_ERR_CUDA, "MLP launch failed");
   }
   float lsum = 0.0f;

@@ -799,6 +799,7 @@ int nl_first_build(hb_forcefield *ff) {
   for (uint32_t v : nent) mx = std::max(mx, v);
   const uint32_t want = mx + mx / 2 + 4;
   if (want > ff->slab) {
+    if (ff->slab) ff->reallocations++;
     cudaFree(ff->d_entry_j);
     cudaFree(ff->d_entry_excl);
     ff->d_entry_j = nullptr;
@@ -820,6 +821,36 @@ int nl_first_build(hb_forcefield *ff) {
   HB_CUDA(cudaStreamSynchronize(s));
   ff->built = true;
   return HB_OK;
+}
+
+// Slabs of a caller-chosen size (capacity tests, and recovery after an
+// overflow): reallocate the entry buffers, clear the capacity bits and
+// rebuild at once into the new slabs.  The fill pass writes at most `slab`
+// entries per tile and raises the overflow bit when a tile has more, so a
+// slab that is too small halts the force field (HB_ERR_NL_OVERFLOW from the
+// caller's status check) without writing past the buffers.
+int nl_set_slab(hb_forcefield *ff, uint32_t slab) {
+  hb_system *sys = ff->sys;
+  if (sys->n == 0) return HB_OK;
+  cudaStream_t s = sys->ctx->stream;
+  HB_CUDA(cudaStreamSynchronize(s));
+  cudaFree(ff->d_entry_j);
+  cudaFree(ff->d_entry_excl);
+  ff->d_entry_j = nullptr;
+  ff->d_entry_excl = nullptr;
+  const size_t cap = (size_t)ff->n_tiles * slab;
+  HB_CUDA(cudaMalloc(&ff->d_entry_j, sizeof(uint32_t) * 32 * cap));
+  HB_CUDA(cudaMalloc(&ff->d_entry_excl, sizeof(uint32_t) * 32 * cap));
+  ff->slab = slab;
+  ff->entry_cap = cap;
+  ff->reallocations++;
+  ff->layout_gen++;
+  uint32_t st = 0;
+  HB_CUDA(cudaMemcpyAsync(&st, ff->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  HB_CUDA(cudaStreamSynchronize(s));
+  st &= ~(HB_ST_ENTRY_HIGHWATER | HB_ST_ENTRY_OVERFLOW);
+  HB_CUDA(cudaMemcpyAsync(ff->d_status, &st, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  return nl_rebuild(ff, false, s);
 }
 
 namespace {

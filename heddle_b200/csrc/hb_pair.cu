@@ -8,26 +8,26 @@
 // polynomial in single precision), per-fragment cutoffs, exclusion scales
 // applied per fragment, energy and virial split 1/2 per atom.
 //
-// Structure (own design): one warp per i-tile walks that tile's entries;
-// each lane owns one i-atom, the 32 j-atoms of an entry rotate through the
-// warp by shuffles (a lock-step diagonal sweep), and both sides accumulate
-// in registers.  The per-entry f32 partial sums are converted to int64
-// fixed point (2^40) and added: i-side in registers across entries (one
-// global atomic per atom at the end), j-side with one global reduction per
-// entry lane.  Integer addition is associative, so forces do not depend on
-// entry order or on scheduling and repeat runs are byte-identical.
-// Exclusions arrive as a 32-bit mask per j-atom built with the list, so an
-// ordinary pair costs no exclusion lookup.  Tiles that satisfy the
-// single-periodic-copy condition shift i and j positions against the tile
-// centre once per entry and skip the per-pair minimum image.
+// Structure (own design): persistent warps take (i-tile, chunk of entries)
+// work items.  Per entry a distance pass over the 32 x 32 slot pairs leaves a
+// hit mask per i-lane, one warp scan places the hits in a lane-major queue,
+// and the math pass gives every lane a run of that queue (k_pair4, every
+// fast step, with or without energies).  Pair forces are summed as integers
+// (int32 shared sums folded into int64 fixed point at 2^40), so forces do
+// not depend on entry order or on scheduling and repeat runs are
+// byte-identical.  Exclusions arrive as a 32-bit mask per (entry, i-lane)
+// built with the list, so an ordinary pair costs no exclusion lookup.  Tiles
+// that satisfy the single-periodic-copy condition shift i and j positions
+// against the tile centre once per entry and skip the per-pair minimum
+// image.  The exact-pair form (k_pair2<.., EXACT>) converts every pair force
+// to int64 fixed point and takes each pair's own minimum image, so forces
+// are functions of the positions alone (the lossless integrator needs that).
 #include <algorithm>
 #include <type_traits>
 
 #include "hb_internal.cuh"
 
 namespace {
-
-#define PAIR_WARPS 4
 
 struct PairParams {
   int n_types;
@@ -54,249 +54,6 @@ __device__ __forceinline__ long long to_fixed(float v) {
 
 __device__ __forceinline__ void red_add(unsigned long long *p, long long v) {
   if (v != 0) atomicAdd(p, (unsigned long long)v);
-}
-
-template <bool EV, bool SCALED, bool SWITCH>
-__global__ void __launch_bounds__(PAIR_WARPS * 32, 8)
-    k_pair(const float4 *__restrict__ tile_posq, const int *__restrict__ tile_type,
-           const float4 *__restrict__ center, const uint32_t *__restrict__ tile_nent,
-           const uint32_t *__restrict__ entry_j, const uint32_t *__restrict__ entry_excl,
-           const DBox *__restrict__ box, const float4 *__restrict__ lj_table,
-           const float *__restrict__ lj_invd, PairParams P,
-           unsigned long long *__restrict__ fp, unsigned long long *__restrict__ e_lj_total,
-           const uint32_t *__restrict__ sorted_ids, const uint32_t *__restrict__ eoff,
-           const uint32_t *__restrict__ epart, const float2 *__restrict__ escale) {
-  extern __shared__ float4 sm_lj[];
-  // per warp: the current entry's j positions / charges and types, read by
-  // lane l at rotation t from slot (l + t) mod 32 (conflict-free)
-  __shared__ float4 sm_jp[PAIR_WARPS][32];
-  __shared__ int sm_jt[PAIR_WARPS][32];
-  const int nt2 = P.n_types * P.n_types;
-  float *sm_ljd = reinterpret_cast<float *>(sm_lj + nt2);
-  for (int k = threadIdx.x; k < nt2; k += blockDim.x) {
-    sm_lj[k] = lj_table[k];
-    sm_ljd[k] = lj_invd[k];
-  }
-  __syncthreads();
-
-  const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  const uint32_t I = blockIdx.x * PAIR_WARPS + w;
-  if (I >= P.n_tiles) return;
-  const DBox b = *box;
-  const float4 c = center[I];
-  const bool spc = ((int)c.w & 1) != 0;
-  const uint32_t si = I * 32u + lane;
-  const bool ivalid = si < P.n;
-  float4 pi = tile_posq[si];
-  if (ivalid) {
-    if (spc) shift_to(pi.x, pi.y, pi.z, c, b);
-  } else {
-    pi = make_float4(-1.0e18f, -1.0e18f, -1.0e18f, 0.0f);
-  }
-  const int ti = ivalid ? tile_type[si] : 0;
-  const uint32_t oi = SCALED ? (ivalid ? sorted_ids[si] : HB_SENTINEL) : 0u;
-  const int ti_row = ti * P.n_types;
-
-  long long ax = 0, ay = 0, az = 0, ae = 0, aw = 0;
-  float elj_warp = 0.0f;
-
-  const uint32_t e0 = I * P.slab;
-  const uint32_t e1 = e0 + min(tile_nent[I], P.slab);
-  const uint32_t nvalid_i = P.n - I * 32u;
-  const bool has_self = nvalid_i >= 2u;
-
-  for (uint32_t e = e0; e < e1; ++e) {
-    const bool self = has_self && (e == e0);
-    uint32_t sj = entry_j[(uint64_t)e * 32u + lane];
-    // exclusions in this lane's rotation order: bit t <-> j of lane (lane+t)
-    const uint32_t xm = entry_excl[(uint64_t)e * 32u + lane];
-    const bool jvalid = sj != HB_SENTINEL;
-    float4 pj;
-    int tj = 0;
-    uint32_t oj = 0u, oj_home = 0u;
-    if (jvalid) {
-      pj = tile_posq[sj];
-      tj = tile_type[sj];
-      if (spc) shift_to(pj.x, pj.y, pj.z, c, b);
-      if (SCALED) oj_home = sorted_ids[sj];
-    } else {
-      pj = make_float4(1.0e18f, 1.0e18f, 1.0e18f, 0.0f);
-    }
-    float fix = 0.f, fiy = 0.f, fiz = 0.f, fie = 0.f, fiw = 0.f;
-    float fjx = 0.f, fjy = 0.f, fjz = 0.f, fje = 0.f, fjw = 0.f;
-    float elj = 0.0f;
-    __syncwarp();
-    sm_jp[w][lane] = pj;
-    sm_jt[w][lane] = tj;
-    __syncwarp();
-
-#define HB_ROTATE()                                                   \
-  {                                                                   \
-    const int src = (lane + 1u) & 31u;                                \
-    fjx = __shfl_sync(0xFFFFFFFFu, fjx, src);                         \
-    fjy = __shfl_sync(0xFFFFFFFFu, fjy, src);                         \
-    fjz = __shfl_sync(0xFFFFFFFFu, fjz, src);                         \
-    if (EV) {                                                         \
-      fje = __shfl_sync(0xFFFFFFFFu, fje, src);                       \
-      fjw = __shfl_sync(0xFFFFFFFFu, fjw, src);                       \
-    }                                                                 \
-  }
-
-    // valid j-slots in this lane's rotation order; padding slots take part
-    // in no pair, whatever their placeholder coordinates give under the
-    // minimum image
-    const uint32_t jv_mask = __ballot_sync(0xFFFFFFFFu, jvalid);
-    const uint32_t jv_rot = ivalid ? __funnelshift_r(jv_mask, jv_mask, lane) : 0u;
-    uint32_t t0 = 0u, t1 = 32u;
-    if (self) {
-      HB_ROTATE();
-      t0 = 1u;
-      t1 = 17u;
-    }
-    for (uint32_t t = t0; t < t1; ++t) {
-      {
-        const uint32_t jl = (lane + t) & 31u;
-        pj = sm_jp[w][jl];
-        tj = sm_jt[w][jl];
-        if (SCALED) oj = __shfl_sync(0xFFFFFFFFu, oj_home, jl);
-      }
-      float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-      if (!spc) hb_min_image(dx, dy, dz, b);
-      const float r2 = dx * dx + dy * dy + dz * dz;
-      const bool excl = (xm >> t) & 1u;
-      bool active = r2 < P.rc2_max && (SCALED || !excl) && ((jv_rot >> t) & 1u);
-      if (self && t == 16u && lane >= 16u) active = false;
-      if (active) {
-        float s_lj = 1.0f, s_c = 1.0f;
-        if (SCALED && excl) {
-          // rare path: per-pair scales from the CSR (jit_composed.rs:1448-1460)
-          s_lj = 0.0f;
-          s_c = 0.0f;
-          for (uint32_t q = eoff[oj]; q < eoff[oj + 1]; ++q) {
-            if (epart[q] == oi) {
-              float2 sc = escale[q];
-              s_lj = sc.x;
-              s_c = sc.y;
-              break;
-            }
-          }
-        }
-        const float inv_r = rsqrtf(r2);
-        const float inv_r2 = inv_r * inv_r;
-        float fac = 0.0f, en = 0.0f;
-        if (P.lj_on) {
-          const float4 L = sm_lj[ti_row + tj];
-          if (r2 <= L.z && L.y != 0.0f && s_lj != 0.0f) {
-            const float sr2 = L.x * inv_r2;
-            const float sr6 = sr2 * sr2 * sr2;
-            const float sr12 = sr6 * sr6;
-            float f = L.y * inv_r2 * (2.0f * sr12 - sr6);
-            float u = (L.y * (1.0f / 6.0f)) * (sr12 - sr6);
-            if (SWITCH && r2 > L.w && L.z > L.w) {
-              const float inv_d = sm_ljd[ti_row + tj];
-              const float tau = (r2 - L.w) * inv_d;
-              const float omt = 1.0f - tau;
-              const float sw = omt * omt * (1.0f + 2.0f * tau);
-              const float chain = 12.0f * tau * omt * inv_d;
-              f = sw * f + chain * u;
-              u = sw * u;
-            }
-            fac += s_lj * f;
-            if (EV) {
-              en += s_lj * u;
-              elj += s_lj * u;
-            }
-          }
-        }
-        if (P.coul_on && r2 <= P.coul_rc2 && s_c != 0.0f) {
-          const float r = r2 * inv_r;
-          const float ar = P.alpha * r;
-          const float g = __expf(-ar * ar);
-          const float tt = __fdividef(1.0f, 1.0f + 0.3275911f * ar);
-          const float poly =
-              0.254829592f +
-              (-0.284496736f + (1.421413741f + (-1.453152027f + 1.061405429f * tt) * tt) * tt) *
-                  tt;
-          const float erfc_ar = poly * tt * g;
-          const float qq = pi.w * pj.w;
-          fac += s_c * qq * inv_r2 * (erfc_ar * inv_r + P.c2a * g);
-          if (EV) en += s_c * qq * erfc_ar * inv_r;
-        }
-        const float fx = fac * dx, fy = fac * dy, fz = fac * dz;
-        fix += fx;
-        fiy += fy;
-        fiz += fz;
-        fjx -= fx;
-        fjy -= fy;
-        fjz -= fz;
-        if (EV) {
-          const float he = 0.5f * en, hw = 0.5f * fac * r2;
-          fie += he;
-          fiw += hw;
-          fje += he;
-          fjw += hw;
-        }
-      }
-      if (t + 1u < t1) HB_ROTATE();
-    }
-    if (self) {
-      // 16 rotations: the j-state of home lane s sits at lane s - 16
-      const int src = (lane + 16u) & 31u;
-      fix += __shfl_sync(0xFFFFFFFFu, fjx, src);
-      fiy += __shfl_sync(0xFFFFFFFFu, fjy, src);
-      fiz += __shfl_sync(0xFFFFFFFFu, fjz, src);
-      if (EV) {
-        fie += __shfl_sync(0xFFFFFFFFu, fje, src);
-        fiw += __shfl_sync(0xFFFFFFFFu, fjw, src);
-      }
-    } else {
-      // 31 rotations: the j-state of home lane s sits at lane s - 31 = s + 1
-      const int src = (lane + 1u) & 31u;
-      fjx = __shfl_sync(0xFFFFFFFFu, fjx, src);
-      fjy = __shfl_sync(0xFFFFFFFFu, fjy, src);
-      fjz = __shfl_sync(0xFFFFFFFFu, fjz, src);
-      if (EV) {
-        fje = __shfl_sync(0xFFFFFFFFu, fje, src);
-        fjw = __shfl_sync(0xFFFFFFFFu, fjw, src);
-      }
-      if (jvalid) {
-        red_add(&fp[0 * (size_t)P.n_tiles * 32u + sj], to_fixed(fjx));
-        red_add(&fp[1 * (size_t)P.n_tiles * 32u + sj], to_fixed(fjy));
-        red_add(&fp[2 * (size_t)P.n_tiles * 32u + sj], to_fixed(fjz));
-        if (EV) {
-          red_add(&fp[3 * (size_t)P.n_tiles * 32u + sj], to_fixed(fje));
-          red_add(&fp[4 * (size_t)P.n_tiles * 32u + sj], to_fixed(fjw));
-        }
-      }
-    }
-    ax += to_fixed(fix);
-    ay += to_fixed(fiy);
-    az += to_fixed(fiz);
-    if (EV) {
-      ae += to_fixed(fie);
-      aw += to_fixed(fiw);
-      elj_warp += elj;
-    }
-  }
-  if (ivalid) {
-    const size_t np = (size_t)P.n_tiles * 32u;
-    red_add(&fp[0 * np + si], ax);
-    red_add(&fp[1 * np + si], ay);
-    red_add(&fp[2 * np + si], az);
-    if (EV) {
-      red_add(&fp[3 * np + si], ae);
-      red_add(&fp[4 * np + si], aw);
-    }
-  }
-  if (EV) {
-    // LJ energy total for the scalar split: per-lane fixed point, then one
-    // integer reduction per warp (order-independent)
-    long long v = to_fixed(elj_warp);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-    if (lane == 0) red_add(e_lj_total, v);
-  }
-#undef HB_ROTATE
 }
 
 // ---------------------------------------------------------------------
@@ -979,18 +736,6 @@ int launch2_t(hb_forcefield *ff, cudaStream_t s, const PairParams &P) {
   return HB_OK;
 }
 
-template <bool EV, bool SCALED, bool SWITCH>
-int launch_t(hb_forcefield *ff, cudaStream_t s, const PairParams &P) {
-  size_t smem = (sizeof(float4) + sizeof(float)) * (size_t)P.n_types * P.n_types;
-  k_pair<EV, SCALED, SWITCH><<<hb_div_up(P.n_tiles, PAIR_WARPS), PAIR_WARPS * 32, smem, s>>>(
-      ff->d_tile_posq, ff->d_tile_type, ff->d_tile_center, ff->d_tile_nent, ff->d_entry_j,
-      ff->d_entry_excl, ff->sys->d_box, ff->d_lj, ff->d_lj_invd, P, ff->d_fp,
-      ff->d_acc,
-      ff->d_sorted_ids, ff->d_excl_off, ff->d_excl_partner, ff->d_excl_scale);
-  HB_CUDA(cudaGetLastError());
-  return HB_OK;
-}
-
 }  // namespace
 
 int pair_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
@@ -1008,15 +753,7 @@ int pair_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
   P.n_tiles = ff->n_tiles;
   P.slab = ff->slab;
   const bool sc = ff->excl_scaled != 0, sw = ff->any_switch != 0;
-  if (ff->pair_variant == 0) {
-    if (ev) {
-      if (sc) return sw ? launch2_t<true, true, true, false>(ff, s, P) : launch2_t<true, true, false, false>(ff, s, P);
-      return sw ? launch2_t<true, false, true, false>(ff, s, P) : launch2_t<true, false, false, false>(ff, s, P);
-    }
-    if (sc) return sw ? launch2_t<false, true, true, false>(ff, s, P) : launch2_t<false, true, false, false>(ff, s, P);
-    return sw ? launch2_t<false, false, true, false>(ff, s, P) : launch2_t<false, false, false, false>(ff, s, P);
-  }
-  if (ff->pair_variant == 2) {
+  if (ff->exact_pairs) {
     if (ev) {
       if (sc) return sw ? launch2_t<true, true, true, true>(ff, s, P) : launch2_t<true, true, false, true>(ff, s, P);
       return sw ? launch2_t<true, false, true, true>(ff, s, P) : launch2_t<true, false, false, true>(ff, s, P);
@@ -1024,18 +761,10 @@ int pair_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
     if (sc) return sw ? launch2_t<false, true, true, true>(ff, s, P) : launch2_t<false, true, false, true>(ff, s, P);
     return sw ? launch2_t<false, false, true, true>(ff, s, P) : launch2_t<false, false, false, true>(ff, s, P);
   }
-  if (ff->pair_variant == 3) {
-    if (ev) {
-      if (sc) return sw ? launch4_t<true, true, true>(ff, s, P) : launch4_t<true, true, false>(ff, s, P);
-      return sw ? launch4_t<true, false, true>(ff, s, P) : launch4_t<true, false, false>(ff, s, P);
-    }
-    if (sc) return sw ? launch4_t<false, true, true>(ff, s, P) : launch4_t<false, true, false>(ff, s, P);
-    return sw ? launch4_t<false, false, true>(ff, s, P) : launch4_t<false, false, false>(ff, s, P);
-  }
   if (ev) {
-    if (sc) return sw ? launch_t<true, true, true>(ff, s, P) : launch_t<true, true, false>(ff, s, P);
-    return sw ? launch_t<true, false, true>(ff, s, P) : launch_t<true, false, false>(ff, s, P);
+    if (sc) return sw ? launch4_t<true, true, true>(ff, s, P) : launch4_t<true, true, false>(ff, s, P);
+    return sw ? launch4_t<true, false, true>(ff, s, P) : launch4_t<true, false, false>(ff, s, P);
   }
-  if (sc) return sw ? launch_t<false, true, true>(ff, s, P) : launch_t<false, true, false>(ff, s, P);
-  return sw ? launch_t<false, false, true>(ff, s, P) : launch_t<false, false, false>(ff, s, P);
+  if (sc) return sw ? launch4_t<false, true, true>(ff, s, P) : launch4_t<false, true, false>(ff, s, P);
+  return sw ? launch4_t<false, false, true>(ff, s, P) : launch4_t<false, false, false>(ff, s, P);
 }

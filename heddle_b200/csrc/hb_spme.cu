@@ -1267,14 +1267,15 @@ int spme_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
 // ---------------------------------------------------------------------
 // Allocation-free SPME reciprocal evaluation (hb_spme_recip_noalloc).
 //
-// For callers that must not allocate device memory -- code running while a
-// stream is being captured into a CUDA graph (cudaMalloc is not allowed
-// then), or a host process whose device memory is owned by another
-// allocator (a framework's caching pool, a fixed-budget serving process)
-// -- this entry point runs the same spread / FFT / convolution / gather
+// For callers that must not allocate device memory -- a host process whose
+// device memory is owned by another allocator (a framework's caching pool,
+// a fixed-budget serving process), where cudaMalloc would take memory that
+// allocator counts on and cudaMalloc / cudaFree would stall the device --
+// this entry point runs the same spread / FFT / convolution / gather
 // kernels as the force field on grids of at most HB_NOALLOC_MAX_POINTS
 // points, with all scratch in one file-scope device array.  Every GPU that
-// loads the library holds that array until the process exits.
+// loads the library holds that array until the process exits.  The array's
+// device address is looked up once per device (primary context) and cached.
 // ---------------------------------------------------------------------
 #include <mutex>
 

@@ -54,9 +54,17 @@ enum {
 
 /* launch-shape parameters of hb_forcefield_set_launch (autotuned) */
 enum {
-  HB_LAUNCH_PAIR_BLOCKS_PER_SM = 0  /* resident blocks of the persistent pair kernel
+  HB_LAUNCH_PAIR_BLOCKS_PER_SM = 0, /* resident blocks of the persistent pair kernel
                                        per SM (1..8, default 8); fewer leave room
                                        for the concurrent reciprocal-space chain */
+  HB_LAUNCH_NL_SLAB = 1             /* packed entries per i-tile slab (>= 2): the
+                                       list is rebuilt at once into slabs of this
+                                       size; more than 3/4 full grows them again
+                                       (the reference's high-water growth,
+                                       src/forces/neighbor_list.rs:400-446), an
+                                       overflow returns HB_ERR_NL_OVERFLOW and
+                                       halts the force field until a larger slab
+                                       is set */
 };
 
 /* pair accumulation modes (hb_forcefield_desc.pair_mode) */
@@ -212,6 +220,12 @@ int hb_neighbor_pairs(hb_forcefield *ff, uint32_t *pairs, uint64_t cap,
 /* Neighbour-list statistics: out[0] tiles, [1] entries, [2] entry capacity,
  * [3] rebuild count, [4] status word, [5] pair slots per step. */
 int hb_neighbor_stats(hb_forcefield *ff, uint64_t out[6]);
+/* Packed-list capacity (the reference's capacity status,
+ * src/forces/neighbor_list.rs:1080-1262 and kernels/neighbor.cu:643-669):
+ * out[0] entries per i-tile slab, [1] most entries of one i-tile in the last
+ * build, [2] slab reallocations so far (high-water growth included), [3]
+ * status word (HB_ST bits: 1 displaced, 2 high water, 8 overflow). */
+int hb_neighbor_capacity(hb_forcefield *ff, uint64_t out[4]);
 
 /* ---- constraints: replaces the Constraint hooks
  * (src/integrator/constraint.rs:43-122) of SETTLE (src/integrator/settle.rs)
@@ -285,6 +299,14 @@ int hb_shake_mlp_predict(hb_shake_mlp *m, const float *features, uint64_t n, flo
  * rows, no update; *loss = that error */
 int hb_shake_mlp_gradients(hb_shake_mlp *m, const float *features, const float *targets,
                            uint32_t n, float *grads, double *loss);
+/* Bounded waits: every mbarrier wait of the network's kernels gives up after
+ * `polls` polls (default 2^22), the kernel frees its tensor memory and the
+ * call (or the integrator step that ran the inference) returns
+ * HB_ERR_DEVICE_TIMEOUT; the rows of a timed-out inference get no
+ * correction.  issue = 0 makes inference issue no tensor-core work, so its
+ * first wait runs out with nothing in flight: the failure-path test, with
+ * no GPU fault.  No reference counterpart. */
+int hb_shake_mlp_set_wait_limit(hb_shake_mlp *m, uint32_t polls, int issue);
 /* epochs of minibatch Adam (seeded shuffles); loss_per_epoch [epochs] */
 int hb_shake_mlp_train(hb_shake_mlp *m, const float *features, const float *targets,
                        uint64_t n, uint32_t epochs, uint32_t batch, double lr, uint64_t seed,
@@ -515,9 +537,10 @@ int hb_reduce_kinetic(hb_system *sys, double out[4]);
 
 /* ---- allocation-free SPME reciprocal evaluation.  No counterpart in the
  * reference: it exists for callers that must not allocate device memory --
- * code that runs while a stream is captured into a CUDA graph (cudaMalloc
- * is not allowed then) or a process whose device memory belongs to another
- * allocator (a framework's caching pool, a fixed-budget serving process).
+ * a process whose device memory belongs to another allocator (a framework's
+ * caching pool, a fixed-budget serving process), where a cudaMalloc would
+ * take memory that allocator counts on, and cudaMalloc / cudaFree would
+ * stall the device.
  *
  * posq: device [4n] floats (x, y, z, q) in any atom order; out: device
  * [4n] floats receiving (fx, fy, fz, per-atom energy share 1/2 q phi -
@@ -530,9 +553,12 @@ int hb_reduce_kinetic(hb_system *sys, double out[4]);
  * one file-scope device array (about 0.7 MB) that every GPU loading the
  * library holds until the process exits; the call allocates nothing.  The
  * first call on a device looks up that array's address (cudaGetSymbolAddress)
- * and caches it: make that first call before any stream capture.  Every call
- * shares the one array, so calls whose GPU work overlaps (different streams
- * or threads) race; serialise them. */
+ * and caches it for the device's primary context: make that first call
+ * before any stream capture, and make no call after cudaDeviceReset (the
+ * cached address would be stale).  Every call shares the one array, which
+ * keeps the last call's contents (each call clears what must start at
+ * zero), so calls whose GPU work overlaps (different streams or threads)
+ * race; serialise them. */
 int hb_spme_recip_noalloc(const float *posq, uint32_t n, const double box[6],
                           const uint32_t grid[3], uint32_t order, double alpha,
                           float *out, double *energy, void *stream);

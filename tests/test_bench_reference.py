@@ -1,6 +1,7 @@
 """The reference arm of bench.py on the CPU: one JSON line with the GPU
-arm's metric, unit and workload config, a cpu_baseline describing the run
-and an e2e block without transfers; rank 0 alone prints it."""
+arm's metric, unit and workload, its own start / barostat / arithmetic
+stated in the config, a cpu_baseline describing the run and an e2e block
+without transfers; rank 0 alone prints it."""
 
 import json
 import os
@@ -38,7 +39,13 @@ def test_reference_line_matches_the_gpu_arm_contract():
                         "d2h_bytes_per_step": 0}
     args = SimpleNamespace(molecules=512, equilibrate=300, barostat=1)
     spec = S.spc_water(512)
-    assert d["config"] == bench.workload_config(args, spec, 1)
+    gpu = bench.workload_config(args, spec, 1)
+    for key in ("workload", "atoms", "grid", "parallelism"):
+        assert d["config"][key] == gpu[key]
+    # what this arm does differently is said, not inherited from the GPU arm
+    assert d["config"]["barostat"].startswith("none")
+    assert d["config"]["start"] == "lattice start, no relaxation"
+    assert "FP64" in d["config"]["arithmetic"]
 
 
 def test_reference_arm_prints_on_rank_zero_only():

@@ -141,3 +141,38 @@ def test_learned_warm_start_saves_sweeps(ctx, chain):
     tol_store = 1e-5  # f32 storage of the constrained positions
     assert shake_residual(pos0, spec) < tol_store and shake_residual(pos1, spec) < tol_store
     net.close()
+
+
+def test_bounded_wait_times_out_and_the_next_call_succeeds(ctx, chain):
+    # the failure path of the tensor-core network without a GPU fault: with
+    # issue=False no MMA is issued, so the first bounded mbarrier wait runs
+    # out (short poll limit), the kernel frees its tensor memory and the
+    # call reports HB_ERR_DEVICE_TIMEOUT; the next call works normally
+    net, p, mean, inv, rng = random_net(ctx, seed=21)
+    x = rng.normal(size=(300, 8)).astype(np.float32)
+    y0 = net.predict(x)
+    net.set_wait_limit(polls=1024, issue=False)
+    with pytest.raises(hb.HeddleError) as e:
+        net.predict(x)
+    assert e.value.name == "HB_ERR_DEVICE_TIMEOUT"
+    net.set_wait_limit()
+    assert np.array_equal(net.predict(x), y0)
+    # inside an integrator step: the step reports the timeout, the timed-out
+    # rows get no correction (plain SHAKE start), the constraints still hold
+    spec = chain
+    sys_ = hb.System.from_spec(ctx, spec)
+    ff = hb.ForceField.from_spec(sys_, spec)
+    cons = hb.Constraints.from_spec(sys_, spec)
+    it = hb.Integrator(sys_, "langevin-baoab", spec.dt, friction=spec.friction,
+                       temperature=spec.temperature, seed=17)
+    cons.set_warm_start(net)
+    net.set_wait_limit(polls=1024, issue=False)
+    with pytest.raises(hb.HeddleError) as e:
+        it.step(ff, cons, n_steps=1)
+    assert e.value.name == "HB_ERR_DEVICE_TIMEOUT"
+    assert shake_residual(sys_.positions(), spec) < 1e-5
+    net.set_wait_limit()
+    it.step(ff, cons, n_steps=2)
+    assert shake_residual(sys_.positions(), spec) < 1e-5
+    for o in (it, cons, ff, sys_, net):
+        o.close()
