@@ -189,6 +189,43 @@ def cpu_baseline(spec, state=None, forces_gpu=None, budget_s=25.0):
     return base, err
 
 
+def reference_cuda(spec, pos, box, skins_A, rebuilds_per_step):
+    """The reference's own CUDA force path (oracle/_ref: its kernels built
+    for sm_100a, its composed pair kernel regenerated from its templates,
+    cuFFT) timed on the same B200 and the same relaxed positions, outside
+    the timed region.  Per skin: mean device ms of one forces-only
+    evaluation and of each of its stages, of one neighbour rebuild, and the
+    force error against the product's forces is the tests' business."""
+    import copy
+
+    from heddle_b200 import units as U
+    from oracle import refpath as R
+
+    if not R.available():
+        return {"unavailable": "oracle/_ref not built (the reference tree was absent at build time)"}
+    out = {"what": "HeddleMD kernels/*.cu + composed LJ+erfc pair kernel + cuFFT, replayed by "
+                   "oracle/ref_harness.cpp with the reference's launch shapes; f32, forces only"}
+    for skin in skins_A:
+        s = copy.copy(spec)
+        s.r_skin = U.angstrom_au(skin)
+        ref = R.RefForceField(s, positions=pos, box=box)
+        try:
+            ref.rebuild()
+            t = ref.time(reps=10, energies=False)
+            st = ref.stats()
+        finally:
+            ref.close()
+        row = {"eval_ms": t["eval"], "rebuild_ms": t["rebuild"],
+               "stage_us": {k: 1e3 * v for k, v in t.items() if k not in ("eval", "rebuild")},
+               "entries": st["entries"], "single_pairs": st["single_pairs"], "cells": st["cells"]}
+        if skin in rebuilds_per_step:
+            row["ms_per_step_estimate"] = t["eval"] + t["rebuild"] * rebuilds_per_step[skin]
+            row["estimate"] = ("evaluation + rebuild x the rebuild rate the product measured at this "
+                               "skin; the integrator and SETTLE kernels are not included")
+        out[f"skin_{skin:g}A"] = row
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -340,7 +377,9 @@ def run_ours(args):
     ctx.timing(False)
     # the state the timed steps ended in and its forces (outside the timed
     # region), for the force error against the FP64 oracle
-    final_state = final_forces = None
+    final_state = final_forces = ref_state = None
+    if rank == 0:
+        ref_state = (sys_.positions(), sys_.box())
     if rank == 0 and not args.no_cpu_baseline:
         ff.step(scalars=False)
         st = sys_.state()
@@ -425,6 +464,13 @@ def run_ours(args):
         }
         if not args.no_cpu_baseline:
             line["cpu_baseline"], line["force_error"] = cpu_baseline(spec, final_state, final_forces)
+        if ref_state is not None:
+            try:
+                line["reference_cuda"] = reference_cuda(
+                    spec, ref_state[0], ref_state[1], [args.skin, 2.7],
+                    {args.skin: rebuilds / args.steps})
+            except Exception as exc:  # the comparison never costs the headline
+                line["reference_cuda"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
         print(json.dumps(line), flush=True)
     it.close()
     if baro:

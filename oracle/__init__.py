@@ -61,6 +61,8 @@ def lib() -> C.CDLL:
         L = C.CDLL(str(LIB))
         L.or_neighbor_pairs_f32.restype = C.c_int64
         L.or_neighbor_pairs_f32.argtypes = [C.c_int32, PF, PF, C.c_float, PU, C.c_int64]
+        L.or_pair_r2_f32.restype = None
+        L.or_pair_r2_f32.argtypes = [C.c_int64, PU, PF, PF, PF]
         L.or_forces.restype = C.c_int
         L.or_forces.argtypes = [C.c_int32, PD, PD, PI, C.POINTER(OrBox), C.POINTER(OrFF), PD, PD, PD, PD, C.c_int]
         L.or_ewald_recip_energy.restype = C.c_double
@@ -187,6 +189,18 @@ def neighbor_pairs_f32(pos_f32: np.ndarray, box, r_search: float) -> np.ndarray:
     L.or_neighbor_pairs_f32(n, x.ctypes.data_as(PF), b.ctypes.data_as(PF),
                             C.c_float(np.float32(r_search)), out.ctypes.data_as(PU), cnt)
     return out[: 2 * cnt].reshape(-1, 2)
+
+
+def pair_r2_f32(pos_f32: np.ndarray, box, pairs: np.ndarray) -> np.ndarray:
+    """f32 squared minimum-image distances of the given (i, j) pairs by the
+    neighbour rule of or_neighbor_pairs_f32 (kernels/pbc.cuh:18-43)."""
+    x = np.ascontiguousarray(pos_f32, dtype=np.float32).reshape(-1)
+    b = np.asarray(box, dtype=np.float32)
+    p = np.ascontiguousarray(pairs, dtype=np.uint32).reshape(-1)
+    out = np.zeros(p.size // 2, dtype=np.float32)
+    lib().or_pair_r2_f32(p.size // 2, p.ctypes.data_as(PU), x.ctypes.data_as(PF),
+                         b.ctypes.data_as(PF), out.ctypes.data_as(PF))
+    return out
 
 
 def ewald_recip_energy(pos, q, box, alpha: float, m_max: int = 8) -> float:

@@ -192,6 +192,19 @@ static int cmp_pair(const void *a, const void *b) {
   return 0;
 }
 
+/* f32 squared minimum-image distance of given pairs (i, j) by the rule
+ * above, for checking another list's pairs against the exact cut. */
+void or_pair_r2_f32(int64_t n_pairs, const uint32_t *pairs, const float *xyz,
+                    const float *box6, float *out_r2) {
+  for (int64_t k = 0; k < n_pairs; ++k) {
+    uint32_t i = pairs[2 * k], j = pairs[2 * k + 1];
+    float dx = xyz[3 * i] - xyz[3 * j];
+    float dy = xyz[3 * i + 1] - xyz[3 * j + 1];
+    float dz = xyz[3 * i + 2] - xyz[3 * j + 2];
+    out_r2[k] = f32_min_image_r2(dx, dy, dz, box6);
+  }
+}
+
 int64_t or_neighbor_pairs_f32(int32_t n, const float *xyz, const float *box6,
                               float r_search, uint32_t *out_pairs,
                               int64_t cap) {

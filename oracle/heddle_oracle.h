@@ -93,6 +93,8 @@ void or_wrap_with_image(const or_box *b, double *x, double *y, double *z,
  * kernels/neighbor.cu:509-529).  xyz holds float positions [3n].
  * Writes min(count, cap) pairs as (i, j) into out_pairs[2*cap], sorted
  * lexicographically; returns the total count. */
+void or_pair_r2_f32(int64_t n_pairs, const uint32_t *pairs, const float *xyz,
+                    const float *box6, float *out_r2);
 int64_t or_neighbor_pairs_f32(int32_t n, const float *xyz, const float *box6,
                               float r_search, uint32_t *out_pairs, int64_t cap);
 

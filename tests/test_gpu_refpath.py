@@ -1,0 +1,145 @@
+"""Parity with the reference's own CUDA build on the same inputs.
+
+oracle/ref_build.py compiles HeddleMD's kernels (kernels/neighbor.cu,
+spme_recip.cu, settle.cu, forces.cu, the PME_ORDER spread / gather and the
+composed LJ + erfc pair kernel regenerated from its templates) and
+oracle/ref_harness.cpp replays the reference's launch sequence, cuFFT
+included.  These tests run that path and the product on the same f32
+positions:
+
+* forces: product vs reference within 1e-5 RMS relative (the contract's
+  f32 tolerance), per class (pair kernel, SPME reciprocal) and in total;
+  energies and virials of the two agree;
+* the FP64 oracle agrees with the reference to the same bar, which pins the
+  oracle to the reference's own outputs;
+* neighbour sets: the reference's canonical pair list (pair_snapshot),
+  cut at r_search by the exact f32 rule, equals the product's bit for bit;
+* SETTLE: the reference's settle_positions and the product's position reset
+  agree to f32 rounding.
+"""
+
+import numpy as np
+import pytest
+
+import heddle_b200 as hb
+import oracle as O
+from heddle_b200 import systems as S
+from oracle import refpath as R
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not R.available(), reason="oracle/_ref not built (reference tree absent)")]
+
+FORCE_RMS_TOL = 1e-5
+
+
+def rms_rel(F, G):
+    return float(np.sqrt(((F - G) ** 2).sum() / (G ** 2).sum()))
+
+
+def tilted(spec):
+    L = spec.box[0]
+    spec.box = np.array([L, L, L, 0.10 * L, -0.06 * L, 0.08 * L])
+    return spec
+
+
+CASES = {
+    # the reference needs >= 3 cells of r_search per box width
+    "water512-rc7": lambda: S.spc_water(512, r_cut_A=7.0, skin_A=1.0, seed=3),
+    "water1000-tilted-rc7": lambda: tilted(S.spc_water(1000, r_cut_A=7.0, skin_A=1.0, seed=5)),
+    "water8192-config2": lambda: S.spc_water(8192, skin_A=2.0),
+}
+
+
+def product_eval(ctx, spec):
+    sys_ = hb.System.from_spec(ctx, spec)
+    ff = hb.ForceField.from_spec(sys_, spec)
+    ff.step(scalars=True)
+    out = dict(pos=sys_.positions(), box=sys_.box(), F=sys_.forces(), sc=ff.scalars(), pe=ff.per_atom())
+    pairs, dups = ff.neighbor_pairs()
+    out["pairs"], out["dups"] = pairs, dups
+    real = hb.ForceField.from_spec(sys_, spec, reciprocal=False)
+    real.step(scalars=False)
+    out["F_real"] = sys_.forces()
+    real.close()
+    ff.close()
+    sys_.close()
+    return out
+
+
+@pytest.fixture(scope="module", params=list(CASES))
+def case(request, ctx):
+    spec = CASES[request.param]()
+    p = product_eval(ctx, spec)
+    ref = R.RefForceField(spec, positions=p["pos"], box=p["box"])
+    ref.rebuild()
+    ref.evaluate(energies=True)
+    r = {k: ref.result(k) for k in ("total", "pair", "recip")}
+    rs = ref.r_search
+    cand = ref.pairs(rs * (1 + 1e-4) + 1e-6)
+    stats = ref.stats()
+    ref.close()
+    yield request.param, spec, p, r, cand, rs, stats
+
+
+def test_forces_match_reference_cuda(case):
+    name, spec, p, r, _, _, stats = case
+    Fr, Er, Wr = r["total"]
+    assert stats["entries"] > 0
+    assert rms_rel(p["F"], Fr) <= FORCE_RMS_TOL, name
+    # per class: the pair kernel (fast class) and the SPME reciprocal part
+    assert rms_rel(p["F_real"], r["pair"][0]) <= FORCE_RMS_TOL
+    F_recip = p["F"] - p["F_real"]
+    err = np.sqrt(((F_recip - r["recip"][0]) ** 2).sum() / (Fr ** 2).sum())
+    assert err <= FORCE_RMS_TOL
+    # energies: the reference's per-atom shares summed in FP64
+    pe = p["sc"]["potential"]
+    assert abs(Er.sum() - pe) <= 1e-5 * abs(pe), (Er.sum(), pe)
+    assert abs(r["recip"][1].sum() - (p["sc"]["recip"] - p["sc"]["self"])) <= 1e-5 * abs(pe)
+    # virial: pair part (the product reports the pair and reciprocal parts)
+    wp = p["sc"]["virial_pair"]
+    assert abs(r["pair"][2].sum() - wp) <= 1e-4 * abs(wp), (r["pair"][2].sum(), wp)
+
+
+def test_oracle_agrees_with_reference_cuda(case):
+    name, spec, p, r, _, _, _ = case
+    import copy
+
+    s = copy.copy(spec)
+    s.box = p["box"]
+    Fo, _, _, To = O.forces(s, p["pos"])
+    Fr, Er, _ = r["total"]
+    assert rms_rel(Fr, Fo) <= FORCE_RMS_TOL, name
+    pe_o = To["lj"] + To["coulomb_real"] + To["recip"] - To["self"]
+    assert abs(Er.sum() - pe_o) <= 1e-5 * abs(pe_o)
+
+
+def test_neighbor_set_matches_reference_cuda(case):
+    name, spec, p, _, cand, rs, _ = case
+    pos32 = p["pos"].astype(np.float32)
+    r2 = O.pair_r2_f32(pos32, p["box"].astype(np.float32), cand)
+    ref_pairs = cand[r2 <= np.float32(rs) * np.float32(rs)]
+    assert p["dups"] == 0
+    assert ref_pairs.shape == p["pairs"].shape, (name, ref_pairs.shape, p["pairs"].shape)
+    assert np.array_equal(ref_pairs, p["pairs"])
+
+
+def test_settle_matches_reference_cuda(ctx):
+    spec = S.spc_water(512, r_cut_A=7.0, skin_A=1.0, seed=3)
+    sys_ = hb.System.from_spec(ctx, spec)
+    cons = hb.Constraints.from_spec(sys_, spec)
+    ref = sys_.positions()
+    cons.before_drift()
+    rng = np.random.default_rng(7)
+    moved = (ref + rng.normal(scale=0.01, size=ref.shape)).astype(np.float32).astype(np.float64)
+    sys_.set_state(moved, np.zeros_like(moved))
+    moved_dev = sys_.positions()
+    cons.after_drift(spec.dt)
+    pos, vel, _, _ = sys_.state()
+    cons.close()
+    sys_.close()
+    p_r, v_r, _ = R.settle(spec, ref, moved_dev, np.zeros_like(moved), spec.dt)
+    d = pos - p_r
+    L = spec.box[:3]
+    d -= L * np.round(d / L)
+    assert np.abs(d).max() < 2e-5
+    assert rms_rel(vel, v_r) < 1e-3

@@ -321,3 +321,60 @@ def test_berendsen_andersen_and_pressure_coupling_limits():
     # the width guard keeps mu = 1 below 2 r_search
     g = OC.pressure_coupling("berendsen", k, w, box, 100.0, 1.0, 1.0, 10.0, 2.0, 0, 0, r_search=14.99)
     assert g["mu"] == 1.0
+
+
+def test_reference_pair_source_regenerates():
+    """The composed LJ + erfc pair kernel of the reference is rebuilt from
+    its own templates (oracle/ref_build.py) with the four entry points the
+    reference's launcher binds (src/forces/jit_composed.rs:84-87)."""
+    from oracle import ref_build
+
+    if not (ref_build.DEFAULT_REF / "src/forces/jit_composed.rs").exists():
+        pytest.skip("reference tree absent")
+    src = ref_build.compose_pair_source(ref_build.DEFAULT_REF, True, 17.0, 17.0)
+    for entry in ("heddle_jit_composed_pair_force_f(", "heddle_jit_composed_pair_force_fev(",
+                  "heddle_jit_composed_pair_force_single_f(", "heddle_jit_composed_pair_force_single_fev("):
+        assert src.count(entry) == 1
+    assert "struct LjPairFunctor" in src and "struct SpmeRealPairFunctor" in src
+    assert "/*HEDDLE_JIT_" not in src
+    # the same inputs give the same text
+    assert src == ref_build.compose_pair_source(ref_build.DEFAULT_REF, True, 17.0, 17.0)
+
+
+def _refcuda_case(name):
+    if name == "refcuda_water512":
+        spec = S.spc_water(512, r_cut_A=7.0, skin_A=1.0, seed=3)
+    else:
+        spec = S.spc_water(1000, r_cut_A=7.0, skin_A=1.0, seed=5)
+        L = spec.box[0]
+        spec.box = np.array([L, L, L, 0.10 * L, -0.06 * L, 0.08 * L])
+    return spec
+
+
+@pytest.mark.parametrize("name", ["refcuda_water512", "refcuda_water1000_tilted"])
+def test_oracle_matches_reference_cuda_outputs(name):
+    """The FP64 oracle against outputs of the reference itself: HeddleMD's
+    own kernels (neighbour list, composed LJ + erfc pair kernel, SPME with
+    cuFFT) run on a B200 by tests/golden/make_refcuda_golden.py.  Forces
+    agree within the 1e-5 RMS contract (per class too), the potential
+    energy to f32 resolution, and the reference's neighbour list, cut at
+    r_search, is the oracle's f32 rule pair for pair."""
+    import hashlib
+
+    g = np.load(GOLD / f"{name}.npz")
+    spec = _refcuda_case(name)
+    assert np.allclose(spec.box, g["box"])
+    pos = g["positions"].astype(np.float64)
+    Fo, _, _, T = O.forces(spec, pos)
+    Fo_real, _, _, _ = O.forces(spec, pos, recip=False)
+    F = g["forces"].astype(np.float64)
+    norm = np.sqrt((Fo ** 2).sum())
+    assert np.sqrt(((F - Fo) ** 2).sum()) / norm <= 1e-5
+    assert np.sqrt(((g["forces_pair"] - Fo_real) ** 2).sum()) / norm <= 1e-5
+    assert np.sqrt(((g["forces_recip"] - (Fo - Fo_real)) ** 2).sum()) / norm <= 1e-5
+    pe = T["lj"] + T["coulomb_real"] + T["recip"] - T["self"]
+    assert abs(g["energy"].astype(np.float64).sum() - pe) <= 1e-6 * abs(pe)
+    pairs = O.neighbor_pairs_f32(g["positions"], spec.box.astype(np.float32), g["r_search"])
+    assert len(pairs) == int(g["n_pairs"])
+    digest = hashlib.sha256(np.ascontiguousarray(pairs, dtype=np.uint32).tobytes()).hexdigest()
+    assert digest == str(g["pairs_sha256"])
