@@ -55,9 +55,11 @@ def parse():
                    help="untimed Langevin steps (friction 50/ps) that relax the lattice start")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", default="water65536",
-                   choices=["water65536", "batch64", "learned_shake"],
+                   choices=["water65536", "batch64", "learned_shake", "argon10000"],
                    help="water65536: the NPT water box (headline); batch64: the 64-box uneven "
-                        "replica batch, batched graph vs 64 sequential plain runs")
+                        "replica batch, batched graph vs 64 sequential plain runs; learned_shake: the "
+                        "solvated chain with the learned SHAKE warm start; argon10000: LJ argon NVE "
+                        "(water65536 with --molecules 8192 --barostat 0 is the 8,192-water NVT box)")
     p.add_argument("--barostat", type=int, default=1,
                    help="1: NPT with the Monte-Carlo barostat at 1 bar (move every 25 steps); 0: NVT")
     p.add_argument("--tune", type=int, default=1, help="autotune the neighbour-list skin (1/0)")
@@ -331,7 +333,9 @@ def run_ours(args):
     spec.r_skin = U.angstrom_au(args.skin)
     ff = hb.ForceField.from_spec(sys_, spec)
     if tune:
-        ff.set_launch(pair_blocks_per_sm=int(tune["pair_blocks_per_sm"]))
+        from heddle_b200.autotune import apply
+
+        apply(ff, tune)
     # phase the step counter so that a barostat move falls in the middle of
     # the timed window: before it run max(3, W) warm-up steps and the stage
     # breakdown's min(K, 20) steps; a move follows every 25th step
@@ -650,9 +654,15 @@ def run_learned_shake(args):
 
     plain = measure(False)
     warm = measure(True)
+    # the product's cost gate: the warm start is attached only when its
+    # step is faster than plain SHAKE's
+    sys_.set_state(pos0, vel0)
+    gate = cons.choose_warm_start(net, ff, "langevin-baoab", spec.dt, steps=args.steps,
+                                  friction=spec.friction, temperature=spec.temperature, seed=99)
+    chosen = warm if gate["chosen"] == "learned" else plain
     line = {
-        "metric": METRIC, "value": warm["atom_steps_per_s"], "unit": UNIT, "n_gpus": 1,
-        "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": warm["ms_per_step"],
+        "metric": METRIC, "value": chosen["atom_steps_per_s"], "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": chosen["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": f"166-atom bonded chain (110 C-H SHAKE constraints, relative tol 1e-8) "
@@ -660,6 +670,8 @@ def run_learned_shake(args):
                                "300 K, dt 2 fs; learned SHAKE warm start",
                    "atoms": spec.n},
         "plain_shake": plain, "learned_warm_start": warm,
+        "cost_gate": gate, "chosen_form": gate["chosen"],
+        "chosen_vs_plain": plain["ms_per_step"] / chosen["ms_per_step"],
         "sweeps_saved_fraction": 1.0 - warm["mean_sweeps_per_group"] / max(plain["mean_sweeps_per_group"], 1e-12),
         "training": {"samples": int(len(targ)), "epochs": 40, "batch": 512,
                      "loss_first_epoch": float(losses[0]), "loss_last_epoch": float(losses[-1]),
@@ -672,6 +684,54 @@ def run_learned_shake(args):
     return 0
 
 
+def run_argon(args):
+    """Config 1: 10,000 LJ argon atoms, velocity Verlet NVE, dt 5 fs, f32,
+    CUDA-graph steps; the force error against the FP64 oracle at the final
+    state."""
+    import torch
+
+    import heddle_b200 as hb
+    import oracle as O
+    from heddle_b200 import systems as S
+
+    torch.cuda.set_device(0)
+    spec = S.lj_argon()
+    ctx = hb.Context(0)
+    sys_ = hb.System.from_spec(ctx, spec)
+    ff = hb.ForceField.from_spec(sys_, spec)
+    it = hb.Integrator(sys_, "velocity-verlet", spec.dt)
+    it.step_graph(ff, None, n_steps=max(3, args.warmup))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda:0")
+    ctx.timing(True)
+    t_ms = 0.0
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            it.step_graph(ff, None, n_steps=1)
+            t_ms += float(ctx.timings()[0])
+    ctx.timing(False)
+    ff.step(scalars=False)
+    pos, F = sys_.positions(), sys_.forces()
+    Fo, _, _, _ = O.forces(spec, pos)
+    rms, mx = force_error(F, Fo)
+    steps_s = args.steps / (t_ms * 1e-3)
+    line = {
+        "metric": METRIC, "value": spec.n * steps_s, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "lj-argon-10000: LJ argon NVE, f32, 10,000 atoms on a 22^3 grid with "
+                               "jitter, r_c 2.5 sigma, velocity Verlet, dt 5 fs, CUDA graph per step",
+                   "atoms": spec.n, "l2": "flushed between timed steps"},
+        "ns_per_day": spec.dt_fs * steps_s * 0.0864, "clocks": clk.summary(),
+        "force_error": {"rms_rel": rms, "max_rel": mx, "vs": "FP64 CPU oracle at the final state"},
+    }
+    print(json.dumps(line), flush=True)
+    for o in (it, ff, sys_, ctx):
+        o.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -680,6 +740,8 @@ def main():
         return run_batch(args)
     if args.workload == "learned_shake":
         return run_learned_shake(args)
+    if args.workload == "argon10000":
+        return run_argon(args)
     return run_ours(args)
 
 

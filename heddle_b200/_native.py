@@ -34,6 +34,9 @@ HB_CONSTRAINT_SETTLE, HB_CONSTRAINT_SHAKE = 0, 1
 HB_PAIRS_FAST, HB_PAIRS_EXACT = 0, 1
 HB_LAUNCH_PAIR_BLOCKS_PER_SM = 0
 HB_LAUNCH_NL_SLAB = 1
+HB_LAUNCH_PAIR_CHUNK = 2
+HB_LAUNCH_FFT_PLANE = 3
+HB_LAUNCH_GATHER_FORM = 4
 
 PD = C.POINTER(C.c_double)
 PU32 = C.POINTER(C.c_uint32)

@@ -353,17 +353,23 @@ class ForceField:
         N.check(self.lib.hb_forcefield_pre_step(self.h, 1 if force else 0, C.byref(r)))
         return bool(r.value)
 
-    def set_launch(self, pair_blocks_per_sm: int | None = None, nl_slab: int | None = None) -> None:
+    def set_launch(self, pair_blocks_per_sm: int | None = None, nl_slab: int | None = None,
+                   pair_chunk: int | None = None, fft_plane: bool | None = None,
+                   gather_per_offset: bool | None = None) -> None:
         """Launch shapes (autotuned): resident blocks per SM of the persistent
-        pair kernel.  nl_slab rebuilds the packed list at once into slabs of
-        that many entries per i-tile (grown again above 3/4 full; too small
-        raises HB_ERR_NL_OVERFLOW and halts the force field until a larger
-        slab is set)."""
-        if pair_blocks_per_sm is not None:
-            N.check(self.lib.hb_forcefield_set_launch(self.h, N.HB_LAUNCH_PAIR_BLOCKS_PER_SM,
-                                                      int(pair_blocks_per_sm)))
-        if nl_slab is not None:
-            N.check(self.lib.hb_forcefield_set_launch(self.h, N.HB_LAUNCH_NL_SLAB, int(nl_slab)))
+        pair kernel and its packed entries per work item; the whole-plane
+        transform pass (where the grid has one) or line passes; the gather
+        with one thread per (atom, c offset) or per atom.  nl_slab rebuilds
+        the packed list at once into slabs of that many entries per i-tile
+        (grown again above 3/4 full; too small raises HB_ERR_NL_OVERFLOW and
+        halts the force field until a larger slab is set)."""
+        for param, v in ((N.HB_LAUNCH_PAIR_BLOCKS_PER_SM, pair_blocks_per_sm),
+                         (N.HB_LAUNCH_PAIR_CHUNK, pair_chunk),
+                         (N.HB_LAUNCH_FFT_PLANE, fft_plane),
+                         (N.HB_LAUNCH_GATHER_FORM, gather_per_offset),
+                         (N.HB_LAUNCH_NL_SLAB, nl_slab)):
+            if v is not None:
+                N.check(self.lib.hb_forcefield_set_launch(self.h, param, int(v)))
 
     def capacity(self) -> dict:
         """Packed-list capacity: entries per slab, the most entries of one
@@ -490,6 +496,40 @@ class Constraints:
     def set_warm_start(self, mlp: "ShakeMLP | None") -> None:
         N.check(self.lib.hb_constraints_set_warm_start(self.h, mlp.h if mlp else None))
         self._mlp = mlp
+
+    def choose_warm_start(self, mlp: "ShakeMLP", ff: "ForceField", kind: str, dt: float,
+                          steps: int = 50, **integrator_kw) -> dict:
+        """Cost gate of the learned warm start: time `steps` CUDA-graph steps
+        with plain SHAKE and with the network's initial multipliers (device
+        time, a scratch integrator of the given kind, the state restored
+        after each run) and attach the network only if its step is faster --
+        the feature pass and the inference cost a fixed time per step, the
+        sweeps they save scale with the SHAKE work.  Returns both timings,
+        the mean sweeps per group solve, and the choice."""
+        sys_ = self.system
+        ctx = sys_.ctx
+        pos, vel, _, _ = sys_.state()
+        box = sys_.box()
+        out = {}
+        for label, net in (("plain", None), ("learned", mlp)):
+            self.set_warm_start(net)
+            it = Integrator(sys_, kind, dt, **integrator_kw)
+            it.step_graph(ff, self, n_steps=3)
+            self.shake_stats(reset=True)
+            ctx.timing(True)
+            it.step_graph(ff, self, n_steps=steps)
+            ms = float(ctx.timings()[0])
+            ctx.timing(False)
+            st = self.shake_stats()
+            it.close()
+            sys_.set_box(box)
+            sys_.set_state(pos, vel)
+            ff.pre_step(force=True)
+            out[label] = {"ms_per_step": ms / steps, "mean_sweeps": st["mean_sweeps"]}
+        use = out["learned"]["ms_per_step"] < out["plain"]["ms_per_step"]
+        self.set_warm_start(mlp if use else None)
+        out["chosen"] = "learned" if use else "plain"
+        return out
 
     def close(self) -> None:
         if getattr(self, "h", None):

@@ -1,4 +1,4 @@
-"""Autotuner for the neighbour-list skin and the pair kernel's launch shape.
+"""Autotuner for the neighbour-list skin and the force path's launch shapes.
 
 The skin trades pair-kernel work (entries grow roughly as (r_cut + skin)^3)
 against rebuild frequency (a rebuild runs when any atom moved more than
@@ -7,7 +7,12 @@ trades its own throughput against room for the reciprocal-space chain that
 runs concurrently on the second stream.  Both depend on the system, so they
 are measured: each candidate skin gets its own force field on the same
 device-resident system, a short run of CUDA-graph steps is timed with CUDA
-events and the fastest wins; then the residency is swept at that skin.
+events and the fastest wins; then, at that skin, one launch-shape knob at a
+time (each kept at its best before the next is swept): the pair kernel's
+residency, its entries per work item (shorter items balance better, longer
+ones reload the i-tile less often), the reciprocal transform form (the
+whole-plane pass or line passes, where both exist) and the gather form
+(one thread per (atom, c offset) or per atom, spline orders 4 and 8).
 Results are keyed by a size class (atoms, grid) and can be kept in a JSON
 cache file.
 """
@@ -18,6 +23,7 @@ import json
 from pathlib import Path
 
 from . import units as U
+from . import _native as N
 from .api import Constraints, ForceField, Integrator, System
 
 
@@ -39,12 +45,15 @@ def _time_steps(ctx, sys_, ff, cons, integrator_kwargs, steps, warm) -> float:
 
 def tune_skin(ctx, sys_: System, spec, cons: Constraints | None, integrator_kwargs: dict,
               candidates_A=(1.2, 1.6, 2.0, 2.5, 3.0), residencies=(4, 5, 6, 7, 8),
-              steps: int = 150, warm: int = 20, cache: Path | None = None) -> dict:
+              chunks=(2, 4, 8, 16), steps: int = 150, warm: int = 20,
+              cache: Path | None = None) -> dict:
     """Time `steps` graph-mode MD steps per candidate skin (angstrom), then
-    per pair-kernel residency at the best skin; return {"best_A": skin,
-    "pair_blocks_per_sm": r, "ms_per_step": {skin: ms}, "residency_ms":
-    {r: ms}}.  Skins the box cannot hold are skipped.  The system state
-    advances during tuning (the runs are real MD steps)."""
+    per launch-shape knob at the best skin; return {"best_A": skin,
+    "pair_blocks_per_sm": r, "pair_chunk": c, "fft_plane": 0/1,
+    "gather_form": 0/1, "ms_per_step": {skin: ms}, "residency_ms": {r: ms},
+    "chunk_ms": {c: ms}, "fft_plane_ms": {...}, "gather_form_ms": {...}}.
+    Skins the box cannot hold are skipped.  The system state advances
+    during tuning (the runs are real MD steps)."""
     from ._native import HeddleError
 
     key = size_class(spec)
@@ -61,18 +70,41 @@ def tune_skin(ctx, sys_: System, spec, cons: Constraints | None, integrator_kwar
         times[skin] = _time_steps(ctx, sys_, ff, cons, integrator_kwargs, steps, warm)
         ff.close()
     best = min(times, key=times.get)
-    res_times = {}
     ff = ForceField.from_spec(sys_, spec, r_skin=U.angstrom_au(best))
-    for r in residencies:
-        ff.set_launch(pair_blocks_per_sm=r)
-        res_times[r] = _time_steps(ctx, sys_, ff, cons, integrator_kwargs, steps, warm)
-    ff.close()
-    best_r = min(res_times, key=res_times.get)
-    result = {"best_A": best, "pair_blocks_per_sm": best_r,
+
+    def sweep(param, values):
+        t = {}
+        for v in values:
+            N.check(ff.lib.hb_forcefield_set_launch(ff.h, param, int(v)))
+            t[v] = _time_steps(ctx, sys_, ff, cons, integrator_kwargs, steps, warm)
+        b = min(t, key=t.get)
+        N.check(ff.lib.hb_forcefield_set_launch(ff.h, param, int(b)))
+        return b, {str(k): v for k, v in t.items()}
+
+    best_r, res_times = sweep(N.HB_LAUNCH_PAIR_BLOCKS_PER_SM, residencies)
+    best_c, chunk_times = sweep(N.HB_LAUNCH_PAIR_CHUNK, chunks)
+    result = {"best_A": best, "pair_blocks_per_sm": best_r, "pair_chunk": best_c,
               "ms_per_step": {str(k): v for k, v in times.items()},
-              "residency_ms": {str(k): v for k, v in res_times.items()}}
+              "residency_ms": res_times, "chunk_ms": chunk_times}
+    grid = spec.grid if spec.alpha is not None else None
+    if grid is not None:
+        if grid[0] == grid[1] and grid[0] in (64, 128):
+            result["fft_plane"], result["fft_plane_ms"] = sweep(N.HB_LAUNCH_FFT_PLANE, (1, 0))
+        if spec.order in (4, 8):
+            result["gather_form"], result["gather_form_ms"] = sweep(N.HB_LAUNCH_GATHER_FORM, (1, 0))
+    ff.close()
     if cache is not None:
         data = json.loads(cache.read_text()) if cache.exists() else {}
         data[key] = result
         cache.write_text(json.dumps(data, indent=1))
     return result
+
+
+def apply(ff: ForceField, tuned: dict) -> None:
+    """Set a force field's launch shapes to an autotuner result."""
+    for key, param in (("pair_blocks_per_sm", N.HB_LAUNCH_PAIR_BLOCKS_PER_SM),
+                       ("pair_chunk", N.HB_LAUNCH_PAIR_CHUNK),
+                       ("fft_plane", N.HB_LAUNCH_FFT_PLANE),
+                       ("gather_form", N.HB_LAUNCH_GATHER_FORM)):
+        if key in tuned:
+            N.check(ff.lib.hb_forcefield_set_launch(ff.h, param, int(tuned[key])))

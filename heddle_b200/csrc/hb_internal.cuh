@@ -239,6 +239,7 @@ struct SpmeState {
   double *d_part = nullptr;                   // energy / virial partials
   int n_part = 0;
   int use_plane = 0;                          // kc-major planes + whole-plane pass
+  int gather_c = 1;                           // orders 4, 8: thread per (atom, c offset)
   double *d_sums = nullptr;                   // [2] E_recip, W_recip
   float4 *d_recip = nullptr;                  // per sorted atom fx, fy, fz, e
   float self_pref = 0.f;                      // alpha / sqrt(pi)
@@ -299,6 +300,7 @@ struct hb_forcefield {
                                      // [3] largest candidate count seen
   uint32_t *h_status = nullptr;      // pinned mirror
   int pair_blocks_per_sm = 8;        // persistent pair kernel residency (tunable)
+  int pair_chunk = 4;                // packed entries per pair work item (tunable)
   uint32_t *d_work = nullptr;        // work counter of the balanced pair kernel
                                      // (zeroed by the combine kernel)
   uint64_t rebuilds_host = 0;
@@ -495,6 +497,8 @@ int pair_launch(hb_forcefield *ff, bool ev, cudaStream_t s);
 int spme_setup(hb_forcefield *ff, const hb_forcefield_desc *d);
 int spme_free(hb_forcefield *ff);
 int spme_launch(hb_forcefield *ff, bool ev, cudaStream_t s);
+// HB_LAUNCH_FFT_PLANE / HB_LAUNCH_GATHER_FORM (hb_forcefield_set_launch)
+int spme_set_form(hb_forcefield *ff, int param, int value);
 // combine (hb_integ.cu): fixed-point + reciprocal -> force (atom order)
 int forces_finalize(hb_forcefield *ff, bool ev, cudaStream_t s);
 int scalars_reduce(hb_forcefield *ff, cudaStream_t s);

@@ -59,9 +59,9 @@ __device__ __forceinline__ void red_add(unsigned long long *p, long long v) {
 // ---------------------------------------------------------------------
 // Balanced form (every step; with EV also per-atom energy and virial).
 // One lane per i-atom of the tile.  Per entry: (1) a distance pass over the
-// 32 rotations (unrolled for ordinary entries) leaves each lane's mask of
-// the rotations whose pair is inside the cutoff (bit t: j-slot
-// (lane + t) mod 32), with exclusions and padding slots masked out; (2) one
+// 32 j-slots (each j position a broadcast shared load) leaves each
+// lane's mask of the j-slots whose pair is inside the cutoff (bit j), with
+// exclusions and padding slots masked out; (2) one
 // warp scan of the mask counts places every lane's pairs contiguously in a
 // per-warp queue (pairs with a Lennard-Jones term first); (3) the math pass
 // gives each lane a run of the queue, so all lanes stay busy whatever the
@@ -87,8 +87,6 @@ __device__ __forceinline__ void red_add(unsigned long long *p, long long v) {
 struct P4Warp {
   float4 ipos[32];
   float4 jpos[32];
-  float2 jxy[64];  // j-slot k's x, y at k and k + 32: rotation t of lane L reads L + t
-  float jz[64];
   int itype[32];
   int jtype[32];
   uint32_t oi[32];
@@ -170,30 +168,37 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
     long long ax = 0, ay = 0, az = 0, ae = 0, aw = 0;
     const bool has_self = P.n - I * 32u >= 2u;
 
+    // software pipeline over the entries: the next entry's j-slots and
+    // exclusion masks are requested at the top of an entry and its j
+    // positions gathered right after the distance pass, so each entry's
+    // dependent global loads are in flight while the previous entry computes
+    const float4 far = make_float4(1.0e18f, 1.0e18f, 1.0e18f, 0.0f);
+    uint32_t sj_n = entry_j[(uint64_t)e0 * 32u + lane];
+    uint32_t xm_n = entry_excl[(uint64_t)e0 * 32u + lane];
+    float4 pj_n = far;
+    int tj_n = 0;
+    if (sj_n != HB_SENTINEL) {
+      pj_n = tile_posq[sj_n];
+      tj_n = tile_type[sj_n];
+    }
+
     for (uint32_t e = e0; e < e1; ++e) {
       const bool self = has_self && (e == tile_e0);
-      const uint32_t sj = entry_j[(uint64_t)e * 32u + lane];
-      const uint32_t xm = entry_excl[(uint64_t)e * 32u + lane];
+      const uint32_t sj = sj_n, xm = xm_n;
       const bool jvalid = sj != HB_SENTINEL;
-      float4 pj = make_float4(1.0e18f, 1.0e18f, 1.0e18f, 0.0f);
-      int tj = 0;
-      if (jvalid) {
-        pj = tile_posq[sj];
-        tj = tile_type[sj];
-        if (spc) shift_to(pj.x, pj.y, pj.z, c, b);
+      float4 pj = pj_n;
+      const int tj = tj_n;
+      if (jvalid && spc) shift_to(pj.x, pj.y, pj.z, c, b);
+      const bool more = e + 1u < e1;
+      if (more) {
+        sj_n = entry_j[(uint64_t)(e + 1u) * 32u + lane];
+        xm_n = entry_excl[(uint64_t)(e + 1u) * 32u + lane];
       }
       __syncwarp();
       S.jpos[lane] = pj;
-      S.jxy[lane] = make_float2(pj.x, pj.y);
-      S.jxy[lane + 32u] = make_float2(pj.x, pj.y);
-      S.jz[lane] = pj.z;
-      S.jz[lane + 32u] = pj.z;
       S.jtype[lane] = tj;
       S.jslot[lane] = self ? si : sj;
-      if (SCALED) {
-        S.oj[lane] = jvalid ? sorted_ids[sj] : HB_SENTINEL;
-        S.xm[lane] = xm;
-      }
+      if (SCALED) S.oj[lane] = jvalid ? sorted_ids[sj] : HB_SENTINEL;
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
         S.fi[q][lane] = 0;
@@ -206,43 +211,48 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
       }
       __syncwarp();
 
-      // (1) distance pass; the tile's single-periodic-copy flag is uniform
-      // over the warp, so each form is its own code path (no per-pair
-      // minimum-image instructions where the shift already placed the atoms)
+      // (1) distance pass: lane L tests its i-atom against the 32 j-slots in
+      // turn, each j position one broadcast shared load (one wavefront), so
+      // bit j of the mask is the pair (L, j); in the self entry only j > L
+      // counts (each pair once).  The tile's single-periodic-copy flag is
+      // uniform over the warp, so each form is its own code path (no
+      // per-pair minimum-image instructions where the shift already placed
+      // the atoms)
       uint32_t m = 0u;
       auto dist_pass = [&](auto sp) {
         constexpr bool SP = decltype(sp)::value;
-        if (!self) {
-#pragma unroll
-          for (uint32_t t = 0; t < 32u; ++t) {
-            const float2 q = S.jxy[lane + t];
-            const float qz = S.jz[lane + t];
-            float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - qz;
-            if constexpr (!SP) hb_min_image(dx, dy, dz, b);
-            const float r2 = dx * dx + dy * dy + dz * dz;
-            m |= (r2 < P.rc2_max ? 1u : 0u) << t;
-          }
-        } else {
-          for (uint32_t t = 1u; t < 17u; ++t) {
-            const float2 q = S.jxy[lane + t];
-            const float qz = S.jz[lane + t];
-            float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - qz;
-            if constexpr (!SP) hb_min_image(dx, dy, dz, b);
-            const float r2 = dx * dx + dy * dy + dz * dz;
-            m |= (r2 < P.rc2_max ? 1u : 0u) << t;
-          }
-          if (lane >= 16u) m &= ~(1u << 16);  // each self pair once
+#pragma unroll 4
+        for (uint32_t t = 0; t < 32u; ++t) {
+          const float4 q = S.jpos[t];
+          float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
+          if constexpr (!SP) hb_min_image(dx, dy, dz, b);
+          const float r2 = dx * dx + dy * dy + dz * dz;
+          m |= (r2 < P.rc2_max ? 1u : 0u) << t;
         }
+        if (self) m &= lane == 31u ? 0u : (0xFFFFFFFFu << (lane + 1u));
       };
       if (spc) dist_pass(std::true_type{});
       else dist_pass(std::false_type{});
+      // the next entry's j positions (its slots have arrived meanwhile)
+      if (more) {
+        pj_n = far;
+        tj_n = 0;
+        if (sj_n != HB_SENTINEL) {
+          pj_n = tile_posq[sj_n];
+          tj_n = tile_type[sj_n];
+        }
+      }
       // padding slots take part in no pair, whatever their placeholder
       // coordinates give under the minimum image
       const uint32_t jv_mask = __ballot_sync(0xFFFFFFFFu, jvalid);
-      m &= ivalid ? __funnelshift_r(jv_mask, jv_mask, lane) : 0u;
-      if (!SCALED) m &= ~xm;
+      m &= ivalid ? jv_mask : 0u;
+      // the list stores each lane's exclusion bits in rotation order (bit t:
+      // j-slot (L + t) mod 32); rotating left by L gives j order
+      const uint32_t xm_j = __funnelshift_l(xm, xm, lane);
+      if (SCALED) S.xm[lane] = xm_j;  // read by the math pass (scaled exclusions)
+      else m &= ~xm_j;
 
-      // (2) lane-major queues of (i-lane, rotation): each lane writes its
+      // (2) lane-major queues of (i-lane, j-slot): each lane writes its
       // pairs with a Lennard-Jones term to [0, n_lj) and its Coulomb-only
       // pairs to [n_lj, n_lj + n_c) at offsets from one warp scan of the
       // packed counts; the LJ arithmetic runs only over the first range
@@ -256,7 +266,7 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
           const uint32_t bal_t = __ballot_sync(0xFFFFFFFFu, tj == q && jvalid);
           if ((lj_types >> q) & 1u) lj_j |= bal_t;
         }
-        lj_rot = __funnelshift_r(lj_j, lj_j, lane);  // bit t <-> j-lane (lane + t) mod 32
+        lj_rot = lj_j;  // bit j <-> j-slot j
       }
       uint32_t mq = m & lj_rot;
       uint32_t mc = P.coul_on ? (m & ~lj_rot) : 0u;
@@ -302,13 +312,13 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
           const uint32_t kk = lane * rounds + it;
           if (kk < cnt_r) {
             const uint32_t pr = S.pairs[q0 + kk];
-            const uint32_t i = pr >> 8, t = pr & 255u, j = (i + t) & 31u;
+            const uint32_t i = pr >> 8, j = pr & 255u;
             const float4 a = S.ipos[i], q = S.jpos[j];
             float dx = a.x - q.x, dy = a.y - q.y, dz = a.z - q.z;
             if constexpr (!SP) hb_min_image(dx, dy, dz, b);
             const float r2 = dx * dx + dy * dy + dz * dz;
             float s_lj = 1.0f, s_c = 1.0f;
-            if (SCALED && ((S.xm[i] >> t) & 1u)) {
+            if (SCALED && ((S.xm[i] >> j) & 1u)) {
               s_lj = 0.0f;
               s_c = 0.0f;
               const uint32_t oi = S.oi[i], oj = S.oj[j];
@@ -480,13 +490,11 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
   }
 }
 
-// entries per work item of the balanced kernel
-#define P4_CHUNK 4
-
 template <bool EV, bool SCALED, bool SWITCH>
 int launch4_t(hb_forcefield *ff, cudaStream_t s, const PairParams &P) {
   size_t smem = (sizeof(float4) + sizeof(float)) * (size_t)P.n_types * P.n_types;
-  const uint32_t chunks = hb_div_up(P.slab, P4_CHUNK);
+  const uint32_t chunk = (uint32_t)ff->pair_chunk;  // entries per work item
+  const uint32_t chunks = hb_div_up(P.slab, chunk);
   // persistent: pair_blocks_per_sm blocks of 4 warps per SM (at most 8 fit),
   // or fewer for small systems
   const uint32_t items = P.n_tiles * chunks;
@@ -495,7 +503,7 @@ int launch4_t(hb_forcefield *ff, cudaStream_t s, const PairParams &P) {
   k_pair4<EV, SCALED, SWITCH><<<std::max(grid, 1u), P4_WARPS * 32, smem, s>>>(
       ff->d_tile_posq, ff->d_tile_type, ff->d_tile_center, ff->d_tile_nent, ff->d_entry_j,
       ff->d_entry_excl, ff->sys->d_box, ff->d_lj, ff->d_lj_invd, P, ff->d_fp, ff->d_sorted_ids,
-      ff->d_excl_off, ff->d_excl_partner, ff->d_excl_scale, ff->d_work, chunks, P4_CHUNK,
+      ff->d_excl_off, ff->d_excl_partner, ff->d_excl_scale, ff->d_work, chunks, chunk,
       ff->d_acc);
   HB_CUDA(cudaGetLastError());
   return HB_OK;

@@ -1166,6 +1166,28 @@ void fft_passes(const SpmeLaunch &q, unsigned long long *rho, float2 *grid, floa
 
 }  // namespace
 
+// energy / virial partials written per step: one per kc plane (plane form)
+// or one per a-pass CTA (line form)
+int spme_n_part(const SpmeState &S) {
+  const int La = lines_per_cta(S.na);
+  return S.use_plane ? S.nch : S.nb * ((S.nch + La - 1) / La);
+}
+
+int spme_set_form(hb_forcefield *ff, int param, int value) {
+  SpmeState &S = ff->spme;
+  HB_REQUIRE(value == 0 || value == 1, HB_ERR_INVALID_ARGUMENT, "form switch is 0 or 1");
+  if (!S.on) return HB_OK;
+  if (param == HB_LAUNCH_FFT_PLANE) {
+    const int use = (value && plane_supported(S.na, S.nb)) ? 1 : 0;
+    if (use && !S.use_plane) HB_TRY(plane_prepare(S.na));
+    S.use_plane = use;
+    S.n_part = spme_n_part(S);
+  } else {
+    S.gather_c = value;
+  }
+  return HB_OK;
+}
+
 int spme_setup(hb_forcefield *ff, const hb_forcefield_desc *d) {
   SpmeState &S = ff->spme;
   S.on = 1;
@@ -1204,11 +1226,13 @@ int spme_setup(hb_forcefield *ff, const hb_forcefield_desc *d) {
   twiddles(S.nc, tw);
   HB_CUDA(cudaMalloc(&S.d_tw, sizeof(float2) * tw.size()));
   HB_CUDA(cudaMemcpy(S.d_tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice));
-  const int La = lines_per_cta(S.na);
   S.use_plane = plane_supported(S.na, S.nb) ? 1 : 0;
   if (S.use_plane) HB_TRY(plane_prepare(S.na));
-  S.n_part = S.use_plane ? S.nch : S.nb * ((S.nch + La - 1) / La);
-  HB_CUDA(cudaMalloc(&S.d_part, sizeof(double) * 2 * S.n_part));
+  S.n_part = spme_n_part(S);
+  // room for the partials of either transform form (HB_LAUNCH_FFT_PLANE)
+  const int La = lines_per_cta(S.na);
+  const int max_part = std::max(S.nch, S.nb * ((S.nch + La - 1) / La));
+  HB_CUDA(cudaMalloc(&S.d_part, sizeof(double) * 2 * max_part));
   HB_CUDA(cudaMalloc(&S.d_sums, sizeof(double) * 2));
   HB_CUDA(cudaMemset(S.d_sums, 0, sizeof(double) * 2));
   HB_CUDA(cudaMalloc(&S.d_recip, sizeof(float4) * std::max(ff->n_pad, 32u)));
@@ -1252,11 +1276,17 @@ int spme_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
              S.alpha, S.d_part, s, S.use_plane != 0, ev);
   if (n > 0) {
     switch (S.order) {
-      case 4: k_gather_c<4><<<hb_div_up((uint64_t)n * 4u, 128), 128, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
+      case 4:
+        if (S.gather_c) k_gather_c<4><<<hb_div_up((uint64_t)n * 4u, 128), 128, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n);
+        else k_gather<4><<<hb_div_up(n, 64), 64, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n);
+        break;
       case 5: k_gather<5><<<hb_div_up(n, 64), 64, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
       case 6: k_gather<6><<<hb_div_up(n, 64), 64, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
       case 7: k_gather<7><<<hb_div_up(n, 64), 64, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
-      case 8: k_gather_c<8><<<hb_div_up((uint64_t)n * 8u, 128), 128, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n); break;
+      case 8:
+        if (S.gather_c) k_gather_c<8><<<hb_div_up((uint64_t)n * 8u, 128), 128, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n);
+        else k_gather<8><<<hb_div_up(n, 64), 64, 0, s>>>(ff->d_tile_posq, S.d_v, sys->d_box, na, nb, nc, S.self_pref, S.d_recip, n);
+        break;
     }
   }
   if (ev) k_spme_sums<<<1, 256, 0, s>>>(S.d_part, S.n_part, S.d_sums);

@@ -57,7 +57,7 @@ enum {
   HB_LAUNCH_PAIR_BLOCKS_PER_SM = 0, /* resident blocks of the persistent pair kernel
                                        per SM (1..8, default 8); fewer leave room
                                        for the concurrent reciprocal-space chain */
-  HB_LAUNCH_NL_SLAB = 1             /* packed entries per i-tile slab (>= 2): the
+  HB_LAUNCH_NL_SLAB = 1,            /* packed entries per i-tile slab (>= 2): the
                                        list is rebuilt at once into slabs of this
                                        size; more than 3/4 full grows them again
                                        (the reference's high-water growth,
@@ -65,6 +65,16 @@ enum {
                                        overflow returns HB_ERR_NL_OVERFLOW and
                                        halts the force field until a larger slab
                                        is set */
+  HB_LAUNCH_PAIR_CHUNK = 2,         /* packed entries per work item of the
+                                       persistent pair kernel (1..64, default 4):
+                                       shorter items balance better, longer ones
+                                       reload the i-tile less often */
+  HB_LAUNCH_FFT_PLANE = 3,          /* 1 (default where supported: 64 x 64 and
+                                       128 x 128 (a, b) planes): whole-plane FFT
+                                       pass; 0: line passes */
+  HB_LAUNCH_GATHER_FORM = 4         /* spline orders 4 and 8: 1 (default) one
+                                       thread per (atom, c offset); 0 one thread
+                                       per atom */
 };
 
 /* pair accumulation modes (hb_forcefield_desc.pair_mode) */

@@ -295,3 +295,33 @@ def test_triclinic_reciprocal_paths_match_oracle(ctx, grid, order):
     assert rms_rel(F, Fo) <= FORCE_RMS_TOL, rms_rel(F, Fo)
     _, _, _, Tp = O.forces(spec, pos, poly_erfc=True)
     assert abs(sc["recip"] - Tp["recip"]) <= 1e-5 * abs(Tp["recip"])
+
+
+def test_launch_shapes_keep_the_forces(ctx):
+    """The autotuner's knobs change launch shapes, not results: any pair
+    entry chunk gives byte-identical forces (integer sums); the line-pass
+    transform and the per-atom gather agree with the defaults to f32
+    rounding and with the FP64 oracle."""
+    from heddle_b200 import _native as N
+
+    spec = S.spc_water(8192, skin_A=2.0)
+    assert spec.grid == (64, 64, 64)
+    sys_ = hb.System.from_spec(ctx, spec)
+    ff = hb.ForceField.from_spec(sys_, spec)
+    ff.step(scalars=True)
+    F0, e0 = sys_.forces(), ff.scalars()["potential"]
+    for chunk in (1, 3, 16):
+        ff.set_launch(pair_chunk=chunk)
+        ff.step(scalars=True)
+        assert np.array_equal(sys_.forces(), F0), chunk
+    Fo, _, _, _ = O.forces(spec, sys_.positions())
+    for param in (N.HB_LAUNCH_FFT_PLANE, N.HB_LAUNCH_GATHER_FORM):
+        N.check(ff.lib.hb_forcefield_set_launch(ff.h, param, 0))
+        ff.step(scalars=True)
+        F = sys_.forces()
+        assert rms_rel(F, F0) < 2e-6
+        assert rms_rel(F, Fo) <= FORCE_RMS_TOL
+        assert abs(ff.scalars()["potential"] - e0) <= 1e-6 * abs(e0)
+        N.check(ff.lib.hb_forcefield_set_launch(ff.h, param, 1))
+    ff.close()
+    sys_.close()

@@ -140,6 +140,21 @@ def test_learned_warm_start_saves_sweeps(ctx, chain):
     assert st1["mean_sweeps"] < 0.75 * st0["mean_sweeps"], (st0, st1)
     tol_store = 1e-5  # f32 storage of the constrained positions
     assert shake_residual(pos0, spec) < tol_store and shake_residual(pos1, spec) < tol_store
+    # the cost gate times both forms, keeps the faster one and leaves the
+    # state as it found it
+    sys_ = hb.System.from_spec(ctx, spec)
+    ff = hb.ForceField.from_spec(sys_, spec)
+    cons = hb.Constraints.from_spec(sys_, spec)
+    p_before = sys_.positions()
+    g = cons.choose_warm_start(net, ff, "langevin-baoab", spec.dt, steps=20, friction=spec.friction,
+                               temperature=spec.temperature, seed=5)
+    assert np.array_equal(sys_.positions(), p_before)
+    faster = "learned" if g["learned"]["ms_per_step"] < g["plain"]["ms_per_step"] else "plain"
+    assert g["chosen"] == faster
+    assert g["learned"]["mean_sweeps"] < g["plain"]["mean_sweeps"]
+    assert (cons._mlp is net) == (faster == "learned")
+    for o in (cons, ff, sys_):
+        o.close()
     net.close()
 
 
