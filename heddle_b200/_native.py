@@ -37,6 +37,7 @@ HB_LAUNCH_NL_SLAB = 1
 HB_LAUNCH_PAIR_CHUNK = 2
 HB_LAUNCH_FFT_PLANE = 3
 HB_LAUNCH_GATHER_FORM = 4
+HB_LAUNCH_PAIR_QUOTA = 5
 
 PD = C.POINTER(C.c_double)
 PU32 = C.POINTER(C.c_uint32)

@@ -355,9 +355,10 @@ class ForceField:
 
     def set_launch(self, pair_blocks_per_sm: int | None = None, nl_slab: int | None = None,
                    pair_chunk: int | None = None, fft_plane: bool | None = None,
-                   gather_per_offset: bool | None = None) -> None:
+                   gather_per_offset: bool | None = None, pair_quota: int | None = None) -> None:
         """Launch shapes (autotuned): resident blocks per SM of the persistent
-        pair kernel and its packed entries per work item; the whole-plane
+        pair kernel, its packed entries per work item and work items per
+        warp (0: persistent blocks); the whole-plane
         transform pass (where the grid has one) or line passes; the gather
         with one thread per (atom, c offset) or per atom.  nl_slab rebuilds
         the packed list at once into slabs of that many entries per i-tile
@@ -365,6 +366,7 @@ class ForceField:
         halts the force field until a larger slab is set)."""
         for param, v in ((N.HB_LAUNCH_PAIR_BLOCKS_PER_SM, pair_blocks_per_sm),
                          (N.HB_LAUNCH_PAIR_CHUNK, pair_chunk),
+                         (N.HB_LAUNCH_PAIR_QUOTA, pair_quota),
                          (N.HB_LAUNCH_FFT_PLANE, fft_plane),
                          (N.HB_LAUNCH_GATHER_FORM, gather_per_offset),
                          (N.HB_LAUNCH_NL_SLAB, nl_slab)):

@@ -690,6 +690,9 @@ extern "C" int hb_forcefield_set_launch(hb_forcefield *ff, int param, int value)
     HB_REQUIRE(value >= 2, HB_ERR_INVALID_ARGUMENT, "neighbour slab must hold at least 2 entries");
     HB_TRY(nl_set_slab(ff, (uint32_t)value));
     return check_status(ff);
+  } else if (param == HB_LAUNCH_PAIR_QUOTA) {
+    HB_REQUIRE(value >= 0 && value <= 4096, HB_ERR_INVALID_ARGUMENT, "pair work quota in 0..4096");
+    ff->pair_quota = value;
   } else if (param == HB_LAUNCH_PAIR_CHUNK) {
     HB_REQUIRE(value >= 1 && value <= 64, HB_ERR_INVALID_ARGUMENT, "pair entry chunk in 1..64");
     ff->pair_chunk = value;

@@ -301,6 +301,7 @@ struct hb_forcefield {
   uint32_t *h_status = nullptr;      // pinned mirror
   int pair_blocks_per_sm = 8;        // persistent pair kernel residency (tunable)
   int pair_chunk = 4;                // packed entries per pair work item (tunable)
+  int pair_quota = 0;                // work items per pair warp (0: persistent; tunable)
   uint32_t *d_work = nullptr;        // work counter of the balanced pair kernel
                                      // (zeroed by the combine kernel)
   uint64_t rebuilds_host = 0;

@@ -59,7 +59,8 @@ __device__ __forceinline__ void red_add(unsigned long long *p, long long v) {
 // ---------------------------------------------------------------------
 // Balanced form (every step; with EV also per-atom energy and virial).
 // One lane per i-atom of the tile.  Per entry: (1) a distance pass over the
-// 32 j-slots (each j position a broadcast shared load) leaves each
+// 32 j-slots (broadcast shared loads; two slots per packed FP32x2 step in
+// single-periodic-copy tiles) leaves each
 // lane's mask of the j-slots whose pair is inside the cutoff (bit j), with
 // exclusions and padding slots masked out; (2) one
 // warp scan of the mask counts places every lane's pairs contiguously in a
@@ -87,6 +88,8 @@ __device__ __forceinline__ void red_add(unsigned long long *p, long long v) {
 struct P4Warp {
   float4 ipos[32];
   float4 jpos[32];
+  float4 jxy2[16];  // j-slots 2k, 2k + 1 negated: (-x, -x', -y, -y') for the packed distance pass
+  float2 jz2[16];   // (-z, -z')
   int itype[32];
   int jtype[32];
   uint32_t oi[32];
@@ -107,7 +110,7 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
             const float *__restrict__ lj_invd, PairParams P, unsigned long long *__restrict__ fp,
             const uint32_t *__restrict__ sorted_ids, const uint32_t *__restrict__ eoff,
             const uint32_t *__restrict__ epart, const float2 *__restrict__ escale,
-            uint32_t *__restrict__ work, uint32_t chunks, uint32_t chunk,
+            uint32_t *__restrict__ work, uint32_t chunks, uint32_t chunk, uint32_t quota,
             unsigned long long *__restrict__ e_lj_total) {
   extern __shared__ float4 sm_lj4[];
   __shared__ P4Warp smw4[P4_WARPS];
@@ -139,8 +142,11 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
   const size_t np_all = (size_t)P.n_tiles * 32u;
   const uint32_t n_items = P.n_tiles * chunks;
 
-  // persistent warps take (tile, chunk of entries) items from a counter
-  for (;;) {
+  // warps take (tile, chunk of entries) items from a counter, at most
+  // `quota` each: a finite quota retires blocks as they finish, so the
+  // concurrent reciprocal-space kernels (a higher-priority stream) get SM
+  // room between pair blocks instead of only what persistent blocks leave
+  for (uint32_t taken = 0; taken < quota; ++taken) {
     uint32_t g = 0u;
     if (lane == 0) g = atomicAdd(work, 1u);
     g = __shfl_sync(0xFFFFFFFFu, g, 0);
@@ -163,7 +169,10 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
     }
     __syncwarp();
     S.ipos[lane] = pi;
-    S.itype[lane] = (ivalid ? tile_type[si] : 0) * P.n_types;
+    const int ti = ivalid ? tile_type[si] : 0;
+    S.itype[lane] = ti * P.n_types;
+    // j-types with a Lennard-Jones term against this lane's i-atom
+    const uint32_t lj_types = few_types ? sm_ljtypes[ti] : 0u;
     if (SCALED) S.oi[lane] = ivalid ? sorted_ids[si] : HB_SENTINEL;
     long long ax = 0, ay = 0, az = 0, ae = 0, aw = 0;
     const bool has_self = P.n - I * 32u >= 2u;
@@ -196,6 +205,12 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
       }
       __syncwarp();
       S.jpos[lane] = pj;
+      {
+        float *jn = reinterpret_cast<float *>(&S.jxy2[lane >> 1]);
+        jn[lane & 1u] = -pj.x;
+        jn[2u + (lane & 1u)] = -pj.y;
+        reinterpret_cast<float *>(&S.jz2[lane >> 1])[lane & 1u] = -pj.z;
+      }
       S.jtype[lane] = tj;
       S.jslot[lane] = self ? si : sj;
       if (SCALED) S.oj[lane] = jvalid ? sorted_ids[sj] : HB_SENTINEL;
@@ -221,13 +236,32 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
       uint32_t m = 0u;
       auto dist_pass = [&](auto sp) {
         constexpr bool SP = decltype(sp)::value;
+        if constexpr (SP) {
+          // two j-slots per step in the packed FP32x2 pipe (FADD2 / FMUL2 /
+          // FFMA2): pi - q is pi + (-q) exactly, each lane of a packed op
+          // rounds like the scalar op
+          const float2 px = make_float2(pi.x, pi.x), py = make_float2(pi.y, pi.y),
+                       pz = make_float2(pi.z, pi.z);
 #pragma unroll 4
-        for (uint32_t t = 0; t < 32u; ++t) {
-          const float4 q = S.jpos[t];
-          float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
-          if constexpr (!SP) hb_min_image(dx, dy, dz, b);
-          const float r2 = dx * dx + dy * dy + dz * dz;
-          m |= (r2 < P.rc2_max ? 1u : 0u) << t;
+          for (uint32_t k = 0; k < 16u; ++k) {
+            const float4 a = S.jxy2[k];
+            const float2 dx = __fadd2_rn(px, make_float2(a.x, a.y));
+            const float2 dy = __fadd2_rn(py, make_float2(a.z, a.w));
+            const float2 dz = __fadd2_rn(pz, S.jz2[k]);
+            float2 r2 = __fmul2_rn(dx, dx);
+            r2 = __ffma2_rn(dy, dy, r2);
+            r2 = __ffma2_rn(dz, dz, r2);
+            m |= ((r2.x < P.rc2_max ? 1u : 0u) | (r2.y < P.rc2_max ? 2u : 0u)) << (2u * k);
+          }
+        } else {
+#pragma unroll 4
+          for (uint32_t t = 0; t < 32u; ++t) {
+            const float4 q = S.jpos[t];
+            float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
+            hb_min_image(dx, dy, dz, b);
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            m |= (r2 < P.rc2_max ? 1u : 0u) << t;
+          }
         }
         if (self) m &= lane == 31u ? 0u : (0xFFFFFFFFu << (lane + 1u));
       };
@@ -260,7 +294,6 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
       if (!P.lj_on) {
         lj_rot = 0u;
       } else if (few_types) {
-        const uint32_t lj_types = sm_ljtypes[S.itype[lane] / P.n_types];
         uint32_t lj_j = 0u;
         for (int q = 0; q < P.n_types; ++q) {
           const uint32_t bal_t = __ballot_sync(0xFFFFFFFFu, tj == q && jvalid);
@@ -435,9 +468,96 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
           atomicAdd(&S.fi[2][ci], sz);
         }
       };
+      // Coulomb-only pairs of single-periodic-copy tiles on force-only steps
+      // (most pairs of a water box): two pairs of a lane's run per step in
+      // the packed FP32x2 pipe (FADD2 / FMUL2 / FFMA2), the transcendentals
+      // and the integer sums per pair as in math_pass
+      auto math_pass_c2 = [&](uint32_t q0, uint32_t cnt_r) {
+        const uint32_t rounds = (((cnt_r + 31u) >> 5) + 1u) & ~1u;  // even: pairs of pairs
+        uint32_t ci = 32u;
+        int sx = 0, sy = 0, sz = 0;
+        constexpr float FLIM = P4_FMAX * P4_SCALE;
+        auto accum = [&](uint32_t i, uint32_t j, float fx, float fy, float fz) {
+          if (fabsf(fx) <= FLIM && fabsf(fy) <= FLIM && fabsf(fz) <= FLIM) {
+            const int ix = __float2int_rn(fx), iy = __float2int_rn(fy), iz = __float2int_rn(fz);
+            atomicAdd(&S.fj[0][jo + j], -ix);
+            atomicAdd(&S.fj[1][jo + j], -iy);
+            atomicAdd(&S.fj[2][jo + j], -iz);
+            if (i != ci) {
+              if (ci < 32u) {
+                atomicAdd(&S.fi[0][ci], sx);
+                atomicAdd(&S.fi[1][ci], sy);
+                atomicAdd(&S.fi[2][ci], sz);
+              }
+              ci = i;
+              sx = sy = sz = 0;
+            }
+            sx += ix;
+            sy += iy;
+            sz += iz;
+          } else {
+            const uint32_t ti_slot = I * 32u + i, tj_slot = S.jslot[j];
+            const long long lx = __float2ll_rn(fx * (HB_FP_SCALE / P4_SCALE)),
+                            ly = __float2ll_rn(fy * (HB_FP_SCALE / P4_SCALE)),
+                            lz = __float2ll_rn(fz * (HB_FP_SCALE / P4_SCALE));
+            red_add(&fp[0 * np_all + ti_slot], lx);
+            red_add(&fp[1 * np_all + ti_slot], ly);
+            red_add(&fp[2 * np_all + ti_slot], lz);
+            red_add(&fp[0 * np_all + tj_slot], -lx);
+            red_add(&fp[1 * np_all + tj_slot], -ly);
+            red_add(&fp[2 * np_all + tj_slot], -lz);
+          }
+        };
+        const float2 alpha2 = make_float2(P.alpha, P.alpha), one2 = make_float2(1.0f, 1.0f),
+                     c2a2 = make_float2(P.c2a, P.c2a), sc2 = make_float2(P4_SCALE, P4_SCALE);
+        for (uint32_t it = 0; it < rounds; it += 2u) {
+          const uint32_t ka = lane * rounds + it;
+          if (ka < cnt_r) {
+            const bool vb = ka + 1u < cnt_r;
+            const uint32_t pa = S.pairs[q0 + ka], pb = vb ? S.pairs[q0 + ka + 1u] : pa;
+            const uint32_t ia = pa >> 8, ja = pa & 255u, ib = pb >> 8, jb = pb & 255u;
+            const float4 a = S.ipos[ia], a2 = S.ipos[ib], qa = S.jpos[ja], qb = S.jpos[jb];
+            const float2 dx = __fadd2_rn(make_float2(a.x, a2.x), make_float2(-qa.x, -qb.x));
+            const float2 dy = __fadd2_rn(make_float2(a.y, a2.y), make_float2(-qa.y, -qb.y));
+            const float2 dz = __fadd2_rn(make_float2(a.z, a2.z), make_float2(-qa.z, -qb.z));
+            float2 r2 = __fmul2_rn(dx, dx);
+            r2 = __ffma2_rn(dy, dy, r2);
+            r2 = __ffma2_rn(dz, dz, r2);
+            const float2 inv_r = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+            const float2 inv_r2 = __fmul2_rn(inv_r, inv_r);
+            const float2 r = __fmul2_rn(r2, inv_r);
+            const float2 ar = __fmul2_rn(alpha2, r);
+            const float2 ea = __fmul2_rn(make_float2(-ar.x, -ar.y), ar);
+            const float2 gg = make_float2(__expf(ea.x), __expf(ea.y));
+            const float2 den = __ffma2_rn(make_float2(0.3275911f, 0.3275911f), ar, one2);
+            const float2 tt = make_float2(__fdividef(1.0f, den.x), __fdividef(1.0f, den.y));
+            float2 poly = __ffma2_rn(make_float2(1.061405429f, 1.061405429f), tt,
+                                     make_float2(-1.453152027f, -1.453152027f));
+            poly = __ffma2_rn(poly, tt, make_float2(1.421413741f, 1.421413741f));
+            poly = __ffma2_rn(poly, tt, make_float2(-0.284496736f, -0.284496736f));
+            poly = __ffma2_rn(poly, tt, make_float2(0.254829592f, 0.254829592f));
+            const float2 pt = __fmul2_rn(poly, tt);
+            const float2 wv = __fmul2_rn(gg, __ffma2_rn(pt, inv_r, c2a2));
+            const float2 qq = __fmul2_rn(make_float2(a.w, a2.w), make_float2(qa.w, qb.w));
+            float2 fac = __fmul2_rn(__fmul2_rn(qq, inv_r2), wv);
+            if (!(r2.x <= P.coul_rc2)) fac.x = 0.0f;
+            if (!(r2.y <= P.coul_rc2)) fac.y = 0.0f;
+            const float2 fs = __fmul2_rn(fac, sc2);
+            const float2 fx = __fmul2_rn(fs, dx), fy = __fmul2_rn(fs, dy), fz = __fmul2_rn(fs, dz);
+            accum(ia, ja, fx.x, fy.x, fz.x);
+            if (vb) accum(ib, jb, fx.y, fy.y, fz.y);
+          }
+        }
+        if (ci < 32u) {
+          atomicAdd(&S.fi[0][ci], sx);
+          atomicAdd(&S.fi[1][ci], sy);
+          atomicAdd(&S.fi[2][ci], sz);
+        }
+      };
       if (spc) {
         math_pass(std::true_type{}, std::true_type{}, 0u, n_lj);
-        math_pass(std::true_type{}, std::false_type{}, n_lj, n_c);
+        if (!EV && !SCALED) math_pass_c2(n_lj, n_c);
+        else math_pass(std::true_type{}, std::false_type{}, n_lj, n_c);
       } else {
         math_pass(std::false_type{}, std::true_type{}, 0u, n_lj);
         math_pass(std::false_type{}, std::false_type{}, n_lj, n_c);
@@ -495,15 +615,22 @@ int launch4_t(hb_forcefield *ff, cudaStream_t s, const PairParams &P) {
   size_t smem = (sizeof(float4) + sizeof(float)) * (size_t)P.n_types * P.n_types;
   const uint32_t chunk = (uint32_t)ff->pair_chunk;  // entries per work item
   const uint32_t chunks = hb_div_up(P.slab, chunk);
-  // persistent: pair_blocks_per_sm blocks of 4 warps per SM (at most 8 fit),
-  // or fewer for small systems
   const uint32_t items = P.n_tiles * chunks;
-  const uint32_t grid = std::min<uint32_t>(
-      (uint32_t)ff->sys->ctx->n_sm * (uint32_t)ff->pair_blocks_per_sm, hb_div_up(items, P4_WARPS));
+  // persistent (quota 0): pair_blocks_per_sm blocks of 4 warps per SM (at
+  // most 8 fit), or fewer for small systems; with a quota of q items per
+  // warp, enough blocks that every item is taken
+  uint32_t grid, quota = 0xFFFFFFFFu;
+  if (ff->pair_quota > 0) {
+    quota = (uint32_t)ff->pair_quota;
+    grid = hb_div_up(items, P4_WARPS * quota);
+  } else {
+    grid = std::min<uint32_t>((uint32_t)ff->sys->ctx->n_sm * (uint32_t)ff->pair_blocks_per_sm,
+                              hb_div_up(items, P4_WARPS));
+  }
   k_pair4<EV, SCALED, SWITCH><<<std::max(grid, 1u), P4_WARPS * 32, smem, s>>>(
       ff->d_tile_posq, ff->d_tile_type, ff->d_tile_center, ff->d_tile_nent, ff->d_entry_j,
       ff->d_entry_excl, ff->sys->d_box, ff->d_lj, ff->d_lj_invd, P, ff->d_fp, ff->d_sorted_ids,
-      ff->d_excl_off, ff->d_excl_partner, ff->d_excl_scale, ff->d_work, chunks, chunk,
+      ff->d_excl_off, ff->d_excl_partner, ff->d_excl_scale, ff->d_work, chunks, chunk, quota,
       ff->d_acc);
   HB_CUDA(cudaGetLastError());
   return HB_OK;

@@ -72,9 +72,14 @@ enum {
   HB_LAUNCH_FFT_PLANE = 3,          /* 1 (default where supported: 64 x 64 and
                                        128 x 128 (a, b) planes): whole-plane FFT
                                        pass; 0: line passes */
-  HB_LAUNCH_GATHER_FORM = 4         /* spline orders 4 and 8: 1 (default) one
+  HB_LAUNCH_GATHER_FORM = 4,        /* spline orders 4 and 8: 1 (default) one
                                        thread per (atom, c offset); 0 one thread
                                        per atom */
+  HB_LAUNCH_PAIR_QUOTA = 5          /* work items per pair-kernel warp (0..4096):
+                                       0 (default) persistent blocks; q > 0
+                                       blocks that retire after q items each, so
+                                       the concurrent reciprocal-space kernels
+                                       are scheduled between them */
 };
 
 /* pair accumulation modes (hb_forcefield_desc.pair_mode) */

@@ -299,7 +299,7 @@ def test_triclinic_reciprocal_paths_match_oracle(ctx, grid, order):
 
 def test_launch_shapes_keep_the_forces(ctx):
     """The autotuner's knobs change launch shapes, not results: any pair
-    entry chunk gives byte-identical forces (integer sums); the line-pass
+    entry chunk or work quota gives byte-identical forces (integer sums); the line-pass
     transform and the per-atom gather agree with the defaults to f32
     rounding and with the FP64 oracle."""
     from heddle_b200 import _native as N
@@ -314,6 +314,10 @@ def test_launch_shapes_keep_the_forces(ctx):
         ff.set_launch(pair_chunk=chunk)
         ff.step(scalars=True)
         assert np.array_equal(sys_.forces(), F0), chunk
+    for quota in (1, 5, 0):
+        ff.set_launch(pair_quota=quota)
+        ff.step(scalars=True)
+        assert np.array_equal(sys_.forces(), F0), quota
     Fo, _, _, _ = O.forces(spec, sys_.positions())
     for param in (N.HB_LAUNCH_FFT_PLANE, N.HB_LAUNCH_GATHER_FORM):
         N.check(ff.lib.hb_forcefield_set_launch(ff.h, param, 0))
