@@ -536,6 +536,22 @@ def run_batch(args):
             t_ms += float(master.timings()[0])
     master.timing(False)
     rebuilds = sum(o[2].stats()["rebuilds"] for o in objs) - rebuilds0
+    one_launch = batch.pair_form()
+    # the same batch with a pair kernel per member (graph branches), for
+    # comparison with the one multi-system pair launch (untimed headline)
+    batch.set_pair_form(False)
+    batch.step(2)
+    master.timing(True)
+    t_per = 0.0
+    k_per = max(3, args.steps // 2)
+    for _ in range(k_per):
+        flush.zero_()
+        torch.cuda.synchronize()
+        batch.step(1)
+        t_per += float(master.timings()[0])
+    master.timing(False)
+    batch.set_pair_form(True)
+    batch.step(1)
     # 64 sequential plain runs (each box's own CUDA-graph steps, one box
     # after another), wall clock
     k_seq = max(1, args.steps // 4)
@@ -567,7 +583,11 @@ def run_batch(args):
                    "atoms": n_atoms, "boxes": len(specs),
                    "l2": "flushed between timed steps (256 MiB write, outside the timed region)"},
         "batched_graph": {"atom_steps_per_s_device": value,
-                          "atom_steps_per_s_wall": n_atoms * k_seq / t_batch_wall},
+                          "atom_steps_per_s_wall": n_atoms * k_seq / t_batch_wall,
+                          "pair_form": ("one persistent pair kernel over all members' work items"
+                                        if one_launch else "a pair kernel per member")},
+        "batched_graph_pair_per_member": {"atom_steps_per_s_device": n_atoms * k_per / (t_per * 1e-3),
+                                          "ms_per_step": t_per / k_per},
         "sequential_plain": {"atom_steps_per_s_wall": n_atoms * k_seq / t_seq, "steps": k_seq},
         "speedup_wall": t_seq / t_batch_wall,
         "rebuilds_in_timed_steps": rebuilds,

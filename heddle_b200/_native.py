@@ -38,6 +38,7 @@ HB_LAUNCH_PAIR_CHUNK = 2
 HB_LAUNCH_FFT_PLANE = 3
 HB_LAUNCH_GATHER_FORM = 4
 HB_LAUNCH_PAIR_QUOTA = 5
+HB_LAUNCH_NL_WAIT_TEST = 6
 
 PD = C.POINTER(C.c_double)
 PU32 = C.POINTER(C.c_uint32)
@@ -257,6 +258,8 @@ SIGNATURES = {
     "hb_batch_destroy": (C.c_int, [VP]),
     "hb_batch_step": (C.c_int, [VP, C.c_uint32]),
     "hb_batch_count_launches": (C.c_int, [VP, PU64]),
+    "hb_batch_set_pair_form": (C.c_int, [VP, C.c_int]),
+    "hb_batch_pair_form": (C.c_int, [VP, C.POINTER(C.c_int)]),
     "hb_reduce_kinetic": (C.c_int, [VP, PD]),
     "hb_spme_recip_noalloc": (C.c_int, [C.c_void_p, C.c_uint32, PD, PU32, C.c_uint32, C.c_double,
                                         C.c_void_p, PD, C.c_void_p]),

@@ -831,6 +831,16 @@ class Batch:
     def step(self, n_steps: int = 1) -> None:
         N.check(self.lib.hb_batch_step(self.h, int(n_steps)))
 
+    def set_pair_form(self, one_launch: bool) -> None:
+        """One multi-system pair kernel for all members (default, when they
+        share the pair physics) or one pair kernel per member."""
+        N.check(self.lib.hb_batch_set_pair_form(self.h, 1 if one_launch else 0))
+
+    def pair_form(self) -> bool:
+        v = C.c_int(0)
+        N.check(self.lib.hb_batch_pair_form(self.h, C.byref(v)))
+        return bool(v.value)
+
     def count_launches(self) -> tuple:
         out = np.zeros(2, dtype=np.uint64)
         N.check(self.lib.hb_batch_count_launches(self.h, out.ctypes.data_as(N.PU64)))

@@ -615,7 +615,12 @@ extern "C" int hb_forcefield_create(hb_system *sys, const hb_forcefield_desc *d,
 
 // ForceField::step body: gated neighbour rebuild, pair kernel on the main
 // stream overlapped with the SPME chain on the second stream, combine.
-static int force_eval(hb_forcefield *ff, bool ev, bool capturing = false) {
+// A force evaluation in three parts: everything before the pair kernel
+// (neighbour check / rebuild, tile-order gather, bonded terms, the
+// reciprocal-space chain forked onto the second stream), the pair kernel,
+// and the join + finalize.  Replica batches put one multi-system pair
+// launch between the members' first and last parts.
+static int force_pre(hb_forcefield *ff, bool ev, bool capturing) {
   hb_context *ctx = ff->sys->ctx;
   cudaStream_t s = ctx->stream, s2 = ctx->stream2;
   cudaEvent_t t0 = stage_begin(s);
@@ -635,12 +640,24 @@ static int force_eval(hb_forcefield *ff, bool ev, bool capturing = false) {
     stage_end(2, t2, s2);
     HB_CUDA(cudaEventRecord(ctx->ev_join, s2));
   }
-  cudaEvent_t t1 = stage_begin(s);
-  HB_TRY(pair_launch(ff, ev, s));
-  stage_end(1, t1, s);
+  return HB_OK;
+}
+
+static int force_post(hb_forcefield *ff, bool ev) {
+  hb_context *ctx = ff->sys->ctx;
+  cudaStream_t s = ctx->stream;
   if (ff->spme.on) HB_CUDA(cudaStreamWaitEvent(s, ctx->ev_join, 0));
   HB_TRY(forces_finalize(ff, ev, s));
   return HB_OK;
+}
+
+static int force_eval(hb_forcefield *ff, bool ev, bool capturing = false) {
+  cudaStream_t s = ff->sys->ctx->stream;
+  HB_TRY(force_pre(ff, ev, capturing));
+  cudaEvent_t t1 = stage_begin(s);
+  HB_TRY(pair_launch(ff, ev, s));
+  stage_end(1, t1, s);
+  return force_post(ff, ev);
 }
 
 // host check of the status word: overflow is an error (the reference's
@@ -650,6 +667,13 @@ static int check_status(hb_forcefield *ff) {
   HB_CUDA(cudaMemcpyAsync(ff->h_status, ff->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   HB_CUDA(cudaStreamSynchronize(s));
   const uint32_t st = ff->h_status[0];
+  if (st & HB_ST_DEVICE_TIMEOUT) {
+    // report once; the list is incomplete, so the next step rebuilds it
+    const uint32_t clr = (st & ~HB_ST_DEVICE_TIMEOUT) | HB_ST_DISPLACED;
+    HB_CUDA(cudaMemcpyAsync(ff->d_status, &clr, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    HB_CUDA(cudaStreamSynchronize(s));
+    return hb_fail(HB_ERR_DEVICE_TIMEOUT, "neighbour tile build: a bounded wait for a staged tile gave up");
+  }
   if (st & HB_ST_ENTRY_OVERFLOW)
     return hb_fail(HB_ERR_NL_OVERFLOW, "packed neighbour entries overflowed their capacity");
   if (st & HB_ST_ENTRY_HIGHWATER) HB_TRY(nl_first_build(ff));
@@ -690,6 +714,10 @@ extern "C" int hb_forcefield_set_launch(hb_forcefield *ff, int param, int value)
     HB_REQUIRE(value >= 2, HB_ERR_INVALID_ARGUMENT, "neighbour slab must hold at least 2 entries");
     HB_TRY(nl_set_slab(ff, (uint32_t)value));
     return check_status(ff);
+  } else if (param == HB_LAUNCH_NL_WAIT_TEST) {
+    HB_REQUIRE(value >= 0, HB_ERR_INVALID_ARGUMENT, "poll limit must be >= 0");
+    ff->nl_polls = value > 0 ? (uint32_t)value : (1u << 20);
+    ff->nl_issue = value > 0 ? 0u : 1u;
   } else if (param == HB_LAUNCH_PAIR_QUOTA) {
     HB_REQUIRE(value >= 0 && value <= 4096, HB_ERR_INVALID_ARGUMENT, "pair work quota in 0..4096");
     ff->pair_quota = value;
@@ -1040,8 +1068,10 @@ extern "C" int hb_integrator_destroy(hb_integrator *it) {
 // forces, velocity projection, final half kick.  Langevin (middle scheme):
 // full kick, velocity projection, half drift, O, half drift, position
 // constraint, forces.
-static int one_step(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons, bool ev,
-                    bool capturing = false) {
+// One MD step = step_head (kicks, drift, constraint positions), a force
+// evaluation with energies when step_force_ev says so, and step_tail (the
+// velocity-Verlet final kick with its constraint and coupling parts).
+static int step_head(hb_integrator *it, hb_constraints *cons) {
   cudaStream_t s = it->sys->ctx->stream;
   cudaEvent_t t4 = stage_begin(s);
   if (it->kind == HB_INTEGRATOR_LANGEVIN) {
@@ -1049,14 +1079,22 @@ static int one_step(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons, 
     if (cons) HB_TRY(cons_velocities(cons, 0.0, false, s));
     HB_TRY(integ_lang_drift_ou(it, s));
     if (cons) HB_TRY(cons_positions(cons, it->dt, s));
-    stage_end(4, t4, s);
-    HB_TRY(force_eval(ff, ev, capturing));
   } else {
     HB_TRY(integ_vv_kick_drift(it, s));
     if (cons) HB_TRY(cons_positions(cons, it->dt, s));
-    stage_end(4, t4, s);
-    // per-step pressure coupling reads the virial of every step
-    HB_TRY(force_eval(ff, ev || it->pc != nullptr, capturing));
+  }
+  stage_end(4, t4, s);
+  return HB_OK;
+}
+
+// per-step pressure coupling reads the virial of every step
+static bool step_force_ev(const hb_integrator *it, bool ev) {
+  return it->kind == HB_INTEGRATOR_LANGEVIN ? ev : (ev || it->pc != nullptr);
+}
+
+static int step_tail(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons) {
+  cudaStream_t s = it->sys->ctx->stream;
+  if (it->kind != HB_INTEGRATOR_LANGEVIN) {
     cudaEvent_t t5 = stage_begin(s);
     if (cons) HB_TRY(cons_velocities(cons, it->dt, true, s));
     if (it->thermo || it->pc) {
@@ -1069,6 +1107,13 @@ static int one_step(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons, 
   }
   it->step++;
   return HB_OK;
+}
+
+static int one_step(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons, bool ev,
+                    bool capturing = false) {
+  HB_TRY(step_head(it, cons));
+  HB_TRY(force_eval(ff, step_force_ev(it, ev), capturing));
+  return step_tail(it, ff, cons);
 }
 
 // Barostat::apply_move on the device: propose + scale, a forces + scalars
@@ -1401,9 +1446,17 @@ struct hb_batch {
   std::vector<hb_forcefield *> ffs;
   std::vector<hb_constraints *> cons;
   std::vector<cudaEvent_t> join;             // one per member
+  std::vector<cudaEvent_t> ready;            // a member's step up to its pair kernel
   std::vector<uint64_t> gens;                // members' layout_gen at capture
-  cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
+  cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr, pair_done = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // one multi-system pair launch for all members (when they share the pair
+  // physics and contexts are distinct); 0 = one pair launch per member
+  int one_pair_launch = 1;
+  bool multi = false;                        // the form of the captured graph
+  void *d_members = nullptr;                 // member table of the multi-system launch
+  uint32_t *d_work = nullptr;                // its work counter
+  uint32_t items = 0;
 };
 
 extern "C" int hb_batch_destroy(hb_batch *b) {
@@ -1413,9 +1466,14 @@ extern "C" int hb_batch_destroy(hb_batch *b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   for (auto e : b->join)
     if (e) cudaEventDestroy(e);
+  for (auto e : b->ready)
+    if (e) cudaEventDestroy(e);
   if (b->fork) cudaEventDestroy(b->fork);
   if (b->t0) cudaEventDestroy(b->t0);
   if (b->t1) cudaEventDestroy(b->t1);
+  if (b->pair_done) cudaEventDestroy(b->pair_done);
+  cudaFree(b->d_members);
+  cudaFree(b->d_work);
   delete b;
   return HB_OK;
 }
@@ -1446,11 +1504,16 @@ extern "C" int hb_batch_create(hb_context *ctx, uint32_t n, hb_integrator *const
   if (cons)
     for (uint32_t k = 0; k < n; ++k) b->cons[k] = cons[k];
   b->join.assign(n, nullptr);
+  b->ready.assign(n, nullptr);
   bool ok = cudaSetDevice(ctx->device) == cudaSuccess &&
             cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess &&
-            cudaEventCreate(&b->t0) == cudaSuccess && cudaEventCreate(&b->t1) == cudaSuccess;
+            cudaEventCreateWithFlags(&b->pair_done, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreate(&b->t0) == cudaSuccess && cudaEventCreate(&b->t1) == cudaSuccess &&
+            cudaMalloc(&b->d_members, pair_member_bytes() * n) == cudaSuccess &&
+            cudaMalloc(&b->d_work, sizeof(uint32_t)) == cudaSuccess;
   for (uint32_t k = 0; ok && k < n; ++k)
-    ok = cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming) == cudaSuccess;
+    ok = cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&b->ready[k], cudaEventDisableTiming) == cudaSuccess;
   if (!ok) {
     hb_batch_destroy(b);
     return hb_fail(HB_ERR_CUDA, "batch event creation failed");
@@ -1459,15 +1522,36 @@ extern "C" int hb_batch_create(hb_context *ctx, uint32_t n, hb_integrator *const
   return HB_OK;
 }
 
-// one graph: fork from the batch stream to every member's stream, capture
-// the member's step there, join back
+// whether the members' pair kernels can run as one multi-system launch:
+// the same pair physics, force-only steps (no per-step pressure coupling),
+// and a context (streams, events) of their own each
+static bool batch_multi_ok(const hb_batch *b) {
+  if (!b->one_pair_launch) return false;
+  const size_t n = b->its.size();
+  for (size_t k = 0; k < n; ++k) {
+    if (step_force_ev(b->its[k], false)) return false;
+    for (size_t q = 0; q < k; ++q)
+      if (b->its[q]->sys->ctx == b->its[k]->sys->ctx) return false;
+  }
+  return pair_batchable(b->ffs.data(), (uint32_t)n);
+}
+
+// one graph: fork from the batch stream to every member's stream and
+// capture the member's step there, join back.  In the multi-system form
+// each member runs up to its pair kernel, the batch stream waits for all
+// of them and launches one pair kernel over every member's work items, and
+// each member then finishes its step (reciprocal-space join, finalize,
+// final kick) after that launch.
 static int batch_capture(hb_batch *b) {
+  const size_t n = b->its.size();
+  b->multi = batch_multi_ok(b);
+  if (b->multi) HB_TRY(pair_batch_table(b->ffs.data(), (uint32_t)n, b->d_members, &b->items));
   cudaStream_t m = b->ctx->stream;
   cudaGraph_t g;
   HB_CUDA(cudaStreamBeginCapture(m, cudaStreamCaptureModeThreadLocal));
   int rc = cudaEventRecord(b->fork, m) == cudaSuccess ? HB_OK : HB_ERR_CUDA;
-  std::vector<uint64_t> steps(b->its.size());
-  for (size_t k = 0; k < b->its.size() && rc == HB_OK; ++k) {
+  std::vector<uint64_t> steps(n);
+  for (size_t k = 0; k < n && rc == HB_OK; ++k) {
     hb_integrator *it = b->its[k];
     cudaStream_t s = it->sys->ctx->stream;
     if (cudaStreamWaitEvent(s, b->fork, 0) != cudaSuccess) {
@@ -1475,11 +1559,38 @@ static int batch_capture(hb_batch *b) {
       break;
     }
     steps[k] = it->step;
-    rc = one_step(it, b->ffs[k], b->cons[k], false, true);
-    it->step = steps[k];
-    if (rc == HB_OK && (cudaEventRecord(b->join[k], s) != cudaSuccess ||
-                        cudaStreamWaitEvent(m, b->join[k], 0) != cudaSuccess))
+    if (!b->multi) {
+      rc = one_step(it, b->ffs[k], b->cons[k], false, true);
+      it->step = steps[k];
+      if (rc == HB_OK && (cudaEventRecord(b->join[k], s) != cudaSuccess ||
+                          cudaStreamWaitEvent(m, b->join[k], 0) != cudaSuccess))
+        rc = hb_fail(HB_ERR_CUDA, "batch join");
+      continue;
+    }
+    rc = step_head(it, b->cons[k]);
+    if (rc == HB_OK) rc = force_pre(b->ffs[k], false, true);
+    if (rc == HB_OK && (cudaEventRecord(b->ready[k], s) != cudaSuccess ||
+                        cudaStreamWaitEvent(m, b->ready[k], 0) != cudaSuccess))
       rc = hb_fail(HB_ERR_CUDA, "batch join");
+  }
+  if (b->multi && rc == HB_OK) {
+    rc = pair_launch_batch(b->ffs.data(), (uint32_t)n, b->d_members, b->items, b->d_work, m);
+    if (rc == HB_OK && cudaEventRecord(b->pair_done, m) != cudaSuccess)
+      rc = hb_fail(HB_ERR_CUDA, "batch pair launch");
+    for (size_t k = 0; k < n && rc == HB_OK; ++k) {
+      hb_integrator *it = b->its[k];
+      cudaStream_t s = it->sys->ctx->stream;
+      if (cudaStreamWaitEvent(s, b->pair_done, 0) != cudaSuccess) {
+        rc = hb_fail(HB_ERR_CUDA, "batch fork");
+        break;
+      }
+      rc = force_post(b->ffs[k], false);
+      if (rc == HB_OK) rc = step_tail(it, b->ffs[k], b->cons[k]);
+      it->step = steps[k];
+      if (rc == HB_OK && (cudaEventRecord(b->join[k], s) != cudaSuccess ||
+                          cudaStreamWaitEvent(m, b->join[k], 0) != cudaSuccess))
+        rc = hb_fail(HB_ERR_CUDA, "batch join");
+    }
   }
   cudaError_t ce = cudaStreamEndCapture(m, &g);
   if (rc != HB_OK) return rc;
@@ -1487,6 +1598,23 @@ static int batch_capture(hb_batch *b) {
   cudaError_t ie = cudaGraphInstantiate(&b->exec, g, 0);
   cudaGraphDestroy(g);
   if (ie != cudaSuccess) return hb_fail(HB_ERR_CUDA, std::string("batch instantiate: ") + cudaGetErrorString(ie));
+  return HB_OK;
+}
+
+extern "C" int hb_batch_set_pair_form(hb_batch *b, int one_launch) {
+  HB_REQUIRE(b, HB_ERR_INVALID_ARGUMENT, "null batch");
+  b->one_pair_launch = one_launch ? 1 : 0;
+  if (b->exec) {
+    cudaStreamSynchronize(b->ctx->stream);
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  return HB_OK;
+}
+
+extern "C" int hb_batch_pair_form(hb_batch *b, int *one_launch) {
+  HB_REQUIRE(b && one_launch, HB_ERR_INVALID_ARGUMENT, "null argument");
+  *one_launch = batch_multi_ok(b) ? 1 : 0;
   return HB_OK;
 }
 
@@ -1544,6 +1672,8 @@ extern "C" int hb_batch_count_launches(hb_batch *b, uint64_t kernels[2]) {
     kernels[0] += c[0];
     kernels[1] += c[1];
   }
+  // the multi-system form: one pair kernel for all members
+  if (batch_multi_ok(b)) kernels[0] -= (uint64_t)(b->its.size() - 1);
   return HB_OK;
 }
 

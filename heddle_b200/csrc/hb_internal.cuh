@@ -58,6 +58,7 @@ int hb_fail(int code, const std::string &msg);
 #define HB_ST_DISPLACED 1u        /* an atom moved more than r_skin / 2 */
 #define HB_ST_ENTRY_OVERFLOW 8u   /* entry capacity exceeded on a rebuild */
 #define HB_ST_ENTRY_HIGHWATER 2u  /* entry count above 3/4 of capacity */
+#define HB_ST_DEVICE_TIMEOUT 16u  /* a bounded wait of the tile build ran out */
 
 // ---------------------------------------------------------------------
 // device box: lattice plus reciprocal helpers, kept in device memory so a
@@ -302,6 +303,8 @@ struct hb_forcefield {
   int pair_blocks_per_sm = 8;        // persistent pair kernel residency (tunable)
   int pair_chunk = 4;                // packed entries per pair work item (tunable)
   int pair_quota = 0;                // work items per pair warp (0: persistent; tunable)
+  uint32_t nl_polls = 1u << 20;      // poll limit of the tile build's bounded waits
+  uint32_t nl_issue = 1;             // 0 (test only): issue no bulk copies, so the waits run out
   uint32_t *d_work = nullptr;        // work counter of the balanced pair kernel
                                      // (zeroed by the combine kernel)
   uint64_t rebuilds_host = 0;
@@ -498,6 +501,12 @@ int pair_launch(hb_forcefield *ff, bool ev, cudaStream_t s);
 int spme_setup(hb_forcefield *ff, const hb_forcefield_desc *d);
 int spme_free(hb_forcefield *ff);
 int spme_launch(hb_forcefield *ff, bool ev, cudaStream_t s);
+// multi-system pair launch of replica batches (hb_pair.cu)
+size_t pair_member_bytes();
+bool pair_batchable(hb_forcefield *const *ffs, uint32_t n);
+int pair_batch_table(hb_forcefield *const *ffs, uint32_t n, void *d_table, uint32_t *items_total);
+int pair_launch_batch(hb_forcefield *const *ffs, uint32_t n, const void *d_table,
+                      uint32_t items_total, uint32_t *d_work, cudaStream_t s);
 // HB_LAUNCH_FFT_PLANE / HB_LAUNCH_GATHER_FORM (hb_forcefield_set_launch)
 int spme_set_form(hb_forcefield *ff, int param, int value);
 // combine (hb_integ.cu): fixed-point + reciprocal -> force (atom order)

@@ -37,6 +37,43 @@ __device__ __forceinline__ bool gate_off(const uint32_t *gate) {
   return gate != nullptr && ((*(volatile const uint32_t *)gate) & HB_ST_DISPLACED) == 0u;
 }
 
+// ---- bulk-copy staging of candidate tiles (cp.async.bulk, TMA engine) ----
+__device__ __forceinline__ uint32_t nl_smem(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void nl_mbar_init(uint64_t *m) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(nl_smem(m)) : "memory");
+}
+
+// one 16-byte-aligned tile of 32 float4 (512 B) from global memory into
+// shared memory; completion (bytes) is signalled on the mbarrier
+__device__ __forceinline__ void nl_bulk_tile(void *dst, const void *src, uint64_t *m, bool issue) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], 512;" ::"r"(nl_smem(m)) : "memory");
+  if (issue)
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], 512, [%2];" ::"r"(
+            nl_smem(dst)),
+        "l"(src), "r"(nl_smem(m))
+        : "memory");
+}
+
+// bounded wait for phase `ph` of the mbarrier: false when `polls` tries
+// (each may suspend briefly) run out
+__device__ __forceinline__ bool nl_mbar_wait(uint64_t *m, uint32_t ph, uint32_t polls) {
+  for (uint32_t i = 0; i < polls; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(nl_smem(m)), "r"(ph)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 // Index of voxel (x, y, z) along the 3-D Hilbert curve of order `bits`,
 // by J. Skilling's transpose method ("Programming the Hilbert curve", AIP
 // Conf. Proc. 707, 2004): undo the excess rotations level by level, Gray
@@ -332,7 +369,8 @@ __global__ void __launch_bounds__(NLT_WARPS * 32, 4)
               uint32_t slab, uint32_t *__restrict__ entry_j, uint32_t *__restrict__ entry_excl,
               uint32_t *__restrict__ status, uint32_t *__restrict__ counters,
               const uint32_t *__restrict__ sorted_ids, const uint32_t *__restrict__ inv_perm,
-              const uint32_t *__restrict__ eoff, const uint32_t *__restrict__ epart) {
+              const uint32_t *__restrict__ eoff, const uint32_t *__restrict__ epart,
+              uint32_t polls, uint32_t issue) {
   if (gate_off(gate)) return;
   extern __shared__ uint32_t sm_nl[];
   uint32_t *cand = sm_nl;             // [maxc] candidate j-tiles
@@ -341,6 +379,10 @@ __global__ void __launch_bounds__(NLT_WARPS * 32, 4)
   __shared__ uint32_t s_cnt[NLT_WARPS];
   __shared__ uint32_t s_ncand;
   __shared__ float4 s_jsh[NLT_WARPS][32], s_jor[NLT_WARPS][32];  // a candidate's j-atoms: shifted, as stored
+  // per warp, two candidate tiles in flight: bulk copies (TMA engine) fill
+  // one buffer while the warp refines the other
+  __shared__ __align__(128) float4 s_jt[NLT_WARPS][2][32];
+  __shared__ __align__(8) uint64_t s_mbar[NLT_WARPS][2];
   const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t I = blockIdx.x;
   const DBox b = *box;
@@ -421,10 +463,38 @@ __global__ void __launch_bounds__(NLT_WARPS * 32, 4)
         sh[q][d] = h >= l ? 0.5f * (h - l) : -1.0f;  // empty sub-tile: never near
       }
   }
-  for (uint32_t c = w; c < ncand; c += NLT_WARPS) {
+  // candidate tiles are staged by bulk copies one candidate ahead; a wait
+  // that runs out sets HB_ST_DEVICE_TIMEOUT (the host returns
+  // HB_ERR_DEVICE_TIMEOUT), drains the copies still in flight and stops
+  if (lane == 0) {
+    nl_mbar_init(&s_mbar[w][0]);
+    nl_mbar_init(&s_mbar[w][1]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (w < ncand) nl_bulk_tile(s_jt[w][0], tile_posq + (size_t)cand[w] * 32u, &s_mbar[w][0], issue != 0);
+  }
+  __syncwarp();
+  uint32_t ph0 = 0u, ph1 = 0u, k_it = 0u;
+  bool timed_out = false;
+  for (uint32_t c = w; c < ncand; c += NLT_WARPS, ++k_it) {
+    const uint32_t buf = k_it & 1u;
+    const uint32_t cn = c + NLT_WARPS;
+    if (lane == 0 && cn < ncand) {
+      // the other buffer was last read in the previous candidate (all lanes
+      // passed the __syncwarp at its end): order those reads before the
+      // async-proxy write
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      nl_bulk_tile(s_jt[w][buf ^ 1u], tile_posq + (size_t)cand[cn] * 32u, &s_mbar[w][buf ^ 1u], issue != 0);
+    }
+    const bool ok = nl_mbar_wait(&s_mbar[w][buf], buf ? ph1 : ph0, polls);
+    if (!__all_sync(0xFFFFFFFFu, ok)) {
+      timed_out = true;
+      break;
+    }
+    if (buf) ph1 ^= 1u;
+    else ph0 ^= 1u;
     const uint32_t kj = cand[c] * 32u + lane;
     const bool jvalid = kj < n;
-    const float4 pj = tile_posq[kj];
+    const float4 pj = s_jt[w][buf][lane];
     float sx = pj.x, sy = pj.y, sz = pj.z;
     if (shift_ok) {
       sx -= b.lx * rintf((sx - ci.x) * b.ilx);
@@ -451,13 +521,12 @@ __global__ void __launch_bounds__(NLT_WARPS * 32, 4)
       s_jsh[w][lane] = make_float4(sx, sy, sz, 0.0f);
       s_jor[w][lane] = pj;
       __syncwarp();
+      // two near j-atoms per step in the packed FP32x2 pipe (plain
+      // distances only decide far from the band, so their rounding is free)
       uint32_t hm = 0u;
-      while (rem != 0u) {
-        const uint32_t jl = (uint32_t)__ffs(rem) - 1u;
-        rem &= rem - 1u;
-        const float4 q = s_jsh[w][jl];
-        const float dx = pim.x - q.x, dy = pim.y - q.y, dz = pim.z - q.z;
-        const float r2 = dx * dx + dy * dy + dz * dz;
+      const float2 px2 = make_float2(pim.x, pim.x), py2 = make_float2(pim.y, pim.y),
+                   pz2 = make_float2(pim.z, pim.z);
+      auto vote = [&](uint32_t jl, float r2) {
         bool hit = __any_sync(0xFFFFFFFFu, r2 < band_lo);
         const bool inb = r2 >= band_lo && r2 <= band_hi;
         if (!hit && __any_sync(0xFFFFFFFFu, inb)) {
@@ -466,6 +535,22 @@ __global__ void __launch_bounds__(NLT_WARPS * 32, 4)
           hit = __any_sync(0xFFFFFFFFu, ex);
         }
         if (hit) hm |= 1u << jl;
+      };
+      while (rem != 0u) {
+        const uint32_t ja = (uint32_t)__ffs(rem) - 1u;
+        rem &= rem - 1u;
+        const bool two = rem != 0u;
+        const uint32_t jb = two ? (uint32_t)__ffs(rem) - 1u : ja;
+        rem &= rem - 1u;
+        const float4 qa = s_jsh[w][ja], qb = s_jsh[w][jb];
+        const float2 dx = __fadd2_rn(px2, make_float2(-qa.x, -qb.x));
+        const float2 dy = __fadd2_rn(py2, make_float2(-qa.y, -qb.y));
+        const float2 dz = __fadd2_rn(pz2, make_float2(-qa.z, -qb.z));
+        float2 r2 = __fmul2_rn(dx, dx);
+        r2 = __ffma2_rn(dy, dy, r2);
+        r2 = __ffma2_rn(dz, dz, r2);
+        vote(ja, r2.x);
+        if (two) vote(jb, r2.y);
       }
       __syncwarp();
       if (lane == 0) hmask[c] = hm;
@@ -500,8 +585,19 @@ __global__ void __launch_bounds__(NLT_WARPS * 32, 4)
     }
     const uint32_t hm = __ballot_sync(0xFFFFFFFFu, hit);
     if (lane == 0) hmask[c] = hm;
+    __syncwarp();
+  }
+  if (timed_out) {
+    // the copies still in flight land before the block's shared memory is
+    // released: one more bounded wait on each buffer's pending phase
+    if (lane == 0) {
+      atomicOr(status, HB_ST_DEVICE_TIMEOUT);
+      nl_mbar_wait(&s_mbar[w][0], ph0, polls);
+      nl_mbar_wait(&s_mbar[w][1], ph1, polls);
+    }
   }
   __syncthreads();
+  if (__syncthreads_or(timed_out ? 1 : 0)) return;
 
   // 3. exclusive prefix of the hit counts (one warp)
   if (w == 0) {
@@ -735,13 +831,14 @@ static int nl_launch(hb_forcefield *ff, const uint32_t *gate, cudaStream_t s, bo
     k_nl_tile<false><<<ff->n_tiles, NLT_WARPS * 32, smem, s>>>(
         gate, ff->d_tile_posq, ff->d_tile_center, ff->d_tile_half, sys->d_box, rs2, rb, band_lo,
         band_hi, n, ff->n_tiles, ff->maxc, ff->d_tile_nent, 0u, nullptr, nullptr, ff->d_status,
-        ff->d_counters, ff->d_sorted_ids, ff->d_inv_perm, ff->d_excl_off, ff->d_excl_partner);
+        ff->d_counters, ff->d_sorted_ids, ff->d_inv_perm, ff->d_excl_off, ff->d_excl_partner,
+        ff->nl_polls, ff->nl_issue);
   } else {
     k_nl_tile<true><<<ff->n_tiles, NLT_WARPS * 32, smem, s>>>(
         gate, ff->d_tile_posq, ff->d_tile_center, ff->d_tile_half, sys->d_box, rs2, rb, band_lo,
         band_hi, n, ff->n_tiles, ff->maxc, ff->d_tile_nent, ff->slab, ff->d_entry_j,
         ff->d_entry_excl, ff->d_status, ff->d_counters, ff->d_sorted_ids, ff->d_inv_perm,
-        ff->d_excl_off, ff->d_excl_partner);
+        ff->d_excl_off, ff->d_excl_partner, ff->nl_polls, ff->nl_issue);
     k_nl_finish<<<1, 1, 0, s>>>(gate, ff->d_status, ff->d_counters, sys->d_box, ff->d_ref_box);
   }
   HB_CUDA(cudaGetLastError());

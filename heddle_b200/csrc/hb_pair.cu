@@ -23,7 +23,9 @@
 // to int64 fixed point and takes each pair's own minimum image, so forces
 // are functions of the positions alone (the lossless integrator needs that).
 #include <algorithm>
+#include <cstring>
 #include <type_traits>
+#include <vector>
 
 #include "hb_internal.cuh"
 
@@ -38,6 +40,20 @@ struct PairParams {
   float c2a;  // 2 alpha / sqrt(pi)
   uint32_t n, n_tiles;
   uint32_t slab;
+};
+
+// one system of the multi-system pair launch: its lists, positions,
+// accumulators and cell, and its first work item in the launch's item space
+struct PairMember {
+  const float4 *tile_posq;
+  const int *tile_type;
+  const float4 *center;
+  const uint32_t *tile_nent;
+  const uint32_t *entry_j;
+  const uint32_t *entry_excl;
+  const DBox *box;
+  unsigned long long *fp;
+  uint32_t n, n_tiles, slab, chunks, item0, pad[3];
 };
 
 __device__ __forceinline__ void shift_to(float &x, float &y, float &z, const float4 &c,
@@ -101,17 +117,20 @@ struct P4Warp {
   uint16_t pairs[1024];
 };
 
-template <bool EV, bool SCALED, bool SWITCH>
-__global__ void __launch_bounds__(P4_WARPS * 32, 8)
-    k_pair4(const float4 *__restrict__ tile_posq, const int *__restrict__ tile_type,
-            const float4 *__restrict__ center, const uint32_t *__restrict__ tile_nent,
-            const uint32_t *__restrict__ entry_j, const uint32_t *__restrict__ entry_excl,
-            const DBox *__restrict__ box, const float4 *__restrict__ lj_table,
-            const float *__restrict__ lj_invd, PairParams P, unsigned long long *__restrict__ fp,
+template <bool EV, bool SCALED, bool SWITCH, bool MULTI>
+__global__ void __launch_bounds__(P4_WARPS * 32, MULTI ? 6 : 8)
+    k_pair4(const float4 *__restrict__ a_tile_posq, const int *__restrict__ a_tile_type,
+            const float4 *__restrict__ a_center, const uint32_t *__restrict__ a_tile_nent,
+            const uint32_t *__restrict__ a_entry_j, const uint32_t *__restrict__ a_entry_excl,
+            const DBox *__restrict__ a_box, const float4 *__restrict__ lj_table,
+            const float *__restrict__ lj_invd, PairParams a_P, unsigned long long *__restrict__ a_fp,
             const uint32_t *__restrict__ sorted_ids, const uint32_t *__restrict__ eoff,
             const uint32_t *__restrict__ epart, const float2 *__restrict__ escale,
-            uint32_t *__restrict__ work, uint32_t chunks, uint32_t chunk, uint32_t quota,
-            unsigned long long *__restrict__ e_lj_total) {
+            uint32_t *__restrict__ work, uint32_t a_chunks, uint32_t chunk, uint32_t quota,
+            unsigned long long *__restrict__ e_lj_total, const PairMember *__restrict__ members,
+            uint32_t n_members, uint32_t n_items_all) {
+  static_assert(!(MULTI && (EV || SCALED)), "the multi-system form is force-only, unscaled");
+  const PairParams &P0 = a_P;
   extern __shared__ float4 sm_lj4[];
   __shared__ P4Warp smw4[P4_WARPS];
   __shared__ uint32_t sm_ljtypes[32];  // per i-type: j-types with a Lennard-Jones term
@@ -120,17 +139,17 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
   // [96, 128); a half above 0.25 hartree takes the int64 path, so the int32
   // sums cannot wrap (32 pairs x 0.25 x 2^28 < 2^31)
   __shared__ int sm_ev[EV ? P4_WARPS * 128 : 1];
-  const int nt2 = P.n_types * P.n_types;
+  const int nt2 = P0.n_types * P0.n_types;
   float *sm_ljd4 = reinterpret_cast<float *>(sm_lj4 + nt2);
   for (int k = threadIdx.x; k < nt2; k += blockDim.x) {
     sm_lj4[k] = lj_table[k];
     sm_ljd4[k] = lj_invd[k];
   }
-  const bool few_types = P.n_types <= 32;
-  if (few_types && (int)threadIdx.x < P.n_types) {
+  const bool few_types = P0.n_types <= 32;
+  if (few_types && (int)threadIdx.x < P0.n_types) {
     uint32_t bits = 0u;
-    for (int q = 0; q < P.n_types; ++q)
-      if (lj_table[threadIdx.x * P.n_types + q].y != 0.0f) bits |= 1u << q;
+    for (int q = 0; q < P0.n_types; ++q)
+      if (lj_table[threadIdx.x * P0.n_types + q].y != 0.0f) bits |= 1u << q;
     sm_ljtypes[threadIdx.x] = bits;
   }
   __syncthreads();
@@ -138,9 +157,8 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
   P4Warp &S = smw4[w];
   int *Ev = sm_ev + (EV ? w * 128u : 0u);
   long long elj_fix = 0;  // LJ energy of this lane's pairs (fixed point)
-  const DBox b = *box;
-  const size_t np_all = (size_t)P.n_tiles * 32u;
-  const uint32_t n_items = P.n_tiles * chunks;
+  const DBox b0 = *a_box;
+  const uint32_t n_items = MULTI ? n_items_all : a_P.n_tiles * a_chunks;
 
   // warps take (tile, chunk of entries) items from a counter, at most
   // `quota` each: a finite quota retires blocks as they finish, so the
@@ -151,6 +169,41 @@ __global__ void __launch_bounds__(P4_WARPS * 32, 8)
     if (lane == 0) g = atomicAdd(work, 1u);
     g = __shfl_sync(0xFFFFFFFFu, g, 0);
     if (g >= n_items) break;
+    // the system this item belongs to: the kernel's own arguments, or (the
+    // multi-system form) the member whose item range holds g
+    const float4 *__restrict__ tile_posq = a_tile_posq;
+    const int *__restrict__ tile_type = a_tile_type;
+    const float4 *__restrict__ center = a_center;
+    const uint32_t *__restrict__ tile_nent = a_tile_nent;
+    const uint32_t *__restrict__ entry_j = a_entry_j;
+    const uint32_t *__restrict__ entry_excl = a_entry_excl;
+    unsigned long long *__restrict__ fp = a_fp;
+    PairParams P = a_P;
+    uint32_t chunks = a_chunks;
+    DBox b = b0;
+    if constexpr (MULTI) {
+      uint32_t lo = 0u, hi = n_members;  // largest m with members[m].item0 <= g
+      while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (members[mid].item0 <= g) lo = mid;
+        else hi = mid;
+      }
+      const PairMember &M = members[lo];
+      g -= M.item0;
+      tile_posq = M.tile_posq;
+      tile_type = M.tile_type;
+      center = M.center;
+      tile_nent = M.tile_nent;
+      entry_j = M.entry_j;
+      entry_excl = M.entry_excl;
+      fp = M.fp;
+      P.n = M.n;
+      P.n_tiles = M.n_tiles;
+      P.slab = M.slab;
+      chunks = M.chunks;
+      b = *M.box;
+    }
+    const size_t np_all = (size_t)P.n_tiles * 32u;
     const uint32_t I = g / chunks, ch = g - I * chunks;
     const uint32_t tile_e0 = I * P.slab;
     const uint32_t tile_e1 = tile_e0 + min(tile_nent[I], P.slab);
@@ -627,11 +680,11 @@ int launch4_t(hb_forcefield *ff, cudaStream_t s, const PairParams &P) {
     grid = std::min<uint32_t>((uint32_t)ff->sys->ctx->n_sm * (uint32_t)ff->pair_blocks_per_sm,
                               hb_div_up(items, P4_WARPS));
   }
-  k_pair4<EV, SCALED, SWITCH><<<std::max(grid, 1u), P4_WARPS * 32, smem, s>>>(
+  k_pair4<EV, SCALED, SWITCH, false><<<std::max(grid, 1u), P4_WARPS * 32, smem, s>>>(
       ff->d_tile_posq, ff->d_tile_type, ff->d_tile_center, ff->d_tile_nent, ff->d_entry_j,
       ff->d_entry_excl, ff->sys->d_box, ff->d_lj, ff->d_lj_invd, P, ff->d_fp, ff->d_sorted_ids,
       ff->d_excl_off, ff->d_excl_partner, ff->d_excl_scale, ff->d_work, chunks, chunk, quota,
-      ff->d_acc);
+      ff->d_acc, nullptr, 0u, 0u);
   HB_CUDA(cudaGetLastError());
   return HB_OK;
 }
@@ -902,4 +955,91 @@ int pair_launch(hb_forcefield *ff, bool ev, cudaStream_t s) {
   }
   if (sc) return sw ? launch4_t<false, true, true>(ff, s, P) : launch4_t<false, true, false>(ff, s, P);
   return sw ? launch4_t<false, false, true>(ff, s, P) : launch4_t<false, false, false>(ff, s, P);
+}
+
+// ---------------------------------------------------------------------
+// Multi-system pair launch (replica batches): one persistent k_pair4 over
+// the work items of every member, each item finding its member by a binary
+// search of the members' first items.  Members must share the pair physics
+// (types, tables, cut-offs, Ewald alpha, switch) and take the force-only,
+// unscaled, tile-shifted form; their own lists, positions, cells and
+// accumulators stay where they are.
+// ---------------------------------------------------------------------
+size_t pair_member_bytes() { return sizeof(PairMember); }
+
+bool pair_batchable(hb_forcefield *const *ffs, uint32_t n) {
+  if (n == 0) return false;
+  const hb_forcefield *a = ffs[0];
+  for (uint32_t k = 0; k < n; ++k) {
+    const hb_forcefield *f = ffs[k];
+    if (f->exact_pairs || f->excl_scaled || f->n_tiles == 0 || f->sys->n < 2) return false;
+    if (f->lj_on != a->lj_on || f->coul_on != a->coul_on || f->any_switch != a->any_switch ||
+        f->n_types != a->n_types || f->rc_max != a->rc_max || f->coul_rc2 != a->coul_rc2 ||
+        f->alpha != a->alpha)
+      return false;
+    // the switch factors (lj_invd) follow from these tables
+    if (f->h_lj.size() != a->h_lj.size()) return false;
+    if (std::memcmp(f->h_lj.data(), a->h_lj.data(), sizeof(float4) * a->h_lj.size()) != 0) return false;
+  }
+  return a->lj_on || a->coul_on;
+}
+
+// the member table (host-built, copied synchronously: call outside capture)
+int pair_batch_table(hb_forcefield *const *ffs, uint32_t n, void *d_table, uint32_t *items_total) {
+  std::vector<PairMember> t(n);
+  uint32_t item0 = 0;
+  const uint32_t chunk = (uint32_t)ffs[0]->pair_chunk;
+  for (uint32_t k = 0; k < n; ++k) {
+    hb_forcefield *f = ffs[k];
+    PairMember &m = t[k];
+    std::memset(&m, 0, sizeof(m));
+    m.tile_posq = f->d_tile_posq;
+    m.tile_type = f->d_tile_type;
+    m.center = f->d_tile_center;
+    m.tile_nent = f->d_tile_nent;
+    m.entry_j = f->d_entry_j;
+    m.entry_excl = f->d_entry_excl;
+    m.box = f->sys->d_box;
+    m.fp = f->d_fp;
+    m.n = f->sys->n;
+    m.n_tiles = f->n_tiles;
+    m.slab = f->slab;
+    m.chunks = hb_div_up(f->slab, chunk);
+    m.item0 = item0;
+    item0 += m.n_tiles * m.chunks;
+  }
+  HB_CUDA(cudaMemcpy(d_table, t.data(), sizeof(PairMember) * n, cudaMemcpyHostToDevice));
+  *items_total = item0;
+  return HB_OK;
+}
+
+int pair_launch_batch(hb_forcefield *const *ffs, uint32_t n, const void *d_table,
+                      uint32_t items_total, uint32_t *d_work, cudaStream_t s) {
+  const hb_forcefield *a = ffs[0];
+  PairParams P;
+  std::memset(&P, 0, sizeof(P));
+  P.n_types = (int)a->n_types;
+  P.lj_on = a->lj_on;
+  P.coul_on = a->coul_on;
+  P.rc2_max = a->rc_max * a->rc_max;
+  P.coul_rc2 = a->coul_rc2;
+  P.alpha = a->alpha;
+  P.c2a = 2.0f * a->alpha / 1.7724538509055160273f;
+  size_t smem = (sizeof(float4) + sizeof(float)) * (size_t)P.n_types * P.n_types;
+  const uint32_t grid = std::min<uint32_t>(
+      (uint32_t)a->sys->ctx->n_sm * (uint32_t)a->pair_blocks_per_sm, hb_div_up(items_total, P4_WARPS));
+  HB_CUDA(cudaMemsetAsync(d_work, 0, sizeof(uint32_t), s));
+  const PairMember *tab = static_cast<const PairMember *>(d_table);
+  if (a->any_switch)
+    k_pair4<false, false, true, true><<<std::max(grid, 1u), P4_WARPS * 32, smem, s>>>(
+        nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, a->sys->d_box, a->d_lj, a->d_lj_invd, P,
+        nullptr, nullptr, nullptr, nullptr, nullptr, d_work, 1u, (uint32_t)a->pair_chunk, 0xFFFFFFFFu,
+        nullptr, tab, n, items_total);
+  else
+    k_pair4<false, false, false, true><<<std::max(grid, 1u), P4_WARPS * 32, smem, s>>>(
+        nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, a->sys->d_box, a->d_lj, a->d_lj_invd, P,
+        nullptr, nullptr, nullptr, nullptr, nullptr, d_work, 1u, (uint32_t)a->pair_chunk, 0xFFFFFFFFu,
+        nullptr, tab, n, items_total);
+  HB_CUDA(cudaGetLastError());
+  return HB_OK;
 }

@@ -75,11 +75,16 @@ enum {
   HB_LAUNCH_GATHER_FORM = 4,        /* spline orders 4 and 8: 1 (default) one
                                        thread per (atom, c offset); 0 one thread
                                        per atom */
-  HB_LAUNCH_PAIR_QUOTA = 5          /* work items per pair-kernel warp (0..4096):
+  HB_LAUNCH_PAIR_QUOTA = 5,         /* work items per pair-kernel warp (0..4096):
                                        0 (default) persistent blocks; q > 0
                                        blocks that retire after q items each, so
                                        the concurrent reciprocal-space kernels
                                        are scheduled between them */
+  HB_LAUNCH_NL_WAIT_TEST = 6        /* failure-path test of the tile build's
+                                       bounded waits: v > 0 issues no bulk
+                                       copies and gives up after v polls (the
+                                       next rebuild returns HB_ERR_DEVICE_TIMEOUT);
+                                       0 restores normal operation */
 };
 
 /* pair accumulation modes (hb_forcefield_desc.pair_mode) */
@@ -544,6 +549,19 @@ int hb_batch_step(hb_batch *b, uint32_t n_steps);
 /* kernels[0] = kernels of one batch step (all members), kernels[1] = sum
  * over members of the kernels of one neighbour rebuild. */
 int hb_batch_count_launches(hb_batch *b, uint64_t kernels[2]);
+/* Pair-kernel form of a batch step (no reference counterpart; the
+ * reference replays one graph per system, src/runner.rs:2803-3000).
+ * one_launch != 0 (the default): when the members share the pair physics
+ * (types, tables, cut-offs, alpha), take force-only steps and each have a
+ * context of their own, every member runs its step up to the pair kernel,
+ * one persistent pair kernel then covers the work items of all members
+ * (each item finds its member in a table), and each member finishes its
+ * step after it; otherwise, and with one_launch = 0, each member launches
+ * its own pair kernel.  Both forms give the same forces bit for bit
+ * (integer accumulation).  The next hb_batch_step recaptures. */
+int hb_batch_set_pair_form(hb_batch *b, int one_launch);
+/* *one_launch = 1 when the next step uses the one-launch form. */
+int hb_batch_pair_form(hb_batch *b, int *one_launch);
 
 /* ---- FP64 deterministic scalar reductions (kernels/nose_hoover.cu:22-103,
  * kernels/barostat.cu:11-78): kinetic energy and the mass-weighted

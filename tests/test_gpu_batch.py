@@ -1,7 +1,8 @@
 """Batched replicas (C ABI): every member's step captured into one CUDA graph
 must advance each member exactly as that member run alone would -- byte for
 byte, including device-side neighbour rebuild decisions -- for boxes of
-uneven sizes and both integrators."""
+uneven sizes and both integrators, with one multi-system pair kernel for
+all members and with a pair kernel per member."""
 
 import numpy as np
 import pytest
@@ -27,8 +28,9 @@ def close_all(objs):
         o.close()
 
 
+@pytest.mark.parametrize("one_launch", [True, False], ids=["one-pair-launch", "pair-per-member"])
 @pytest.mark.parametrize("kind", ["velocity-verlet", "langevin-baoab"])
-def test_batch_matches_members_run_alone(ctx, kind):
+def test_batch_matches_members_run_alone(ctx, kind, one_launch):
     specs = [S.spc_water(n, r_cut_A=7.0, skin_A=0.8, seed=20 + n) for n in (216, 300, 512, 343)]
     steps = 30
     # alone: each member's own graph steps
@@ -45,6 +47,10 @@ def test_batch_matches_members_run_alone(ctx, kind):
         members.append((it, ff, cons))
         objs.append((c, sys_, ff, cons, it))
     batch = hb.Batch(ctx, members)
+    batch.set_pair_form(one_launch)
+    # the members share the pair physics: one multi-system pair kernel
+    # replaces their pair launches when asked to
+    assert batch.pair_form() == one_launch
     top, body = batch.count_launches()
     assert top > 0 and body == 10 * len(specs)
     batch.step(steps)

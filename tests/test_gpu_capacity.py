@@ -97,3 +97,32 @@ def test_overflow_halts_with_nl_overflow_until_a_larger_slab(ctx, water):
     pairs, dups = ff.neighbor_pairs()
     assert dups == 0 and np.array_equal(pairs, oracle_pairs(spec, sys_))
     ff.close(), sys_.close()
+
+
+def test_tile_build_bounded_wait_times_out_and_the_next_rebuild_works(ctx, water):
+    """The tile build stages candidate tiles with bulk copies completing on
+    mbarriers; every wait is bounded.  With the test knob no copy is issued,
+    so the first wait runs out: the kernel flags it, drains its copies and
+    returns, the call reports HB_ERR_DEVICE_TIMEOUT, and once the knob is
+    cleared the next rebuild gives the exact list and forces again (no GPU
+    fault is involved)."""
+    from heddle_b200 import _native as N
+
+    spec = water
+    sys_ = hb.System.from_spec(ctx, spec)
+    ff = hb.ForceField.from_spec(sys_, spec)
+    ff.step(scalars=False)
+    F0 = sys_.forces()
+    N.check(ff.lib.hb_forcefield_set_launch(ff.h, N.HB_LAUNCH_NL_WAIT_TEST, 256))
+    with pytest.raises(hb.HeddleError) as e:
+        ff.pre_step(force=True)
+    assert e.value.name == "HB_ERR_DEVICE_TIMEOUT"
+    N.check(ff.lib.hb_forcefield_set_launch(ff.h, N.HB_LAUNCH_NL_WAIT_TEST, 0))
+    ff.pre_step(force=True)
+    pairs, dups = ff.neighbor_pairs()
+    assert dups == 0
+    assert np.array_equal(pairs, oracle_pairs(spec, sys_))
+    ff.step(scalars=False)
+    assert np.array_equal(sys_.forces(), F0)
+    ff.close()
+    sys_.close()
