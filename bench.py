@@ -50,7 +50,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--molecules", type=int, default=65536)
     p.add_argument("--skin", type=float, default=1.0, help="neighbour-list skin in angstrom")
-    p.add_argument("--e2e-steps", type=int, default=10)
+    p.add_argument("--e2e-steps", type=int, default=20)
     p.add_argument("--equilibrate", type=int, default=300,
                    help="untimed Langevin steps (friction 50/ps) that relax the lattice start")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -400,20 +400,28 @@ def run_ours(args):
     clocks = clk.summary()
 
     # end to end through the C ABI with page-locked host buffers: every step
-    # uploads positions and velocities and reads the whole state back
-    host = tuple(torch.empty((spec.n, 3), dtype=dt, pin_memory=True).numpy()
-                 for dt in (torch.float64, torch.float64, torch.int32, torch.float64))
-    sys_.state(out=host)
-    pos_h, vel_h = host[0], host[1]
+    # uploads positions and velocities and reads the whole state back, in
+    # single precision (the reference's own buffer precision) and, for
+    # comparison, in FP64
     k2 = max(1, min(args.e2e_steps, args.steps))
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(k2):
-        sys_.set_state(pos_h, vel_h)
+
+    def e2e(dtype):
+        host = tuple(torch.empty((spec.n, 3), dtype=dt, pin_memory=True).numpy()
+                     for dt in (dtype, dtype, torch.int32, dtype))
+        get = sys_.state_f32 if dtype == torch.float32 else (lambda out: sys_.state(out=out))
+        put = sys_.set_state_f32 if dtype == torch.float32 else sys_.set_state
+        get(host)
         run(ff, cons, n_steps=1)
-        sys_.state(out=host)
-    t_e2e = time.perf_counter() - t0
-    t_e2e = max_over_ranks(t_e2e, dist, f"cuda:{local}")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(k2):
+            put(host[0], host[1])
+            run(ff, cons, n_steps=1)
+            get(host)
+        return max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
+
+    t_e2e = e2e(torch.float32)
+    t_e2e64 = e2e(torch.float64)
     e2e_value = world * spec.n * k2 / t_e2e
 
     peak, peak_kind = measured_peaks()
@@ -459,11 +467,15 @@ def run_ours(args):
                               "achieved_gbs": step_bytes / (t_ms / args.steps * 1e-3) / 1e9,
                               "frac": step_bytes / (t_ms / args.steps * 1e-3) / 1e9 / peak},
             "clocks": clocks,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 3 * 8 * spec.n,
-                    "d2h_bytes_per_step": (3 * 3 * 8 + 3 * 4) * spec.n,
-                    "note": "per step, page-locked host buffers: positions + velocities (f64) "
-                            "in; positions, velocities, forces (f64) and images (i32) out; wall "
-                            "clock"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 3 * 4 * spec.n,
+                    "d2h_bytes_per_step": (3 * 3 * 4 + 3 * 4) * spec.n,
+                    "note": "per step, page-locked host buffers: positions + velocities (f32) "
+                            "in; positions, velocities, forces (f32) and images (i32) out; wall "
+                            "clock, over the C ABI (hb_system_set_state_f32 / hb_integrator step "
+                            "/ hb_system_get_state_f32)",
+                    "f64_exchange": {"value": world * spec.n * k2 / t_e2e64,
+                                     "h2d_bytes_per_step": 2 * 3 * 8 * spec.n,
+                                     "d2h_bytes_per_step": (3 * 3 * 8 + 3 * 4) * spec.n}},
             "gpu_launches": (per_step_kernels * args.steps + rebuild_kernels * rebuilds +
                              move_kernels * moves),
             "barostat": ({"moves_in_timed_steps": moves, "volume_A3": baro_stats["volume"] *
@@ -537,9 +549,9 @@ def run_batch(args):
     master.timing(False)
     rebuilds = sum(o[2].stats()["rebuilds"] for o in objs) - rebuilds0
     one_launch = batch.pair_form()
-    # the same batch with a pair kernel per member (graph branches), for
-    # comparison with the one multi-system pair launch (untimed headline)
-    batch.set_pair_form(False)
+    # the same batch with one multi-system pair launch for all members, for
+    # comparison with the default (a pair kernel per member)
+    batch.set_pair_form(True)
     batch.step(2)
     master.timing(True)
     t_per = 0.0
@@ -550,7 +562,7 @@ def run_batch(args):
         batch.step(1)
         t_per += float(master.timings()[0])
     master.timing(False)
-    batch.set_pair_form(True)
+    batch.set_pair_form(False)
     batch.step(1)
     # 64 sequential plain runs (each box's own CUDA-graph steps, one box
     # after another), wall clock
@@ -586,8 +598,10 @@ def run_batch(args):
                           "atom_steps_per_s_wall": n_atoms * k_seq / t_batch_wall,
                           "pair_form": ("one persistent pair kernel over all members' work items"
                                         if one_launch else "a pair kernel per member")},
-        "batched_graph_pair_per_member": {"atom_steps_per_s_device": n_atoms * k_per / (t_per * 1e-3),
-                                          "ms_per_step": t_per / k_per},
+        "batched_graph_one_pair_launch": {"atom_steps_per_s_device": n_atoms * k_per / (t_per * 1e-3),
+                                          "ms_per_step": t_per / k_per,
+                                          "pair_form": "one persistent pair kernel over all members' "
+                                                       "work items"},
         "sequential_plain": {"atom_steps_per_s_wall": n_atoms * k_seq / t_seq, "steps": k_seq},
         "speedup_wall": t_seq / t_batch_wall,
         "rebuilds_in_timed_steps": rebuilds,

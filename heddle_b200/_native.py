@@ -198,6 +198,8 @@ SIGNATURES = {
     "hb_system_destroy": (C.c_int, [VP]),
     "hb_system_set_state": (C.c_int, [VP, PD, PD]),
     "hb_system_get_state": (C.c_int, [VP, PD, PD, PI32, PD]),
+    "hb_system_set_state_f32": (C.c_int, [VP, PF32, PF32]),
+    "hb_system_get_state_f32": (C.c_int, [VP, PF32, PF32, PI32, PF32]),
     "hb_system_set_box": (C.c_int, [VP, PD]),
     "hb_system_get_box": (C.c_int, [VP, PD]),
     "hb_system_flip_velocities": (C.c_int, [VP]),

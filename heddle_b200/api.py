@@ -108,6 +108,25 @@ class System:
         N.check(self.lib.hb_system_get_state(self.h, N.dptr(pos), N.dptr(vel), N.i32ptr(img), N.dptr(frc)))
         return pos.reshape(-1, 3), vel.reshape(-1, 3), img.reshape(-1, 3), frc.reshape(-1, 3)
 
+    def state_f32(self, out):
+        """Download into four C-contiguous (n, 3) arrays (float32, float32,
+        int32, float32): the single-precision exchange, half the bytes of
+        state()."""
+        pos, vel, img, frc = out
+        for a, dt in ((pos, np.float32), (vel, np.float32), (img, np.int32), (frc, np.float32)):
+            if a.dtype != dt or not a.flags["C_CONTIGUOUS"] or a.size != 3 * self.n:
+                raise ValueError("state_f32(out=...): four C-contiguous (n, 3) arrays of the right types")
+        N.check(self.lib.hb_system_get_state_f32(self.h, N.f32ptr(pos), N.f32ptr(vel), N.i32ptr(img),
+                                                 N.f32ptr(frc)))
+        return out
+
+    def set_state_f32(self, positions=None, velocities=None) -> None:
+        """Upload C-contiguous float32 (n, 3) arrays (None = keep)."""
+        for a in (positions, velocities):
+            if a is not None and (a.dtype != np.float32 or not a.flags["C_CONTIGUOUS"] or a.size != 3 * self.n):
+                raise ValueError("set_state_f32: C-contiguous float32 (n, 3) arrays")
+        N.check(self.lib.hb_system_set_state_f32(self.h, N.f32ptr(positions), N.f32ptr(velocities)))
+
     def positions(self) -> np.ndarray:
         pos = np.zeros(3 * self.n)
         N.check(self.lib.hb_system_get_state(self.h, N.dptr(pos), None, None, None))
@@ -832,8 +851,8 @@ class Batch:
         N.check(self.lib.hb_batch_step(self.h, int(n_steps)))
 
     def set_pair_form(self, one_launch: bool) -> None:
-        """One multi-system pair kernel for all members (default, when they
-        share the pair physics) or one pair kernel per member."""
+        """One multi-system pair kernel for all members (when they share the
+        pair physics) or one pair kernel per member (default, faster)."""
         N.check(self.lib.hb_batch_set_pair_form(self.h, 1 if one_launch else 0))
 
     def pair_form(self) -> bool:

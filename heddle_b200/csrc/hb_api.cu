@@ -271,8 +271,8 @@ extern "C" int hb_system_destroy(hb_system *s) {
 // transfers and two small kernels.
 namespace {
 
-__global__ void k_state_check(const double *__restrict__ pos, uint32_t *__restrict__ bad,
-                              uint32_t n) {
+template <class T>
+__global__ void k_state_check(const T *__restrict__ pos, uint32_t *__restrict__ bad, uint32_t n) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   if (!isfinite(pos[3 * i]) || !isfinite(pos[3 * i + 1]) || !isfinite(pos[3 * i + 2]))
@@ -280,12 +280,17 @@ __global__ void k_state_check(const double *__restrict__ pos, uint32_t *__restri
 }
 
 // wrap into the primary cell in FP64, operation by operation as the host
-// upload does it (no contraction), keeping image counts continuous
-__global__ void k_state_in(const double *__restrict__ pos, const double *__restrict__ vel,
+// upload does it (no contraction), keeping image counts continuous.  With a
+// `bad` word (set by k_state_check earlier on the same stream) nothing is
+// written when some position is not finite, so the state is left as it was
+template <class T>
+__global__ void k_state_in(const T *__restrict__ pos, const T *__restrict__ vel,
                            const double *__restrict__ b, float4 *__restrict__ posq,
-                           float4 *__restrict__ v, int4 *__restrict__ image, uint32_t n) {
+                           float4 *__restrict__ v, int4 *__restrict__ image,
+                           const uint32_t *__restrict__ bad, uint32_t n) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (bad && *bad != 0xFFFFFFFFu) return;
   if (pos) {
     double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
     const double sc = __ddiv_rn(z, b[2]);
@@ -318,10 +323,11 @@ __global__ void k_state_in(const double *__restrict__ pos, const double *__restr
   }
 }
 
+template <class T>
 __global__ void k_state_out(const float4 *__restrict__ posq, const float4 *__restrict__ vel,
                             const float4 *__restrict__ force, const int4 *__restrict__ image,
-                            double *__restrict__ pos, double *__restrict__ velo,
-                            double *__restrict__ frc, int32_t *__restrict__ img, uint32_t n) {
+                            T *__restrict__ pos, T *__restrict__ velo, T *__restrict__ frc,
+                            int32_t *__restrict__ img, uint32_t n) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   if (pos) {
@@ -361,39 +367,46 @@ int stage_alloc(hb_system *sys) {
 
 }  // namespace
 
-extern "C" int hb_system_set_state(hb_system *sys, const double *positions,
-                                   const double *velocities) {
+namespace {
+
+// Upload: both host arrays and the finite check are queued before the one
+// synchronisation; the conversion writes nothing when a position is not
+// finite (checked on the device), so a rejected call leaves the state as it
+// was.  T is the host element type (double or float).
+template <class T>
+int set_state_t(hb_system *sys, const T *positions, const T *velocities) {
   HB_REQUIRE(sys, HB_ERR_INVALID_ARGUMENT, "null system");
   const uint32_t n = sys->n;
   if (!n || (!positions && !velocities)) return HB_OK;
   HB_TRY(stage_alloc(sys));
   cudaStream_t s = sys->ctx->stream;
-  double *dp = sys->d_stage, *dv = sys->d_stage + 3 * (size_t)n;
+  T *dp = reinterpret_cast<T *>(sys->d_stage), *dv = dp + 3 * (size_t)n;
   const unsigned g = hb_div_up(n, 256);
+  const uint32_t none = 0xFFFFFFFFu;
   if (positions) {
-    HB_CUDA(cudaMemcpyAsync(dp, positions, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
-    const uint32_t none = 0xFFFFFFFFu;
+    HB_CUDA(cudaMemcpyAsync(dp, positions, sizeof(T) * 3 * n, cudaMemcpyHostToDevice, s));
     HB_CUDA(cudaMemcpyAsync(sys->d_bad, &none, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-    k_state_check<<<g, 256, 0, s>>>(dp, sys->d_bad, n);
-    uint32_t bad = none;
-    HB_CUDA(cudaMemcpyAsync(&bad, sys->d_bad, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    HB_CUDA(cudaStreamSynchronize(s));
-    if (bad != none)
-      return hb_fail(HB_ERR_NOT_FINITE, "non-finite position for atom " + std::to_string(bad));
+    k_state_check<T><<<g, 256, 0, s>>>(dp, sys->d_bad, n);
   }
   if (velocities)
-    HB_CUDA(cudaMemcpyAsync(dv, velocities, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
-  sys->fix_valid = false;
-  k_state_in<<<g, 256, 0, s>>>(positions ? dp : nullptr, velocities ? dv : nullptr,
-                               sys->d_box64, sys->d_posq, sys->d_vel, sys->d_image, n);
+    HB_CUDA(cudaMemcpyAsync(dv, velocities, sizeof(T) * 3 * n, cudaMemcpyHostToDevice, s));
+  k_state_in<T><<<g, 256, 0, s>>>(positions ? dp : nullptr, velocities ? dv : nullptr,
+                                  sys->d_box64, sys->d_posq, sys->d_vel, sys->d_image,
+                                  positions ? sys->d_bad : nullptr, n);
   HB_CUDA(cudaGetLastError());
+  uint32_t bad = none;
+  if (positions)
+    HB_CUDA(cudaMemcpyAsync(&bad, sys->d_bad, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   // the host arrays may be reused as soon as the call returns
   HB_CUDA(cudaStreamSynchronize(s));
+  if (bad != none)
+    return hb_fail(HB_ERR_NOT_FINITE, "non-finite position for atom " + std::to_string(bad));
+  sys->fix_valid = false;
   return HB_OK;
 }
 
-extern "C" int hb_system_get_state(hb_system *sys, double *positions, double *velocities,
-                                   int32_t *images, double *forces) {
+template <class T>
+int get_state_t(hb_system *sys, T *positions, T *velocities, int32_t *images, T *forces) {
   HB_REQUIRE(sys, HB_ERR_INVALID_ARGUMENT, "null system");
   const uint32_t n = sys->n;
   if (!n || (!positions && !velocities && !images && !forces)) return HB_OK;
@@ -403,22 +416,44 @@ extern "C" int hb_system_get_state(hb_system *sys, double *positions, double *ve
   // evaluation; wait for it anyway in case a caller queued some there
   HB_CUDA(cudaStreamSynchronize(sys->ctx->stream2));
   const size_t n3 = 3 * (size_t)n;
-  double *dp = sys->d_stage, *dv = dp + n3, *df = dv + n3;
-  k_state_out<<<hb_div_up(n, 256), 256, 0, s>>>(
+  T *dp = reinterpret_cast<T *>(sys->d_stage), *dv = dp + n3, *df = dv + n3;
+  k_state_out<T><<<hb_div_up(n, 256), 256, 0, s>>>(
       sys->d_posq, sys->d_vel, sys->d_force, sys->d_image, positions ? dp : nullptr,
       velocities ? dv : nullptr, forces ? df : nullptr, images ? sys->d_stage_img : nullptr, n);
   HB_CUDA(cudaGetLastError());
   if (positions)
-    HB_CUDA(cudaMemcpyAsync(positions, dp, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
+    HB_CUDA(cudaMemcpyAsync(positions, dp, sizeof(T) * n3, cudaMemcpyDeviceToHost, s));
   if (velocities)
-    HB_CUDA(cudaMemcpyAsync(velocities, dv, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
+    HB_CUDA(cudaMemcpyAsync(velocities, dv, sizeof(T) * n3, cudaMemcpyDeviceToHost, s));
   if (forces)
-    HB_CUDA(cudaMemcpyAsync(forces, df, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
+    HB_CUDA(cudaMemcpyAsync(forces, df, sizeof(T) * n3, cudaMemcpyDeviceToHost, s));
   if (images)
     HB_CUDA(cudaMemcpyAsync(images, sys->d_stage_img, sizeof(int32_t) * n3,
                             cudaMemcpyDeviceToHost, s));
   HB_CUDA(cudaStreamSynchronize(s));
   return HB_OK;
+}
+
+}  // namespace
+
+extern "C" int hb_system_set_state(hb_system *sys, const double *positions,
+                                   const double *velocities) {
+  return set_state_t<double>(sys, positions, velocities);
+}
+
+extern "C" int hb_system_get_state(hb_system *sys, double *positions, double *velocities,
+                                   int32_t *images, double *forces) {
+  return get_state_t<double>(sys, positions, velocities, images, forces);
+}
+
+extern "C" int hb_system_set_state_f32(hb_system *sys, const float *positions,
+                                       const float *velocities) {
+  return set_state_t<float>(sys, positions, velocities);
+}
+
+extern "C" int hb_system_get_state_f32(hb_system *sys, float *positions, float *velocities,
+                                       int32_t *images, float *forces) {
+  return get_state_t<float>(sys, positions, velocities, images, forces);
 }
 
 extern "C" int hb_system_set_box(hb_system *sys, const double box[6]) {
@@ -1450,9 +1485,11 @@ struct hb_batch {
   std::vector<uint64_t> gens;                // members' layout_gen at capture
   cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr, pair_done = nullptr;
   cudaGraphExec_t exec = nullptr;
-  // one multi-system pair launch for all members (when they share the pair
-  // physics and contexts are distinct); 0 = one pair launch per member
-  int one_pair_launch = 1;
+  // 1: one multi-system pair launch for all members (when they share the
+  // pair physics and contexts are distinct); 0 (default, measured faster:
+  // members that skip a rebuild start their pair kernels early instead of
+  // waiting at the join) = one pair launch per member
+  int one_pair_launch = 0;
   bool multi = false;                        // the form of the captured graph
   void *d_members = nullptr;                 // member table of the multi-system launch
   uint32_t *d_work = nullptr;                // its work counter

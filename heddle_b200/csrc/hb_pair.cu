@@ -139,6 +139,13 @@ __global__ void __launch_bounds__(P4_WARPS * 32, MULTI ? 6 : 8)
   // [96, 128); a half above 0.25 hartree takes the int64 path, so the int32
   // sums cannot wrap (32 pairs x 0.25 x 2^28 < 2^31)
   __shared__ int sm_ev[EV ? P4_WARPS * 128 : 1];
+  // multi-system form: the members' first work items, for the per-item
+  // member search (members beyond the table search global memory)
+  constexpr uint32_t MT = 128u;
+  __shared__ uint32_t sm_item0[MULTI ? MT : 1];
+  if constexpr (MULTI) {
+    for (uint32_t k = threadIdx.x; k < MT && k < n_members; k += blockDim.x) sm_item0[k] = members[k].item0;
+  }
   const int nt2 = P0.n_types * P0.n_types;
   float *sm_ljd4 = reinterpret_cast<float *>(sm_lj4 + nt2);
   for (int k = threadIdx.x; k < nt2; k += blockDim.x) {
@@ -185,7 +192,7 @@ __global__ void __launch_bounds__(P4_WARPS * 32, MULTI ? 6 : 8)
       uint32_t lo = 0u, hi = n_members;  // largest m with members[m].item0 <= g
       while (hi - lo > 1u) {
         const uint32_t mid = (lo + hi) >> 1;
-        if (members[mid].item0 <= g) lo = mid;
+        if ((mid < MT ? sm_item0[mid] : members[mid].item0) <= g) lo = mid;
         else hi = mid;
       }
       const PairMember &M = members[lo];

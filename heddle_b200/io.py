@@ -211,7 +211,8 @@ def _minimization(m: dict, base: Path) -> MinimizationConfig:
               "trajectory_every": int(out.get("trajectory_every", 0)),
               "include_images": bool(out.get("include_images", True)),
               "minlog_path": _out_path(base, out.get("minlog_path")),
-              "trajectory_path": _out_path(base, out.get("trajectory_path"))}
+              "trajectory_path": _out_path(base, out.get("trajectory_path")),
+              "timings_path": _out_path(base, out.get("timings_path"))}
     return MinimizationConfig(name, a, output)
 
 
@@ -266,7 +267,8 @@ def load_config(path) -> Config:
                   "include_images": bool(out.get("include_images", True)),
                   "log_every": int(out.get("log_every", 100)),
                   "trajectory_path": _out_path(base, out.get("trajectory_path")),
-                  "log_path": _out_path(base, out.get("log_path"))}
+                  "log_path": _out_path(base, out.get("log_path")),
+                  "timings_path": _out_path(base, out.get("timings_path"))}
         md_phases.append(PhaseConfig(name, n_steps, dt, integ, thermo, baro, output))
     min_phases = [_minimization(m, base) for m in doc.get("minimization", [])]
     # [[phase]] and [[minimization]] run in document order
@@ -569,3 +571,43 @@ def read_topology(path) -> Topology:
             else:
                 raise ConfigError(f"topology: unknown section [{section}]")
     return t
+
+
+class StageTimes:
+    """Per-stage count, total, min and max time of one phase -- the
+    reference's timings accumulator (src/timings.rs:120-150, 440-505).
+    Device stages arrive per call of several steps (the library times the
+    stages of a whole call), so a call of k steps adds k samples whose
+    min / max are the call's mean per step; host stages add one sample per
+    measurement."""
+
+    def __init__(self):
+        self.acc = {}
+
+    def record(self, name: str, seconds: float, count: int = 1) -> None:
+        if count <= 0:
+            return
+        ns = seconds * 1e9
+        per = ns / count
+        a = self.acc.get(name)
+        if a is None:
+            self.acc[name] = [count, ns, per, per]
+        else:
+            a[0] += count
+            a[1] += ns
+            a[2] = min(a[2], per)
+            a[3] = max(a[3], per)
+
+    def rows(self):
+        return [(k, int(v[0]), v[1], v[2], v[3]) for k, v in self.acc.items() if v[0] > 0]
+
+
+def write_timings(path, times: StageTimes) -> None:
+    """The `.timings` table of src/timings.rs:513-548: one row per stage
+    with count, total ms, mean / min / max us; an existing file is an error
+    (the reference's OutputExists)."""
+    with open(path, "x") as f:
+        f.write(f"{'stage':<28} {'count':>10} {'total_ms':>14} {'mean_us':>13} {'min_us':>11} {'max_us':>11}\n")
+        for name, count, total_ns, min_ns, max_ns in times.rows():
+            f.write(f"{name:<28} {count:>10} {total_ns / 1e6:>14.3f} {total_ns / 1e3 / count:>13.1f} "
+                    f"{min_ns / 1e3:>11.1f} {max_ns / 1e3:>11.1f}\n")

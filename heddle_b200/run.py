@@ -6,7 +6,8 @@
 reads the configuration, the initial extended-XYZ frame and the topology,
 builds the system, force field (LJ, SPME, bonded terms, exclusions by the
 topology rules), constraint groups and each phase's integrator / barostat,
-and writes `<root>.out.<phase>.xyz` and `<root>.out.<phase>.log` beside the
+and writes `<root>.out.<phase>.xyz`, `<root>.out.<phase>.log` and
+`<root>.out.<phase>.timings` (per-stage device and host times) beside the
 configuration (`<root>` = file name without `.toml` and one `.in`), in SI
 units like the reference.  Initial velocities, when the XYZ frame has none,
 are Maxwell-Boltzmann at [simulation].temperature from the ChaCha8 seed.
@@ -15,14 +16,15 @@ are Maxwell-Boltzmann at [simulation].temperature from the ChaCha8 seed.
 from __future__ import annotations
 
 import sys
+import time
 from pathlib import Path
 
 import numpy as np
 
 from . import api as A
 from . import units as U
-from .io import (ConfigError, LogWriter, MinimizationConfig, MinlogWriter, TrajectoryWriter,
-                 load_config, read_topology, read_xyz)
+from .io import (ConfigError, LogWriter, MinimizationConfig, MinlogWriter, StageTimes,
+                 TrajectoryWriter, load_config, read_topology, read_xyz, write_timings)
 from .systems import settle_geometry
 from .topology import effective_exclusions, exclusion_csr
 from .velocities import generate_velocities
@@ -273,21 +275,40 @@ def minimize(ph, sys_, ff, cons, names, base: Path, root: str) -> list:
     return written
 
 
+# device stages reported by the library per call (hb_timing_get)
+DEVICE_STAGES = [(1, "pair_force"), (2, "spme_reciprocal"), (3, "neighbor_list"),
+                 (4, "integrate_constrain"), (0, "step_total")]
+
+
 def run(config_path, ctx=None) -> list:
     """Run every phase; returns the written output paths."""
+    t_run = time.perf_counter()
+    t0 = time.perf_counter()
     cfg = load_config(config_path)
+    pre = StageTimes()  # the setup stages, replayed into the first phase's timings
+    pre.record("config_load", time.perf_counter() - t0)
     own = ctx is None
+    t0 = time.perf_counter()
     ctx = ctx or A.Context(0)
+    pre.record("gpu_init", time.perf_counter() - t0)
+    t0 = time.perf_counter()
     sys_, ff, cons, names, extra = build(cfg, ctx)
+    pre.record("init_load", time.perf_counter() - t0)
     root = config_root(Path(cfg.path))
     base = Path(cfg.path).parent
     written = []
     n = sys_.n
     dof = max(3 * n - extra["n_constraints"] - 3, 1)
     step = 0
-    for ph in cfg.phases:
+    for k_ph, ph in enumerate(cfg.phases):
+        times = pre if k_ph == 0 else StageTimes()
+        t_phase = time.perf_counter()
+        tpath = ph.output.get("timings_path") or base / f"{root}.out.{ph.name}.timings"
         if isinstance(ph, MinimizationConfig):
             written += minimize(ph, sys_, ff, cons, names, base, root)
+            times.record("total_runtime", time.perf_counter() - (t_run if k_ph == 0 else t_phase))
+            write_timings(tpath, times)
+            written.append(tpath)
             continue
         kw = dict(ph.integrator)
         kind = kw.pop("kind")
@@ -322,23 +343,37 @@ def run(config_path, ctx=None) -> list:
         types = None
         done = 0
         cadence = [c for c in (out["trajectory_every"], out["log_every"]) if c > 0]
+        ctx.timing(True)
         while done < ph.n_steps:
             k = ph.n_steps - done
             for c in cadence:
                 k = min(k, c - (done % c))
             it.step(ff, cons, n_steps=k, scalar_every=k if (log and (done + k) % out["log_every"] == 0) else 0)
+            t_dev = ctx.timings()
+            for idx, name in DEVICE_STAGES:
+                times.record(name, t_dev[idx] * 1e-3, k)
             done += k
             t_au = (step + done) * ph.dt
             if traj and done % out["trajectory_every"] == 0:
+                t0 = time.perf_counter()
                 pos, vel, img, _ = sys_.state()
+                times.record("device_to_host_download", time.perf_counter() - t0)
                 if types is None:
                     types = np.asarray(sys_._t)
+                t0 = time.perf_counter()
                 traj.write(step + done, t_au, sys_.box(), types, pos, vel, img)
+                times.record("trajectory_write", time.perf_counter() - t0)
             if log and done % out["log_every"] == 0:
+                t0 = time.perf_counter()
                 ke = sys_.kinetic()[0]
                 log.write(step + done, t_au, ke, 2.0 * ke / dof,
                           log_values(ph, ke, ff.scalars()["potential"], thermo, baro))
+                times.record("log_write", time.perf_counter() - t0)
+        ctx.timing(False)
         step += ph.n_steps
+        times.record("total_runtime", time.perf_counter() - (t_run if k_ph == 0 else t_phase))
+        write_timings(tpath, times)
+        written.append(tpath)
         for w in (traj, log):
             if w:
                 w.close()

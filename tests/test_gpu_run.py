@@ -31,9 +31,20 @@ def test_argon_run_is_byte_identical_and_conserves_energy(ctx, tmp_path):
         d = tmp_path / f"r{k}"
         d.mkdir()
         paths = R.run(staged(d, "argon"), ctx=ctx)
-        assert [p.name for p in paths] == ["argon.out.run.xyz", "argon.out.run.log"]
-        outs.append([p.read_bytes() for p in paths])
+        assert [p.name for p in paths] == ["argon.out.run.xyz", "argon.out.run.log", "argon.out.run.timings"]
+        # trajectories and logs are byte-identical run to run; the timings are times
+        outs.append([p.read_bytes() for p in paths[:2]])
     assert outs[0] == outs[1]
+    # the .timings table (src/timings.rs:513-548): header, device stages
+    # counted per step, host stages, the whole run
+    rows = (tmp_path / "r0" / "argon.out.run.timings").read_text().splitlines()
+    assert rows[0].split() == ["stage", "count", "total_ms", "mean_us", "min_us", "max_us"]
+    table = {r.split()[0]: r.split()[1:] for r in rows[1:]}
+    for stage in ("pair_force", "neighbor_list", "integrate_constrain", "step_total"):
+        assert int(table[stage][0]) == 100
+    for stage in ("config_load", "gpu_init", "init_load", "trajectory_write", "log_write", "total_runtime"):
+        assert stage in table
+    assert float(table["total_runtime"][1]) >= float(table["step_total"][1])
     logf = tmp_path / "r0" / "argon.out.run.log"
     # an NVE phase logs only the base columns (src/io/log_output.rs:40-60)
     assert logf.read_text().splitlines()[0] == "step,time,kinetic_energy,temperature"
@@ -66,7 +77,8 @@ def test_water_csvr_c_rescale_run(ctx, tmp_path):
         shutil.copy(f, tmp_path / f.name)
     cfg = staged(tmp_path, "water_cr")
     paths = R.run(cfg, ctx=ctx)
-    assert [p.name for p in paths] == ["water_cr.out.npt.xyz", "water_cr.out.npt.log"]
+    assert [p.name for p in paths] == ["water_cr.out.npt.xyz", "water_cr.out.npt.log",
+                                       "water_cr.out.npt.timings"]
     lines = (tmp_path / "water_cr.out.npt.log").read_text().splitlines()
     assert lines[0] == ("step,time,kinetic_energy,temperature,csvr_conserved,pressure,box_volume,"
                         "c_rescale_conserved")
@@ -91,7 +103,8 @@ def test_argon_minimization_then_md(ctx, tmp_path):
     cfg = staged(tmp_path, "argon_min")
     paths = R.run(cfg, ctx=ctx)
     assert [p.name for p in paths] == ["argon_min.out.relax.minlog", "argon_min.out.relax.xyz",
-                                       "argon_min.out.run.xyz", "argon_min.out.run.log"]
+                                       "argon_min.out.relax.timings", "argon_min.out.run.xyz",
+                                       "argon_min.out.run.log", "argon_min.out.run.timings"]
     lines = (tmp_path / "argon_min.out.relax.minlog").read_text().splitlines()
     assert lines[0] == "iter,energy,max_force,step,accepted"
     rows = np.loadtxt(tmp_path / "argon_min.out.relax.minlog", delimiter=",", skiprows=1)

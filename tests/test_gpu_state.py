@@ -78,3 +78,29 @@ def test_state_into_page_locked_arrays(ctx):
     with pytest.raises(ValueError):
         sys_.state(out=(host[0], host[1], host[0], host[3]))  # wrong dtype for the images
     sys_.close()
+
+
+def test_single_precision_exchange(ctx):
+    """hb_system_set_state_f32 / hb_system_get_state_f32: the same state as
+    the FP64 exchange (the device holds f32), a round trip changes nothing,
+    and a non-finite position is rejected with nothing changed."""
+    sys_ = make(ctx, seed=6)
+    p64, v64, i64, f64 = sys_.state()
+    out = tuple(np.zeros((sys_.n, 3), dtype=dt) for dt in (np.float32, np.float32, np.int32, np.float32))
+    sys_.state_f32(out)
+    assert np.array_equal(out[0].astype(np.float64), p64)
+    assert np.array_equal(out[1].astype(np.float64), v64)
+    assert np.array_equal(out[2], i64)
+    assert np.array_equal(out[3].astype(np.float64), f64)
+    sys_.set_state_f32(out[0], out[1])
+    p1, v1, i1, _ = sys_.state()
+    assert np.array_equal(p1, p64) and np.array_equal(v1, v64) and np.array_equal(i1, i64)
+    bad = out[0].copy()
+    bad[7, 2] = np.inf
+    with pytest.raises(hb.HeddleError, match="non-finite position for atom 7"):
+        sys_.set_state_f32(bad, np.zeros_like(out[1]))
+    p2, v2, i2, _ = sys_.state()
+    assert np.array_equal(p2, p64) and np.array_equal(v2, v64) and np.array_equal(i2, i64)
+    with pytest.raises(ValueError):
+        sys_.set_state_f32(p64, None)  # float64 arrays belong to set_state
+    sys_.close()

@@ -196,3 +196,26 @@ def test_topology_sections_and_molecules():
     # the 14-atom chain is one molecule, every water another
     assert off[1] == 14 and len(off) - 1 == 1 + (638 - 14) // 3
     assert config_root(Path("a/b/chain.in.toml")) == "chain"
+
+
+def test_timings_table_format_and_no_overwrite(tmp_path):
+    """The `.timings` writer follows src/timings.rs:513-548: a header row and
+    one row per stage (count, total ms, mean / min / max us), and it never
+    overwrites an existing file (the reference's OutputExists)."""
+    from heddle_b200.io import StageTimes, write_timings
+
+    t = StageTimes()
+    t.record("pair_force", 3e-3, 10)    # one call of 10 steps: mean 300 us
+    t.record("pair_force", 1e-3, 5)     # 5 steps: mean 200 us
+    t.record("log_write", 2e-4)
+    path = tmp_path / "x.out.run.timings"
+    write_timings(path, t)
+    rows = path.read_text().splitlines()
+    assert rows[0] == (f"{'stage':<28} {'count':>10} {'total_ms':>14} {'mean_us':>13} "
+                       f"{'min_us':>11} {'max_us':>11}")
+    f = rows[1].split()
+    assert f[0] == "pair_force" and f[1] == "15" and f[2] == "4.000"
+    assert f[3] == "266.7" and f[4] == "200.0" and f[5] == "300.0"
+    assert rows[2].split()[:2] == ["log_write", "1"]
+    with pytest.raises(FileExistsError):
+        write_timings(path, t)
