@@ -584,6 +584,23 @@ def run_batch(args):
     torch.cuda.synchronize()
     t_batch_wall = time.perf_counter() - t0
     value = n_atoms * args.steps / (t_ms * 1e-3)
+    # force error against the FP64 oracle for the smallest, a middle and the
+    # largest box at the state the timed steps ended in (outside the timed
+    # region)
+    import copy
+
+    import oracle as O
+
+    order = sorted(range(len(specs)), key=lambda k: specs[k].n)
+    ferr = {}
+    for k in (order[0], order[len(order) // 2], order[-1]):
+        c, sys_k, ff_k, _, _ = objs[k]
+        ff_k.step(scalars=False)
+        sp = copy.copy(specs[k])
+        sp.box = sys_k.box()
+        Fo, _, _, _ = O.forces(sp, sys_k.positions(), n_threads=os.cpu_count() or 1)
+        rms, mx = force_error(sys_k.forces(), Fo)
+        ferr[f"box{k}_{sp.n // 3}mol"] = {"rms_rel": rms, "max_rel": mx}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": max(3, args.warmup) + args.equilibrate, "ms_per_step": t_ms / args.steps,
@@ -604,6 +621,7 @@ def run_batch(args):
                                                        "work items"},
         "sequential_plain": {"atom_steps_per_s_wall": n_atoms * k_seq / t_seq, "steps": k_seq},
         "speedup_wall": t_seq / t_batch_wall,
+        "force_error": dict(ferr, vs="FP64 CPU oracle at the final state"),
         "rebuilds_in_timed_steps": rebuilds,
         "clocks": clk.summary(),
         "gpu_launches": per_step_kernels * args.steps + (rebuild_kernels // len(specs)) * rebuilds,
@@ -626,6 +644,7 @@ def run_learned_shake(args):
     import heddle_b200 as hb
     from heddle_b200 import systems as S
     from heddle_b200 import units as U
+    import oracle as O
     from oracle import mlp as M
 
     torch.cuda.set_device(0)
@@ -692,6 +711,9 @@ def run_learned_shake(args):
 
     plain = measure(False)
     warm = measure(True)
+    ff.step(scalars=False)
+    Fo, _, _, _ = O.forces(spec, sys_.positions(), n_threads=os.cpu_count() or 1)
+    f_rms, f_max = force_error(sys_.forces(), Fo)
     # the product's cost gate: the warm start is attached only when its
     # step is faster than plain SHAKE's
     sys_.set_state(pos0, vel0)
@@ -709,6 +731,8 @@ def run_learned_shake(args):
                    "atoms": spec.n},
         "plain_shake": plain, "learned_warm_start": warm,
         "cost_gate": gate, "chosen_form": gate["chosen"],
+        "force_error": {"rms_rel": f_rms, "max_rel": f_max, "vs": "FP64 CPU oracle (bonded + LJ + "
+                        "SPME) at the state the warm-started run ended in"},
         "chosen_vs_plain": plain["ms_per_step"] / chosen["ms_per_step"],
         "sweeps_saved_fraction": 1.0 - warm["mean_sweeps_per_group"] / max(plain["mean_sweeps_per_group"], 1e-12),
         "training": {"samples": int(len(targ)), "epochs": 40, "batch": 512,
