@@ -405,23 +405,32 @@ def run_ours(args):
     # comparison, in FP64
     k2 = max(1, min(args.e2e_steps, args.steps))
 
-    def e2e(dtype):
+    def e2e(dtype, fused):
         host = tuple(torch.empty((spec.n, 3), dtype=dt, pin_memory=True).numpy()
                      for dt in (dtype, dtype, torch.int32, dtype))
         get = sys_.state_f32 if dtype == torch.float32 else (lambda out: sys_.state(out=out))
         put = sys_.set_state_f32 if dtype == torch.float32 else sys_.set_state
         get(host)
-        run(ff, cons, n_steps=1)
+        if fused:  # one call per step: upload, step, read-out (captures its graph here)
+            it.step_exchange(ff, cons, 1, host[0], host[1], host)
+        else:
+            run(ff, cons, n_steps=1)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(k2):
-            put(host[0], host[1])
-            run(ff, cons, n_steps=1)
-            get(host)
+            if fused:
+                # the inputs alias the outputs: the upload completes before the step
+                it.step_exchange(ff, cons, 1, host[0], host[1], host)
+            else:
+                put(host[0], host[1])
+                run(ff, cons, n_steps=1)
+                get(host)
         return max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
 
-    t_e2e = e2e(torch.float32)
-    t_e2e64 = e2e(torch.float64)
+    fused = bool(args.graphs)
+    t_e2e = e2e(torch.float32, fused)
+    t_e2e_sep = e2e(torch.float32, False) if fused else t_e2e
+    t_e2e64 = e2e(torch.float64, False)
     e2e_value = world * spec.n * k2 / t_e2e
 
     peak, peak_kind = measured_peaks()
@@ -471,8 +480,14 @@ def run_ours(args):
                     "d2h_bytes_per_step": (3 * 3 * 4 + 3 * 4) * spec.n,
                     "note": "per step, page-locked host buffers: positions + velocities (f32) "
                             "in; positions, velocities, forces (f32) and images (i32) out; wall "
-                            "clock, over the C ABI (hb_system_set_state_f32 / hb_integrator step "
-                            "/ hb_system_get_state_f32)",
+                            "clock, over the C ABI: " + (
+                                "one hb_integrator_step_exchange_f32 call per step (positions "
+                                "and images copied out during the force evaluation)" if fused else
+                                "hb_system_set_state_f32 / hb_integrator_step / "
+                                "hb_system_get_state_f32"),
+                    "separate_calls": {"value": world * spec.n * k2 / t_e2e_sep,
+                                       "calls": "hb_system_set_state_f32 / hb_integrator "
+                                                "step / hb_system_get_state_f32"},
                     "f64_exchange": {"value": world * spec.n * k2 / t_e2e64,
                                      "h2d_bytes_per_step": 2 * 3 * 8 * spec.n,
                                      "d2h_bytes_per_step": (3 * 3 * 8 + 3 * 4) * spec.n}},

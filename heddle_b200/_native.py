@@ -238,6 +238,8 @@ SIGNATURES = {
     "hb_integrator_destroy": (C.c_int, [VP]),
     "hb_integrator_step": (C.c_int, [VP, VP, VP, C.c_uint32, C.c_uint32]),
     "hb_integrator_step_graph": (C.c_int, [VP, VP, VP, C.c_uint32]),
+    "hb_integrator_step_exchange_f32": (C.c_int, [VP, VP, VP, C.c_uint32, PF32, PF32, PF32, PF32,
+                                                   PI32, PF32]),
     "hb_integrator_count_launches": (C.c_int, [VP, VP, VP, PU64]),
     "hb_barostat_create": (C.c_int, [VP, C.POINTER(BarostatDesc), PVP]),
     "hb_barostat_destroy": (C.c_int, [VP]),

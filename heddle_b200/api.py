@@ -594,6 +594,26 @@ class Integrator:
     def step_graph(self, ff: ForceField, cons: Constraints | None = None, n_steps: int = 1) -> None:
         N.check(self.lib.hb_integrator_step_graph(self.h, ff.h, cons.h if cons else None, int(n_steps)))
 
+    def step_exchange(self, ff: ForceField, cons: Constraints | None = None, n_steps: int = 1,
+                      positions_in=None, velocities_in=None, out=None):
+        """Upload float32 (n, 3) positions / velocities (None = keep), run
+        n_steps graph steps and read the state after the last one into
+        `out` = (positions, velocities, images, forces) arrays (float32,
+        float32, int32, float32; any None).  With page-locked arrays the
+        read-out of positions and images overlaps the last step's force
+        evaluation."""
+        want = ((np.float32, positions_in), (np.float32, velocities_in))
+        pos, vel, img, frc = out if out is not None else (None, None, None, None)
+        want += ((np.float32, pos), (np.float32, vel), (np.int32, img), (np.float32, frc))
+        n = self.system.n
+        for dt, a in want:
+            if a is not None and (a.dtype != dt or not a.flags["C_CONTIGUOUS"] or a.size != 3 * n):
+                raise ValueError("step_exchange: C-contiguous (n, 3) arrays of the right types")
+        N.check(self.lib.hb_integrator_step_exchange_f32(
+            self.h, ff.h, cons.h if cons else None, int(n_steps), N.f32ptr(positions_in),
+            N.f32ptr(velocities_in), N.f32ptr(pos), N.f32ptr(vel), N.i32ptr(img), N.f32ptr(frc)))
+        return out
+
     def count_launches(self, ff: ForceField, cons: Constraints | None = None) -> tuple:
         """(kernels every step, kernels of one neighbour rebuild, kernels of
         one barostat move or 0)."""

@@ -54,8 +54,11 @@ extern "C" int hb_context_create(int device_ordinal, hb_context **out) {
   HB_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
   HB_CUDA(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, prio_hi));
   HB_CUDA(cudaStreamCreateWithFlags(&c->stream3, cudaStreamNonBlocking));
+  HB_CUDA(cudaStreamCreateWithFlags(&c->stream4, cudaStreamNonBlocking));
   HB_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
   HB_CUDA(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+  HB_CUDA(cudaEventCreateWithFlags(&c->ev_xfork, cudaEventDisableTiming));
+  HB_CUDA(cudaEventCreateWithFlags(&c->ev_xjoin, cudaEventDisableTiming));
   *out = c;
   return HB_OK;
 }
@@ -68,9 +71,12 @@ extern "C" int hb_context_destroy(hb_context *ctx) {
   for (auto e : ctx->tev) cudaEventDestroy(e);
   cudaEventDestroy(ctx->ev_fork);
   cudaEventDestroy(ctx->ev_join);
+  cudaEventDestroy(ctx->ev_xfork);
+  cudaEventDestroy(ctx->ev_xjoin);
   cudaStreamDestroy(ctx->stream);
   cudaStreamDestroy(ctx->stream2);
   cudaStreamDestroy(ctx->stream3);
+  cudaStreamDestroy(ctx->stream4);
   delete ctx;
   return HB_OK;
 }
@@ -1090,6 +1096,8 @@ extern "C" int hb_integrator_destroy(hb_integrator *it) {
   cudaStreamSynchronize(it->sys->ctx->stream);
   if (it->graph_exec) cudaGraphExecDestroy(it->graph_exec);
   if (it->graph_exec_move) cudaGraphExecDestroy(it->graph_exec_move);
+  if (it->graph_exec_x) cudaGraphExecDestroy(it->graph_exec_x);
+  if (it->graph_exec_x_move) cudaGraphExecDestroy(it->graph_exec_x_move);
   cudaFree(it->d_step);
   if (it->g_ev0) cudaEventDestroy(it->g_ev0);
   if (it->g_ev1) cudaEventDestroy(it->g_ev1);
@@ -1367,11 +1375,42 @@ static int capture_step(hb_integrator *it, hb_forcefield *ff, hb_constraints *co
   return HB_OK;
 }
 
+static void drop_exchange_graphs(hb_integrator *it) {
+  if (it->graph_exec_x) cudaGraphExecDestroy(it->graph_exec_x);
+  if (it->graph_exec_x_move) cudaGraphExecDestroy(it->graph_exec_x_move);
+  it->graph_exec_x = nullptr;
+  it->graph_exec_x_move = nullptr;
+  for (auto &k : it->graph_x_key) k = nullptr;
+}
+
 static void drop_graphs(hb_integrator *it) {
   if (it->graph_exec) cudaGraphExecDestroy(it->graph_exec);
   if (it->graph_exec_move) cudaGraphExecDestroy(it->graph_exec_move);
   it->graph_exec = nullptr;
   it->graph_exec_move = nullptr;
+  drop_exchange_graphs(it);
+}
+
+// the graphs of the plain step (and of the step with a volume move), captured
+// again whenever an attached object or the force field's buffers changed
+static int ensure_step_graphs(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons) {
+  const uint64_t cons_uid = cons ? cons->uid : 0, baro_uid = it->baro ? it->baro->uid : 0;
+  const uint64_t thermo_uid = it->thermo ? it->thermo->uid : 0, pc_uid = it->pc ? it->pc->uid : 0;
+  if (it->graph_exec && it->graph_ff == ff->uid && it->graph_cons == cons_uid &&
+      it->graph_baro == baro_uid && it->graph_gen == ff->layout_gen &&
+      it->graph_thermo == thermo_uid && it->graph_pc == pc_uid)
+    return HB_OK;
+  drop_graphs(it);
+  HB_CUDA(cudaStreamSynchronize(it->sys->ctx->stream));
+  HB_TRY(capture_step(it, ff, cons, false, &it->graph_exec));
+  if (it->baro) HB_TRY(capture_step(it, ff, cons, true, &it->graph_exec_move));
+  it->graph_ff = ff->uid;
+  it->graph_cons = cons_uid;
+  it->graph_baro = baro_uid;
+  it->graph_gen = ff->layout_gen;
+  it->graph_thermo = thermo_uid;
+  it->graph_pc = pc_uid;
+  return HB_OK;
 }
 
 extern "C" int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
@@ -1386,22 +1425,7 @@ extern "C" int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
     HB_TRY(force_eval(ff, false));
     it->forces_valid = true;
   }
-  const uint64_t cons_uid = cons ? cons->uid : 0, baro_uid = it->baro ? it->baro->uid : 0;
-  const uint64_t thermo_uid = it->thermo ? it->thermo->uid : 0, pc_uid = it->pc ? it->pc->uid : 0;
-  if (!it->graph_exec || it->graph_ff != ff->uid || it->graph_cons != cons_uid ||
-      it->graph_baro != baro_uid || it->graph_gen != ff->layout_gen ||
-      it->graph_thermo != thermo_uid || it->graph_pc != pc_uid) {
-    drop_graphs(it);
-    HB_CUDA(cudaStreamSynchronize(s));
-    HB_TRY(capture_step(it, ff, cons, false, &it->graph_exec));
-    if (it->baro) HB_TRY(capture_step(it, ff, cons, true, &it->graph_exec_move));
-    it->graph_ff = ff->uid;
-    it->graph_cons = cons_uid;
-    it->graph_baro = baro_uid;
-    it->graph_gen = ff->layout_gen;
-    it->graph_thermo = thermo_uid;
-    it->graph_pc = pc_uid;
-  }
+  HB_TRY(ensure_step_graphs(it, ff, cons));
   if (ctx->timing) HB_CUDA(cudaEventRecord(it->g_ev0, s));
   for (uint32_t k = 0; k < n_steps; ++k) {
     const bool move = move_due(it, it->step + 1);
@@ -1419,6 +1443,159 @@ extern "C" int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
   HB_TRY(check_status(ff));
   if (cons && cons->mlp) HB_TRY(mlp_status(cons->mlp));
   // buffers or sizes changed: the captured graphs are stale
+  if (ff->layout_gen != it->graph_gen) drop_graphs(it);
+  return HB_OK;
+}
+
+// ---- exchange steps: upload, steps and read-out in one call --------------
+//
+// Replaces the runner's "steps, then ParticleState::download_from" sequence
+// (src/runner.rs:2709-2716, src/state.rs:140-216).  Positions and image
+// counts are final once a step's head has run (kicks, drift, constraint
+// projection), and so are the velocities of the Langevin middle scheme; the
+// force evaluation only reads them.  Their conversion and device-to-host copy
+// therefore run on a side stream concurrently with the force evaluation; the
+// forces (and the velocity-Verlet velocities) follow the step's tail.  A step
+// that ends with a volume move or scales positions in its tail (per-step
+// pressure coupling) reads everything at its end.
+
+struct ExchangeOut {
+  float *pos, *vel, *force;
+  int32_t *img;
+};
+
+// convert the requested fields into the output half of the staging buffer
+// (the upload uses the first 6n floats) and copy them to the host arrays
+static int readout_f32(hb_system *sys, cudaStream_t st, float *pos, float *vel, int32_t *img,
+                       float *force) {
+  if (!pos && !vel && !img && !force) return HB_OK;
+  const size_t n = sys->n, n3 = 3 * n;
+  float *base = reinterpret_cast<float *>(sys->d_stage);
+  float *dp = base + 2 * n3, *dv = base + 3 * n3, *df = base + 4 * n3;
+  k_state_out<float><<<hb_div_up(sys->n, 256), 256, 0, st>>>(
+      sys->d_posq, sys->d_vel, sys->d_force, sys->d_image, pos ? dp : nullptr,
+      vel ? dv : nullptr, force ? df : nullptr, img ? sys->d_stage_img : nullptr, sys->n);
+  HB_CUDA(cudaGetLastError());
+  if (pos) HB_CUDA(cudaMemcpyAsync(pos, dp, sizeof(float) * n3, cudaMemcpyDeviceToHost, st));
+  if (vel) HB_CUDA(cudaMemcpyAsync(vel, dv, sizeof(float) * n3, cudaMemcpyDeviceToHost, st));
+  if (force) HB_CUDA(cudaMemcpyAsync(force, df, sizeof(float) * n3, cudaMemcpyDeviceToHost, st));
+  if (img)
+    HB_CUDA(cudaMemcpyAsync(img, sys->d_stage_img, sizeof(int32_t) * n3, cudaMemcpyDeviceToHost,
+                            st));
+  return HB_OK;
+}
+
+// one step (with its volume move when `move`) whose state lands in `xo`
+static int exchange_step(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons, bool move,
+                         bool capturing, const ExchangeOut &xo) {
+  hb_system *sys = it->sys;
+  hb_context *ctx = sys->ctx;
+  cudaStream_t s = ctx->stream, sx = ctx->stream4;
+  const bool early_pos = !move && (it->kind == HB_INTEGRATOR_LANGEVIN || !it->pc);
+  const bool early_vel = !move && it->kind == HB_INTEGRATOR_LANGEVIN;
+  ExchangeOut e{early_pos ? xo.pos : nullptr, early_vel ? xo.vel : nullptr, nullptr,
+                early_pos ? xo.img : nullptr};
+  const bool fork = e.pos || e.vel || e.img;
+  HB_TRY(step_head(it, cons));
+  if (fork) {
+    HB_CUDA(cudaEventRecord(ctx->ev_xfork, s));
+    HB_CUDA(cudaStreamWaitEvent(sx, ctx->ev_xfork, 0));
+    HB_TRY(readout_f32(sys, sx, e.pos, e.vel, e.img, nullptr));
+  }
+  HB_TRY(force_eval(ff, step_force_ev(it, move), capturing));
+  HB_TRY(step_tail(it, ff, cons));
+  if (move) HB_TRY(baro_move(it->baro, ff, capturing));
+  HB_TRY(readout_f32(sys, s, e.pos ? nullptr : xo.pos, e.vel ? nullptr : xo.vel,
+                     e.img ? nullptr : xo.img, xo.force));
+  if (fork) {
+    HB_CUDA(cudaEventRecord(ctx->ev_xjoin, sx));
+    HB_CUDA(cudaStreamWaitEvent(s, ctx->ev_xjoin, 0));
+  }
+  return HB_OK;
+}
+
+static int capture_exchange(hb_integrator *it, hb_forcefield *ff, hb_constraints *cons, bool move,
+                            const ExchangeOut &xo, cudaGraphExec_t *exec) {
+  cudaStream_t s = it->sys->ctx->stream;
+  cudaGraph_t g;
+  HB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  const uint64_t step = it->step;
+  int rc = exchange_step(it, ff, cons, move, true, xo);
+  it->step = step;
+  cudaError_t ce = cudaStreamEndCapture(s, &g);
+  if (rc != HB_OK) return rc;
+  if (ce != cudaSuccess) return hb_fail(HB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+  cudaError_t ie = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  if (ie != cudaSuccess) return hb_fail(HB_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+  return HB_OK;
+}
+
+static bool page_locked(const void *p) {
+  if (!p) return true;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+extern "C" int hb_integrator_step_exchange_f32(hb_integrator *it, hb_forcefield *ff,
+                                               hb_constraints *cons, uint32_t n_steps,
+                                               const float *positions_in,
+                                               const float *velocities_in, float *positions,
+                                               float *velocities, int32_t *images,
+                                               float *forces) {
+  HB_REQUIRE(it && ff, HB_ERR_INVALID_ARGUMENT, "null argument");
+  HB_REQUIRE(ff->sys == it->sys && (!cons || cons->sys == it->sys), HB_ERR_INVALID_ARGUMENT,
+             "integrator, force field and constraints must share one system");
+  HB_REQUIRE(n_steps >= 1, HB_ERR_INVALID_ARGUMENT, "an exchange call takes at least one step");
+  hb_system *sys = it->sys;
+  HB_TRY(set_state_t<float>(sys, positions_in, velocities_in));
+  const ExchangeOut xo{positions, velocities, forces, images};
+  if (!page_locked(positions) || !page_locked(velocities) || !page_locked(forces) ||
+      !page_locked(images)) {
+    // pageable host arrays cannot be graph copy targets: steps, then read-out
+    HB_TRY(hb_integrator_step_graph(it, ff, cons, n_steps));
+    return get_state_t<float>(sys, positions, velocities, images, forces);
+  }
+  HB_TRY(lossless_prologue(it, cons));
+  hb_context *ctx = sys->ctx;
+  cudaStream_t s = ctx->stream;
+  if (!it->forces_valid) {
+    HB_TRY(force_eval(ff, false));
+    it->forces_valid = true;
+  }
+  HB_TRY(stage_alloc(sys));
+  HB_TRY(ensure_step_graphs(it, ff, cons));
+  const void *key[4] = {positions, velocities, forces, images};
+  if (!std::equal(key, key + 4, it->graph_x_key)) {
+    drop_exchange_graphs(it);
+    HB_CUDA(cudaStreamSynchronize(s));
+    HB_TRY(capture_exchange(it, ff, cons, false, xo, &it->graph_exec_x));
+    if (it->baro) HB_TRY(capture_exchange(it, ff, cons, true, xo, &it->graph_exec_x_move));
+    std::copy(key, key + 4, it->graph_x_key);
+  }
+  if (ctx->timing) HB_CUDA(cudaEventRecord(it->g_ev0, s));
+  for (uint32_t k = 0; k < n_steps; ++k) {
+    const bool move = move_due(it, it->step + 1);
+    cudaGraphExec_t g = k + 1 < n_steps ? (move ? it->graph_exec_move : it->graph_exec)
+                                        : (move ? it->graph_exec_x_move : it->graph_exec_x);
+    HB_CUDA(cudaGraphLaunch(g, s));
+    it->step++;
+  }
+  if (ctx->timing) {
+    HB_CUDA(cudaEventRecord(it->g_ev1, s));
+    HB_CUDA(cudaEventSynchronize(it->g_ev1));
+    float ms = 0.f;
+    HB_CUDA(cudaEventElapsedTime(&ms, it->g_ev0, it->g_ev1));
+    for (int q = 0; q < 8; ++q) ctx->t_ms[q] = 0.0;
+    ctx->t_ms[0] = ms;
+  }
+  // check_status synchronises the stream: the host arrays are filled
+  HB_TRY(check_status(ff));
+  if (cons && cons->mlp) HB_TRY(mlp_status(cons->mlp));
   if (ff->layout_gen != it->graph_gen) drop_graphs(it);
   return HB_OK;
 }

@@ -188,7 +188,9 @@ struct hb_context {
   cudaStream_t stream = nullptr;    // main stream
   cudaStream_t stream2 = nullptr;   // SPME runs here, overlapping the pair kernel
   cudaStream_t stream3 = nullptr;   // captures the bodies of conditional graph nodes
+  cudaStream_t stream4 = nullptr;   // host read-out overlapping a step's force evaluation
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_xfork = nullptr, ev_xjoin = nullptr;
   bool timing = false;
   // stage timers (accumulated over the last hb_integrator_step call)
   std::vector<cudaEvent_t> tev;
@@ -384,6 +386,11 @@ struct hb_integrator {
   hb_thermostat *thermo = nullptr;
   hb_pcouple *pc = nullptr;
   uint64_t graph_thermo = 0, graph_pc = 0;
+  // exchange steps (hb_integrator_step_exchange_f32): the last step of a
+  // call as a graph that also copies the state into page-locked host arrays
+  // (with and without a volume move), captured for one set of host pointers
+  cudaGraphExec_t graph_exec_x = nullptr, graph_exec_x_move = nullptr;
+  const void *graph_x_key[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 // Device-resident state of the Monte-Carlo barostat (FP64).  The whole move

@@ -366,6 +366,27 @@ int hb_integrator_step(hb_integrator *it, hb_forcefield *ff,
  * lives on the device, so replays draw fresh noise). */
 int hb_integrator_step_graph(hb_integrator *it, hb_forcefield *ff,
                              hb_constraints *cons, uint32_t n_steps);
+/* Upload, steps and read-out in one call: replaces the runner's steps
+ * followed by ParticleState::download_from (src/runner.rs:2709-2716,
+ * src/state.rs:140-216).  positions_in / velocities_in (f32 [3n], either may
+ * be NULL) are uploaded as by hb_system_set_state_f32 (the forces of the
+ * last evaluation are kept); n_steps >= 1 steps run as by
+ * hb_integrator_step_graph; then the state after the last step is written
+ * to positions / velocities / forces (f32 [3n]) and images (i32 [3n]), any
+ * of which may be NULL.  With page-locked host arrays the last step is one
+ * CUDA graph whose positions and image counts (and the Langevin velocities)
+ * are copied out while its force evaluation runs; a step that ends with a
+ * barostat move or scales positions in its tail copies them at its end.
+ * The graph is captured again when a host pointer changes.  Pageable host
+ * arrays are filled after the steps instead.  The input arrays may be the
+ * output arrays (the upload completes before the steps).  Returns when the
+ * host arrays are filled. */
+int hb_integrator_step_exchange_f32(hb_integrator *it, hb_forcefield *ff,
+                                    hb_constraints *cons, uint32_t n_steps,
+                                    const float *positions_in,
+                                    const float *velocities_in, float *positions,
+                                    float *velocities, int32_t *images,
+                                    float *forces);
 
 /* Kernel launches of one step: the step is captured into a throwaway CUDA
  * graph (nothing runs) and its kernel nodes are counted: kernels[0] = the
