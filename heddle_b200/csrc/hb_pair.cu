@@ -302,6 +302,7 @@ __global__ void __launch_bounds__(P4_WARPS * 32, MULTI ? 6 : 8)
           // rounds like the scalar op
           const float2 px = make_float2(pi.x, pi.x), py = make_float2(pi.y, pi.y),
                        pz = make_float2(pi.z, pi.z);
+          const float2 nrc = make_float2(-P.rc2_max, -P.rc2_max);
 #pragma unroll 4
           for (uint32_t k = 0; k < 16u; ++k) {
             const float4 a = S.jxy2[k];
@@ -311,7 +312,11 @@ __global__ void __launch_bounds__(P4_WARPS * 32, MULTI ? 6 : 8)
             float2 r2 = __fmul2_rn(dx, dx);
             r2 = __ffma2_rn(dy, dy, r2);
             r2 = __ffma2_rn(dz, dz, r2);
-            m |= ((r2.x < P.rc2_max ? 1u : 0u) | (r2.y < P.rc2_max ? 2u : 0u)) << (2u * k);
+            // r2 < rc2 exactly when r2 - rc2 is negative (the difference of
+            // two distinct finite floats is never zero): its sign bits are
+            // the two mask bits
+            const float2 d = __fadd2_rn(r2, nrc);
+            m |= ((__float_as_uint(d.x) >> 31) | ((__float_as_uint(d.y) >> 30) & 2u)) << (2u * k);
           }
         } else {
 #pragma unroll 4
