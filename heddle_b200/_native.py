@@ -221,6 +221,7 @@ SIGNATURES = {
     "hb_constraints_get_virial": (C.c_int, [VP, PD]),
     "hb_constraints_shake_stats": (C.c_int, [VP, PD, C.c_int]),
     "hb_constraints_record": (C.c_int, [VP, C.c_int]),
+    "hb_constraints_fuse_head": (C.c_int, [VP, C.c_int]),
     "hb_constraints_get_record": (C.c_int, [VP, PF32, PD, PD, PD, PU32]),
     "hb_constraints_set_warm_start": (C.c_int, [VP, VP]),
     "hb_shake_mlp_create": (C.c_int, [VP, C.c_uint64, PVP]),

@@ -504,6 +504,12 @@ class Constraints:
     def record(self, enable: bool = True) -> None:
         N.check(self.lib.hb_constraints_record(self.h, 1 if enable else 0))
 
+    def fuse_head(self, enable: bool = True) -> None:
+        """Langevin steps of an all-SETTLE system: the head (kick, velocity
+        projection, drift / O / drift, position reset) as one kernel (True,
+        the default) or as four (False); the results are identical."""
+        N.check(self.lib.hb_constraints_fuse_head(self.h, 1 if enable else 0))
+
     def get_record(self) -> dict:
         m = C.c_uint32(0)
         N.check(self.lib.hb_constraints_get_record(self.h, None, None, None, None, C.byref(m)))

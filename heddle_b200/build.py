@@ -25,6 +25,13 @@ SOURCES = ["hb_api.cu", "hb_nlist.cu", "hb_pair.cu", "hb_spme.cu", "hb_integ.cu"
            "hb_baro.cu", "hb_bonded.cu", "hb_mlp.cu", "hb_couple.cu", "hb_min.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# Units whose kernels must round alike however their device functions are
+# combined: the Langevin + SETTLE step head runs either as four kernels or
+# as one fused kernel built from the same device functions, and the
+# velocity-Verlet final kick runs plain or fused with a thermostat's
+# rescale; without multiply-add contraction every form rounds each
+# operation the same way.
+FILE_FLAGS = {name: ["-fmad=false"] for name in ("hb_cons.cu", "hb_integ.cu", "hb_couple.cu")}
 NVCC_FLAGS = [
     "-O3",
     "-std=c++17",
@@ -61,15 +68,15 @@ def _newer(src: Path, dst: Path, deps: list[Path]) -> bool:
 def build(verbose: bool = False, extra: list[str] | None = None) -> Path:
     BUILD.mkdir(exist_ok=True)
     nvcc = nvcc_path()
-    deps = list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+    deps = list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h")) + [Path(__file__)]
     objs = []
     for name in SOURCES:
         src = CSRC / name
         obj = BUILD / (src.stem + ".o")
         objs.append(obj)
         if _newer(src, obj, deps):
-            cmd = [nvcc, *host_compiler(), *ARCH, *NVCC_FLAGS, *(extra or []),
-                   "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
+            cmd = [nvcc, *host_compiler(), *ARCH, *NVCC_FLAGS, *FILE_FLAGS.get(name, []),
+                   *(extra or []), "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
             if verbose:
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)

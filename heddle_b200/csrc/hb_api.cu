@@ -998,6 +998,15 @@ extern "C" int hb_constraints_record(hb_constraints *c, int enable) {
   return HB_OK;
 }
 
+extern "C" int hb_constraints_fuse_head(hb_constraints *c, int enable) {
+  HB_REQUIRE(c, HB_ERR_INVALID_ARGUMENT, "null constraints");
+  if (c->fuse_head != (enable != 0)) {
+    c->fuse_head = enable != 0;
+    c->uid = hb_next_uid();  // graphs captured with the other form are stale
+  }
+  return HB_OK;
+}
+
 extern "C" int hb_constraints_get_record(hb_constraints *c, float *features, double *lam1,
                                          double *lscale, double *lam, uint32_t *m) {
   HB_REQUIRE(c, HB_ERR_INVALID_ARGUMENT, "null constraints");
@@ -1074,6 +1083,8 @@ extern "C" int hb_integrator_create(hb_system *sys, const hb_integrator_desc *d,
   it->step = d->step0;
   if (cudaMalloc(&it->d_step, sizeof(uint64_t)) != cudaSuccess ||
       cudaMemcpy(it->d_step, &it->step, sizeof(uint64_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMalloc(&it->d_done, sizeof(uint32_t)) != cudaSuccess ||
+      cudaMemset(it->d_done, 0, sizeof(uint32_t)) != cudaSuccess ||
       cudaEventCreate(&it->g_ev0) != cudaSuccess || cudaEventCreate(&it->g_ev1) != cudaSuccess) {
     hb_integrator_destroy(it);
     return hb_fail(HB_ERR_CUDA, "integrator state allocation failed");
@@ -1099,6 +1110,7 @@ extern "C" int hb_integrator_destroy(hb_integrator *it) {
   if (it->graph_exec_x) cudaGraphExecDestroy(it->graph_exec_x);
   if (it->graph_exec_x_move) cudaGraphExecDestroy(it->graph_exec_x_move);
   cudaFree(it->d_step);
+  cudaFree(it->d_done);
   if (it->g_ev0) cudaEventDestroy(it->g_ev0);
   if (it->g_ev1) cudaEventDestroy(it->g_ev1);
   delete it;
@@ -1117,7 +1129,12 @@ extern "C" int hb_integrator_destroy(hb_integrator *it) {
 static int step_head(hb_integrator *it, hb_constraints *cons) {
   cudaStream_t s = it->sys->ctx->stream;
   cudaEvent_t t4 = stage_begin(s);
-  if (it->kind == HB_INTEGRATOR_LANGEVIN) {
+  if (it->kind == HB_INTEGRATOR_LANGEVIN && cons_lang_head_fusable(cons)) {
+    // every atom in a SETTLE water: the four parts in one kernel
+    HB_TRY(cons_lang_settle_head(cons, (float)it->dt, (float)std::exp(-it->friction * it->dt),
+                                 (float)it->temperature, (uint32_t)it->seed,
+                                 (uint32_t)(it->seed >> 32), it->d_step, it->d_done, s));
+  } else if (it->kind == HB_INTEGRATOR_LANGEVIN) {
     HB_TRY(integ_lang_kick(it, s));
     if (cons) HB_TRY(cons_velocities(cons, 0.0, false, s));
     HB_TRY(integ_lang_drift_ou(it, s));

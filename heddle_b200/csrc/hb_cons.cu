@@ -41,20 +41,15 @@ __device__ __forceinline__ V3 unit(V3 a) {
   return l > 0.0f ? (1.0f / l) * a : v3(0.f, 0.f, 0.f);
 }
 
-__global__ void k_settle_pos(const uint4 *__restrict__ atoms, const float4 *__restrict__ geom,
-                             const float2 *__restrict__ mass, float4 *__restrict__ posq,
-                             float4 *__restrict__ vel, const float4 *__restrict__ prev,
-                             const DBox *__restrict__ box, float dt, float *__restrict__ virial,
-                             uint32_t ng) {
-  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= ng) return;
-  const DBox bx = *box;
-  const uint4 at = atoms[g];
-  const float4 ge = geom[g];
+// SETTLE position reset of one water in registers: P = pre-drift snapshot,
+// Q = drifted positions (reset in place), V = velocities (corrected by
+// dx / dt in place), vir = the position-level virial of each atom
+__device__ __forceinline__ void settle_pos_core(const float4 &P0, const float4 &P1,
+                                                const float4 &P2, float4 (&Q)[3], float4 (&V)[3],
+                                                const float4 &ge, float mo, float mh,
+                                                const DBox &bx, float dt, float (&vir)[3]) {
   const float ra = ge.x, rb = ge.y, rc = ge.z;
-  const float mo = mass[g].x, mh = mass[g].y;
-  const float4 P0 = prev[at.x], P1 = prev[at.y], P2 = prev[at.z];
-  const float4 Q0 = posq[at.x], Q1 = posq[at.y], Q2 = posq[at.z];
+  const float4 Q0 = Q[0], Q1 = Q[1], Q2 = Q[2];
   // reference frame: snapshot bond vectors relative to the snapshot oxygen
   const V3 b0 = mi(v3(P1.x - P0.x, P1.y - P0.y, P1.z - P0.z), bx);
   const V3 c0 = mi(v3(P2.x - P0.x, P2.y - P0.y, P2.z - P0.z), bx);
@@ -102,23 +97,40 @@ __global__ void k_settle_pos(const uint4 *__restrict__ atoms, const float4 *__re
   const V3 rc3 = c3.x * ex + c3.y * ey + c3.z * ez;
   const V3 corr[3] = {(com + ra3) - ua, (com + rb3) - ub, (com + rc3) - uc};
   const V3 rel[3] = {ra3, rb3, rc3};
-  const uint32_t id[3] = {at.x, at.y, at.z};
   const float ms[3] = {mo, mh, mh};
-  const float4 Q[3] = {Q0, Q1, Q2};
   const float inv_dt = dt != 0.0f ? 1.0f / dt : 0.0f;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    float4 q = Q[a];
-    q.x += corr[a].x;
-    q.y += corr[a].y;
-    q.z += corr[a].z;
-    posq[id[a]] = q;
-    float4 v = vel[id[a]];
-    v.x += corr[a].x * inv_dt;
-    v.y += corr[a].y * inv_dt;
-    v.z += corr[a].z * inv_dt;
-    vel[id[a]] = v;
-    if (virial) virial[id[a]] = ms[a] * inv_dt * inv_dt * dot(corr[a], rel[a]);
+    Q[a].x += corr[a].x;
+    Q[a].y += corr[a].y;
+    Q[a].z += corr[a].z;
+    V[a].x += corr[a].x * inv_dt;
+    V[a].y += corr[a].y * inv_dt;
+    V[a].z += corr[a].z * inv_dt;
+    vir[a] = ms[a] * inv_dt * inv_dt * dot(corr[a], rel[a]);
+  }
+}
+
+__global__ void k_settle_pos(const uint4 *__restrict__ atoms, const float4 *__restrict__ geom,
+                             const float2 *__restrict__ mass, float4 *__restrict__ posq,
+                             float4 *__restrict__ vel, const float4 *__restrict__ prev,
+                             const DBox *__restrict__ box, float dt, float *__restrict__ virial,
+                             uint32_t ng) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ng) return;
+  const DBox bx = *box;
+  const uint4 at = atoms[g];
+  const uint32_t id[3] = {at.x, at.y, at.z};
+  float4 Q[3] = {posq[at.x], posq[at.y], posq[at.z]};
+  float4 V[3] = {vel[at.x], vel[at.y], vel[at.z]};
+  float vir[3];
+  settle_pos_core(prev[at.x], prev[at.y], prev[at.z], Q, V, geom[g], mass[g].x, mass[g].y, bx,
+                  dt, vir);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    posq[id[a]] = Q[a];
+    vel[id[a]] = V[a];
+    if (virial) virial[id[a]] = vir[a];
   }
 }
 
@@ -142,21 +154,16 @@ __device__ __forceinline__ bool solve3(const float m[3][3], const float r[3], fl
 
 // velocity projection: impulses g_k along r_k (O-H1, O-H2, H1-H2) that
 // zero the relative velocity along every bond
-__global__ void k_settle_vel(const uint4 *__restrict__ atoms, const float2 *__restrict__ mass,
-                             const float4 *__restrict__ posq, float4 *__restrict__ vel,
-                             const DBox *__restrict__ box, float dt, float *__restrict__ virial,
-                             uint32_t ng) {
-  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= ng) return;
-  const DBox bx = *box;
-  const uint4 at = atoms[g];
-  const float mo = mass[g].x, mh = mass[g].y;
+// velocity projection of one water in registers (W in place); with dt > 0
+// the impulses' virial of each atom goes to vir
+__device__ __forceinline__ void settle_vel_core(const float4 &p0, const float4 &p1,
+                                                const float4 &p2, float4 &w0, float4 &w1,
+                                                float4 &w2, float mo, float mh, const DBox &bx,
+                                                float dt, float (&vir)[3]) {
   const float io = 1.0f / mo, ih = 1.0f / mh;
-  const float4 p0 = posq[at.x], p1 = posq[at.y], p2 = posq[at.z];
   const V3 x0 = v3(p0.x, p0.y, p0.z);
   const V3 x1 = x0 + mi(v3(p1.x - p0.x, p1.y - p0.y, p1.z - p0.z), bx);
   const V3 x2 = x0 + mi(v3(p2.x - p0.x, p2.y - p0.y, p2.z - p0.z), bx);
-  float4 w0 = vel[at.x], w1 = vel[at.y], w2 = vel[at.z];
   const V3 v0 = v3(w0.x, w0.y, w0.z), v1 = v3(w1.x, w1.y, w1.z), v2 = v3(w2.x, w2.y, w2.z);
   const V3 r1 = x0 - x1, r2 = x0 - x2, r3 = x1 - x2;
   const float d11 = dot(r1, r1), d22 = dot(r2, r2), d33 = dot(r3, r3);
@@ -173,15 +180,92 @@ __global__ void k_settle_vel(const uint4 *__restrict__ atoms, const float2 *__re
   w0.x += dv0.x; w0.y += dv0.y; w0.z += dv0.z;
   w1.x += dv1.x; w1.y += dv1.y; w1.z += dv1.z;
   w2.x += dv2.x; w2.y += dv2.y; w2.z += dv2.z;
+  if (dt > 0.0f) {
+    const float inv_dt = 1.0f / dt;
+    const V3 com = (1.0f / (mo + 2.0f * mh)) * (mo * x0 + mh * x1 + mh * x2);
+    vir[0] = mo * inv_dt * dot(dv0, x0 - com);
+    vir[1] = mh * inv_dt * dot(dv1, x1 - com);
+    vir[2] = mh * inv_dt * dot(dv2, x2 - com);
+  }
+}
+
+__global__ void k_settle_vel(const uint4 *__restrict__ atoms, const float2 *__restrict__ mass,
+                             const float4 *__restrict__ posq, float4 *__restrict__ vel,
+                             const DBox *__restrict__ box, float dt, float *__restrict__ virial,
+                             uint32_t ng) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ng) return;
+  const DBox bx = *box;
+  const uint4 at = atoms[g];
+  float4 w0 = vel[at.x], w1 = vel[at.y], w2 = vel[at.z];
+  float vir[3] = {0.f, 0.f, 0.f};
+  settle_vel_core(posq[at.x], posq[at.y], posq[at.z], w0, w1, w2, mass[g].x, mass[g].y, bx,
+                  virial ? dt : 0.0f, vir);
   vel[at.x] = w0;
   vel[at.y] = w1;
   vel[at.z] = w2;
   if (virial && dt > 0.0f) {
-    const float inv_dt = 1.0f / dt;
-    const V3 com = (1.0f / (mo + 2.0f * mh)) * (mo * x0 + mh * x1 + mh * x2);
-    virial[at.x] += mo * inv_dt * dot(dv0, x0 - com);
-    virial[at.y] += mh * inv_dt * dot(dv1, x1 - com);
-    virial[at.z] += mh * inv_dt * dot(dv2, x2 - com);
+    virial[at.x] += vir[0];
+    virial[at.y] += vir[1];
+    virial[at.z] += vir[2];
+  }
+}
+
+// The whole Langevin head of a step for a system whose every atom is in a
+// SETTLE water, one thread per water with every value in registers: the
+// kick of its three atoms, the velocity projection, drift / O / drift with
+// the wrap, and the position reset with its virial -- the same arithmetic
+// per atom as k_lang_kick, k_settle_vel (dt = 0), k_lang_drift_ou and
+// k_settle_pos in turn.  The block that finishes last (a completion
+// counter, no waiting) advances the Langevin draw counter, which every
+// thread read first.
+__global__ void __launch_bounds__(128) k_lang_settle_head(
+    const uint4 *__restrict__ atoms, const float4 *__restrict__ geom,
+    const float2 *__restrict__ mass, float4 *__restrict__ posq, float4 *__restrict__ vel,
+    int4 *__restrict__ image, float4 *__restrict__ prev, const float4 *__restrict__ force,
+    const DBox *__restrict__ box, float dt, float a, float kt, uint32_t s_lo, uint32_t s_hi,
+    uint64_t *__restrict__ step_ptr, uint32_t *__restrict__ done, float *__restrict__ virial,
+    uint32_t ng) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t step = *step_ptr;
+  if (g < ng) {
+    const DBox bx = *box;
+    const uint4 at = atoms[g];
+    const uint32_t id[3] = {at.x, at.y, at.z};
+    const float mo = mass[g].x, mh = mass[g].y;
+    float4 Q[3], V[3], P[3];
+    int4 M[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      V[k] = vel[id[k]];
+      hb_lang_kick(V[k], force[id[k]], dt);
+      P[k] = posq[id[k]];
+    }
+    float vir[3] = {0.f, 0.f, 0.f};
+    settle_vel_core(P[0], P[1], P[2], V[0], V[1], V[2], mo, mh, bx, 0.0f, vir);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      Q[k] = P[k];
+      M[k] = image[id[k]];
+      hb_lang_drift_ou(Q[k], V[k], M[k], dt, a, kt, s_lo, s_hi, step, id[k], bx);
+      prev[id[k]] = P[k];
+      image[id[k]] = M[k];
+    }
+    settle_pos_core(P[0], P[1], P[2], Q, V, geom[g], mo, mh, bx, dt, vir);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      posq[id[k]] = Q[k];
+      vel[id[k]] = V[k];
+      if (virial) virial[id[k]] = vir[k];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(done, 1u) == gridDim.x - 1u) {
+      *step_ptr = step + 1ull;
+      *done = 0u;
+    }
   }
 }
 
@@ -597,6 +681,22 @@ int cons_positions(hb_constraints *c, double dt, cudaStream_t s) {
         (rec && !pred) ? c->d_feat : nullptr, c->d_lam1, c->d_lsc, rec ? c->d_lam : nullptr, 0,
         c->n_shake);
   }
+  HB_CUDA(cudaGetLastError());
+  return HB_OK;
+}
+
+bool cons_lang_head_fusable(const hb_constraints *c) {
+  return c && c->fuse_head && c->n_shake == 0 && c->n_settle > 0 &&
+         3ull * c->n_settle == c->sys->n;
+}
+
+int cons_lang_settle_head(hb_constraints *c, float dt, float a, float kt, uint32_t s_lo,
+                          uint32_t s_hi, uint64_t *d_step, uint32_t *d_done, cudaStream_t s) {
+  hb_system *sys = c->sys;
+  k_lang_settle_head<<<hb_div_up(c->n_settle, 128), 128, 0, s>>>(
+      c->d_settle_atoms, c->d_settle_geom, c->d_settle_mass, sys->d_posq, sys->d_vel,
+      sys->d_image, sys->d_pos_prev, sys->d_force, sys->d_box, dt, a, kt, s_lo, s_hi, d_step,
+      d_done, c->d_virial, c->n_settle);
   HB_CUDA(cudaGetLastError());
   return HB_OK;
 }

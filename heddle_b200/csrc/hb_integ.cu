@@ -93,16 +93,6 @@ __global__ void k_scalars(unsigned long long *__restrict__ acc,
   acc[3] = 0ull;
 }
 
-// Box-Muller cosine branch on the first two words, u = (x + 1/2) 2^-32
-// (kernels/philox.cuh:135-150), evaluated in single precision.
-__device__ __forceinline__ float gaussian(uint32_t s_lo, uint32_t s_hi, uint64_t step,
-                                          uint32_t atom, uint32_t axis) {
-  uint32_t o0, o1;
-  hb_philox(s_lo, s_hi, (uint32_t)step, (uint32_t)(step >> 32), atom, axis, o0, o1);
-  const float u1 = ((float)(o0 >> 8) + 0.5f) * (1.0f / 16777216.0f);
-  const float u2 = ((float)(o1 >> 8) + 0.5f) * (1.0f / 16777216.0f);
-  return sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
-}
 
 __global__ void k_vv_kick_drift(float4 *__restrict__ posq, float4 *__restrict__ vel,
                                 int4 *__restrict__ image, const float4 *__restrict__ force,
@@ -277,11 +267,7 @@ __global__ void k_lang_kick(float4 *__restrict__ vel, const float4 *__restrict__
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float4 v = vel[i];
-  const float4 f = force[i];
-  const float h = dt * v.w;
-  v.x += f.x * h;
-  v.y += f.y * h;
-  v.z += f.z * h;
+  hb_lang_kick(v, force[i], dt);
   vel[i] = v;
 }
 
@@ -297,23 +283,8 @@ __global__ void k_lang_drift_ou(float4 *__restrict__ posq, float4 *__restrict__ 
   float4 p = posq[i];
   float4 v = vel[i];
   prev[i] = p;
-  const float hdt = 0.5f * dt;
-  p.x += v.x * hdt;
-  p.y += v.y * hdt;
-  p.z += v.z * hdt;
-  const float sig = sqrtf((1.0f - a * a) * kt * v.w);
-  v.x = a * v.x + sig * gaussian(s_lo, s_hi, step, i, 0u);
-  v.y = a * v.y + sig * gaussian(s_lo, s_hi, step, i, 1u);
-  v.z = a * v.z + sig * gaussian(s_lo, s_hi, step, i, 2u);
-  p.x += v.x * hdt;
-  p.y += v.y * hdt;
-  p.z += v.z * hdt;
-  int ka, kb, kc;
-  hb_wrap(p.x, p.y, p.z, ka, kb, kc, b);
   int4 im = image[i];
-  im.x += ka;
-  im.y += kb;
-  im.z += kc;
+  hb_lang_drift_ou(p, v, im, dt, a, kt, s_lo, s_hi, step, i, b);
   image[i] = im;
   posq[i] = p;
   vel[i] = v;

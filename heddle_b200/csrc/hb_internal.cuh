@@ -140,6 +140,52 @@ __host__ __device__ inline void hb_philox(uint32_t k0, uint32_t k1, uint32_t c0,
   o1 = c1;
 }
 
+#ifdef __CUDACC__
+// Box-Muller cosine branch on the first two words, u = (x + 1/2) 2^-32
+// (kernels/philox.cuh:135-150), evaluated in single precision.
+__device__ __forceinline__ float hb_gaussian(uint32_t s_lo, uint32_t s_hi, uint64_t step,
+                                             uint32_t atom, uint32_t axis) {
+  uint32_t o0, o1;
+  hb_philox(s_lo, s_hi, (uint32_t)step, (uint32_t)(step >> 32), atom, axis, o0, o1);
+  const float u1 = ((float)(o0 >> 8) + 0.5f) * (1.0f / 16777216.0f);
+  const float u2 = ((float)(o1 >> 8) + 0.5f) * (1.0f / 16777216.0f);
+  return sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
+}
+
+// Langevin middle scheme, per atom (kernels/langevin.cu:13-80): the full
+// kick v += F dt / m ...
+__device__ __forceinline__ void hb_lang_kick(float4 &v, const float4 &f, float dt) {
+  const float h = dt * v.w;
+  v.x += f.x * h;
+  v.y += f.y * h;
+  v.z += f.z * h;
+}
+
+// ... and half drift, O step (friction factor a, k_B T, the atom's Philox
+// stream at the step's draw counter), half drift and the wrap into the
+// cell with the image counts carried
+__device__ __forceinline__ void hb_lang_drift_ou(float4 &p, float4 &v, int4 &im, float dt,
+                                                 float a, float kt, uint32_t s_lo, uint32_t s_hi,
+                                                 uint64_t step, uint32_t i, const DBox &b) {
+  const float hdt = 0.5f * dt;
+  p.x += v.x * hdt;
+  p.y += v.y * hdt;
+  p.z += v.z * hdt;
+  const float sig = sqrtf((1.0f - a * a) * kt * v.w);
+  v.x = a * v.x + sig * hb_gaussian(s_lo, s_hi, step, i, 0u);
+  v.y = a * v.y + sig * hb_gaussian(s_lo, s_hi, step, i, 1u);
+  v.z = a * v.z + sig * hb_gaussian(s_lo, s_hi, step, i, 2u);
+  p.x += v.x * hdt;
+  p.y += v.y * hdt;
+  p.z += v.z * hdt;
+  int ka, kb, kc;
+  hb_wrap(p.x, p.y, p.z, ka, kb, kc, b);
+  im.x += ka;
+  im.y += kb;
+  im.z += kc;
+}
+#endif
+
 // lower-triangular lattice (lx, ly, lz, xy, xz, yz) -> the single-precision
 // box the kernels read
 __host__ __device__ inline DBox hb_make_dbox(const double b[6]) {
@@ -353,6 +399,7 @@ struct hb_constraints {
   // learned warm start and its training data (per SHAKE constraint)
   hb_shake_mlp *mlp = nullptr;       // warm start when set
   bool record = false;               // write features and converged multipliers
+  bool fuse_head = true;             // Langevin head in one kernel where it applies
   float *d_feat = nullptr;           // [n_shake_cons * 8]
   double *d_lam1 = nullptr;          // first Gauss-Seidel multiplier
   double *d_lsc = nullptr;           // multiplier -> sigma-unit scale
@@ -370,6 +417,7 @@ struct hb_integrator {
   double dt = 0.0, friction = 0.0, temperature = 0.0;
   uint64_t seed = 0, step = 0;
   uint64_t *d_step = nullptr;   // Philox draw counter read by the O step
+  uint32_t *d_done = nullptr;   // completion counter of the fused Langevin + SETTLE head
   bool forces_valid = false;
   // graph mode
   cudaGraphExec_t graph_exec = nullptr;
@@ -547,6 +595,12 @@ int mlp_status(hb_shake_mlp *m);
 // constraints (hb_cons.cu)
 int cons_positions(hb_constraints *c, double dt, cudaStream_t s);
 int cons_velocities(hb_constraints *c, double dt, bool virial, cudaStream_t s);
+// Langevin head (kick, velocity projection, drift / O / drift, position
+// reset) in one kernel when every atom is in a SETTLE water and there is no
+// SHAKE group
+bool cons_lang_head_fusable(const hb_constraints *c);
+int cons_lang_settle_head(hb_constraints *c, float dt, float a, float kt, uint32_t s_lo,
+                          uint32_t s_hi, uint64_t *d_step, uint32_t *d_done, cudaStream_t s);
 // position-only projection (minimiser); skip: optional device no-op flag
 int cons_project(hb_constraints *c, const int *skip, cudaStream_t s);
 // steepest descent (hb_min.cu): warm-up report, trial step, decision + report

@@ -302,6 +302,14 @@ int hb_constraints_shake_stats(hb_constraints *c, double out[3], int reset);
 int hb_constraints_record(hb_constraints *c, int enable);
 int hb_constraints_get_record(hb_constraints *c, float *features, double *lam1, double *lscale,
                               double *lam, uint32_t *m);
+/* With a Langevin integrator and every atom in a SETTLE water (no SHAKE
+ * group), a step's kick, velocity projection, drift / O / drift and
+ * position reset run as one kernel, one thread per water, with the same
+ * per-atom arithmetic as the four separate kernels (enable = 1, the
+ * default); enable = 0 launches the four.  No reference counterpart: the
+ * reference launches them in turn (kernels/langevin.cu:13-80,
+ * kernels/settle.cu:145-492). */
+int hb_constraints_fuse_head(hb_constraints *c, int enable);
 /* Warm-start SHAKE from the network (NULL switches it off): features ->
  * network -> lam0 = lam1 + prediction / ls, then the usual sweeps to the
  * same tolerance. */

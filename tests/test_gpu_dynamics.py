@@ -152,7 +152,9 @@ def test_langevin_graph_replay_equals_eager(ctx):
     for a, b in zip(st_a, st_b):
         assert np.array_equal(a, b)
     top, body, _ = ib.count_launches(fb, cb)
-    assert top > 10 and body > 5
+    # fused step head + displacement check, the reciprocal chain, the pair
+    # kernel and the finalize every step; the rebuild's kernels in the IF node
+    assert top >= 8 and body > 5
     close(ia, ca, fa, sa, ib, cb, fb, sb)
 
 
