@@ -389,6 +389,10 @@ __global__ void __launch_bounds__(NLT_WARPS * 32, 4)
   const float4 ci = center[I], hi = half[I];
   const bool ortho = ((int)ci.w & 2) != 0;
   const float rb2 = rb * rb;
+  // corner distance^2 below which a sub-tile's atoms all lie inside the
+  // plain-hit band (a relative margin far above the rounding of the boxes
+  // and of the distances)
+  const float acc2 = band_lo * (1.0f - 1.0e-5f);
   if (threadIdx.x == 0) s_ncand = 0u;
   __syncthreads();
 
@@ -503,27 +507,36 @@ __global__ void __launch_bounds__(NLT_WARPS * 32, 4)
     }
     if (shift_ok) {
       uint32_t qm = 0u;
+      bool inside = false;
       if (jvalid) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          const float ex = fmaxf(fabsf(sx - sc[q][0]) - sh[q][0], 0.0f);
-          const float ey = fmaxf(fabsf(sy - sc[q][1]) - sh[q][1], 0.0f);
-          const float ez = fmaxf(fabsf(sz - sc[q][2]) - sh[q][2], 0.0f);
+          const float ax = fabsf(sx - sc[q][0]), ay = fabsf(sy - sc[q][1]),
+                      az = fabsf(sz - sc[q][2]);
+          const float ex = fmaxf(ax - sh[q][0], 0.0f);
+          const float ey = fmaxf(ay - sh[q][1], 0.0f);
+          const float ez = fmaxf(az - sh[q][2], 0.0f);
           if (sh[q][0] >= 0.0f && ex * ex + ey * ey + ez * ez <= rb2) qm |= 1u << q;
+          // the box's farthest corner well inside the band: every i-atom of
+          // the (non-empty) sub-tile is, so the vote would find a plain hit
+          const float fx = ax + sh[q][0], fy = ay + sh[q][1], fz = az + sh[q][2];
+          if (sh[q][0] >= 0.0f && fx * fx + fy * fy + fz * fz < acc2) inside = true;
         }
       }
       // the j-atoms near a sub-tile box are refined one at a time with the
       // lanes as i-atoms: each lane tests its own i-atom against the
       // broadcast j-atom and one vote decides (padding i-slots sit at 1e18
       // and never hit); the exact rule runs only when some pair falls in
-      // the band
-      uint32_t rem = __ballot_sync(0xFFFFFFFFu, qm != 0u);
+      // the band.  The j-atoms found inside a sub-tile's reach above need
+      // no vote.
+      const uint32_t sure = __ballot_sync(0xFFFFFFFFu, inside);
+      uint32_t rem = __ballot_sync(0xFFFFFFFFu, qm != 0u && !inside);
       s_jsh[w][lane] = make_float4(sx, sy, sz, 0.0f);
       s_jor[w][lane] = pj;
       __syncwarp();
       // two near j-atoms per step in the packed FP32x2 pipe (plain
       // distances only decide far from the band, so their rounding is free)
-      uint32_t hm = 0u;
+      uint32_t hm = sure;
       const float2 px2 = make_float2(pim.x, pim.x), py2 = make_float2(pim.y, pim.y),
                    pz2 = make_float2(pim.z, pim.z);
       auto vote = [&](uint32_t jl, float r2) {
