@@ -575,13 +575,28 @@ __global__ void __launch_bounds__(P4_WARPS * 32, MULTI ? 6 : 8)
         };
         const float2 alpha2 = make_float2(P.alpha, P.alpha), one2 = make_float2(1.0f, 1.0f),
                      c2a2 = make_float2(P.c2a, P.c2a), sc2 = make_float2(P4_SCALE, P4_SCALE);
+        // the i-atom of a lane's run changes rarely: its position stays in
+        // registers and is reloaded only when the i-lane changes
+        uint32_t pi_idx = 32u;
+        float4 pi_c = make_float4(0.f, 0.f, 0.f, 0.f);
         for (uint32_t it = 0; it < rounds; it += 2u) {
           const uint32_t ka = lane * rounds + it;
           if (ka < cnt_r) {
             const bool vb = ka + 1u < cnt_r;
             const uint32_t pa = S.pairs[q0 + ka], pb = vb ? S.pairs[q0 + ka + 1u] : pa;
             const uint32_t ia = pa >> 8, ja = pa & 255u, ib = pb >> 8, jb = pb & 255u;
-            const float4 a = S.ipos[ia], a2 = S.ipos[ib], qa = S.jpos[ja], qb = S.jpos[jb];
+            if (ia != pi_idx) {
+              pi_c = S.ipos[ia];
+              pi_idx = ia;
+            }
+            const float4 a = pi_c;
+            float4 a2 = pi_c;
+            if (ib != ia) {
+              a2 = S.ipos[ib];
+              pi_c = a2;
+              pi_idx = ib;
+            }
+            const float4 qa = S.jpos[ja], qb = S.jpos[jb];
             const float2 dx = __fadd2_rn(make_float2(a.x, a2.x), make_float2(-qa.x, -qb.x));
             const float2 dy = __fadd2_rn(make_float2(a.y, a2.y), make_float2(-qa.y, -qb.y));
             const float2 dz = __fadd2_rn(make_float2(a.z, a2.z), make_float2(-qa.z, -qb.z));
