@@ -303,7 +303,7 @@ __global__ void __launch_bounds__(P4_WARPS * 32, MULTI ? 6 : 8)
           const float2 px = make_float2(pi.x, pi.x), py = make_float2(pi.y, pi.y),
                        pz = make_float2(pi.z, pi.z);
           const float2 nrc = make_float2(-P.rc2_max, -P.rc2_max);
-#pragma unroll 4
+#pragma unroll
           for (uint32_t k = 0; k < 16u; ++k) {
             const float4 a = S.jxy2[k];
             const float2 dx = __fadd2_rn(px, make_float2(a.x, a.y));
