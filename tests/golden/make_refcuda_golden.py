@@ -5,9 +5,9 @@ oracle/ref_harness.cpp) on seeded SPC water boxes and stores the inputs and
 the reference's outputs, so that CPU tests can check the FP64 oracle
 against the reference itself without a GPU:
 
-  python tests/golden/make_refcuda_golden.py OUT_DIR
+  python tests/golden/make_refcuda_golden.py [OUT_DIR]
 
-writes OUT_DIR/refcuda_water512.npz (orthorhombic, r_c 7 A) and
+writes (by default into tests/golden/) OUT_DIR/refcuda_water512.npz (orthorhombic, r_c 7 A) and
 OUT_DIR/refcuda_water1000_tilted.npz (triclinic, r_c 7 A): f32 positions and
 box, reference total / pair / reciprocal forces, per-atom energies and
 virials, and the reference's canonical pair list cut at r_search (stored as
@@ -82,4 +82,4 @@ def main(out_dir: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "gpurun_out/golden")
+    main(sys.argv[1] if len(sys.argv) > 1 else str(Path(__file__).resolve().parent))
