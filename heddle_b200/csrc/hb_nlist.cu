@@ -396,31 +396,37 @@ __global__ void __launch_bounds__(NLT_WARPS * 32, 4)
   if (threadIdx.x == 0) s_ncand = 0u;
   __syncthreads();
 
-  // 1. ordered candidate sweep
-  for (uint32_t base = I + 1u; base < n_tiles; base += 32u * NLT_WARPS) {
-    const uint32_t J = base + w * 32u + lane;
-    bool pass = false;
-    if (J < n_tiles) {
-      if (!ortho) {
-        pass = true;
-      } else {
-        const float4 cj = center[J], hj = half[J];
-        float dx = ci.x - cj.x, dy = ci.y - cj.y, dz = ci.z - cj.z;
-        hb_min_image(dx, dy, dz, b);
-        const float ex = fmaxf(fabsf(dx) - (hi.x + hj.x), 0.0f);
-        const float ey = fmaxf(fabsf(dy) - (hi.y + hj.y), 0.0f);
-        const float ez = fmaxf(fabsf(dz) - (hi.z + hj.z), 0.0f);
-        pass = ex * ex + ey * ey + ez * ez <= rb2;
-      }
-    }
-    const uint32_t bal = __ballot_sync(0xFFFFFFFFu, pass);
-    if (lane == 0) s_cnt[w] = __popc(bal);
+  // 1. ordered candidate sweep, 64 tiles per warp and 512 per block step
+  // (warp w takes tiles base + 64 w .. base + 64 w + 63, its lanes the first
+  // and then the second 32 of them, so the list stays in tile order)
+  auto box_near = [&](uint32_t J) {
+    if (J >= n_tiles) return false;
+    if (!ortho) return true;
+    const float4 cj = center[J], hj = half[J];
+    float dx = ci.x - cj.x, dy = ci.y - cj.y, dz = ci.z - cj.z;
+    hb_min_image(dx, dy, dz, b);
+    const float ex = fmaxf(fabsf(dx) - (hi.x + hj.x), 0.0f);
+    const float ey = fmaxf(fabsf(dy) - (hi.y + hj.y), 0.0f);
+    const float ez = fmaxf(fabsf(dz) - (hi.z + hj.z), 0.0f);
+    return ex * ex + ey * ey + ez * ez <= rb2;
+  };
+  for (uint32_t base = I + 1u; base < n_tiles; base += 64u * NLT_WARPS) {
+    const uint32_t J0 = base + w * 64u + lane, J1 = J0 + 32u;
+    const bool pass0 = box_near(J0), pass1 = box_near(J1);
+    const uint32_t bal0 = __ballot_sync(0xFFFFFFFFu, pass0);
+    const uint32_t bal1 = __ballot_sync(0xFFFFFFFFu, pass1);
+    if (lane == 0) s_cnt[w] = __popc(bal0) + __popc(bal1);
     __syncthreads();
     uint32_t off = s_ncand;
     for (uint32_t k = 0; k < w; ++k) off += s_cnt[k];
-    if (pass) {
-      const uint32_t pos = off + __popc(bal & ((1u << lane) - 1u));
-      if (pos < maxc) cand[pos] = J;
+    const uint32_t below = (1u << lane) - 1u;
+    if (pass0) {
+      const uint32_t pos = off + __popc(bal0 & below);
+      if (pos < maxc) cand[pos] = J0;
+    }
+    if (pass1) {
+      const uint32_t pos = off + __popc(bal0) + __popc(bal1 & below);
+      if (pos < maxc) cand[pos] = J1;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
