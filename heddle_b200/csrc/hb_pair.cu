@@ -533,11 +533,14 @@ __global__ void __launch_bounds__(P4_WARPS * 32, MULTI ? 6 : 8)
           atomicAdd(&S.fi[2][ci], sz);
         }
       };
-      // Coulomb-only pairs of single-periodic-copy tiles on force-only steps
-      // (most pairs of a water box): two pairs of a lane's run per step in
-      // the packed FP32x2 pipe (FADD2 / FMUL2 / FFMA2), the transcendentals
-      // and the integer sums per pair as in math_pass
-      auto math_pass_c2 = [&](uint32_t q0, uint32_t cnt_r) {
+      // Pairs of single-periodic-copy tiles on force-only steps (every pair
+      // of a water box): two pairs of a lane's run per step in the packed
+      // FP32x2 pipe (FADD2 / FMUL2 / FFMA2), the transcendentals and the
+      // integer sums per pair as in math_pass.  LJQ: the range with a
+      // Lennard-Jones term (unswitched kernels), then the Coulomb term where
+      // the force field has one; otherwise the Coulomb-only range
+      auto math_pass_2 = [&](auto ljc, uint32_t q0, uint32_t cnt_r) {
+        constexpr bool LJQ = decltype(ljc)::value;
         const uint32_t rounds = (((cnt_r + 31u) >> 5) + 1u) & ~1u;  // even: pairs of pairs
         uint32_t ci = 32u;
         int sx = 0, sy = 0, sz = 0;
@@ -605,23 +608,55 @@ __global__ void __launch_bounds__(P4_WARPS * 32, MULTI ? 6 : 8)
             r2 = __ffma2_rn(dz, dz, r2);
             const float2 inv_r = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
             const float2 inv_r2 = __fmul2_rn(inv_r, inv_r);
-            const float2 r = __fmul2_rn(r2, inv_r);
-            const float2 ar = __fmul2_rn(alpha2, r);
-            const float2 ea = __fmul2_rn(make_float2(-ar.x, -ar.y), ar);
-            const float2 gg = make_float2(__expf(ea.x), __expf(ea.y));
-            const float2 den = __ffma2_rn(make_float2(0.3275911f, 0.3275911f), ar, one2);
-            const float2 tt = make_float2(__fdividef(1.0f, den.x), __fdividef(1.0f, den.y));
-            float2 poly = __ffma2_rn(make_float2(1.061405429f, 1.061405429f), tt,
-                                     make_float2(-1.453152027f, -1.453152027f));
-            poly = __ffma2_rn(poly, tt, make_float2(1.421413741f, 1.421413741f));
-            poly = __ffma2_rn(poly, tt, make_float2(-0.284496736f, -0.284496736f));
-            poly = __ffma2_rn(poly, tt, make_float2(0.254829592f, 0.254829592f));
-            const float2 pt = __fmul2_rn(poly, tt);
-            const float2 wv = __fmul2_rn(gg, __ffma2_rn(pt, inv_r, c2a2));
-            const float2 qq = __fmul2_rn(make_float2(a.w, a2.w), make_float2(qa.w, qb.w));
-            float2 fac = __fmul2_rn(__fmul2_rn(qq, inv_r2), wv);
-            if (!(r2.x <= P.coul_rc2)) fac.x = 0.0f;
-            if (!(r2.y <= P.coul_rc2)) fac.y = 0.0f;
+            float2 fac = make_float2(0.0f, 0.0f);
+            if constexpr (LJQ) {
+              const int tpa = S.itype[ia] + S.jtype[ja], tpb = S.itype[ib] + S.jtype[jb];
+              const float4 La = sm_lj4[tpa], Lb = sm_lj4[tpb];
+              const float2 eps = make_float2(La.y, Lb.y);
+              const float2 sr2 = __fmul2_rn(make_float2(La.x, Lb.x), inv_r2);
+              const float2 sr6 = __fmul2_rn(__fmul2_rn(sr2, sr2), sr2);
+              const float2 sr12 = __fmul2_rn(sr6, sr6);
+              const float2 nsr6 = make_float2(-sr6.x, -sr6.y);
+              float2 f = __fmul2_rn(__fmul2_rn(eps, inv_r2),
+                                    __ffma2_rn(make_float2(2.0f, 2.0f), sr12, nsr6));
+              if (SWITCH && (r2.x > La.w || r2.y > Lb.w)) {
+                const float2 u = __fmul2_rn(__fmul2_rn(eps, make_float2(1.0f / 6.0f, 1.0f / 6.0f)),
+                                            __fadd2_rn(sr12, nsr6));
+                const float2 inv_d = make_float2(sm_ljd4[tpa], sm_ljd4[tpb]);
+                const float2 tau = __fmul2_rn(__fadd2_rn(r2, make_float2(-La.w, -Lb.w)), inv_d);
+                const float2 omt = __fadd2_rn(one2, make_float2(-tau.x, -tau.y));
+                const float2 sw = __fmul2_rn(__fmul2_rn(omt, omt),
+                                             __ffma2_rn(make_float2(2.0f, 2.0f), tau, one2));
+                const float2 chain =
+                    __fmul2_rn(__fmul2_rn(__fmul2_rn(make_float2(12.0f, 12.0f), tau), omt), inv_d);
+                const float2 fsw = __ffma2_rn(sw, f, __fmul2_rn(chain, u));
+                if (r2.x > La.w) f.x = fsw.x;
+                if (r2.y > Lb.w) f.y = fsw.y;
+              }
+              if (r2.x <= La.z && La.y != 0.0f) fac.x = f.x;
+              if (r2.y <= Lb.z && Lb.y != 0.0f) fac.y = f.y;
+            }
+            if (!LJQ || P.coul_on) {
+              const float2 r = __fmul2_rn(r2, inv_r);
+              const float2 ar = __fmul2_rn(alpha2, r);
+              const float2 ea = __fmul2_rn(make_float2(-ar.x, -ar.y), ar);
+              const float2 gg = make_float2(__expf(ea.x), __expf(ea.y));
+              const float2 den = __ffma2_rn(make_float2(0.3275911f, 0.3275911f), ar, one2);
+              const float2 tt = make_float2(__fdividef(1.0f, den.x), __fdividef(1.0f, den.y));
+              float2 poly = __ffma2_rn(make_float2(1.061405429f, 1.061405429f), tt,
+                                       make_float2(-1.453152027f, -1.453152027f));
+              poly = __ffma2_rn(poly, tt, make_float2(1.421413741f, 1.421413741f));
+              poly = __ffma2_rn(poly, tt, make_float2(-0.284496736f, -0.284496736f));
+              poly = __ffma2_rn(poly, tt, make_float2(0.254829592f, 0.254829592f));
+              const float2 pt = __fmul2_rn(poly, tt);
+              const float2 wv = __fmul2_rn(gg, __ffma2_rn(pt, inv_r, c2a2));
+              const float2 qq = __fmul2_rn(make_float2(a.w, a2.w), make_float2(qa.w, qb.w));
+              float2 fc = __fmul2_rn(__fmul2_rn(qq, inv_r2), wv);
+              if (!(r2.x <= P.coul_rc2)) fc.x = 0.0f;
+              if (!(r2.y <= P.coul_rc2)) fc.y = 0.0f;
+              if constexpr (LJQ) fac = __fadd2_rn(fac, fc);
+              else fac = fc;
+            }
             const float2 fs = __fmul2_rn(fac, sc2);
             const float2 fx = __fmul2_rn(fs, dx), fy = __fmul2_rn(fs, dy), fz = __fmul2_rn(fs, dz);
             accum(ia, ja, fx.x, fy.x, fz.x);
@@ -634,10 +669,15 @@ __global__ void __launch_bounds__(P4_WARPS * 32, MULTI ? 6 : 8)
           atomicAdd(&S.fi[2][ci], sz);
         }
       };
-      if (spc) {
+      if (spc && !EV && !SCALED) {
+        // the switched Lennard-Jones range stays scalar: packed, its live
+        // values exceed the 64-register budget of this kernel
+        if constexpr (SWITCH) math_pass(std::true_type{}, std::true_type{}, 0u, n_lj);
+        else math_pass_2(std::true_type{}, 0u, n_lj);
+        math_pass_2(std::false_type{}, n_lj, n_c);
+      } else if (spc) {
         math_pass(std::true_type{}, std::true_type{}, 0u, n_lj);
-        if (!EV && !SCALED) math_pass_c2(n_lj, n_c);
-        else math_pass(std::true_type{}, std::false_type{}, n_lj, n_c);
+        math_pass(std::true_type{}, std::false_type{}, n_lj, n_c);
       } else {
         math_pass(std::false_type{}, std::true_type{}, 0u, n_lj);
         math_pass(std::false_type{}, std::false_type{}, n_lj, n_c);
