@@ -340,9 +340,17 @@ __device__ __forceinline__ void grid_setup(float x, float y, float z, const DBox
     float u = (s[d] + 0.5f) * (float)n[d];
     float f = floorf(u);
     t[d] = u - f;
+    // s lies in [-1/2, 1/2] up to rounding after the wrap, so fi is in
+    // [-1, n]: one conditional step gives the residue mod n; positions far
+    // outside any cell (a system blowing up) take the full residue, so the
+    // index stays inside the grid whatever the input
     int fi = (int)f;
-    fi %= n[d];
-    if (fi < 0) fi += n[d];
+    if (fi >= n[d]) fi -= n[d];
+    else if (fi < 0) fi += n[d];
+    if ((unsigned)fi >= (unsigned)n[d]) {
+      fi %= n[d];
+      if (fi < 0) fi += n[d];
+    }
     g0[d] = fi;
   }
 }
