@@ -328,6 +328,7 @@ __device__ __forceinline__ uint32_t excl_mask(uint32_t sj, uint32_t I,
 }
 
 #define NLT_WARPS 8
+#define NLT_SWEEP 4  // 32-tile groups per warp and block step of the candidate sweep
 
 // k-th set bit (0-based) of a 32-bit mask
 // (k < popc(m)), by a binary search on the popcounts of low halves
@@ -396,9 +397,9 @@ __global__ void __launch_bounds__(NLT_WARPS * 32, 4)
   if (threadIdx.x == 0) s_ncand = 0u;
   __syncthreads();
 
-  // 1. ordered candidate sweep, 64 tiles per warp and 512 per block step
-  // (warp w takes tiles base + 64 w .. base + 64 w + 63, its lanes the first
-  // and then the second 32 of them, so the list stays in tile order)
+  // 1. ordered candidate sweep, NLT_SWEEP x 32 tiles per warp per block
+  // step (warp w takes the w-th run of them, its lanes one 32-tile group
+  // after another, so the list stays in tile order)
   auto box_near = [&](uint32_t J) {
     if (J >= n_tiles) return false;
     if (!ortho) return true;
@@ -410,23 +411,27 @@ __global__ void __launch_bounds__(NLT_WARPS * 32, 4)
     const float ez = fmaxf(fabsf(dz) - (hi.z + hj.z), 0.0f);
     return ex * ex + ey * ey + ez * ez <= rb2;
   };
-  for (uint32_t base = I + 1u; base < n_tiles; base += 64u * NLT_WARPS) {
-    const uint32_t J0 = base + w * 64u + lane, J1 = J0 + 32u;
-    const bool pass0 = box_near(J0), pass1 = box_near(J1);
-    const uint32_t bal0 = __ballot_sync(0xFFFFFFFFu, pass0);
-    const uint32_t bal1 = __ballot_sync(0xFFFFFFFFu, pass1);
-    if (lane == 0) s_cnt[w] = __popc(bal0) + __popc(bal1);
+  for (uint32_t base = I + 1u; base < n_tiles; base += 32u * NLT_SWEEP * NLT_WARPS) {
+    const uint32_t J0 = base + w * 32u * NLT_SWEEP + lane;
+    uint32_t bal[NLT_SWEEP];
+    uint32_t tot = 0u;
+#pragma unroll
+    for (int q = 0; q < NLT_SWEEP; ++q) {
+      bal[q] = __ballot_sync(0xFFFFFFFFu, box_near(J0 + 32u * q));
+      tot += __popc(bal[q]);
+    }
+    if (lane == 0) s_cnt[w] = tot;
     __syncthreads();
     uint32_t off = s_ncand;
     for (uint32_t k = 0; k < w; ++k) off += s_cnt[k];
     const uint32_t below = (1u << lane) - 1u;
-    if (pass0) {
-      const uint32_t pos = off + __popc(bal0 & below);
-      if (pos < maxc) cand[pos] = J0;
-    }
-    if (pass1) {
-      const uint32_t pos = off + __popc(bal0) + __popc(bal1 & below);
-      if (pos < maxc) cand[pos] = J1;
+#pragma unroll
+    for (int q = 0; q < NLT_SWEEP; ++q) {
+      if ((bal[q] >> lane) & 1u) {
+        const uint32_t pos = off + __popc(bal[q] & below);
+        if (pos < maxc) cand[pos] = J0 + 32u * q;
+      }
+      off += __popc(bal[q]);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
