@@ -1485,7 +1485,7 @@ struct ExchangeOut {
 // (the upload uses the first 6n floats) and copy them to the host arrays
 static int readout_f32(hb_system *sys, cudaStream_t st, float *pos, float *vel, int32_t *img,
                        float *force) {
-  if (!pos && !vel && !img && !force) return HB_OK;
+  if (!sys->n || (!pos && !vel && !img && !force)) return HB_OK;
   const size_t n = sys->n, n3 = 3 * n;
   float *base = reinterpret_cast<float *>(sys->d_stage);
   float *dp = base + 2 * n3, *dv = base + 3 * n3, *df = base + 4 * n3;
